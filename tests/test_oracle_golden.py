@@ -1,0 +1,63 @@
+"""Pin the oracle against golden vectors produced by running the reference (CPU path).
+
+Tolerances: FP32 oracle vs FP32 reference -- summation order differs (numpy vs torch), so
+results agree to FP32 rounding: rel-L2 <= 5e-6 on residuals/gradients, <= 1e-6 on states.
+FP64 oracle vs FP64 reference -- the oracle runs on FP32-built geometry, the FP64 reference on
+FP64 geometry; rel-L2 <= 1e-4 on residuals, <= 1e-6 on states.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from oracle import fvm_oracle as O
+
+
+def test_residual_fp32(golden):
+    g, spec, T, cfg = golden
+    res = O.OracleResidual(T, cfg, np.float32)
+    r1, g1 = res.forward(g["prim0"])
+    assert rel_l2(r1, g["res1"]) < 5e-6
+    assert rel_l2(g1, g["grads1"]) < 5e-6
+    r2, g2 = res.forward(g["prim2"], g["grads1"])
+    assert rel_l2(r2, g["res2"]) < 5e-6
+    assert rel_l2(g2, g["grads2"]) < 5e-6
+
+
+def test_residual_fp64(golden):
+    g, spec, T, cfg = golden
+    res = O.OracleResidual(T, cfg, np.float64)
+    r1, g1 = res.forward(g["prim0"].astype(np.float64))
+    assert rel_l2(r1, g["res1_f64"]) < 1e-4
+    # FP32 reference is within its own rounding of the FP64 reference
+    assert rel_l2(g["res1"], g["res1_f64"]) < 1e-4
+
+
+@pytest.mark.parametrize("name,key", [("RK4", "rk4_step1"), ("SSP_RK3", "ssprk3_step1")])
+def test_butcher_step(golden, name, key):
+    g, spec, T, cfg = golden
+    s = O.OracleSolver(O.OracleResidual(T, cfg, np.float32), g["state0"], float(g["dt"]))
+    s.butcher_step(name)
+    assert rel_l2(s.state, g[key]) < 1e-6
+    s64 = O.OracleSolver(O.OracleResidual(T, cfg, np.float64), g["state0"].astype(np.float64), float(g["dt"]))
+    s64.butcher_step(name)
+    assert rel_l2(s64.state, g[key + "_f64"]) < 1e-6
+
+
+def test_ten_steps(golden):
+    g, spec, T, cfg = golden
+    s = O.OracleSolver(O.OracleResidual(T, cfg, np.float32), g["state0"], float(g["dt"]))
+    for _ in range(10):
+        s.butcher_step("SSP_RK3")
+    assert rel_l2(s.state, g["ssprk3_step10"]) < 2e-6
+
+
+def test_adaptive_steps(golden):
+    g, spec, T, cfg = golden
+    s = O.OracleSolver(O.OracleResidual(T, cfg, np.float32), g["state0"], float(g["dt"]))
+    s.adapt_step("RK3_SSP4")
+    assert rel_l2(s.state, g["adapt_step1"]) < 1e-6
+    assert abs(float(s.dt) / float(g["adapt_dt1"]) - 1) < 1e-5
+    s = O.OracleSolver(O.OracleResidual(T, cfg, np.float32), g["state0"], float(g["dt"]))
+    s.rk3ssp4_step()
+    assert rel_l2(s.state, g["rk3ssp4_step1"]) < 1e-6
+    assert abs(float(s.dt) / float(g["rk3ssp4_dt1"]) - 1) < 1e-5

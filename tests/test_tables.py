@@ -1,0 +1,44 @@
+"""Host table build: bit-exact against the reference's packed ELL operators (golden vectors)."""
+import numpy as np
+import torch
+
+from fvm_solver_b200 import tables as tb
+
+
+def test_ell_operators_bit_exact(golden):
+    g, spec, T, cfg = golden
+    for name, A in [("G", T.ops.G_mats), ("flux", T.ops.flux_mat), ("Afg", T.ops.A_face_grad),
+                    ("Abc", T.ops.A_bc), ("Acorr", T.ops.A_corr)]:
+        v, c = tb.coo_to_ell(A)
+        assert np.array_equal(v.numpy(), g[f"ell_{name}_vals"]), name
+        assert np.array_equal(c.numpy(), g[f"ell_{name}_cols"]), name
+    assert np.array_equal(T.ops.b_face_grad.numpy(), g["b_face_grad"])
+    # b_bc is uninitialised (torch.empty) on characteristic rows in the reference: compare the rest
+    m = (T.bc.dirich_mask | T.bc.neumann_mask).reshape(-1).numpy()
+    assert np.array_equal(T.ops.b_bc.numpy()[m], g["b_bc"][m])
+
+
+def test_kernel_tables_consistent(golden):
+    """The slot-major kernel tables encode the same operators as the reference-format ones."""
+    g, spec, T, cfg = golden
+    K = T.kernel
+    N, dim = K.n_cells, K.dim
+    gv = g["ell_G_vals"].reshape(N, dim, -1)
+    gc = g["ell_G_cols"].reshape(N, dim, -1)
+    assert np.array_equal(K.g_vals.numpy(), gv.transpose(1, 2, 0))
+    assert np.array_equal(K.g_cols.numpy(), gc[:, 0].T)
+    assert np.array_equal(K.f_vals.numpy(), g["ell_flux_vals"].T)
+    assert np.array_equal(K.f_cols.numpy(), g["ell_flux_cols"].T)
+    # neighbour slots decode to neigh_combine
+    slots = np.stack([(K.nb_slot.numpy() >> (4 * j)) & 15 for j in range(dim + 1)], 1)
+    nb = np.take_along_axis(K.g_cols.numpy().T, slots, 1)
+    assert np.array_equal(nb, T.neigh_combine.numpy())
+
+
+def test_coo_to_ell_overflow():
+    A = torch.sparse_coo_tensor(torch.tensor([[0, 0, 1], [0, 1, 1]]), torch.ones(3), (2, 2))
+    try:
+        tb.coo_to_ell(A, K=1)
+    except ValueError:
+        return
+    raise AssertionError("expected ValueError")
