@@ -1,0 +1,880 @@
+// Fused finite-volume residual and explicit time-stepping kernels.
+//
+// One residual evaluation (FVMEquation.forward, time_fvm/fvm_equation.py:406-435) is four
+// kernels instead of the reference's ~60 eager PyTorch ops:
+//
+//   k_bc        boundary facets: A_bc U + b_bc + A_corr grads_prev, then the characteristic BC
+//               (facet_boundary.py:124-168, 418-512).  Each block recomputes the group mean of the
+//               interior sound speed in the same order, so no grid-wide synchronisation is needed.
+//   k_cell      per cell: LSQ gradient (G_mats spMM, facet_process.py:409-418), slope limiter
+//               (facet_process.py:387-407, limiter.py), limited facet values scattered straight to
+//               the [F][2][C] facet table (facet_process.py:349-351), limited gradient.
+//   k_face      per facet: averaged gradients, normal gradient (A_face_grad spMV) and
+//               non-orthogonal correction (facet_process.py:362-385), EOS and stress
+//               (fvm_equation.py:62-187), advection + pressure + viscous + heating + Kurganov-Tadmor
+//               fluxes (fvm_equation.py:199-368).
+//   k_div_stage per cell: divergence (flux_mat spMM, fvm_equation.py:428-435) fused with the
+//               Runge-Kutta / Adams stage combination, the conserved -> primitive conversion of
+//               the next stage input (fvm_equation.py:35-44) and, on the last stage, the FP64
+//               reductions for the adaptive step size (integrators.py:42-62), the CFL time step and
+//               the conservation sums.
+//
+// All four are memory-bound gathers: one thread per cell / facet, slot-major tables so warps read
+// coalesced, AoS [row][C] state so each gathered neighbour is one or two 32-byte sectors.
+#include <math.h>
+
+#include "fvm_common.cuh"
+
+namespace fvm {
+
+struct Phys {
+    float T_0, mu, mu_b, S, C_v, gamma, kappa, v_factor;
+    float R, gR, inv_Cv, T0pS, T0sq;  // derived, rounded to float as the reference's scalars are
+    int lim_p;
+};
+
+// Stage descriptor built on the host from a tableau.
+struct StageArgs {
+    int s;          // index of the increment computed by this stage (k[s] = dt * f)
+    int store_k;    // write k[s] to memory (needed by a later combination)
+    int final_;     // 1: combination is the new state (written to state); 0: next stage input
+    int n_terms;    // combination U0 + sum_t coef[t] * k[idx[t]]
+    int idx[FVM_MAX_STAGES];
+    float coef[FVM_MAX_STAGES];
+    int n_lo;       // embedded low-order combination (adaptive error estimate)
+    int idx_lo[FVM_MAX_STAGES];
+    float coef_lo[FVM_MAX_STAGES];
+    int adaptive, cfl, cons;
+};
+
+// ------------------------------------------------------------------------------------------
+// Slope limiters (limiter.py:29-77).  delta: allowed range, dU: unlimited increment.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ float limiter_phi(int p, float delta, float dU, float eps) {
+    if (p == 4) {
+        const float a = fabsf(delta), b = fabsf(dU), b2 = 2.f * b;
+        const float a2 = a * a;
+        const float a_eps = a2 * a2 + eps;
+        const float S = b2 * fmaf(b2, b2 - a, a2);
+        const float phi = fmaf(a, S, a_eps) / fmaf(b, delta * delta * delta + S, a_eps);
+        return a < b2 ? phi : 1.f;
+    }
+    if (p == 1) {
+        const float s = 2.f * ((dU > 0.f ? 1.f : 0.f) - 0.5f) * (fabsf(dU) + 1e-8f);
+        return fminf(fmaxf(delta / s, 0.f), 1.f);
+    }
+    if (p == 2) {
+        return (delta * delta + eps + 2.f * delta * dU) / (delta * delta + 2.f * dU * dU + delta * dU + eps);
+    }
+    const float a = fabsf(delta), b = fabsf(dU);
+    if (p == 3) {
+        const float a_eps = a * a * a + eps, S = 4.f * b * b;
+        const float phi = (a_eps + a * S) / (a_eps + b * (delta * delta + S));
+        return a < 2.f * b ? phi : 1.f;
+    }
+    // p == 5
+    const float a2 = a * a;
+    const float a_eps = a2 * a2 * a + eps;
+    const float S = 8.f * b * b * (a2 - 2.f * b * (a - b));
+    const float d2 = delta * delta;
+    const float phi = (a_eps + a * S) / (a_eps + b * (d2 * d2 + S));
+    return a < 2.f * b ? phi : 1.f;
+}
+
+// ------------------------------------------------------------------------------------------
+// k_bc: boundary facet values.
+// ------------------------------------------------------------------------------------------
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+                                                const float* __restrict__ grads,
+                                                const int32_t* __restrict__ has_grads,
+                                                float* __restrict__ bcv, float* __restrict__ face_vals) {
+    constexpr int C = DIM + 2;
+    __shared__ double red[32];
+    float scale = 0.f;
+    if (m.n_char > 0) {
+        // Group mean of the interior sound speed c = sqrt(gamma R T) (facet_boundary.py:427),
+        // recomputed identically by every block.
+        double acc = 0.0;
+        for (int t = threadIdx.x; t < m.n_char; t += blockDim.x) {
+            const int cell = __ldg(m.ch_cell + t);
+            acc += (double)sqrtf(p.gR * __ldg(prims + (int64_t)cell * C + DIM + 1));
+        }
+        double v[1] = {acc};
+        block_sum<1>(v, red);
+        __shared__ float s_scale;
+        if (threadIdx.x == 0) s_scale = 10.0f / (float)(v[0] / (double)m.n_char);
+        __syncthreads();
+        scale = s_scale;
+    }
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m.n_bc) return;
+    const int cell = __ldg(m.bc_cell + b);
+    float U[C];
+    load_row<C>(prims + (int64_t)cell * C, U);
+    const bool prev = *has_grads != 0;
+    float out[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        const int kind = __ldg(m.bc_kind + b * C + c);
+        float v = (kind == 2 ? U[c] : 0.f) + __ldg(m.bc_b + b * C + c);
+        if (prev && kind == 2) {
+            float corr = 0.f;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d)
+                corr = fmaf(__ldg(m.bc_l + b * DIM + d), grads[((int64_t)cell * DIM + d) * C + c], corr);
+            v += corr;
+        }
+        out[c] = v;
+    }
+    const int ch = __ldg(m.bc_char + b);
+    if (ch >= 0) {
+        // Characteristic BC (facet_boundary.py:436-512).
+        float n[DIM], vt[DIM];
+        float vn = 0.f;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            n[d] = __ldg(m.ch_normal + ch * DIM + d);
+            vn = fmaf(U[d], n[d], vn);
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) vt[d] = U[d] - vn * n[d];
+        const float rho = U[DIM], T = U[DIM + 1];
+        const float pr = p.R * rho * T;
+        const float c = sqrtf(p.gR * T);
+        const float drho = __ldg(m.ch_rho + ch) - rho;
+        const float dvn = __ldg(m.ch_vn + ch) - vn;
+        const float dp = __ldg(m.ch_p + ch) - pr;
+        const float inv_c = 1.f / c;
+        const float inv_c2 = inv_c * inv_c;
+        const float h_dp = 0.5f * inv_c2 * dp;
+        const float h_dvn = 0.5f * rho * inv_c * dvn;
+        float x0 = -h_dvn + h_dp, x1 = drho - inv_c2 * dp, x2 = h_dvn + h_dp;
+        const float g0 = 0.5f * (1.f - tanhf(scale * (vn - c)));
+        const float g1 = 0.5f * (1.f - tanhf(scale * vn));
+        const float g2 = 0.5f * (1.f - tanhf(scale * (vn + c)));
+        x0 *= g0; x1 *= g1; x2 *= g2;
+        const float cor = c / rho;
+        const float rho_b = rho + (x0 + x1 + x2);
+        const float vn_b = vn + (-cor * x0 + cor * x2);
+        const float p_b = pr + (c * c) * (x0 + x2);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            const float vtb = g1 * vt[d] + (1.f - g1) * __ldg(m.ch_vt + ch * DIM + d);
+            out[d] = vn_b * n[d] + vtb;
+        }
+        out[DIM] = rho_b;
+        out[DIM + 1] = p_b / (p.R * rho_b);
+    }
+    store_row<C>(bcv + (int64_t)b * C, out);
+    const int f = __ldg(m.bc_face + b), sd = __ldg(m.bc_side + b);
+    store_row<C>(face_vals + ((int64_t)f * 2 + sd) * C, out);
+}
+
+// ------------------------------------------------------------------------------------------
+// k_cell: gradient, limiter, limited facet values, limited gradient.
+// ------------------------------------------------------------------------------------------
+template <int DIM, int KG>
+__global__ void __launch_bounds__(kBlock) k_cell(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+                                                  const float* __restrict__ bcv,
+                                                  float* __restrict__ face_vals,
+                                                  float* __restrict__ grads,
+                                                  int32_t* __restrict__ has_grads) {
+    constexpr int C = DIM + 2, K = DIM + 1;
+    const int N = m.n_cells;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *has_grads = 1;
+    if (i >= N) return;
+    float U[C];
+    load_row<C>(prims + (int64_t)i * C, U);
+    const int meta = __ldg(m.nb_slot + i);
+    const int nvalid = (meta >> 24) & 31;
+    float g[DIM][C];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+#pragma unroll
+        for (int c = 0; c < C; ++c) g[d][c] = 0.f;
+    float up[C], lo[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) up[c] = lo[c] = U[c];
+#pragma unroll
+    for (int k = 0; k < KG; ++k) {
+        const int col = __ldg(m.g_cols + (int64_t)k * N + i);
+        float X[C];
+        if (col < N) load_row<C>(prims + (int64_t)col * C, X);
+        else load_row_cg<C>(bcv + (int64_t)(col - N) * C, X);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            const float w = __ldg(m.g_vals + ((int64_t)d * KG + k) * N + i);
+#pragma unroll
+            for (int c = 0; c < C; ++c) g[d][c] = fmaf(w, X[c], g[d][c]);
+        }
+        if (k < nvalid) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                up[c] = fmaxf(up[c], X[c]);
+                lo[c] = fminf(lo[c], X[c]);
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        up[c] -= U[c];
+        lo[c] -= U[c];
+    }
+    const float eps = __ldg(m.eps + i);
+    float dU[K][C], phim[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) phim[c] = INFINITY;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        float r[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) r[d] = __ldg(m.disp + ((int64_t)j * DIM + d) * N + i);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            float du = g[0][c] * r[0];
+#pragma unroll
+            for (int d = 1; d < DIM; ++d) du = fmaf(g[d][c], r[d], du);
+            dU[j][c] = du;
+            const float num = du > 0.f ? up[c] : lo[c];
+            phim[c] = fminf(phim[c], limiter_phi(p.lim_p, num, du, eps));
+        }
+    }
+    const int sides = __ldg(m.side + i);
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        float fv[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) fv[c] = fmaf(dU[j][c], phim[c], U[c]);
+        const int f = __ldg(m.c2f + (int64_t)j * N + i);
+        store_row<C>(face_vals + ((int64_t)f * 2 + ((sides >> j) & 1)) * C, fv);
+    }
+    float* go = grads + (int64_t)i * DIM * C;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        float gd[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) gd[c] = g[d][c] * phim[c];
+        store_row<C>(go + d * C, gd);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// k_face: facet fluxes.
+// ------------------------------------------------------------------------------------------
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_face(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+                                                  const float* __restrict__ face_vals,
+                                                  const float* __restrict__ grads,
+                                                  float* __restrict__ flux) {
+    constexpr int C = DIM + 2, NG = DIM + 1;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.n_facets) return;
+    const int cL = __ldg(m.fcell + 2 * f), cR = __ldg(m.fcell + 2 * f + 1);
+    const int b = __ldg(m.fbc + f);
+    float n[DIM], nh[DIM], xo[DIM];
+    const float size = __ldg(m.fsize + f);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        n[d] = __ldg(m.normals + f * DIM + d);
+        nh[d] = n[d] / size;
+        xo[d] = __ldg(m.xorth + f * DIM + d);
+    }
+    float UL[C], UR[C];
+    load_row_cg<C>(face_vals + (int64_t)f * 2 * C, UL);
+    load_row_cg<C>(face_vals + ((int64_t)f * 2 + 1) * C, UR);
+
+    // Facet-averaged limited gradients of (V, T): gls[d][k] (facet_process.py:362-371).
+    float gls[DIM][NG];
+    const float* gA = grads + (int64_t)cL * DIM * C;
+    const float* gB = grads + (int64_t)cR * DIM * C;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+#pragma unroll
+        for (int k = 0; k < NG; ++k) {
+            const int comp = k < DIM ? k : DIM + 1;
+            gls[d][k] = (__ldcg(gA + d * C + comp) + __ldcg(gB + d * C + comp)) / 2.f;
+        }
+    // Normal gradient (A_face_grad row, facet_process.py:420-450).
+    float dn[NG];
+    if (b < 0) {
+        const float w = __ldg(m.inv_d + f);
+#pragma unroll
+        for (int k = 0; k < NG; ++k) {
+            const int comp = k < DIM ? k : DIM + 1;
+            const float x0 = __ldg(prims + (int64_t)cL * C + comp);
+            const float x1 = __ldg(prims + (int64_t)cR * C + comp);
+            dn[k] = cL < cR ? fmaf(w, x1, (-w) * x0) : fmaf(-w, x0, w * x1);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < NG; ++k) {
+            const int comp = k < DIM ? k : DIM + 1;
+            const float x = __ldg(prims + (int64_t)cL * C + comp);
+            dn[k] = __ldg(m.bc_ga + b * C + comp) * x + __ldg(m.bc_gb + b * C + comp);
+        }
+    }
+    // Non-orthogonal correction (facet_process.py:377-385).
+    float dFdn[NG], gF[DIM][NG];
+#pragma unroll
+    for (int k = 0; k < NG; ++k) {
+        float sx = gls[0][k] * xo[0], sn = gls[0][k] * nh[0];
+#pragma unroll
+        for (int d = 1; d < DIM; ++d) {
+            sx = fmaf(gls[d][k], xo[d], sx);
+            sn = fmaf(gls[d][k], nh[d], sn);
+        }
+        dFdn[k] = dn[k] - sx;
+        const float corr = dFdn[k] - sn;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) gF[d][k] = fmaf(corr, nh[d], gls[d][k]);
+    }
+    const float grad_T_n = dFdn[DIM];
+
+    // Side quantities.
+    float mom[2][DIM], rho[2], T[2], Q[2], P[2], cs[2], phi[2], vm2[2];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        const float* Us = s == 0 ? UL : UR;
+        rho[s] = Us[DIM];
+        T[s] = Us[DIM + 1];
+        float v2 = 0.f, ph = 0.f;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            mom[s][d] = Us[d] * rho[s];
+            v2 = fmaf(Us[d], Us[d], v2);
+            ph = fmaf(Us[d], n[d], ph);
+        }
+        vm2[s] = v2;
+        phi[s] = ph;
+        Q[s] = rho[s] * (p.C_v * T[s] + 0.5f * v2);
+        P[s] = p.R * rho[s] * T[s];
+        cs[s] = sqrtf(p.gR * T[s]);
+    }
+    // Stress (fvm_equation.py:101-120, 149-170).  I1 = D00 + D11 also in 3D, as in the reference.
+    const float Tm = (T[0] + T[1]) / 2.f;
+    float D[DIM][DIM];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) D[a][c] = 0.5f * (gF[a][c] + gF[c][a]);
+    const float I1 = D[0][0] + D[1][1];
+    const float mu = p.mu * powf(Tm / p.T_0, 1.5f) * p.T0pS / (Tm + p.S);
+    const float mub = p.mu_b * (Tm * Tm) / p.T0sq;
+    const float a0 = -mub * I1, a1 = -2.f * mu;
+    float tau[DIM][DIM];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) tau[a][c] = (a == c ? a0 : 0.f) + a1 * D[a][c];
+
+    float F[C];
+    // Advection (fvm_equation.py:210-231)
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) F[d] = (mom[0][d] * phi[0] + mom[1][d] * phi[1]) / 2.f;
+    F[DIM] = (rho[0] * phi[0] + rho[1] * phi[1]) / 2.f;
+    F[DIM + 1] = ((Q[0] + P[0]) * phi[0] + (Q[1] + P[1]) * phi[1]) / 2.f;
+    // Pressure (fvm_equation.py:309-321)
+    const float Pm = (P[0] + P[1]) / 2.f;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) F[d] += Pm * n[d];
+    // Viscous force (fvm_equation.py:246-257)
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+        float s = tau[0][c] * n[0];
+#pragma unroll
+        for (int a = 1; a < DIM; ++a) s = fmaf(tau[a][c], n[a], s);
+        F[c] += s;
+    }
+    // Heating and conduction (fvm_equation.py:272-294)
+    float heat = 0.f;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+            const float Vm = (UL[c] + UR[c]) / 2.f;
+            heat = fmaf(tau[a][c] * Vm, n[a], heat);
+        }
+    heat = fmaf(-p.kappa * grad_T_n, size, heat);
+    F[DIM + 1] += heat;
+    // Kurganov-Tadmor diffusion (fvm_equation.py:337-368)
+    const float vmax = fmaxf(sqrtf(vm2[0]), sqrtf(vm2[1]));
+    const float cmax = fmaxf(cs[0], cs[1]);
+    const float M = fabsf(vmax / (cmax + 1e-8f));
+    const float vf = fminf(fmaxf(M, p.v_factor), 1.f);
+    const float a_vel = vf * cmax + vmax, a_oth = cmax + vmax;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) F[d] += 0.5f * (a_vel * (mom[0][d] - mom[1][d])) * size;
+    F[DIM] += 0.5f * (a_oth * (rho[0] - rho[1])) * size;
+    F[DIM + 1] += 0.5f * (a_oth * (Q[0] - Q[1])) * size;
+    store_row<C>(flux + (int64_t)f * C, F);
+}
+
+// ------------------------------------------------------------------------------------------
+// k_div_stage: divergence + stage combination.
+// ------------------------------------------------------------------------------------------
+template <int C>
+__device__ __forceinline__ void state_to_prim(const float (&U)[C], float inv_Cv, float (&P)[C]) {
+    constexpr int DIM = C - 2;
+    const float rho = U[DIM];
+    float v2 = 0.f;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        P[d] = U[d] / rho;
+        v2 = fmaf(P[d], P[d], v2);
+    }
+    P[DIM] = rho;
+    P[DIM + 1] = inv_Cv * (U[DIM + 1] / rho - 0.5f * v2);
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_div_stage(fvm_mesh_t m, Phys p, const float* __restrict__ flux,
+                                                       StageArgs a, float* __restrict__ state,
+                                                       float* __restrict__ prims, float* __restrict__ kbuf,
+                                                       const float* __restrict__ dt,
+                                                       double* __restrict__ red,
+                                                       float* __restrict__ dudt) {
+    constexpr int C = DIM + 2;
+    const int N = m.n_cells;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < N;
+    float r[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) r[c] = 0.f;
+    if (live) {
+        for (int k = 0; k < m.kf; ++k) {
+            const float w = __ldg(m.f_vals + (int64_t)k * N + i);
+            float Fk[C];
+            load_row_cg<C>(flux + (int64_t)__ldg(m.f_cols + (int64_t)k * N + i) * C, Fk);
+#pragma unroll
+            for (int c = 0; c < C; ++c) r[c] = fmaf(w, Fk[c], r[c]);
+        }
+    }
+    if (dudt) {  // residual only
+        if (live) store_row<C>(dudt + (int64_t)i * C, r);
+        return;
+    }
+    const float h = *dt;
+    float kk[C], U0[C], inc[C], U[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        kk[c] = h * r[c];
+        inc[c] = 0.f;
+    }
+    if (live) {
+        if (a.store_k) store_row<C>(kbuf + ((int64_t)a.s * N + i) * C, kk);
+        load_row_cg<C>(state + (int64_t)i * C, U0);
+        for (int t = 0; t < a.n_terms; ++t) {
+            float kt[C];
+            if (a.idx[t] == a.s) {
+#pragma unroll
+                for (int c = 0; c < C; ++c) kt[c] = kk[c];
+            } else {
+                load_row_cg<C>(kbuf + ((int64_t)a.idx[t] * N + i) * C, kt);
+            }
+#pragma unroll
+            for (int c = 0; c < C; ++c) inc[c] = fmaf(a.coef[t], kt[c], inc[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) U[c] = U0[c] + inc[c];
+        if (a.final_) store_row<C>(state + (int64_t)i * C, U);
+        float P[C];
+        state_to_prim<C>(U, p.inv_Cv, P);
+        store_row<C>(prims + (int64_t)i * C, P);
+    }
+    if (!a.final_) return;
+    __shared__ double smem[32 * 3 * C];
+    if (a.adaptive) {
+        // Column norms of dU_high - dU_low, dU_high and U0 (integrators.py:54), in FP64.
+        double v[3 * C];
+#pragma unroll
+        for (int c = 0; c < 3 * C; ++c) v[c] = 0.0;
+        if (live) {
+            float lo[C];
+#pragma unroll
+            for (int c = 0; c < C; ++c) lo[c] = 0.f;
+            for (int t = 0; t < a.n_lo; ++t) {
+                float kt[C];
+                if (a.idx_lo[t] == a.s) {
+#pragma unroll
+                    for (int c = 0; c < C; ++c) kt[c] = kk[c];
+                } else {
+                    load_row_cg<C>(kbuf + ((int64_t)a.idx_lo[t] * N + i) * C, kt);
+                }
+#pragma unroll
+                for (int c = 0; c < C; ++c) lo[c] = fmaf(a.coef_lo[t], kt[c], lo[c]);
+            }
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const double e = (double)inc[c] - (double)lo[c];
+                v[c] = e * e;
+                v[C + c] = (double)inc[c] * inc[c];
+                v[2 * C + c] = (double)U0[c] * U0[c];
+            }
+        }
+        block_sum<3 * C>(v, smem);
+        if (threadIdx.x == 0)
+            for (int c = 0; c < 3 * C; ++c) atomicAdd(red + c, v[c]);
+        __syncthreads();
+    }
+    if (a.cons) {
+        double v[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) v[c] = live ? __ldg(m.volumes + i) * (double)U[c] : 0.0;
+        block_sum<C>(v, smem);
+        if (threadIdx.x == 0)
+            for (int c = 0; c < C; ++c) atomicAdd(red + 24 + c, v[c]);
+        __syncthreads();
+    }
+    if (a.cfl) {
+        double s = 0.0;
+        if (live) {
+            double v2 = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) v2 += (double)U[d] / U[DIM] * ((double)U[d] / U[DIM]);
+            const double T = ((double)U[DIM + 1] / U[DIM] - 0.5 * v2) / (double)p.C_v;
+            s = __ldg(m.inv_h + i) * (sqrt(v2) + sqrt((double)p.gamma * (double)p.R * fmax(T, 0.0)));
+        }
+        s = block_max(s, smem);
+        if (threadIdx.x == 0) atomic_max_pos(red + 16, s);
+    }
+}
+
+// Step-end bookkeeping: adaptive dt (integrators.py:42-62) or CFL dt, conservation sums.
+__global__ void k_finalize(int C, int adaptive, float atol, float rtol, float mtol, float alpha_hi,
+                           float alpha_lo, float order, float cfl, int cons, double* red, float* dt,
+                           double* cons_out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (adaptive) {
+        double E = 0.0;
+        for (int c = 0; c < C; ++c) {
+            const double nd = sqrt(red[c]), nh = sqrt(red[C + c]), nu = sqrt(red[2 * C + c]);
+            E += nd / ((double)atol + (double)rtol * nh + (double)mtol * nu);
+            red[c] = red[C + c] = red[2 * C + c] = 0.0;
+        }
+        E /= C;
+        const float Ef = (float)E;
+        const float factor = 0.9f * powf(Ef, -1.f / order);
+        const float alpha = Ef > 1.f ? alpha_hi : alpha_lo;
+        dt[0] = dt[0] * (alpha + (1.f - alpha) * factor);
+        red[40] = E;
+    }
+    if (cfl > 0.f) {
+        const double smax = red[16];
+        if (smax > 0.0) dt[0] = (float)((double)cfl / smax);
+        red[16] = 0.0;
+    }
+    if (cons) {
+        for (int c = 0; c < C; ++c) {
+            if (cons_out) cons_out[c] = red[24 + c];
+            red[24 + c] = 0.0;
+        }
+    }
+}
+
+template <int C>
+__global__ void __launch_bounds__(kBlock) k_state_to_prims(int N, float inv_Cv, const float* __restrict__ state,
+                                                            float* __restrict__ prims) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float U[C], P[C];
+    load_row<C>(state + (int64_t)i * C, U);
+    state_to_prim<C>(U, inv_Cv, P);
+    store_row<C>(prims + (int64_t)i * C, P);
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_reduce_state(fvm_mesh_t m, Phys p, const float* __restrict__ state,
+                                                          int want_cfl, int want_cons, double* red) {
+    constexpr int C = DIM + 2;
+    __shared__ double smem[32 * C];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < m.n_cells;
+    float U[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) U[c] = 1.f;
+    if (live) load_row<C>(state + (int64_t)i * C, U);
+    if (want_cons) {
+        double v[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) v[c] = live ? __ldg(m.volumes + i) * (double)U[c] : 0.0;
+        block_sum<C>(v, smem);
+        if (threadIdx.x == 0)
+            for (int c = 0; c < C; ++c) atomicAdd(red + 24 + c, v[c]);
+        __syncthreads();
+    }
+    if (want_cfl) {
+        double s = 0.0;
+        if (live) {
+            double v2 = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) v2 += (double)U[d] / U[DIM] * ((double)U[d] / U[DIM]);
+            const double T = ((double)U[DIM + 1] / U[DIM] - 0.5 * v2) / (double)p.C_v;
+            s = __ldg(m.inv_h + i) * (sqrt(v2) + sqrt((double)p.gamma * (double)p.R * fmax(T, 0.0)));
+        }
+        s = block_max(s, smem);
+        if (threadIdx.x == 0) atomic_max_pos(red + 16, s);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Host side
+// ------------------------------------------------------------------------------------------
+static Phys make_phys(const fvm_physics_t* ph) {
+    Phys p;
+    p.T_0 = ph->T_0;
+    p.mu = ph->mu;
+    p.mu_b = ph->mu_b;
+    p.S = ph->S_const;
+    p.C_v = ph->C_v;
+    p.gamma = ph->gamma;
+    p.kappa = ph->kappa;
+    p.v_factor = ph->v_factor;
+    p.lim_p = ph->lim_p;
+    // Python-scalar constants of the reference, evaluated in double and rounded once to float.
+    const double R = (double)ph->C_v * ((double)ph->gamma - 1.0);
+    p.R = (float)R;
+    p.gR = (float)((double)ph->gamma * R);
+    p.inv_Cv = (float)(1.0 / (double)ph->C_v);
+    p.T0pS = (float)((double)ph->T_0 + (double)ph->S_const);
+    p.T0sq = (float)((double)ph->T_0 * (double)ph->T_0);
+    return p;
+}
+
+static bool mesh_ok(const fvm_mesh_t* m) {
+    if (!m || (m->dim != 2 && m->dim != 3) || m->n_comp != m->dim + 2) return false;
+    if (m->n_cells <= 0 || m->n_facets <= 0 || m->n_bc < 0 || m->n_char < 0) return false;
+    if (m->kg != m->dim + 2 || m->kf < 1 || m->kf > 8) return false;
+    if (!m->g_vals || !m->g_cols || !m->nb_slot || !m->disp || !m->eps || !m->c2f || !m->side ||
+        !m->f_vals || !m->f_cols || !m->fcell || !m->fbc || !m->normals || !m->fsize || !m->xorth ||
+        !m->inv_d || !m->inv_h || !m->volumes)
+        return false;
+    if (m->n_bc > 0 && (!m->bc_face || !m->bc_side || !m->bc_cell || !m->bc_kind || !m->bc_b ||
+                        !m->bc_l || !m->bc_ga || !m->bc_gb || !m->bc_char))
+        return false;
+    if (m->n_char > 0 && (!m->ch_cell || !m->ch_normal || !m->ch_rho || !m->ch_vn || !m->ch_p || !m->ch_vt))
+        return false;
+    return true;
+}
+
+static bool work_ok(const fvm_mesh_t* m, const fvm_work_t* w) {
+    return w && w->face_vals && w->flux && w->red && (m->n_bc == 0 || w->bc_vals);
+}
+
+static inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+// bc -> cell -> face for the primitives `prims`; leaves fluxes in work->flux.
+template <int DIM>
+static int launch_fluxes(const fvm_mesh_t* m, const Phys& p, const float* prims, float* grads,
+                         int32_t* has_grads, const fvm_work_t* w, cudaStream_t s) {
+    if (m->n_bc > 0)
+        FVM_LAUNCH(KID_BC, s, k_bc<DIM><<<blocks_for(m->n_bc), kBlock, 0, s>>>(*m, p, prims, grads, has_grads,
+                                                                               w->bc_vals, w->face_vals));
+    FVM_LAUNCH(KID_CELL, s, k_cell<DIM, DIM + 2><<<blocks_for(m->n_cells), kBlock, 0, s>>>(
+                                *m, p, prims, w->bc_vals, w->face_vals, grads, has_grads));
+    FVM_LAUNCH(KID_FACE, s, k_face<DIM><<<blocks_for(m->n_facets), kBlock, 0, s>>>(*m, p, prims, w->face_vals,
+                                                                                   grads, w->flux));
+    return launch_status();
+}
+
+template <int DIM>
+static int residual_impl(const fvm_mesh_t* m, const Phys& p, const float* prims, float* grads,
+                         int32_t* has_grads, float* dudt, const fvm_work_t* w, cudaStream_t s) {
+    int rc = launch_fluxes<DIM>(m, p, prims, grads, has_grads, w, s);
+    if (rc) return rc;
+    StageArgs a{};
+    FVM_LAUNCH(KID_DIV_STAGE, s, k_div_stage<DIM><<<blocks_for(m->n_cells), kBlock, 0, s>>>(
+                                     *m, p, w->flux, a, nullptr, nullptr, nullptr, nullptr, nullptr, dudt));
+    return launch_status();
+}
+
+static StageArgs stage_args(const fvm_tableau_t* tab, int s) {
+    StageArgs a{};
+    const int S = tab->stages;
+    a.s = s;
+    a.final_ = s == S - 1;
+    if (!a.final_) {
+        for (int j = 0; j <= s; ++j)
+            if (tab->a[s + 1][j] != 0.f) {
+                a.idx[a.n_terms] = j;
+                a.coef[a.n_terms++] = tab->a[s + 1][j];
+            }
+        bool needed = tab->b[s] != 0.f || (tab->adaptive && tab->b2[s] != 0.f);
+        for (int i = s + 2; i < S; ++i) needed = needed || tab->a[i][s] != 0.f;
+        a.store_k = needed;
+    } else {
+        for (int j = 0; j < S; ++j)
+            if (tab->b[j] != 0.f) {
+                a.idx[a.n_terms] = j;
+                a.coef[a.n_terms++] = tab->b[j];
+            }
+        if (tab->adaptive) {
+            for (int j = 0; j < S; ++j)
+                if (tab->b2[j] != 0.f) {
+                    a.idx_lo[a.n_lo] = j;
+                    a.coef_lo[a.n_lo++] = tab->b2[j];
+                }
+        }
+        a.store_k = 0;
+        a.adaptive = tab->adaptive;
+        a.cfl = tab->cfl > 0.f;
+    }
+    return a;
+}
+
+template <int DIM>
+static int stage_impl(const fvm_mesh_t* m, const Phys& p, const fvm_tableau_t* tab, int s,
+                      const fvm_solver_bufs_t* b, const fvm_work_t* w, cudaStream_t st) {
+    int rc = launch_fluxes<DIM>(m, p, b->prims, b->grads, b->has_grads, w, st);
+    if (rc) return rc;
+    StageArgs a = stage_args(tab, s);
+    a.cons = a.final_ && b->cons != nullptr;
+    FVM_LAUNCH(KID_DIV_STAGE, st, k_div_stage<DIM><<<blocks_for(m->n_cells), kBlock, 0, st>>>(
+                                      *m, p, w->flux, a, b->state, b->prims, b->k, b->dt, w->red, nullptr));
+    rc = launch_status();
+    if (rc) return rc;
+    if (a.final_ && (a.adaptive || a.cfl || a.cons)) {
+        FVM_LAUNCH(KID_FINALIZE, st,
+                   k_finalize<<<1, 32, 0, st>>>(m->n_comp, tab->adaptive, tab->atol, tab->rtol, tab->mtol,
+                                                tab->alpha_hi_err, tab->alpha_lo_err, tab->order, tab->cfl,
+                                                a.cons, w->red, b->dt, b->cons));
+        rc = launch_status();
+    }
+    return rc;
+}
+
+template <int DIM>
+static int multistep_impl(const fvm_mesh_t* m, const Phys& p, int store, int n_terms, const int32_t* idx,
+                          const float* coef, const fvm_solver_bufs_t* b, const fvm_work_t* w,
+                          cudaStream_t st) {
+    int rc = launch_fluxes<DIM>(m, p, b->prims, b->grads, b->has_grads, w, st);
+    if (rc) return rc;
+    StageArgs a{};
+    a.s = store;
+    a.store_k = 1;
+    a.final_ = 1;
+    a.n_terms = n_terms;
+    for (int t = 0; t < n_terms; ++t) {
+        a.idx[t] = idx[t];
+        a.coef[t] = coef[t];
+    }
+    a.cons = b->cons != nullptr;
+    FVM_LAUNCH(KID_DIV_STAGE, st, k_div_stage<DIM><<<blocks_for(m->n_cells), kBlock, 0, st>>>(
+                                      *m, p, w->flux, a, b->state, b->prims, b->k, b->dt, w->red, nullptr));
+    rc = launch_status();
+    if (rc) return rc;
+    if (a.cons) {
+        FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<1, 32, 0, st>>>(m->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f,
+                                                                   0.f, 1, w->red, b->dt, b->cons));
+        rc = launch_status();
+    }
+    return rc;
+}
+
+}  // namespace fvm
+
+using namespace fvm;
+
+extern "C" int fvm_residual(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const float* prims,
+                            float* grads, int32_t* has_grads, float* dudt, const fvm_work_t* work,
+                            void* stream) {
+    if (!mesh_ok(mesh)) return mesh && mesh->kg != mesh->dim + 2 ? FVM_E_UNSUPPORTED : FVM_E_ARG;
+    if (!phys || !prims || !grads || !has_grads || !dudt || !work_ok(mesh, work)) return FVM_E_ARG;
+    const Phys p = make_phys(phys);
+    cudaStream_t s = (cudaStream_t)stream;
+    return mesh->dim == 2 ? residual_impl<2>(mesh, p, prims, grads, has_grads, dudt, work, s)
+                          : residual_impl<3>(mesh, p, prims, grads, has_grads, dudt, work, s);
+}
+
+static bool bufs_ok(const fvm_solver_bufs_t* b) {
+    return b && b->state && b->prims && b->grads && b->k && b->dt && b->has_grads;
+}
+
+static bool tab_ok(const fvm_tableau_t* t) { return t && t->stages >= 1 && t->stages <= FVM_MAX_STAGES; }
+
+extern "C" int fvm_stage(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const fvm_tableau_t* tab,
+                         int32_t s, const fvm_solver_bufs_t* bufs, const fvm_work_t* work, void* stream) {
+    if (!mesh_ok(mesh) || !phys || !tab_ok(tab) || s < 0 || s >= tab->stages || !bufs_ok(bufs) ||
+        !work_ok(mesh, work))
+        return FVM_E_ARG;
+    const Phys p = make_phys(phys);
+    cudaStream_t st = (cudaStream_t)stream;
+    return mesh->dim == 2 ? stage_impl<2>(mesh, p, tab, s, bufs, work, st)
+                          : stage_impl<3>(mesh, p, tab, s, bufs, work, st);
+}
+
+extern "C" int fvm_step(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const fvm_tableau_t* tab,
+                        const fvm_solver_bufs_t* bufs, const fvm_work_t* work, void* stream) {
+    if (!mesh_ok(mesh) || !phys || !tab_ok(tab) || !bufs_ok(bufs) || !work_ok(mesh, work)) return FVM_E_ARG;
+    const Phys p = make_phys(phys);
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int s = 0; s < tab->stages; ++s) {
+        const int rc = mesh->dim == 2 ? stage_impl<2>(mesh, p, tab, s, bufs, work, st)
+                                      : stage_impl<3>(mesh, p, tab, s, bufs, work, st);
+        if (rc) return rc;
+    }
+    return FVM_OK;
+}
+
+extern "C" int fvm_multistep(const fvm_mesh_t* mesh, const fvm_physics_t* phys, int32_t store,
+                             int32_t n_terms, const int32_t* idx, const float* coef,
+                             const fvm_solver_bufs_t* bufs, const fvm_work_t* work, void* stream) {
+    if (!mesh_ok(mesh) || !phys || !bufs_ok(bufs) || !work_ok(mesh, work) || n_terms < 0 ||
+        n_terms > FVM_MAX_STAGES || (n_terms > 0 && (!idx || !coef)) || store < 0)
+        return FVM_E_ARG;
+    const Phys p = make_phys(phys);
+    cudaStream_t st = (cudaStream_t)stream;
+    return mesh->dim == 2 ? multistep_impl<2>(mesh, p, store, n_terms, idx, coef, bufs, work, st)
+                          : multistep_impl<3>(mesh, p, store, n_terms, idx, coef, bufs, work, st);
+}
+
+extern "C" int fvm_state_to_prims(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const float* state,
+                                  float* prims, void* stream) {
+    if (!mesh_ok(mesh) || !phys || !state || !prims) return FVM_E_ARG;
+    const Phys p = make_phys(phys);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (mesh->dim == 2)
+        FVM_LAUNCH(KID_STATE_TO_PRIMS, st, k_state_to_prims<4><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
+                                               mesh->n_cells, p.inv_Cv, state, prims));
+    else
+        FVM_LAUNCH(KID_STATE_TO_PRIMS, st, k_state_to_prims<5><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
+                                               mesh->n_cells, p.inv_Cv, state, prims));
+    return launch_status();
+}
+
+extern "C" int fvm_cfl_dt(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const float* state, float cfl,
+                          float* dt, const fvm_work_t* work, void* stream) {
+    if (!mesh_ok(mesh) || !phys || !state || !dt || !work || !work->red || !(cfl > 0.f)) return FVM_E_ARG;
+    const Phys p = make_phys(phys);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (mesh->dim == 2)
+        FVM_LAUNCH(KID_REDUCE_STATE, st, k_reduce_state<2><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
+                                             *mesh, p, state, 1, 0, work->red));
+    else
+        FVM_LAUNCH(KID_REDUCE_STATE, st, k_reduce_state<3><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
+                                             *mesh, p, state, 1, 0, work->red));
+    int rc = launch_status();
+    if (rc) return rc;
+    FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<1, 32, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, cfl,
+                                                               0, work->red, dt, nullptr));
+    return launch_status();
+}
+
+extern "C" int fvm_conservation(const fvm_mesh_t* mesh, const float* state, double* out, const fvm_work_t* work,
+                                void* stream) {
+    if (!mesh_ok(mesh) || !state || !out || !work || !work->red) return FVM_E_ARG;
+    Phys p{};
+    cudaStream_t st = (cudaStream_t)stream;
+    if (mesh->dim == 2)
+        FVM_LAUNCH(KID_REDUCE_STATE, st, k_reduce_state<2><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
+                                             *mesh, p, state, 0, 1, work->red));
+    else
+        FVM_LAUNCH(KID_REDUCE_STATE, st, k_reduce_state<3><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
+                                             *mesh, p, state, 0, 1, work->red));
+    int rc = launch_status();
+    if (rc) return rc;
+    FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<1, 32, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f,
+                                                               1, work->red, nullptr, out));
+    return launch_status();
+}

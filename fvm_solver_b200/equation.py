@@ -1,0 +1,227 @@
+"""Residual seam: ``FluidConstitution2D/3D``, ``FVMCells``, ``FVMEquation``.
+
+Mirrors ``time_fvm/fvm_equation.py`` and ``time_fvm/time_solvers/t_solvers.py:15-42``.
+
+``FVMEquation(cfg, phy_setup, mesh, n_comp, bc_tag, us_init)`` has the reference's signature.
+``mesh`` may be this package's ``FVMMesh2D/3D`` or any object with the reference mesh's raw inputs
+(``vertices``, ``cells``, ``facets``, ``bc_facet_mask``; e.g. a reference ``FVMMesh2D``): the host
+tables are rebuilt from them bit-identically.  ``forward(primatives)`` returns dU/dt through the
+fused CUDA residual (``fvm_residual``) and, like the reference, carries the limited cell
+gradients (``cell_grads``) into the next call's boundary correction.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import torch
+
+from . import _lib
+from .config import ConfigFVM
+from .fvm_mesh import FVMMesh, FVMMesh2D, FVMMesh3D
+from .tables import FVMTables, KernelTables
+
+
+class FluidConstitution:
+    """Ideal gas with Sutherland viscosity (``fvm_equation.py:16-87``).
+
+    The conversions below are setup/inspection utilities (torch ops); the time loop converts on
+    the device inside the stage kernels.
+    """
+    dim: int
+
+    def __init__(self, cfg: ConfigFVM, dim: int):
+        self.device = cfg.device
+        self.dim = dim
+        self.T_0 = cfg.T_0
+        self.mu = cfg.viscosity
+        self.mu_b = cfg.visc_bulk
+        self.S_const = cfg.S_const
+        self.C_v = cfg.C_v
+        self.gamma = cfg.gamma
+        self.R = self.C_v * (cfg.gamma - 1)
+
+    def state_to_primative(self, state: torch.Tensor):
+        d = self.dim
+        momentum, rho, Q = state[:, :d], state[:, d:d + 1], state[:, d + 1:d + 2]
+        V = momentum / rho
+        T = 1 / self.C_v * (Q / rho - 0.5 * V.square().sum(dim=1, keepdim=True))
+        return torch.cat([V, rho, T], dim=-1), state
+
+    def primatives_to_state(self, V, rho, T):
+        momentum = V * rho
+        Q = rho * (self.C_v * T + 0.5 * V.square().sum(dim=-1, keepdim=True))
+        return momentum, rho, Q
+
+    def eos_c(self, rho, T):
+        return torch.sqrt(self.gamma * self.R * T)
+
+    def eos_P(self, rho, T):
+        return self.R * rho * T
+
+    def eos_T(self, rho, P):
+        return P / (self.R * rho)
+
+    def physics_struct(self, cfg: ConfigFVM) -> _lib.Physics:
+        return _lib.Physics(T_0=self.T_0, mu=self.mu, mu_b=self.mu_b, S_const=self.S_const, C_v=self.C_v,
+                            gamma=self.gamma, kappa=cfg.thermal_cond, v_factor=cfg.v_factor,
+                            lim_p=cfg.lim_p)
+
+
+class FluidConstitution2D(FluidConstitution):
+    def __init__(self, cfg: ConfigFVM, dim: int = 2):
+        super().__init__(cfg, dim)
+        assert self.dim == 2, "Only for 2D fluids"
+
+
+class FluidConstitution3D(FluidConstitution):
+    def __init__(self, cfg: ConfigFVM, dim: int = 3):
+        super().__init__(cfg, dim)
+        assert self.dim == 3, "Only for 3D fluids"
+
+
+class DeviceMesh:
+    """Kernel tables uploaded to one device, plus the ``fvm_mesh_t`` struct pointing at them."""
+
+    _ptr_fields = [f for f, _ in _lib.Mesh._fields_[8:]]
+
+    def __init__(self, kt: KernelTables, device):
+        self.device = torch.device(device)
+        self.t = kt.to(self.device)
+        self.dim, self.n_comp, self.n_cells = kt.dim, kt.n_comp, kt.n_cells
+        self.n_facets, self.n_bc = kt.n_facets, kt.n_bc
+        m = _lib.Mesh(dim=kt.dim, n_comp=kt.n_comp, n_cells=kt.n_cells, n_facets=kt.n_facets,
+                      n_bc=kt.n_bc, n_char=kt.n_char, kg=kt.kg, kf=kt.kf)
+        for f in self._ptr_fields:
+            setattr(m, f, _lib.ptr(getattr(self.t, f)))
+        self.struct = m
+
+    def work(self) -> "Work":
+        return Work(self)
+
+    def bytes(self) -> int:
+        return sum(v.numel() * v.element_size() for v in self.t.__dict__.values() if isinstance(v, torch.Tensor))
+
+
+class Work:
+    """Caller-owned scratch of one mesh (``fvm_work_t``)."""
+
+    def __init__(self, dm: DeviceMesh):
+        C, dev = dm.n_comp, dm.device
+        self.bc_vals = torch.zeros((max(dm.n_bc, 1), C), device=dev)
+        self.face_vals = torch.zeros((dm.n_facets, 2, C), device=dev)
+        self.flux = torch.zeros((dm.n_facets, C), device=dev)
+        self.red = torch.zeros(_lib.FVM_RED_DOUBLES, device=dev, dtype=torch.float64)
+        self.struct = _lib.Work(bc_vals=_lib.ptr(self.bc_vals), face_vals=_lib.ptr(self.face_vals),
+                                flux=_lib.ptr(self.flux), red=_lib.ptr(self.red))
+
+
+def _host_mesh(mesh, dim_hint=None) -> FVMMesh:
+    if isinstance(mesh, FVMMesh):
+        return mesh
+    cls = FVMMesh2D if mesh.vertices.shape[1] == 2 else FVMMesh3D
+    kw = {}
+    if getattr(mesh, "period", None) is not None:
+        kw = dict(period=mesh.period, cell_shifts=mesh.cell_shifts, facet_shifts=mesh.facet_shifts)
+    return cls(mesh.vertices.float().cpu(), mesh.cells.cpu(), mesh.facets.cpu(), mesh.bc_facet_mask.cpu(), **kw)
+
+
+class FVMCells:
+    """Conserved state on the device (``t_solvers.py:15-42``)."""
+
+    def __init__(self, n_cells, n_comp, phys_setup: FluidConstitution, init_val=None, device="cuda"):
+        self.device = device
+        self.phys_setup = phys_setup
+        if init_val is None:
+            state = torch.zeros(n_cells, n_comp, device=device)
+        else:
+            assert init_val.shape == (n_cells, n_comp), f"Incorrect us init shape {init_val.shape = }"
+            state = init_val.to(device=device, dtype=torch.float32)
+        self._state = state.contiguous()
+        self.version = 0
+
+    @property
+    def state(self) -> torch.Tensor:
+        return self._state
+
+    @state.setter
+    def state(self, value: torch.Tensor):
+        self._state.copy_(value)
+        self.version += 1
+
+    def update_cells(self, state_new):
+        self.state = state_new
+
+    def get_values(self):
+        return self.phys_setup.state_to_primative(self._state)
+
+    def convert_state_to_value(self, state):
+        return self.phys_setup.state_to_primative(state)
+
+    def save(self, name="state.pt"):
+        torch.save(self._state, name)
+
+    def load(self, name="state.pt"):
+        self.state = torch.load(name, weights_only=True).to(self.device)
+
+
+class FVMEquation:
+    """``FVMEquation`` (``fvm_equation.py:371-435``) on the B200 kernels."""
+
+    def __init__(self, cfg: ConfigFVM, phy_setup: FluidConstitution, mesh, n_comp, bc_tag, us_init=None,
+                 build_solver: bool = True):
+        if getattr(cfg, "backend", "b200") != "b200":
+            raise ValueError(f"unknown backend {cfg.backend!r}")
+        self.cfg = cfg
+        self.phy_setup = phy_setup
+        self.device = torch.device(cfg.device)
+        if self.device.type != "cuda":
+            raise RuntimeError("fvm_solver_b200 runs on CUDA devices only (no CPU fallback)")
+        self.lib = _lib.load()
+        self.mesh = _host_mesh(mesh)
+        self.n_comp = n_comp
+        assert n_comp == self.mesh.dim + 2, "n_comp must be dim + 2"
+        self.tables = FVMTables(self.mesh, cfg, n_comp, bc_tag)
+        self.dev = DeviceMesh(self.tables.kernel, self.device)
+        self.work = self.dev.work()
+        self.phys = phy_setup.physics_struct(cfg)
+        N, dim = self.mesh.n_cells, self.mesh.dim
+        self.grads = torch.zeros((N, dim, n_comp), device=self.device)
+        self.has_grads = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self._has_grads_host = False
+        self.cells = FVMCells(N, n_comp, init_val=us_init, phys_setup=phy_setup, device=self.device)
+        self.t_solver = None
+        if build_solver:
+            from .solvers import get_solver
+            self.t_solver = get_solver(self.cells, self, cfg)
+
+    @property
+    def cell_grads(self):
+        """Limited cell gradients of the last evaluation [N, dim, C], or None before the first."""
+        return self.grads if self._has_grads_host else None
+
+    def reset_gradients(self):
+        """Forget the carried gradients (the next evaluation behaves like the reference's first)."""
+        self.has_grads.zero_()
+        self._has_grads_host = False
+
+    def solve(self):
+        self.t_solver.solve()
+
+    def forward(self, primatives: torch.Tensor) -> torch.Tensor:
+        """dU/dt [N, C] of the primitives [N, C] (V, rho, T)."""
+        prims = primatives.to(device=self.device, dtype=torch.float32).contiguous()
+        assert prims.shape == (self.mesh.n_cells, self.n_comp), f"bad primatives shape {tuple(prims.shape)}"
+        out = torch.empty_like(prims)
+        _lib.check(self.lib.fvm_residual(ct.byref(self.dev.struct), ct.byref(self.phys), _lib.ptr(prims),
+                                         _lib.ptr(self.grads), _lib.ptr(self.has_grads), _lib.ptr(out),
+                                         ct.byref(self.work.struct), _lib.stream_ptr()), "fvm_residual")
+        self._has_grads_host = True
+        return out
+
+    def conservation(self, state: torch.Tensor | None = None) -> torch.Tensor:
+        """FP64 totals sum_i vol_i U_i [C] of ``state`` (default: the current cell state)."""
+        s = (self.cells.state if state is None else state).contiguous()
+        out = torch.empty(self.n_comp, dtype=torch.float64, device=self.device)
+        _lib.check(self.lib.fvm_conservation(ct.byref(self.dev.struct), _lib.ptr(s), _lib.ptr(out),
+                                             ct.byref(self.work.struct), _lib.stream_ptr()), "fvm_conservation")
+        return out

@@ -1,0 +1,285 @@
+"""Time integrators on the device (mirrors ``time_fvm/time_solvers/integrators.py`` / ``t_solvers.py``).
+
+Every solver advances ``FVMCells.state`` with ``fvm_step`` / ``fvm_multistep``: the stage
+combinations, the conserved -> primitive conversion and the step-size update all run inside the
+stage kernels; ``dt`` lives on the device, so a step issues no host synchronisation and whole
+steps can be captured in a CUDA graph (``TSolver.graph_steps``).
+
+* ``Butcher(name)``       -- fixed (or CFL) dt, tableau ``name`` (``integrators.py:349-393``)
+* ``ButcherAdapt(name)``  -- embedded error estimate + ``Adaptive.update_stepsize``
+                             (``integrators.py:42-62, 305-346``)
+* ``RK3_SSP4``            -- the hand-unrolled four-stage SSP-RK3 (``integrators.py:65-94``): the
+                             same tableau as ``Butcher_Tables("RK3_SSP4")`` with the low-order
+                             estimate ``U_b - U_0 = (k1 + k2) / 2``
+* ``AB3``                 -- Adams-Bashforth 3 after two SSP-RK3 start-up steps (restated; the
+                             reference's ``Adams3PC`` cannot run, ``integrators.py:111``)
+* ``SSP_RK3``             -- three-stage Shu-Osher SSP-RK3 tableau (restated from
+                             ``integrators_bad.py:13-35``)
+
+``cfg.cfl`` (when set) recomputes dt = cfl * min h / (|u| + c) in FP64 after every step.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import torch
+
+from . import _lib
+
+_T = {
+    # integrators.py:216-226
+    "RK4": ([[0, 0, 0, 0], [0.5, 0, 0, 0], [0, 0.5, 0, 0], [0, 0, 1.0, 0]],
+            [1 / 6, 1 / 3, 1 / 3, 1 / 6], [1 / 4] * 4),
+    # integrators.py:228-238
+    "RK3_SSP4": ([[0, 0, 0, 0], [0.5, 0, 0, 0], [0.5, 0.5, 0, 0], [1 / 6, 1 / 6, 1 / 6, 0]],
+                 [1 / 6, 1 / 6, 1 / 6, 1 / 2], [1 / 4] * 4),
+    # integrators.py:240-251
+    "RK3_SSP5": ([[0, 0, 0, 0, 0],
+                  [0.37726891511710, 0, 0, 0, 0],
+                  [0.37726891511710, 0.37726891511710, 0, 0, 0],
+                  [0.16352294089771, 0.16352294089771, 0.16352294089771, 0, 0],
+                  [0.14904059394856, 0.14831273384724, 0.14831273384724, 0.34217696850008, 0]],
+                 [0.19707596384481, 0.11780316509765, 0.11709725193772, 0.27015874934251, 0.29786487010104],
+                 [1 / 5] * 5),
+    # integrators.py:253-265
+    "RK3_SSP6": ([[0, 0, 0, 0, 0, 0],
+                  [0.28422, 0, 0, 0, 0, 0],
+                  [0.28422, 0.28422, 0, 0, 0, 0],
+                  [0.23071, 0.23071, 0.23071, 0, 0, 0],
+                  [0.13416, 0.13416, 0.13416, 0.16528, 0, 0],
+                  [0.13416, 0.13416, 0.13416, 0.16528, 0.28422, 0]],
+                 [0.17016, 0.17016, 0.10198, 0.12563, 0.21604, 0.21604], [1 / 6] * 6),
+    # integrators.py:267-278
+    "RK4_SSP5": ([[0, 0, 0, 0, 0],
+                  [0.39175222700392, 0, 0, 0, 0],
+                  [0.21766909633821, 0.36841059262959, 0, 0, 0],
+                  [0.08269208670950, 0.13995850206999, 0.25189177424738, 0, 0],
+                  [0.06796628370320, 0.11503469844438, 0.20703489864929, 0.54497475021237, 0]],
+                 [0.14681187618661, 0.24848290924556, 0.10425883036650, 0.27443890091960, 0.22600748319395],
+                 [1 / 5] * 5),
+    # integrators.py:280-296
+    "RK4_SSP10": ([[0] * 10,
+                   [1 / 6] + [0] * 9,
+                   [1 / 6] * 2 + [0] * 8,
+                   [1 / 6] * 3 + [0] * 7,
+                   [1 / 6] * 4 + [0] * 6,
+                   [1 / 15] * 5 + [0] * 5,
+                   [1 / 15] * 5 + [1 / 6] + [0] * 4,
+                   [1 / 15] * 5 + [1 / 6] * 2 + [0] * 3,
+                   [1 / 15] * 5 + [1 / 6] * 3 + [0] * 2,
+                   [1 / 15] * 5 + [1 / 6] * 4 + [0]],
+                  [1 / 10] * 10, [1 / 5, 0, 0, 3 / 10, 0, 0, 1 / 5, 0, 3 / 10, 0]),
+    # three-stage Shu-Osher SSP-RK3
+    "SSP_RK3": ([[0, 0, 0], [1, 0, 0], [0.25, 0.25, 0]], [1 / 6, 1 / 6, 2 / 3], [0.5, 0.5, 0]),
+}
+
+
+def tableau_names():
+    return sorted(_T)
+
+
+def make_tableau(name: str, adaptive=False, cfl: float | None = None, b2=None, atol=2e-3, rtol=2e-3,
+                 mtol=1e-6, alphas=(0.8, 0.995), order=4) -> _lib.Tableau:
+    if name not in _T:
+        raise NotImplementedError("Unknown Butcher tableau")
+    A, b, b2d = _T[name]
+    b2 = b2d if b2 is None else b2
+    t = _lib.Tableau()
+    t.stages = len(b)
+    for i, row in enumerate(A):
+        for j, v in enumerate(row):
+            t.a[i][j] = float(torch.tensor(v, dtype=torch.float32))
+    for j in range(len(b)):
+        t.b[j] = float(torch.tensor(b[j], dtype=torch.float32))
+        t.b2[j] = float(torch.tensor(b2[j], dtype=torch.float32))
+    t.adaptive = int(adaptive)
+    t.atol, t.rtol, t.mtol = atol, rtol, mtol
+    t.alpha_hi_err, t.alpha_lo_err = alphas
+    t.order = order
+    t.cfl = float(cfl) if cfl else 0.0
+    return t
+
+
+class TSolver:
+    """Device time stepper for one ``FVMEquation``."""
+
+    n_k = 0
+
+    def __init__(self, cells, eq, cfg):
+        self.cfg = cfg
+        self.cells = cells
+        self.eq = eq
+        self.lib = eq.lib
+        dev = eq.device
+        self.n_steps = cfg.n_iter
+        self.end_t = cfg.end_t
+        self.print_i = cfg.print_i
+        N, C = eq.mesh.n_cells, eq.n_comp
+        self.prims = torch.zeros((N, C), device=dev)
+        self.k = torch.zeros((max(self.n_k, 1), N, C), device=dev)
+        self.dt = torch.tensor([cfg.dt if cfg.dt is not None else 0.0], dtype=torch.float32, device=dev)
+        self.cons = None
+        self._prims_version = -1
+        self.t = 0.0
+        self.steps_done = 0
+        self.bufs = _lib.SolverBufs(state=_lib.ptr(cells.state), prims=_lib.ptr(self.prims),
+                                    grads=_lib.ptr(eq.grads), k=_lib.ptr(self.k), dt=_lib.ptr(self.dt),
+                                    has_grads=_lib.ptr(eq.has_grads), cons=None)
+        self.cfl = cfg.cfl
+        if self.cfl:
+            self.update_cfl_dt()
+
+    # -- helpers ------------------------------------------------------------------------------
+    def track_conservation(self, on: bool = True):
+        """Record the FP64 totals sum vol * U after every step in ``self.cons`` (device)."""
+        if on and self.cons is None:
+            self.cons = torch.zeros(self.eq.n_comp, dtype=torch.float64, device=self.eq.device)
+        self.bufs.cons = _lib.ptr(self.cons) if on else None
+
+    def update_cfl_dt(self, cfl: float | None = None):
+        cfl = cfl or self.cfl
+        _lib.check(self.lib.fvm_cfl_dt(ct.byref(self.eq.dev.struct), ct.byref(self.eq.phys),
+                                       _lib.ptr(self.cells.state), float(cfl), _lib.ptr(self.dt),
+                                       ct.byref(self.eq.work.struct), _lib.stream_ptr()), "fvm_cfl_dt")
+
+    def _sync_prims(self):
+        if self._prims_version != self.cells.version:
+            _lib.check(self.lib.fvm_state_to_prims(ct.byref(self.eq.dev.struct), ct.byref(self.eq.phys),
+                                                   _lib.ptr(self.cells.state), _lib.ptr(self.prims),
+                                                   _lib.stream_ptr()), "fvm_state_to_prims")
+            self._prims_version = self.cells.version
+
+    def _step(self):
+        raise NotImplementedError
+
+    def _solve_step(self, t=None):
+        self._sync_prims()
+        self._step()
+        self.eq._has_grads_host = True
+        self.steps_done += 1
+
+    def step(self, n: int = 1):
+        for _ in range(n):
+            self._solve_step()
+
+    def graph_steps(self, n: int):
+        """Capture ``n`` steps in a CUDA graph; returns a callable that replays them."""
+        self._sync_prims()
+        s = torch.cuda.Stream(device=self.eq.device)
+        s.wait_stream(torch.cuda.current_stream())
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(s):
+            # the capture must not start with an un-synced conversion
+            with torch.cuda.graph(g, stream=s):
+                for _ in range(n):
+                    self._step()
+        torch.cuda.current_stream().wait_stream(s)
+
+        def replay():
+            g.replay()
+            self.eq._has_grads_host = True
+            self.steps_done += n
+
+        replay.graph = g
+        return replay
+
+    def solve(self):
+        """Run ``n_iter`` steps (or until ``end_t`` with host-side time accounting)."""
+        if self.n_steps is None and self.end_t is None:
+            raise ValueError("Either n_iter or end_t must be set in ConfigFVM")
+        i = 0
+        while True:
+            if self.n_steps is not None and i >= self.n_steps:
+                break
+            if self.end_t is not None and self.t >= self.end_t:
+                break
+            dt = float(self.dt.item()) if self.end_t is not None else 0.0
+            self._solve_step()
+            self.t += dt
+            if self.print_i and i % self.print_i == 0:
+                if not torch.isfinite(self.cells.state).all():
+                    raise ValueError("Nan detected in primatives")
+            i += 1
+
+
+class Butcher(TSolver):
+    def __init__(self, cells, eq, name, cfg, adaptive=False, **kw):
+        self.name = name
+        self.tab = make_tableau(name, adaptive=adaptive, cfl=None if adaptive else cfg.cfl, **kw)
+        self.n_k = self.tab.stages
+        self.stages = self.tab.stages
+        super().__init__(cells, eq, cfg)
+
+    def _step(self):
+        _lib.check(self.lib.fvm_step(ct.byref(self.eq.dev.struct), ct.byref(self.eq.phys), ct.byref(self.tab),
+                                     ct.byref(self.bufs), ct.byref(self.eq.work.struct), _lib.stream_ptr()),
+                   "fvm_step")
+
+
+class ButcherAdapt(Butcher):
+    def __init__(self, cells, eq, name, cfg):
+        super().__init__(cells, eq, name, cfg, adaptive=True, atol=2e-3, rtol=2e-3, mtol=1e-6,
+                         alphas=(0.8, 0.995), order=4)
+
+
+class RK3_SSP4(Butcher):
+    def __init__(self, cells, eq, cfg):
+        super().__init__(cells, eq, "RK3_SSP4", cfg, adaptive=True, b2=[0.5, 0.5, 0.0, 0.0], atol=2e-3,
+                         rtol=2e-3, mtol=1e-6, alphas=(0.8, 0.995), order=4)
+
+
+class AB3(TSolver):
+    """Adams-Bashforth 3 (fixed dt) after two three-stage SSP-RK3 start-up steps."""
+    n_k = 3
+    COEF = (23 / 12, -16 / 12, 5 / 12)
+
+    def __init__(self, cells, eq, cfg):
+        self.rk = make_tableau("SSP_RK3", cfl=None)
+        super().__init__(cells, eq, cfg)
+        self.n_hist = 0
+        self.head = 0
+        self.rk_k = torch.zeros((3, eq.mesh.n_cells, eq.n_comp), device=eq.device)
+        self.rk_bufs = _lib.SolverBufs(state=self.bufs.state, prims=self.bufs.prims, grads=self.bufs.grads,
+                                       k=_lib.ptr(self.rk_k), dt=self.bufs.dt, has_grads=self.bufs.has_grads,
+                                       cons=None)
+        self._idx = (ct.c_int32 * 3)()
+        self._coef = (ct.c_float * 3)()
+
+    def _multistep(self, n_terms, idx, coef):
+        for t in range(n_terms):
+            self._idx[t] = idx[t]
+            self._coef[t] = coef[t]
+        _lib.check(self.lib.fvm_multistep(ct.byref(self.eq.dev.struct), ct.byref(self.eq.phys), idx[0], n_terms,
+                                          ct.cast(self._idx, ct.c_void_p), ct.cast(self._coef, ct.c_void_p),
+                                          ct.byref(self.bufs), ct.byref(self.eq.work.struct), _lib.stream_ptr()),
+                   "fvm_multistep")
+
+    def _step(self):
+        h = self.head
+        if self.n_hist < 2:
+            # Start-up: an SSP-RK3 step from U_n; its first increment dt * f(U_n) joins the history.
+            _lib.check(self.lib.fvm_step(ct.byref(self.eq.dev.struct), ct.byref(self.eq.phys), ct.byref(self.rk),
+                                         ct.byref(self.rk_bufs), ct.byref(self.eq.work.struct), _lib.stream_ptr()),
+                       "fvm_step")
+            self.k[h].copy_(self.rk_k[0])
+        else:
+            idx = [h, (h - 1) % 3, (h - 2) % 3]
+            self._multistep(3, idx, list(self.COEF))
+        self.n_hist = min(self.n_hist + 1, 3)
+        self.head = (h + 1) % 3
+
+
+def get_solver(cells, equation, cfg):
+    """``get_solver`` (``integrators.py:11-27``)."""
+    name, extra = cfg.solver_name, cfg.solver_extra
+    if name == "RK3_SSP4":
+        return RK3_SSP4(cells, equation, cfg)
+    if name == "Butcher_adapt":
+        return ButcherAdapt(cells, equation, extra, cfg)
+    if name == "Butcher":
+        return Butcher(cells, equation, extra, cfg)
+    if name == "AB3":
+        return AB3(cells, equation, cfg)
+    if name in ("Adams3_PC", "Adams4_PC", "Euler"):
+        raise NotImplementedError(f"{name} is not provided (its reference implementation cannot run)")
+    raise NotImplementedError("Invalid solver.")

@@ -198,6 +198,7 @@ class KernelTables:
     bc_ga: torch.Tensor       # [Fb, C] f32 face-gradient coefficient on the cell value
     bc_gb: torch.Tensor       # [Fb, C] f32 face-gradient offset
     bc_char: torch.Tensor     # [Fb] i32 index into the characteristic arrays or -1
+    ch_cell: torch.Tensor     # [Fc] i32 cell of each characteristic facet
     ch_normal: torch.Tensor   # [Fc, dim] f32
     ch_rho: torch.Tensor      # [Fc] f32
     ch_vn: torch.Tensor       # [Fc] f32
@@ -435,6 +436,9 @@ class FVMTables:
         nb_slot = torch.zeros(N, dtype=torch.int64)
         for j in range(K):
             nb_slot |= slot[:, j].long() << (4 * j)
+        # bits 24..28: number of valid (unpadded) slots of the cell's gradient row
+        row_nnz = torch.bincount(self.ops.G_mats.coalesce().indices()[0], minlength=N * dim).view(N, dim)[:, 0]
+        nb_slot |= row_nnz.long() << 24
         disp = self.mesh.cent_to_facet_disp.permute(1, 2, 0).contiguous()          # [K, dim, N]
         eps = self.eps_p.reshape(-1).contiguous()
         c2f = self.mesh.cell_to_facet.t().contiguous().to(i32)
@@ -488,9 +492,11 @@ class FVMTables:
         if ch is None:
             z = torch.zeros(0, dtype=torch.float32)
             ch_n, ch_r, ch_vn, ch_vt, ch_p = torch.zeros((0, dim)), z, z, torch.zeros((0, dim)), z
+            ch_cell = torch.zeros(0, dtype=i32)
             nchar = 0
         else:
             ch_n, ch_r, ch_vn, ch_vt, ch_p = ch.normals, ch.rho_inf, ch.v_n_inf, ch.v_t_inf, ch.p_inf
+            ch_cell = ch.cells.to(i32)
             nchar = int(ch.bc_idx.shape[0])
 
         return KernelTables(
@@ -504,7 +510,7 @@ class FVMTables:
             inv_d=inv_d,
             bc_face=self.bc_locations.to(i32), bc_side=self.bc_facet_side.to(i32),
             bc_cell=self.facet_to_cell_bc.to(i32), bc_kind=bc_kind, bc_b=bc_b, bc_l=bc_l,
-            bc_ga=bc_ga, bc_gb=bc_gb, bc_char=bc_char,
+            bc_ga=bc_ga, bc_gb=bc_gb, bc_char=bc_char, ch_cell=ch_cell,
             ch_normal=ch_n.float().contiguous(), ch_rho=ch_r.float(), ch_vn=ch_vn.float(),
             ch_vt=ch_vt.float().contiguous(), ch_p=ch_p.float(),
         )

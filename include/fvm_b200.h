@@ -1,0 +1,182 @@
+/*
+ * fvm_b200.h -- C ABI of the B200 finite-volume residual library (libfvm_b200.so).
+ *
+ * All pointers are device pointers unless stated otherwise; all arrays are dense and
+ * row-major as documented per field.  Every entry point returns 0 on success or a negative
+ * FVM_E_* code (the CUDA launch error, if any, is folded into FVM_E_CUDA and can be read
+ * with fvm_last_cuda_error()).  Work is enqueued on `stream` (a cudaStream_t passed as
+ * void*, NULL = legacy default stream); nothing synchronises the host.
+ *
+ * The reference (Merlotec/fvm_solver) is Python; the interfaces replaced here are its
+ * sparse-operator seam and its residual / integrator seam:
+ *   fvm_ell_spmv / fvm_ell_spmm   <- time_fvm/utils/ell_kernel.py:135 (ell_spmv),
+ *                                    :176 (ell_spmm); called through SPM.spMV / SPM.spMM
+ *                                    (time_fvm/utils/sparse.py:14-21, 34-38)
+ *   fvm_residual                  <- FVMEquation.forward (time_fvm/fvm_equation.py:406-435),
+ *                                    including FacetCalc.compute_facet
+ *                                    (time_fvm/fvm_stepping/facet_process.py:332-385)
+ *   fvm_stage / fvm_step          <- Butcher._step / ButcherAdapt._step / RK3_SSP4._step and
+ *                                    Adaptive.update_stepsize
+ *                                    (time_fvm/time_solvers/integrators.py:42-94, 322-393)
+ *   fvm_cfl_dt                    <- no reference counterpart (CFL time step, FP64 reduction)
+ *   fvm_conservation              <- no reference counterpart (FP64 sum of vol * U)
+ */
+#ifndef FVM_B200_H
+#define FVM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FVM_OK 0
+#define FVM_E_ARG (-1)      /* invalid argument (null pointer, size out of range) */
+#define FVM_E_CUDA (-2)     /* a CUDA launch failed; see fvm_last_cuda_error() */
+#define FVM_E_UNSUPPORTED (-3)
+
+#define FVM_MAX_STAGES 12
+#define FVM_MAX_KG 16
+#define FVM_RED_DOUBLES 64
+
+/* Mesh tables (see fvm_solver_b200/tables.py KernelTables for how they are built).
+ * N cells, F facets, Fb boundary facets, Fc characteristic facets, K = dim + 1. */
+typedef struct fvm_mesh {
+    int32_t dim, n_comp, n_cells, n_facets, n_bc, n_char, kg, kf;
+    /* cells (slot-major: [slot][cell]) */
+    const float *g_vals;      /* [dim][kg][N]  LSQ gradient weights                       */
+    const int32_t *g_cols;    /* [kg][N]       columns into [prims ; boundary values]      */
+    const int32_t *nb_slot;   /* [N]           4 bits per local facet: slot of neighbour   */
+    const float *disp;        /* [K][dim][N]   centroid -> facet midpoint                  */
+    const float *eps;         /* [N]           limiter epsilon                             */
+    const int32_t *c2f;       /* [K][N]        cell -> facet                               */
+    const int32_t *side;      /* [N]           bit j: side of local facet j (0 left)       */
+    const float *f_vals;      /* [kf][N]       divergence weights +-1/vol                  */
+    const int32_t *f_cols;    /* [kf][N]       facet indices                               */
+    const double *inv_h;      /* [N]           max facet area / volume                     */
+    const double *volumes;    /* [N]                                                       */
+    /* facets */
+    const int32_t *fcell;     /* [F][2]        side-0 / side-1 cell (boundary: cell twice)  */
+    const int32_t *fbc;       /* [F]           boundary-local index or -1                  */
+    const float *normals;     /* [F][dim]      area-weighted normals                       */
+    const float *fsize;       /* [F]           |normal|                                    */
+    const float *xorth;       /* [F][dim]      non-orthogonal correction vector            */
+    const float *inv_d;       /* [F]           1 / projected centroid distance             */
+    /* boundary facets */
+    const int32_t *bc_face, *bc_side, *bc_cell;   /* [Fb]                                  */
+    const int32_t *bc_kind;   /* [Fb][C] 1 Dirichlet, 2 Neumann, 0 other                    */
+    const float *bc_b;        /* [Fb][C] face-value offset                                 */
+    const float *bc_l;        /* [Fb][dim] tangential lever arm (non-orthogonal correction) */
+    const float *bc_ga;       /* [Fb][C] face-gradient coefficient                         */
+    const float *bc_gb;       /* [Fb][C] face-gradient offset                              */
+    const int32_t *bc_char;   /* [Fb] index into the characteristic arrays or -1            */
+    const int32_t *ch_cell;   /* [Fc] cell adjacent to each characteristic facet            */
+    const float *ch_normal;   /* [Fc][dim] outward unit normals                            */
+    const float *ch_rho, *ch_vn, *ch_p;            /* [Fc]                                 */
+    const float *ch_vt;       /* [Fc][dim]                                                 */
+} fvm_mesh_t;
+
+/* Gas and scheme constants (ConfigFVM fields, time_fvm/config_fvm.py:52-63). */
+typedef struct fvm_physics {
+    float T_0, mu, mu_b, S_const, C_v, gamma, kappa, v_factor;
+    int32_t lim_p;
+} fvm_physics_t;
+
+/* Caller-owned scratch for one mesh. */
+typedef struct fvm_work {
+    float *bc_vals;     /* [Fb][C]                                   */
+    float *face_vals;   /* [F][2][C]                                 */
+    float *flux;        /* [F][C]                                    */
+    double *red;        /* [FVM_RED_DOUBLES], zero-initialised once  */
+} fvm_work_t;
+
+/* Explicit Runge-Kutta tableau (optionally with an embedded low-order row). */
+typedef struct fvm_tableau {
+    int32_t stages;
+    float a[FVM_MAX_STAGES][FVM_MAX_STAGES];
+    float b[FVM_MAX_STAGES];
+    float b2[FVM_MAX_STAGES];
+    int32_t adaptive;                 /* 1: Adaptive.update_stepsize after the step            */
+    float atol, rtol, mtol, alpha_hi_err, alpha_lo_err, order;
+    float cfl;                        /* > 0: dt = cfl * min h / (|u| + c) after the step      */
+} fvm_tableau_t;
+
+/* Time-stepping buffers (caller-owned). */
+typedef struct fvm_solver_bufs {
+    float *state;       /* [N][C] conserved state, updated in place                      */
+    float *prims;       /* [N][C] primitives of the current stage input                   */
+    float *grads;       /* [N][dim][C] limited gradients, carried across evaluations      */
+    float *k;           /* [stages][N][C] stage increments dt * f                          */
+    float *dt;          /* [1] time step (device)                                         */
+    int32_t *has_grads; /* [1] device flag: grads hold a previous evaluation              */
+    double *cons;       /* [C] optional: FP64 sum of vol * U after each step (may be NULL) */
+} fvm_solver_bufs_t;
+
+/* Last CUDA error recorded by this library (cudaError_t value), 0 if none. */
+int fvm_last_cuda_error(void);
+/* Library build identifier, e.g. "fvm_b200 sm_100a". Host string. */
+const char *fvm_version(void);
+
+/* Launch profiling (no reference counterpart).  Between fvm_profile_start(capacity) and
+ * fvm_profile_stop() every kernel this library launches is bracketed by two CUDA events recorded
+ * on its stream (also when the launches are captured into a CUDA graph).  fvm_profile_stop returns
+ * the number of launches recorded (FVM_E_ARG if more than `capacity` were attempted);
+ * fvm_profile_read fills host arrays with each launch's kernel id and duration in ms, waiting for
+ * the events.  Kernel ids: 0 ell_spmv, 1 ell_spmm, 2 bc, 3 cell, 4 face, 5 div_stage,
+ * 6 finalize, 7 state_to_prims, 8 reduce_state, 9 batched. */
+int fvm_profile_start(int32_t capacity);
+int fvm_profile_stop(void);
+int fvm_profile_read(int32_t n, int32_t *ids, float *ms);
+
+/* y[M] = A x (+ bias).  A in slot-major ELL: vals[K][M], cols[K][M] (int32).  x is read with
+ * stride incx, y written with stride incy.  bias may be NULL. */
+int fvm_ell_spmv(const float *vals, const int32_t *cols, int64_t M, int32_t K,
+                 const float *x, int64_t incx, const float *bias, float *y, int64_t incy,
+                 void *stream);
+
+/* Y[M][B] = A X (+ bias[:, None]).  X is [N][B] with leading dimension ldx, Y [M][B] with ldy. */
+int fvm_ell_spmm(const float *vals, const int32_t *cols, int64_t M, int32_t K,
+                 const float *X, int64_t ldx, int32_t B, const float *bias, float *Y, int64_t ldy,
+                 void *stream);
+
+/* dU/dt [N][C] (conserved variables) of the primitives prims [N][C].  grads [N][dim][C] is
+ * read as the previous limited gradient when the device flag *has_grads != 0 (the reference's
+ * FacetCalc.cell_grads is not None) and overwritten with this evaluation's limited gradient;
+ * the call sets *has_grads = 1.  Returns FVM_E_UNSUPPORTED if mesh->kg != dim + 2. */
+int fvm_residual(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *prims,
+                 float *grads, int32_t *has_grads, float *dudt, const fvm_work_t *work,
+                 void *stream);
+
+/* One explicit stage s of `tab` (residual of bufs->prims, then the stage combination); the
+ * last stage writes the new state and, per `tab`, updates dt. */
+int fvm_stage(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const fvm_tableau_t *tab,
+              int32_t s, const fvm_solver_bufs_t *bufs, const fvm_work_t *work, void *stream);
+
+/* A whole step: all stages and the dt update.  bufs->prims must hold the primitives of
+ * bufs->state when the step starts (fvm_state_to_prims after setting the state); every step
+ * leaves them consistent for the next one. */
+int fvm_step(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const fvm_tableau_t *tab,
+             const fvm_solver_bufs_t *bufs, const fvm_work_t *work, void *stream);
+
+/* Multistep combination U <- U + sum_j coef[j] * k[idx[j]] (Adams-Bashforth); the residual of
+ * the current state is stored, times dt, into k[store]. */
+int fvm_multistep(const fvm_mesh_t *mesh, const fvm_physics_t *phys, int32_t store,
+                  int32_t n_terms, const int32_t *idx, const float *coef,
+                  const fvm_solver_bufs_t *bufs, const fvm_work_t *work, void *stream);
+
+/* prims [N][C] <- primitives of state [N][C]. */
+int fvm_state_to_prims(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *state,
+                       float *prims, void *stream);
+
+/* dt[0] <- cfl * min_i 1 / (inv_h_i (|u_i| + c_i)) of state (FP64 reduction). */
+int fvm_cfl_dt(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *state,
+               float cfl, float *dt, const fvm_work_t *work, void *stream);
+
+/* out[C] <- sum_i vol_i * state[i][c] in FP64. */
+int fvm_conservation(const fvm_mesh_t *mesh, const float *state, double *out,
+                     const fvm_work_t *work, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FVM_B200_H */

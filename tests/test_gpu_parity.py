@@ -1,0 +1,212 @@
+"""CUDA path vs the reference (golden vectors) and vs the oracle.  Needs a B200.
+
+Tolerances (written per check):
+* residuals / limited gradients vs the FP32 reference: rel-L2 <= 1e-5 (FP32 rounding; the
+  reference's own FP32-vs-FP64 gap on these cases is ~1e-6 .. 1e-5);
+* states after one or ten steps vs the FP32 reference: rel-L2 <= 1e-5 (the per-step parity bar);
+* ELL operators vs torch sparse (FP32): rel-L2 <= 1e-6.
+The FP64 error of every result is also checked to stay within the reference's own FP32 error x 10.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+from gpu_helpers import make_equation, to_np
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["c2d", "b3d"]
+
+
+@pytest.fixture(autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("needs CUDA")
+
+
+# -- ELL operators ----------------------------------------------------------------------------
+@pytest.mark.parametrize("K", [1, 2, 5, 16])
+@pytest.mark.parametrize("B", [1, 4, 5, 9])
+def test_ell_random_vs_torch_sparse(K, B):
+    from fvm_solver_b200.sparse import SPMB200
+    g = torch.Generator().manual_seed(K * 100 + B)
+    M, N = 3001, 2003
+    nnz_row = torch.randint(0, K + 1, (M,), generator=g)          # ragged rows incl. empty ones
+    rows = torch.repeat_interleave(torch.arange(M), nnz_row)
+    cols = torch.randint(0, N, (rows.numel(),), generator=g)
+    vals = torch.randn(rows.numel(), generator=g)
+    A = torch.sparse_coo_tensor(torch.stack([rows, cols]), vals, (M, N)).coalesce()
+    op = SPMB200(A, "cuda")
+    X = torch.randn(N, B, generator=g).cuda()
+    b = torch.randn(M, generator=g).cuda()
+    Ad = A.cuda()
+    ref = torch.sparse.mm(Ad, X)
+    assert rel_l2(to_np(op.spMM(X)), to_np(ref)) < 1e-6
+    assert rel_l2(to_np(op.spMM(X, b)), to_np(ref + b[:, None])) < 1e-6
+    x = X[:, 0]                                   # strided 1-D view when B > 1
+    y = op.spMV(x, b)
+    assert y.shape == (M,)
+    assert rel_l2(to_np(y), to_np(torch.sparse.mm(Ad, x[:, None])[:, 0] + b)) < 1e-6
+
+
+def test_ell_empty_and_zero_width():
+    from fvm_solver_b200.sparse import SPMB200
+    A = torch.sparse_coo_tensor(torch.zeros((2, 0), dtype=torch.long), torch.zeros(0), (7, 5))
+    op = SPMB200(A, "cuda")
+    x = torch.randn(5, 3, device="cuda")
+    assert torch.equal(op.spMM(x), torch.zeros(7, 3, device="cuda"))
+    b = torch.arange(7.0, device="cuda")
+    assert torch.equal(op.spMV(x[:, 0], b), b)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_reference_operators_on_device(case):
+    """SPMB200 built from the reference-format operators reproduces the oracle ELL products."""
+    from fvm_solver_b200.sparse import SPMB200
+    from oracle import fvm_oracle as O
+    from conftest import golden_setup
+    g, spec, T, cfg = golden_setup(case)
+    for A in (T.ops.G_mats, T.ops.flux_mat, T.ops.A_face_grad):
+        op = SPMB200(A, "cuda")
+        v, c = O.ell_from_coo(A)
+        X = np.random.default_rng(0).standard_normal((A.shape[1], 4)).astype(np.float32)
+        want = O.ell_spmm(v, c, X)
+        got = to_np(op.spMM(torch.from_numpy(X).cuda()))
+        assert rel_l2(got, want) < 1e-6
+
+
+# -- residual ------------------------------------------------------------------------------------
+@pytest.mark.parametrize("case", CASES)
+def test_residual_vs_reference(case):
+    g, eq, T, cfg = make_equation(case)
+    r1 = eq.forward(torch.from_numpy(g["prim0"]))
+    assert rel_l2(to_np(r1), g["res1"]) < 1e-5
+    assert rel_l2(to_np(eq.cell_grads), g["grads1"]) < 1e-5
+    # second call carries the limited gradients into the boundary correction
+    r2 = eq.forward(torch.from_numpy(g["prim2"]))
+    assert rel_l2(to_np(r2), g["res2"]) < 1e-5
+    assert rel_l2(to_np(eq.cell_grads), g["grads2"]) < 1e-5
+    # FP64 error: no worse than 10x the reference's own FP32 error
+    e32 = rel_l2(g["res1"], g["res1_f64"])
+    eq.reset_gradients()
+    r1b = eq.forward(torch.from_numpy(g["prim0"]))
+    assert rel_l2(to_np(r1b), g["res1_f64"]) < max(10 * e32, 1e-6)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_residual_deterministic(case):
+    g, eq, T, cfg = make_equation(case)
+    p = torch.from_numpy(g["prim0"])
+    a = eq.forward(p)
+    eq.reset_gradients()
+    b = eq.forward(p)
+    assert torch.equal(a, b)
+
+
+# -- integrators ---------------------------------------------------------------------------------
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("extra,key", [("RK4", "rk4_step1"), ("SSP_RK3", "ssprk3_step1")])
+def test_butcher_one_step(case, extra, key):
+    g, eq, T, cfg = make_equation(case, "Butcher", extra)
+    eq.t_solver.step(1)
+    st = to_np(eq.cells.state)
+    assert rel_l2(st, g[key]) < 1e-5
+    assert rel_l2(st, g[key + "_f64"]) < 1e-5
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_ten_steps(case):
+    g, eq, T, cfg = make_equation(case, "Butcher", "SSP_RK3")
+    eq.t_solver.step(10)
+    assert rel_l2(to_np(eq.cells.state), g["ssprk3_step10"]) < 1e-5
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("name,extra,key", [("Butcher_adapt", "RK3_SSP4", "adapt"), ("RK3_SSP4", "", "rk3ssp4")])
+def test_adaptive_step(case, name, extra, key):
+    g, eq, T, cfg = make_equation(case, name, extra)
+    eq.t_solver.step(1)
+    assert rel_l2(to_np(eq.cells.state), g[f"{key}_step1"]) < 1e-5
+    dt = float(eq.t_solver.dt.item())
+    assert abs(dt / float(g[f"{key}_dt1"]) - 1) < 1e-4
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_ab3_vs_oracle(case):
+    from oracle import fvm_oracle as O
+    g, eq, T, cfg = make_equation(case, "AB3", "")
+    s = O.OracleSolver(O.OracleResidual(T, cfg, np.float32), g["state0"], float(g["dt"]))
+    s.ab3_start()
+    for _ in range(3):
+        s.ab3_step()
+    eq.t_solver.step(5)
+    assert rel_l2(to_np(eq.cells.state), s.state) < 1e-5
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_cfl_and_conservation(case):
+    from oracle import fvm_oracle as O
+    g, eq, T, cfg = make_equation(case, "Butcher", "SSP_RK3", cfl=0.5)
+    want = O.cfl_dt(g["state0"], int(g["dim"]), cfg.C_v, cfg.gamma, T.kernel.inv_h.numpy(), 0.5)
+    got = float(eq.t_solver.dt.item())
+    assert abs(got / want - 1) < 1e-6
+    tot = to_np(eq.conservation())
+    vol = T.kernel.volumes.numpy()
+    want_tot = (vol[:, None] * g["state0"].astype(np.float64)).sum(0)
+    assert np.allclose(tot, want_tot, rtol=1e-12, atol=1e-9)
+    # CFL after a step is computed in the step's last stage kernel
+    eq.t_solver.step(1)
+    want = O.cfl_dt(to_np(eq.cells.state), int(g["dim"]), cfg.C_v, cfg.gamma, T.kernel.inv_h.numpy(), 0.5)
+    assert abs(float(eq.t_solver.dt.item()) / want - 1) < 1e-6
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_graph_replay_matches_eager(case):
+    g, eq, T, cfg = make_equation(case, "Butcher", "RK4", cfl=0.5)
+    g2, eq2, _, _ = make_equation(case, "Butcher", "RK4", cfl=0.5)
+    eq.t_solver.step(4)
+    replay = eq2.t_solver.graph_steps(2)
+    replay()
+    replay()
+    assert torch.equal(eq.cells.state, eq2.cells.state)
+    assert torch.equal(eq.t_solver.dt, eq2.t_solver.dt)
+
+
+def test_periodic_box_vs_oracle():
+    """Periodic tetrahedral box (no reference counterpart): CUDA path vs oracle, residual and step."""
+    from fvm_solver_b200 import config as cf, equation as E, fvm_mesh as fm, meshgen as mg, tables as tb
+    from oracle import fvm_oracle as O
+    spec = mg.periodic_box(8, seed=5)
+    cfg = cf.TaylorGreenConfig(device="cuda")
+    tabs = tb.FVMTables(fm.mesh_from_spec(spec), cfg, 5, {})
+    rng = np.random.default_rng(1)
+    N = spec.n_cells
+    prim = np.zeros((N, 5), np.float32)
+    prim[:, :3] = rng.standard_normal((N, 3)) * 0.5
+    prim[:, 3] = 1 + 0.05 * rng.standard_normal(N)
+    prim[:, 4] = 100 + rng.standard_normal(N)
+    phy = E.FluidConstitution3D(cfg)
+    eq = E.FVMEquation(cfg, phy, spec, 5, {}, us_init=torch.from_numpy(O.prim_to_state(prim, 3, cfg.C_v)))
+    orc = O.OracleResidual(tabs, cfg, np.float32)
+    want, wg = orc.forward(prim)
+    got = eq.forward(torch.from_numpy(prim))
+    assert rel_l2(to_np(got), want) < 1e-5
+    assert rel_l2(to_np(eq.cell_grads), wg) < 1e-5
+
+
+def test_free_stream_preservation_periodic():
+    """Uniform flow on a periodic mesh: every facet flux is identical, so dU/dt ~ 0 (size-independent)."""
+    from fvm_solver_b200 import config as cf, equation as E, meshgen as mg
+    spec = mg.periodic_box(24, seed=2)
+    cfg = cf.TaylorGreenConfig(device="cuda")
+    phy = E.FluidConstitution3D(cfg)
+    N = spec.n_cells
+    prim = torch.zeros(N, 5)
+    prim[:, 0], prim[:, 1], prim[:, 2], prim[:, 3], prim[:, 4] = 0.7, -0.3, 0.2, 1.0, 100.0
+    V, rho, T = prim[:, :3], prim[:, 3:4], prim[:, 4:]
+    m, r, Q = phy.primatives_to_state(V, rho, T)
+    eq = E.FVMEquation(cfg, phy, spec, 5, {}, us_init=torch.cat([m, r, Q], 1))
+    d = eq.forward(prim)
+    scale = float(eq.dev.t.f_vals.abs().max()) * 250.0   # |flux| ~ rho E u |S|
+    assert float(d.abs().max()) < 1e-4 * scale

@@ -31,6 +31,7 @@ def test_kernel_tables_consistent(golden):
     assert np.array_equal(K.f_cols.numpy(), g["ell_flux_cols"].T)
     # neighbour slots decode to neigh_combine
     slots = np.stack([(K.nb_slot.numpy() >> (4 * j)) & 15 for j in range(dim + 1)], 1)
+    assert np.all((K.nb_slot.numpy() >> 24) == K.kg)
     nb = np.take_along_axis(K.g_cols.numpy().T, slots, 1)
     assert np.array_equal(nb, T.neigh_combine.numpy())
 
