@@ -48,6 +48,10 @@ def parse():
     ap.add_argument("--sample-n", type=int, default=20, help="points per axis of the CPU sample box")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="taylor_green", choices=["taylor_green", "channel_cylinder", "ensemble"],
+                    help="taylor_green: the headline 3D box; channel_cylinder: the 2D cylinder case (11k cells); "
+                         "ensemble: batched 2D ensemble vs the same cases run one by one")
+    ap.add_argument("--cases", type=int, default=256, help="ensemble size")
     return ap.parse_args()
 
 
@@ -161,10 +165,98 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def secondary(args):
+    """Secondary workloads (single GPU): the 2D channel-cylinder case and the batched ensemble."""
+    from fvm_solver_b200 import _lib, workloads as W
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+
+    def timed(sol, steps):
+        replay = sol.graph_steps(steps)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        replay()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    if args.workload == "channel_cylinder":
+        case = W.channel_cylinder(device="cuda")
+        eq = case.equation()
+        sol = eq.t_solver
+        sol.step(args.warmup)
+        with ClockSampler(0) as clk:
+            ms = timed(sol, args.steps)
+        N = eq.mesh.n_cells
+        cpu = None
+        if not args.no_cpu_baseline:
+            from oracle import fvm_oracle as O
+            T = eq.tables
+            res = O.OracleResidual(T, case.cfg, np.float32)
+            s = O.OracleSolver(res, case.state0.numpy(), 1e-4)
+            inv_h = T.kernel.inv_h.numpy()
+            t0, n = time.perf_counter(), 0
+            while time.perf_counter() - t0 < 15.0:
+                s.dt = res.dt(O.cfl_dt(s.state, 2, case.cfg.C_v, case.cfg.gamma, inv_h, 0.5))
+                s.butcher_step("SSP_RK3")
+                n += 1
+            el = time.perf_counter() - t0
+            cpu = {"value": N * n / el, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+                   "sample": f"numpy oracle, same mesh ({N} cells), {n} SSP-RK3 steps, {el:.1f} s"}
+        out = {"metric": "cell-steps/s", "value": N * args.steps / (ms / 1e3), "unit": "cell-steps/s", "n_gpus": 1,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+               "dtype": "f32", "data": "synthetic",
+               "config": {"workload": "channel_cylinder_2d_ssprk3_cfl0.5", "cells": N, "facets": eq.dev.n_facets,
+                          "l2": "working set fits in L2 (launch/latency bound case)", "timing": "cuda graph replay"},
+               "cpu_baseline": cpu, "clocks": clk.summary()}
+        print(json.dumps(out))
+        return
+
+    # ensemble: batched vs one-by-one
+    from fvm_solver_b200 import batched as B
+    from fvm_solver_b200.equation import FVMEquation, FluidConstitution2D
+    t0 = time.time()
+    parts = B.build_ensemble_tables(args.cases, workers=min(16, os.cpu_count() or 1))
+    t_build = time.time() - t0
+    cfg = W.ensemble_case(0, device="cuda", cfl=0.3).cfg
+    batch = B.BatchedFVM(parts, cfg, device="cuda")
+    Nt = batch.n_cells
+    batch.t_solver.step(max(args.warmup, 3))
+    with ClockSampler(0) as clk:
+        ms_b = timed(batch.t_solver, args.steps)
+    del batch
+    torch.cuda.empty_cache()
+    # plain: every case alone, each with its own captured graph of the same number of steps
+    ms_p, cells_p = 0.0, 0
+    for k, p in enumerate(parts):
+        c = W.ensemble_case(k, device="cuda", cfl=0.3).cfg
+        eq = FVMEquation.from_kernel_tables(c, FluidConstitution2D(c), p.kt, p.state0)
+        eq.t_solver.step(max(args.warmup, 3))
+        ms_p += timed(eq.t_solver, args.steps)
+        cells_p += p.kt.n_cells
+        del eq
+    vb = Nt * args.steps / (ms_b / 1e3)
+    vp = cells_p * args.steps / (ms_p / 1e3)
+    sizes = [p.kt.n_cells for p in parts]
+    out = {"metric": "cell-steps/s", "value": vb, "unit": "cell-steps/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_b / args.steps, "higher_is_better": True, "dtype": "f32",
+           "data": "synthetic",
+           "config": {"workload": "ensemble_2d_ab3_batched", "cases": args.cases, "cells_total": Nt,
+                      "cells_min": min(sizes), "cells_max": max(sizes), "integrator": "AB3 (SSP-RK3 start), CFL 0.3",
+                      "timing": "cuda graph replay", "table_build_s": t_build},
+           "plain": {"value": vp, "unit": "cell-steps/s", "ms_per_step_all_cases": ms_p / args.steps,
+                     "how": "each case alone, own CUDA graph, sequential"},
+           "batched_over_plain": vb / vp, "clocks": clk.summary()}
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "taylor_green":
+        return secondary(args)
 
     import torch.distributed as dist
     from fvm_solver_b200 import _lib, workloads as W

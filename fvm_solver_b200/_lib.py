@@ -25,7 +25,11 @@ class Mesh(ct.Structure):
         (n, _P) for n in ("g_vals", "g_cols", "nb_slot", "disp", "eps", "c2f", "side", "f_vals", "f_cols",
                           "inv_h", "volumes", "fcell", "fbc", "normals", "fsize", "xorth", "inv_d",
                           "bc_face", "bc_side", "bc_cell", "bc_kind", "bc_b", "bc_l", "bc_ga", "bc_gb",
-                          "bc_char", "ch_cell", "ch_normal", "ch_rho", "ch_vn", "ch_p", "ch_vt")]
+                          "bc_char", "ch_cell", "ch_normal", "ch_rho", "ch_vn", "ch_p", "ch_vt")] + [
+        ("n_cases", ct.c_int32)] + [
+        (n, _P) for n in ("cell_case", "face_case", "bc_case", "ch_off", "case_mu", "case_mu_b", "case_kappa")]
+
+MESH_PTR_FIELDS = [f for f, t in Mesh._fields_ if t is _P]
 
 
 class Physics(ct.Structure):

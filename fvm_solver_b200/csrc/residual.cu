@@ -84,31 +84,55 @@ __device__ __forceinline__ float limiter_phi(int p, float delta, float dU, float
 // ------------------------------------------------------------------------------------------
 // k_bc: boundary facet values.
 // ------------------------------------------------------------------------------------------
+// Sum of the interior sound speed over characteristic facets [lo, hi): every caller uses the same
+// thread -> element mapping and reduction tree, so batched and single-mesh runs agree bitwise.
+template <int C>
+__device__ __forceinline__ double char_c_sum(const fvm_mesh_t& m, const Phys& p, const float* prims, int lo,
+                                             int hi, double* red) {
+    constexpr int DIM = C - 2;
+    double acc = 0.0;
+    for (int t = lo + threadIdx.x; t < hi; t += blockDim.x) {
+        const int cell = __ldg(m.ch_cell + t);
+        acc += (double)sqrtf(p.gR * __ldg(prims + (int64_t)cell * C + DIM + 1));
+    }
+    double v[1] = {acc};
+    block_sum<1>(v, red);
+    return v[0];
+}
+
+// Batched meshes: per-case characteristic gating scale 10 / mean(c), one block per case.
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_char_scale(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+                                                        double* __restrict__ red_out) {
+    constexpr int C = DIM + 2;
+    __shared__ double red[32];
+    const int c = blockIdx.x;
+    const int lo = __ldg(m.ch_off + c), hi = __ldg(m.ch_off + c + 1);
+    const double sum = char_c_sum<C>(m, p, prims, lo, hi, red);
+    if (threadIdx.x == 0) red_out[FVM_RED_DOUBLES + 8 * c + 6] = hi > lo ? (double)(10.0f / (float)(sum / (double)(hi - lo))) : 0.0;
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
                                                 const float* __restrict__ grads,
                                                 const int32_t* __restrict__ has_grads,
-                                                float* __restrict__ bcv, float* __restrict__ face_vals) {
+                                                float* __restrict__ bcv, float* __restrict__ face_vals,
+                                                const double* __restrict__ wred) {
     constexpr int C = DIM + 2;
     __shared__ double red[32];
     float scale = 0.f;
-    if (m.n_char > 0) {
+    if (m.n_char > 0 && m.n_cases == 0) {
         // Group mean of the interior sound speed c = sqrt(gamma R T) (facet_boundary.py:427),
         // recomputed identically by every block.
-        double acc = 0.0;
-        for (int t = threadIdx.x; t < m.n_char; t += blockDim.x) {
-            const int cell = __ldg(m.ch_cell + t);
-            acc += (double)sqrtf(p.gR * __ldg(prims + (int64_t)cell * C + DIM + 1));
-        }
-        double v[1] = {acc};
-        block_sum<1>(v, red);
+        const double sum = char_c_sum<C>(m, p, prims, 0, m.n_char, red);
         __shared__ float s_scale;
-        if (threadIdx.x == 0) s_scale = 10.0f / (float)(v[0] / (double)m.n_char);
+        if (threadIdx.x == 0) s_scale = 10.0f / (float)(sum / (double)m.n_char);
         __syncthreads();
         scale = s_scale;
     }
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= m.n_bc) return;
+    if (m.n_cases > 0) scale = (float)wred[FVM_RED_DOUBLES + 8 * __ldg(m.bc_case + b) + 6];
     const int cell = __ldg(m.bc_cell + b);
     float U[C];
     load_row<C>(prims + (int64_t)cell * C, U);
@@ -354,14 +378,21 @@ __global__ void __launch_bounds__(kBlock) k_face(fvm_mesh_t m, Phys p, const flo
     }
     // Stress (fvm_equation.py:101-120, 149-170).  I1 = D00 + D11 also in 3D, as in the reference.
     const float Tm = (T[0] + T[1]) / 2.f;
+    float mu0 = p.mu, mub0 = p.mu_b, kappa = p.kappa;
+    if (m.n_cases > 0) {
+        const int cs_ = __ldg(m.face_case + f);
+        mu0 = __ldg(m.case_mu + cs_);
+        mub0 = __ldg(m.case_mu_b + cs_);
+        kappa = __ldg(m.case_kappa + cs_);
+    }
     float D[DIM][DIM];
 #pragma unroll
     for (int a = 0; a < DIM; ++a)
 #pragma unroll
         for (int c = 0; c < DIM; ++c) D[a][c] = 0.5f * (gF[a][c] + gF[c][a]);
     const float I1 = D[0][0] + D[1][1];
-    const float mu = p.mu * powf(Tm / p.T_0, 1.5f) * p.T0pS / (Tm + p.S);
-    const float mub = p.mu_b * (Tm * Tm) / p.T0sq;
+    const float mu = mu0 * powf(Tm / p.T_0, 1.5f) * p.T0pS / (Tm + p.S);
+    const float mub = mub0 * (Tm * Tm) / p.T0sq;
     const float a0 = -mub * I1, a1 = -2.f * mu;
     float tau[DIM][DIM];
 #pragma unroll
@@ -396,7 +427,7 @@ __global__ void __launch_bounds__(kBlock) k_face(fvm_mesh_t m, Phys p, const flo
             const float Vm = (UL[c] + UR[c]) / 2.f;
             heat = fmaf(tau[a][c] * Vm, n[a], heat);
         }
-    heat = fmaf(-p.kappa * grad_T_n, size, heat);
+    heat = fmaf(-kappa * grad_T_n, size, heat);
     F[DIM + 1] += heat;
     // Kurganov-Tadmor diffusion (fvm_equation.py:337-368)
     const float vmax = fmaxf(sqrtf(vm2[0]), sqrtf(vm2[1]));
@@ -428,6 +459,71 @@ __device__ __forceinline__ void state_to_prim(const float (&U)[C], float inv_Cv,
     P[DIM + 1] = inv_Cv * (U[DIM + 1] / rho - 0.5f * v2);
 }
 
+// Speed scale inv_h (|u| + c) of a conserved state, FP64 (CFL time step).
+template <int DIM>
+__device__ __forceinline__ double cfl_speed(const fvm_mesh_t& m, const Phys& p, const float* U, int i) {
+    double v2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v2 += (double)U[d] / U[DIM] * ((double)U[d] / U[DIM]);
+    const double T = ((double)U[DIM + 1] / U[DIM] - 0.5 * v2) / (double)p.C_v;
+    return __ldg(m.inv_h + i) * (sqrt(v2) + sqrt((double)p.gamma * (double)p.R * fmax(T, 0.0)));
+}
+
+// Conservation sums sum vol U and CFL speed max of the block's cells into red (single mesh) or
+// into the per-case slots red[FVM_RED_DOUBLES + 8 case + {0: max speed, 1..C: sums}] (batched).
+// Batched: warps whose lanes all belong to one case reduce first; mixed warps use per-lane atomics.
+template <int DIM>
+__device__ __forceinline__ void reduce_cons_cfl(const fvm_mesh_t& m, const Phys& p, const float* U, bool live,
+                                                int cse, int want_cons, int want_cfl, double* red,
+                                                double* smem) {
+    constexpr int C = DIM + 2;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m.n_cases == 0) {
+        if (want_cons) {
+            double v[C];
+#pragma unroll
+            for (int c = 0; c < C; ++c) v[c] = live ? __ldg(m.volumes + i) * (double)U[c] : 0.0;
+            block_sum<C>(v, smem);
+            if (threadIdx.x == 0)
+                for (int c = 0; c < C; ++c) atomicAdd(red + 24 + c, v[c]);
+            __syncthreads();
+        }
+        if (want_cfl) {
+            double sp = live ? cfl_speed<DIM>(m, p, U, i) : 0.0;
+            sp = block_max(sp, smem);
+            if (threadIdx.x == 0) atomic_max_pos(red + 16, sp);
+        }
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    const int c0 = __shfl_sync(0xffffffffu, cse, 0);
+    const bool uniform = __all_sync(0xffffffffu, !live || cse == c0);
+    double* slot = red + FVM_RED_DOUBLES + 8 * cse;
+    if (want_cfl) {
+        double sp = live ? cfl_speed<DIM>(m, p, U, i) : 0.0;
+        if (uniform) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sp = fmax(sp, __shfl_down_sync(0xffffffffu, sp, o));
+            if (lane == 0 && sp > 0.0) atomic_max_pos(red + FVM_RED_DOUBLES + 8 * c0, sp);
+        } else if (live) {
+            atomic_max_pos(slot, sp);
+        }
+    }
+    if (want_cons) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            double v = live ? __ldg(m.volumes + i) * (double)U[c] : 0.0;
+            if (uniform) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                if (lane == 0) atomicAdd(red + FVM_RED_DOUBLES + 8 * c0 + 1 + c, v);
+            } else if (live) {
+                atomicAdd(slot + 1 + c, v);
+            }
+        }
+    }
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(kBlock) k_div_stage(fvm_mesh_t m, Phys p, const float* __restrict__ flux,
                                                        StageArgs a, float* __restrict__ state,
@@ -455,7 +551,8 @@ __global__ void __launch_bounds__(kBlock) k_div_stage(fvm_mesh_t m, Phys p, cons
         if (live) store_row<C>(dudt + (int64_t)i * C, r);
         return;
     }
-    const float h = *dt;
+    const int cse = (m.n_cases > 0 && live) ? __ldg(m.cell_case + i) : 0;
+    const float h = dt[cse];
     float kk[C], U0[C], inc[C], U[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) {
@@ -518,33 +615,30 @@ __global__ void __launch_bounds__(kBlock) k_div_stage(fvm_mesh_t m, Phys p, cons
             for (int c = 0; c < 3 * C; ++c) atomicAdd(red + c, v[c]);
         __syncthreads();
     }
-    if (a.cons) {
-        double v[C];
-#pragma unroll
-        for (int c = 0; c < C; ++c) v[c] = live ? __ldg(m.volumes + i) * (double)U[c] : 0.0;
-        block_sum<C>(v, smem);
-        if (threadIdx.x == 0)
-            for (int c = 0; c < C; ++c) atomicAdd(red + 24 + c, v[c]);
-        __syncthreads();
-    }
-    if (a.cfl) {
-        double s = 0.0;
-        if (live) {
-            double v2 = 0.0;
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) v2 += (double)U[d] / U[DIM] * ((double)U[d] / U[DIM]);
-            const double T = ((double)U[DIM + 1] / U[DIM] - 0.5 * v2) / (double)p.C_v;
-            s = __ldg(m.inv_h + i) * (sqrt(v2) + sqrt((double)p.gamma * (double)p.R * fmax(T, 0.0)));
-        }
-        s = block_max(s, smem);
-        if (threadIdx.x == 0) atomic_max_pos(red + 16, s);
-    }
+    reduce_cons_cfl<DIM>(m, p, U, live, cse, a.cons, a.cfl, red, smem);
 }
 
 // Step-end bookkeeping: adaptive dt (integrators.py:42-62) or CFL dt, conservation sums.
+// Batched meshes (n_cases > 0): one thread per case handles its CFL dt and sums.
 __global__ void k_finalize(int C, int adaptive, float atol, float rtol, float mtol, float alpha_hi,
                            float alpha_lo, float order, float cfl, int cons, double* red, float* dt,
-                           double* cons_out) {
+                           double* cons_out, int n_cases) {
+    if (n_cases > 0) {
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cases; c += gridDim.x * blockDim.x) {
+            double* slot = red + FVM_RED_DOUBLES + 8 * c;
+            if (cfl > 0.f) {
+                if (slot[0] > 0.0) dt[c] = (float)((double)cfl / slot[0]);
+                slot[0] = 0.0;
+            }
+            if (cons) {
+                for (int k = 0; k < C; ++k) {
+                    if (cons_out) cons_out[c * C + k] = slot[1 + k];
+                    slot[1 + k] = 0.0;
+                }
+            }
+        }
+        return;
+    }
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (adaptive) {
         double E = 0.0;
@@ -595,27 +689,8 @@ __global__ void __launch_bounds__(kBlock) k_reduce_state(fvm_mesh_t m, Phys p, c
 #pragma unroll
     for (int c = 0; c < C; ++c) U[c] = 1.f;
     if (live) load_row<C>(state + (int64_t)i * C, U);
-    if (want_cons) {
-        double v[C];
-#pragma unroll
-        for (int c = 0; c < C; ++c) v[c] = live ? __ldg(m.volumes + i) * (double)U[c] : 0.0;
-        block_sum<C>(v, smem);
-        if (threadIdx.x == 0)
-            for (int c = 0; c < C; ++c) atomicAdd(red + 24 + c, v[c]);
-        __syncthreads();
-    }
-    if (want_cfl) {
-        double s = 0.0;
-        if (live) {
-            double v2 = 0.0;
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) v2 += (double)U[d] / U[DIM] * ((double)U[d] / U[DIM]);
-            const double T = ((double)U[DIM + 1] / U[DIM] - 0.5 * v2) / (double)p.C_v;
-            s = __ldg(m.inv_h + i) * (sqrt(v2) + sqrt((double)p.gamma * (double)p.R * fmax(T, 0.0)));
-        }
-        s = block_max(s, smem);
-        if (threadIdx.x == 0) atomic_max_pos(red + 16, s);
-    }
+    const int cse = (m.n_cases > 0 && live) ? __ldg(m.cell_case + i) : 0;
+    reduce_cons_cfl<DIM>(m, p, U, live, cse, want_cons, want_cfl, red, smem);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -655,6 +730,10 @@ static bool mesh_ok(const fvm_mesh_t* m) {
         return false;
     if (m->n_char > 0 && (!m->ch_cell || !m->ch_normal || !m->ch_rho || !m->ch_vn || !m->ch_p || !m->ch_vt))
         return false;
+    if (m->n_cases < 0) return false;
+    if (m->n_cases > 0 && (!m->cell_case || !m->face_case || !m->ch_off || !m->case_mu || !m->case_mu_b ||
+                           !m->case_kappa || (m->n_bc > 0 && !m->bc_case)))
+        return false;
     return true;
 }
 
@@ -663,14 +742,18 @@ static bool work_ok(const fvm_mesh_t* m, const fvm_work_t* w) {
 }
 
 static inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+static inline unsigned fin_blocks(const fvm_mesh_t* m) { return m->n_cases > 0 ? (unsigned)((m->n_cases + 127) / 128) : 1u; }
 
 // bc -> cell -> face for the primitives `prims`; leaves fluxes in work->flux.
 template <int DIM>
 static int launch_fluxes(const fvm_mesh_t* m, const Phys& p, const float* prims, float* grads,
                          int32_t* has_grads, const fvm_work_t* w, cudaStream_t s) {
-    if (m->n_bc > 0)
+    if (m->n_bc > 0) {
+        if (m->n_cases > 0 && m->n_char > 0)
+            FVM_LAUNCH(KID_BC, s, k_char_scale<DIM><<<m->n_cases, kBlock, 0, s>>>(*m, p, prims, w->red));
         FVM_LAUNCH(KID_BC, s, k_bc<DIM><<<blocks_for(m->n_bc), kBlock, 0, s>>>(*m, p, prims, grads, has_grads,
-                                                                               w->bc_vals, w->face_vals));
+                                                                               w->bc_vals, w->face_vals, w->red));
+    }
     FVM_LAUNCH(KID_CELL, s, k_cell<DIM, DIM + 2><<<blocks_for(m->n_cells), kBlock, 0, s>>>(
                                 *m, p, prims, w->bc_vals, w->face_vals, grads, has_grads));
     FVM_LAUNCH(KID_FACE, s, k_face<DIM><<<blocks_for(m->n_facets), kBlock, 0, s>>>(*m, p, prims, w->face_vals,
@@ -736,9 +819,9 @@ static int stage_impl(const fvm_mesh_t* m, const Phys& p, const fvm_tableau_t* t
     if (rc) return rc;
     if (a.final_ && (a.adaptive || a.cfl || a.cons)) {
         FVM_LAUNCH(KID_FINALIZE, st,
-                   k_finalize<<<1, 32, 0, st>>>(m->n_comp, tab->adaptive, tab->atol, tab->rtol, tab->mtol,
+                   k_finalize<<<fin_blocks(m), 128, 0, st>>>(m->n_comp, tab->adaptive, tab->atol, tab->rtol, tab->mtol,
                                                 tab->alpha_hi_err, tab->alpha_lo_err, tab->order, tab->cfl,
-                                                a.cons, w->red, b->dt, b->cons));
+                                                a.cons, w->red, b->dt, b->cons, m->n_cases));
         rc = launch_status();
     }
     return rc;
@@ -765,8 +848,8 @@ static int multistep_impl(const fvm_mesh_t* m, const Phys& p, int store, int n_t
     rc = launch_status();
     if (rc) return rc;
     if (a.cons) {
-        FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<1, 32, 0, st>>>(m->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f,
-                                                                   0.f, 1, w->red, b->dt, b->cons));
+        FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(m), 128, 0, st>>>(m->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f,
+                                                                   0.f, 1, w->red, b->dt, b->cons, m->n_cases));
         rc = launch_status();
     }
     return rc;
@@ -776,10 +859,15 @@ static int multistep_impl(const fvm_mesh_t* m, const Phys& p, int store, int n_t
 
 using namespace fvm;
 
+static int check_common(const fvm_mesh_t* mesh) {
+    if (mesh && mesh->dim >= 2 && mesh->dim <= 3 && mesh->kg != mesh->dim + 2) return FVM_E_UNSUPPORTED;
+    return mesh_ok(mesh) ? FVM_OK : FVM_E_ARG;
+}
+
 extern "C" int fvm_residual(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const float* prims,
                             float* grads, int32_t* has_grads, float* dudt, const fvm_work_t* work,
                             void* stream) {
-    if (!mesh_ok(mesh)) return mesh && mesh->kg != mesh->dim + 2 ? FVM_E_UNSUPPORTED : FVM_E_ARG;
+    if (const int rc = check_common(mesh)) return rc;
     if (!phys || !prims || !grads || !has_grads || !dudt || !work_ok(mesh, work)) return FVM_E_ARG;
     const Phys p = make_phys(phys);
     cudaStream_t s = (cudaStream_t)stream;
@@ -793,11 +881,13 @@ static bool bufs_ok(const fvm_solver_bufs_t* b) {
 
 static bool tab_ok(const fvm_tableau_t* t) { return t && t->stages >= 1 && t->stages <= FVM_MAX_STAGES; }
 
+
 extern "C" int fvm_stage(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const fvm_tableau_t* tab,
                          int32_t s, const fvm_solver_bufs_t* bufs, const fvm_work_t* work, void* stream) {
-    if (!mesh_ok(mesh) || !phys || !tab_ok(tab) || s < 0 || s >= tab->stages || !bufs_ok(bufs) ||
-        !work_ok(mesh, work))
+    if (const int rc = check_common(mesh)) return rc;
+    if (!phys || !tab_ok(tab) || s < 0 || s >= tab->stages || !bufs_ok(bufs) || !work_ok(mesh, work))
         return FVM_E_ARG;
+    if (mesh->n_cases > 0 && tab->adaptive) return FVM_E_UNSUPPORTED;
     const Phys p = make_phys(phys);
     cudaStream_t st = (cudaStream_t)stream;
     return mesh->dim == 2 ? stage_impl<2>(mesh, p, tab, s, bufs, work, st)
@@ -806,7 +896,9 @@ extern "C" int fvm_stage(const fvm_mesh_t* mesh, const fvm_physics_t* phys, cons
 
 extern "C" int fvm_step(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const fvm_tableau_t* tab,
                         const fvm_solver_bufs_t* bufs, const fvm_work_t* work, void* stream) {
-    if (!mesh_ok(mesh) || !phys || !tab_ok(tab) || !bufs_ok(bufs) || !work_ok(mesh, work)) return FVM_E_ARG;
+    if (const int rc = check_common(mesh)) return rc;
+    if (!phys || !tab_ok(tab) || !bufs_ok(bufs) || !work_ok(mesh, work)) return FVM_E_ARG;
+    if (mesh->n_cases > 0 && tab->adaptive) return FVM_E_UNSUPPORTED;
     const Phys p = make_phys(phys);
     cudaStream_t st = (cudaStream_t)stream;
     for (int s = 0; s < tab->stages; ++s) {
@@ -820,7 +912,8 @@ extern "C" int fvm_step(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const
 extern "C" int fvm_multistep(const fvm_mesh_t* mesh, const fvm_physics_t* phys, int32_t store,
                              int32_t n_terms, const int32_t* idx, const float* coef,
                              const fvm_solver_bufs_t* bufs, const fvm_work_t* work, void* stream) {
-    if (!mesh_ok(mesh) || !phys || !bufs_ok(bufs) || !work_ok(mesh, work) || n_terms < 0 ||
+    if (const int rc = check_common(mesh)) return rc;
+    if (!phys || !bufs_ok(bufs) || !work_ok(mesh, work) || n_terms < 0 ||
         n_terms > FVM_MAX_STAGES || (n_terms > 0 && (!idx || !coef)) || store < 0)
         return FVM_E_ARG;
     const Phys p = make_phys(phys);
@@ -856,8 +949,8 @@ extern "C" int fvm_cfl_dt(const fvm_mesh_t* mesh, const fvm_physics_t* phys, con
                                              *mesh, p, state, 1, 0, work->red));
     int rc = launch_status();
     if (rc) return rc;
-    FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<1, 32, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, cfl,
-                                                               0, work->red, dt, nullptr));
+    FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(mesh), 128, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, cfl,
+                                                               0, work->red, dt, nullptr, mesh->n_cases));
     return launch_status();
 }
 
@@ -874,7 +967,7 @@ extern "C" int fvm_conservation(const fvm_mesh_t* mesh, const float* state, doub
                                              *mesh, p, state, 0, 1, work->red));
     int rc = launch_status();
     if (rc) return rc;
-    FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<1, 32, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f,
-                                                               1, work->red, nullptr, out));
+    FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(mesh), 128, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f,
+                                                               1, work->red, nullptr, out, mesh->n_cases));
     return launch_status();
 }

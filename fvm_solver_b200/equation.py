@@ -82,7 +82,8 @@ class FluidConstitution3D(FluidConstitution):
 class DeviceMesh:
     """Kernel tables uploaded to one device, plus the ``fvm_mesh_t`` struct pointing at them."""
 
-    _ptr_fields = [f for f, _ in _lib.Mesh._fields_[8:]]
+    _ptr_fields = [f for f in _lib.MESH_PTR_FIELDS if f not in
+                   ("cell_case", "face_case", "bc_case", "ch_off", "case_mu", "case_mu_b", "case_kappa")]
 
     def __init__(self, kt: KernelTables, device):
         self.device = torch.device(device)
@@ -123,6 +124,12 @@ def _host_mesh(mesh, dim_hint=None) -> FVMMesh:
     if getattr(mesh, "period", None) is not None:
         kw = dict(period=mesh.period, cell_shifts=mesh.cell_shifts, facet_shifts=mesh.facet_shifts)
     return cls(mesh.vertices.float().cpu(), mesh.cells.cpu(), mesh.facets.cpu(), mesh.bc_facet_mask.cpu(), **kw)
+
+
+class _MeshInfo:
+    def __init__(self, n_cells, dim):
+        self.n_cells = n_cells
+        self.dim = dim
 
 
 class FVMCells:
@@ -194,6 +201,30 @@ class FVMEquation:
             from .solvers import get_solver
             self.t_solver = get_solver(self.cells, self, cfg)
 
+    @classmethod
+    def from_kernel_tables(cls, cfg: ConfigFVM, phy_setup: FluidConstitution, kt: KernelTables, us_init,
+                           build_solver: bool = True) -> "FVMEquation":
+        """Construct from prebuilt kernel tables (e.g. built once and shared with a batch)."""
+        self = cls.__new__(cls)
+        self.cfg, self.phy_setup = cfg, phy_setup
+        self.device = torch.device(cfg.device)
+        self.lib = _lib.load()
+        self.mesh = _MeshInfo(kt.n_cells, kt.dim)
+        self.n_comp = kt.n_comp
+        self.tables = None
+        self.dev = DeviceMesh(kt, self.device)
+        self.work = self.dev.work()
+        self.phys = phy_setup.physics_struct(cfg)
+        self.grads = torch.zeros((kt.n_cells, kt.dim, kt.n_comp), device=self.device)
+        self.has_grads = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self._has_grads_host = False
+        self.cells = FVMCells(kt.n_cells, kt.n_comp, init_val=us_init, phys_setup=phy_setup, device=self.device)
+        self.t_solver = None
+        if build_solver:
+            from .solvers import get_solver
+            self.t_solver = get_solver(self.cells, self, cfg)
+        return self
+
     @property
     def cell_grads(self):
         """Limited cell gradients of the last evaluation [N, dim, C], or None before the first."""
@@ -221,7 +252,7 @@ class FVMEquation:
     def conservation(self, state: torch.Tensor | None = None) -> torch.Tensor:
         """FP64 totals sum_i vol_i U_i [C] of ``state`` (default: the current cell state)."""
         s = (self.cells.state if state is None else state).contiguous()
-        out = torch.empty(self.n_comp, dtype=torch.float64, device=self.device)
+        out = torch.empty((1, self.n_comp), dtype=torch.float64, device=self.device)
         _lib.check(self.lib.fvm_conservation(ct.byref(self.dev.struct), _lib.ptr(s), _lib.ptr(out),
                                              ct.byref(self.work.struct), _lib.stream_ptr()), "fvm_conservation")
-        return out
+        return out[0]

@@ -117,7 +117,9 @@ class TSolver:
         N, C = eq.mesh.n_cells, eq.n_comp
         self.prims = torch.zeros((N, C), device=dev)
         self.k = torch.zeros((max(self.n_k, 1), N, C), device=dev)
-        self.dt = torch.tensor([cfg.dt if cfg.dt is not None else 0.0], dtype=torch.float32, device=dev)
+        self.n_cases = max(1, int(getattr(eq, "n_cases", 0) or 0))
+        self.dt = torch.full((self.n_cases,), cfg.dt if cfg.dt is not None else 0.0, dtype=torch.float32,
+                             device=dev)
         self.cons = None
         self._prims_version = -1
         self.t = 0.0
@@ -133,7 +135,7 @@ class TSolver:
     def track_conservation(self, on: bool = True):
         """Record the FP64 totals sum vol * U after every step in ``self.cons`` (device)."""
         if on and self.cons is None:
-            self.cons = torch.zeros(self.eq.n_comp, dtype=torch.float64, device=self.eq.device)
+            self.cons = torch.zeros((self.n_cases, self.eq.n_comp), dtype=torch.float64, device=self.eq.device)
         self.bufs.cons = _lib.ptr(self.cons) if on else None
 
     def update_cfl_dt(self, cfl: float | None = None):

@@ -74,6 +74,17 @@ typedef struct fvm_mesh {
     const float *ch_normal;   /* [Fc][dim] outward unit normals                            */
     const float *ch_rho, *ch_vn, *ch_p;            /* [Fc]                                 */
     const float *ch_vt;       /* [Fc][dim]                                                 */
+    /* Batched meshes: n_cases > 0 means the tables are several independent meshes
+     * concatenated (cells, facets, boundary and characteristic facets each contiguous per
+     * case, all indices global).  Each case has its own time step (dt[case]), gas transport
+     * coefficients, characteristic-BC sound-speed mean, CFL and conservation reductions.
+     * n_cases = 0 and NULL pointers: a single mesh. */
+    int32_t n_cases;
+    const int32_t *cell_case; /* [N]  case of each cell                                    */
+    const int32_t *face_case; /* [F]  case of each facet                                   */
+    const int32_t *bc_case;   /* [Fb] case of each boundary facet                          */
+    const int32_t *ch_off;    /* [n_cases + 1] characteristic-facet offsets per case        */
+    const float *case_mu, *case_mu_b, *case_kappa;   /* [n_cases] transport coefficients   */
 } fvm_mesh_t;
 
 /* Gas and scheme constants (ConfigFVM fields, time_fvm/config_fvm.py:52-63). */
@@ -87,7 +98,7 @@ typedef struct fvm_work {
     float *bc_vals;     /* [Fb][C]                                   */
     float *face_vals;   /* [F][2][C]                                 */
     float *flux;        /* [F][C]                                    */
-    double *red;        /* [FVM_RED_DOUBLES], zero-initialised once  */
+    double *red;        /* [FVM_RED_DOUBLES + 8 * n_cases], zero-initialised once */
 } fvm_work_t;
 
 /* Explicit Runge-Kutta tableau (optionally with an embedded low-order row). */
@@ -107,9 +118,10 @@ typedef struct fvm_solver_bufs {
     float *prims;       /* [N][C] primitives of the current stage input                   */
     float *grads;       /* [N][dim][C] limited gradients, carried across evaluations      */
     float *k;           /* [stages][N][C] stage increments dt * f                          */
-    float *dt;          /* [1] time step (device)                                         */
+    float *dt;          /* [max(1, n_cases)] time step per case (device)                  */
     int32_t *has_grads; /* [1] device flag: grads hold a previous evaluation              */
-    double *cons;       /* [C] optional: FP64 sum of vol * U after each step (may be NULL) */
+    double *cons;       /* [max(1, n_cases)][C] optional: FP64 sum of vol * U after each step
+                         * (may be NULL)                                                  */
 } fvm_solver_bufs_t;
 
 /* Last CUDA error recorded by this library (cudaError_t value), 0 if none. */
@@ -148,7 +160,8 @@ int fvm_residual(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float 
                  void *stream);
 
 /* One explicit stage s of `tab` (residual of bufs->prims, then the stage combination); the
- * last stage writes the new state and, per `tab`, updates dt. */
+ * last stage writes the new state and, per `tab`, updates dt.  Adaptive tableaus are
+ * single-mesh only (FVM_E_UNSUPPORTED for batched meshes). */
 int fvm_stage(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const fvm_tableau_t *tab,
               int32_t s, const fvm_solver_bufs_t *bufs, const fvm_work_t *work, void *stream);
 
@@ -168,11 +181,11 @@ int fvm_multistep(const fvm_mesh_t *mesh, const fvm_physics_t *phys, int32_t sto
 int fvm_state_to_prims(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *state,
                        float *prims, void *stream);
 
-/* dt[0] <- cfl * min_i 1 / (inv_h_i (|u_i| + c_i)) of state (FP64 reduction). */
+/* dt[case] <- cfl * min_i 1 / (inv_h_i (|u_i| + c_i)) over the case's cells (FP64 reduction). */
 int fvm_cfl_dt(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *state,
                float cfl, float *dt, const fvm_work_t *work, void *stream);
 
-/* out[C] <- sum_i vol_i * state[i][c] in FP64. */
+/* out[case][C] <- sum_i vol_i * state[i][c] over the case's cells, in FP64. */
 int fvm_conservation(const fvm_mesh_t *mesh, const float *state, double *out,
                      const fvm_work_t *work, void *stream);
 
