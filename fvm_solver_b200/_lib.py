@@ -13,7 +13,8 @@ import torch
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfvm_b200.so")
 
-FVM_OK, FVM_E_ARG, FVM_E_CUDA, FVM_E_UNSUPPORTED = 0, -1, -2, -3
+FVM_OK, FVM_E_ARG, FVM_E_CUDA, FVM_E_UNSUPPORTED, FVM_E_CAPACITY = 0, -1, -2, -3, -4
+FVM_NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024
 FVM_MAX_STAGES = 12
 FVM_RED_DOUBLES = 64
 
@@ -74,6 +75,7 @@ _SIGS = [
     ("fvm_state_to_prims", ct.c_int, [ct.POINTER(Mesh), ct.POINTER(Physics), _P, _P, _P]),
     ("fvm_cfl_dt", ct.c_int, [ct.POINTER(Mesh), ct.POINTER(Physics), _P, ct.c_float, _P, ct.POINTER(Work), _P]),
     ("fvm_conservation", ct.c_int, [ct.POINTER(Mesh), _P, _P, ct.POINTER(Work), _P]),
+    ("fvm_residual_noalloc", ct.c_int, [ct.POINTER(Mesh), ct.POINTER(Physics), _P, _P, _P, _P, _P]),
     ("fvm_profile_start", ct.c_int, [ct.c_int32]),
     ("fvm_profile_stop", ct.c_int, []),
     ("fvm_profile_read", ct.c_int, [ct.c_int32, _P, _P]),
@@ -108,7 +110,9 @@ def check(rc: int, what: str):
         if rc == FVM_E_CUDA:
             extra = f" (cudaError {load(False).fvm_last_cuda_error()})"
         kind = {FVM_E_ARG: "invalid argument", FVM_E_CUDA: "CUDA launch failure",
-                FVM_E_UNSUPPORTED: "unsupported configuration"}.get(rc, f"error {rc}")
+                FVM_E_UNSUPPORTED: "unsupported configuration",
+                FVM_E_CAPACITY: f"mesh too large for the {FVM_NOALLOC_SCRATCH_BYTES >> 20} MiB static scratch"
+                }.get(rc, f"error {rc}")
         raise RuntimeError(f"{what}: {kind}{extra}")
 
 

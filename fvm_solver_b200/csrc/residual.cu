@@ -875,6 +875,40 @@ extern "C" int fvm_residual(const fvm_mesh_t* mesh, const fvm_physics_t* phys, c
                           : residual_impl<3>(mesh, p, prims, grads, has_grads, dudt, work, s);
 }
 
+// ------------------------------------------------------------------------------------------
+// Allocation-free residual (fvm_residual_noalloc).
+//
+// Some callers cannot allocate device memory where they call the residual: an application whose
+// own pool allocator has already reserved the GPU's memory, or a time-critical loop that forbids
+// allocation once it runs (cudaMalloc / cudaFree can also wait for the whole device to go idle,
+// stalling unrelated streams).  This variant takes its scratch -- boundary values, the facet-value
+// table and the fluxes (plus per-case slots of batched meshes) -- from one file-scope device array
+// of FVM_NOALLOC_SCRATCH_BYTES, which every GPU that loads this library keeps until the process
+// exits.  The residual overwrites every scratch element it reads before reading it, so nothing has
+// to be cleared between calls.  All calls on a device share the array: calls that overlap on the
+// GPU (different streams, or different host threads) race and must be serialised by the caller.
+// ------------------------------------------------------------------------------------------
+constexpr int64_t kNoAllocFloats = FVM_NOALLOC_SCRATCH_BYTES / 4;
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocFloats];
+
+static constexpr int kMaxDevices = 64;
+static float* g_noalloc_dev_ptr[kMaxDevices];   // device address of g_noalloc_scratch, per device
+
+// The symbol's device address, looked up once per device with that device current (host code may
+// not use the symbol's name as an address).  Returns nullptr on failure.
+static float* noalloc_scratch_address() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    float* p = __atomic_load_n(&g_noalloc_dev_ptr[dev], __ATOMIC_ACQUIRE);
+    if (p) return p;
+    void* addr = nullptr;
+    if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || addr == nullptr) return nullptr;
+    __atomic_store_n(&g_noalloc_dev_ptr[dev], static_cast<float*>(addr), __ATOMIC_RELEASE);
+    return static_cast<float*>(addr);
+}
+
+static inline int64_t align64(int64_t n) { return (n + 63) / 64 * 64; }   // 256-byte units of floats
+
 static bool bufs_ok(const fvm_solver_bufs_t* b) {
     return b && b->state && b->prims && b->grads && b->k && b->dt && b->has_grads;
 }
@@ -970,4 +1004,30 @@ extern "C" int fvm_conservation(const fvm_mesh_t* mesh, const float* state, doub
     FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(mesh), 128, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f,
                                                                1, work->red, nullptr, out, mesh->n_cases));
     return launch_status();
+}
+
+extern "C" int fvm_residual_noalloc(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const float* prims,
+                                    float* grads, int32_t* has_grads, float* dudt, void* stream) {
+    if (const int rc = check_common(mesh)) return rc;
+    if (!phys || !prims || !grads || !has_grads || !dudt) return FVM_E_ARG;
+    const int64_t C = mesh->n_comp;
+    const int64_t n_bc = align64((int64_t)mesh->n_bc * C);
+    const int64_t n_face = align64((int64_t)mesh->n_facets * 2 * C);
+    const int64_t n_flux = align64((int64_t)mesh->n_facets * C);
+    const int64_t n_red = align64(2 * ((int64_t)FVM_RED_DOUBLES + 8 * (int64_t)mesh->n_cases));
+    if (n_bc + n_face + n_flux + n_red > kNoAllocFloats) return FVM_E_CAPACITY;
+    float* base = noalloc_scratch_address();
+    if (!base) {
+        launch_status();
+        return FVM_E_CUDA;
+    }
+    fvm_work_t w;
+    w.bc_vals = base;
+    w.face_vals = base + n_bc;
+    w.flux = base + n_bc + n_face;
+    w.red = reinterpret_cast<double*>(base + n_bc + n_face + n_flux);
+    const Phys p = make_phys(phys);
+    cudaStream_t s = (cudaStream_t)stream;
+    return mesh->dim == 2 ? residual_impl<2>(mesh, p, prims, grads, has_grads, dudt, &w, s)
+                          : residual_impl<3>(mesh, p, prims, grads, has_grads, dudt, &w, s);
 }

@@ -249,6 +249,26 @@ class FVMEquation:
         self._has_grads_host = True
         return out
 
+    def forward_noalloc(self, primatives: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+        """``forward`` through ``fvm_residual_noalloc``: writes dU/dt into the caller's ``out``.
+
+        For callers that cannot allocate device memory at the call: the library allocates nothing
+        (its scratch is a 16 MiB static device array shared by all calls on the device, so calls
+        must not overlap on the GPU), and ``primatives`` / ``out`` must already be contiguous
+        float32 CUDA tensors of shape [N, C].  Raises ``RuntimeError`` if the mesh needs more
+        scratch than the static array holds.
+        """
+        N, C = self.mesh.n_cells, self.n_comp
+        for t in (primatives, out):
+            if not (t.is_cuda and t.dtype == torch.float32 and t.is_contiguous() and tuple(t.shape) == (N, C)):
+                raise ValueError("forward_noalloc needs contiguous float32 CUDA tensors of shape [N, C]")
+        _lib.check(self.lib.fvm_residual_noalloc(ct.byref(self.dev.struct), ct.byref(self.phys),
+                                                 _lib.ptr(primatives), _lib.ptr(self.grads),
+                                                 _lib.ptr(self.has_grads), _lib.ptr(out), _lib.stream_ptr()),
+                   "fvm_residual_noalloc")
+        self._has_grads_host = True
+        return out
+
     def conservation(self, state: torch.Tensor | None = None) -> torch.Tensor:
         """FP64 totals sum_i vol_i U_i [C] of ``state`` (default: the current cell state)."""
         s = (self.cells.state if state is None else state).contiguous()

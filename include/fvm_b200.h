@@ -34,10 +34,12 @@ extern "C" {
 #define FVM_E_ARG (-1)      /* invalid argument (null pointer, size out of range) */
 #define FVM_E_CUDA (-2)     /* a CUDA launch failed; see fvm_last_cuda_error() */
 #define FVM_E_UNSUPPORTED (-3)
+#define FVM_E_CAPACITY (-4)    /* the mesh needs more scratch than fvm_residual_noalloc has */
 
 #define FVM_MAX_STAGES 12
 #define FVM_MAX_KG 16
 #define FVM_RED_DOUBLES 64
+#define FVM_NOALLOC_SCRATCH_BYTES (16 * 1024 * 1024)
 
 /* Mesh tables (see fvm_solver_b200/tables.py KernelTables for how they are built).
  * N cells, F facets, Fb boundary facets, Fc characteristic facets, K = dim + 1. */
@@ -158,6 +160,23 @@ int fvm_ell_spmm(const float *vals, const int32_t *cols, int64_t M, int32_t K,
 int fvm_residual(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *prims,
                  float *grads, int32_t *has_grads, float *dudt, const fvm_work_t *work,
                  void *stream);
+
+/* Allocation-free fvm_residual.  No counterpart in the reference: it exists for callers that
+ * cannot allocate device memory where they call the residual -- an application whose own pool
+ * allocator has already reserved the GPU's memory, or a time-critical loop that forbids
+ * allocation once it runs (cudaMalloc / cudaFree can also wait for the device to go idle).
+ * Same arguments and results as fvm_residual, minus `work`: the scratch (boundary values,
+ * facet-value table, fluxes) lives in one static device array of FVM_NOALLOC_SCRATCH_BYTES
+ * (16 MiB) that every GPU loading the library keeps until the process exits.  A mesh whose
+ * scratch does not fit -- 4 * (align64(Fb*C) + align64(2*F*C) + align64(F*C)
+ * + align64(2*(64 + 8*n_cases))) bytes, i.e. up to about 280 000 facets in 3D or 350 000 in 2D --
+ * is rejected with FVM_E_CAPACITY before anything is launched.  The function never allocates;
+ * the first call on each device looks up the array's device address (with that device
+ * current), so make that first call before any stream capture.  Every call overwrites the
+ * scratch it reads, so no clearing is needed; all calls on a device share the array, so calls
+ * that overlap on the GPU race and must be serialised by the caller. */
+int fvm_residual_noalloc(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *prims,
+                         float *grads, int32_t *has_grads, float *dudt, void *stream);
 
 /* One explicit stage s of `tab` (residual of bufs->prims, then the stage combination); the
  * last stage writes the new state and, per `tab`, updates dt.  Adaptive tableaus are
