@@ -329,9 +329,9 @@ def main():
     tot = sum(v["ms_total"] for v in kern.values())
     for v in kern.values():
         v["share"] = v["ms_total"] / tot
-    kb = kernel_bytes(3, N, F, Fb, eq.dev.t.kf)
+    kb = kernel_bytes(3, N, F, Fb, eq.dev.kf)
     per_launch = {"cell": kb["cell"], "face": kb["face"], "bc": kb["bc"]}
-    dsb = div_stage_bytes(3, N, F, Fb, tableau_terms(sol.tab), eq.dev.t.kf)
+    dsb = div_stage_bytes(3, N, F, Fb, tableau_terms(sol.tab), eq.dev.kf)
     per_launch["div_stage"] = float(np.mean(dsb))
     dom = max((k for k in kern if k in per_launch), key=lambda k: kern[k]["ms_total"])
     peak, peak_kind = measured_peaks()

@@ -23,9 +23,8 @@ _P = ct.c_void_p
 
 class Mesh(ct.Structure):
     _fields_ = [(n, ct.c_int32) for n in ("dim", "n_comp", "n_cells", "n_facets", "n_bc", "n_char", "kg", "kf")] + [
-        (n, _P) for n in ("g_vals", "g_cols", "nb_slot", "disp", "eps", "c2f", "side", "f_vals", "f_cols",
-                          "inv_h", "volumes", "fcell", "fbc", "normals", "fsize", "xorth", "inv_d",
-                          "bc_face", "bc_side", "bc_cell", "bc_kind", "bc_b", "bc_l", "bc_ga", "bc_gb",
+        (n, _P) for n in ("cell_rec", "div_rec", "inv_h", "volumes", "face_rec",
+                          "bc_cell", "bc_kind", "bc_b", "bc_l", "bc_ga", "bc_gb",
                           "bc_char", "ch_cell", "ch_normal", "ch_rho", "ch_vn", "ch_p", "ch_vt")] + [
         ("n_cases", ct.c_int32)] + [
         (n, _P) for n in ("cell_case", "face_case", "bc_case", "ch_off", "case_mu", "case_mu_b", "case_kappa")]
@@ -39,7 +38,7 @@ class Physics(ct.Structure):
 
 
 class Work(ct.Structure):
-    _fields_ = [("bc_vals", _P), ("face_vals", _P), ("flux", _P), ("red", _P)]
+    _fields_ = [("bc_vals", _P), ("prims", _P), ("flux", _P), ("red", _P)]
 
 
 class Tableau(ct.Structure):

@@ -134,7 +134,7 @@ class BatchedDeviceMesh:
         self.t = self.base.t
         self.device = self.base.device
         self.n_comp, self.n_cells, self.n_facets, self.n_bc = kt.n_comp, kt.n_cells, kt.n_facets, kt.n_bc
-        self.dim = kt.dim
+        self.dim, self.row, self.grow, self.kf = kt.dim, self.base.row, self.base.grow, kt.kf
         self.case = {k: v.contiguous().to(self.device) for k, v in case_arrays.items()}
         m = self.base.struct
         m.n_cases = int(case_arrays["case_mu"].numel())
@@ -166,7 +166,7 @@ class BatchedFVM:
         self.work = Work(self.dev)
         self.work.red = torch.zeros(_lib.FVM_RED_DOUBLES + 8 * self.n_cases, dtype=torch.float64, device=self.device)
         self.work.struct.red = _lib.ptr(self.work.red)
-        self.grads = torch.zeros((kt.n_cells, kt.dim, C), device=self.device)
+        self.grads = torch.zeros((kt.n_cells, self.dev.grow), device=self.device)
         self.has_grads = torch.zeros(1, dtype=torch.int32, device=self.device)
         self._has_grads_host = False
         phy = (FluidConstitution2D if kt.dim == 2 else FluidConstitution3D)(cfg)

@@ -1,26 +1,32 @@
 // Fused finite-volume residual and explicit time-stepping kernels.
 //
-// One residual evaluation (FVMEquation.forward, time_fvm/fvm_equation.py:406-435) is four
-// kernels instead of the reference's ~60 eager PyTorch ops:
+// One residual evaluation (FVMEquation.forward, time_fvm/fvm_equation.py:406-435) is three
+// kernels (four with boundaries) instead of the reference's ~60 eager PyTorch ops:
 //
 //   k_bc        boundary facets: A_bc U + b_bc + A_corr grads_prev, then the characteristic BC
 //               (facet_boundary.py:124-168, 418-512).  Each block recomputes the group mean of the
 //               interior sound speed in the same order, so no grid-wide synchronisation is needed.
 //   k_cell      per cell: LSQ gradient (G_mats spMM, facet_process.py:409-418), slope limiter
-//               (facet_process.py:387-407, limiter.py), limited facet values scattered straight to
-//               the [F][2][C] facet table (facet_process.py:349-351), limited gradient.
-//   k_face      per facet: averaged gradients, normal gradient (A_face_grad spMV) and
-//               non-orthogonal correction (facet_process.py:362-385), EOS and stress
-//               (fvm_equation.py:62-187), advection + pressure + viscous + heating + Kurganov-Tadmor
-//               fluxes (fvm_equation.py:199-368).
+//               (facet_process.py:387-407, limiter.py) and the limited gradient
+//               (FacetCalc.cell_grads, facet_process.py:345-346).
+//   k_face      per facet: limited facet values of both sides, rebuilt from each cell's primitives
+//               and limited gradient (U + grad_lim . r, the reference's addcmul(U, dU, phi) of
+//               facet_process.py:405 with the limiter applied to the gradient), averaged gradients,
+//               normal gradient (A_face_grad spMV) and non-orthogonal correction
+//               (facet_process.py:362-385), EOS and stress (fvm_equation.py:62-187), advection +
+//               pressure + viscous + heating + Kurganov-Tadmor fluxes (fvm_equation.py:199-368).
 //   k_div_stage per cell: divergence (flux_mat spMM, fvm_equation.py:428-435) fused with the
 //               Runge-Kutta / Adams stage combination, the conserved -> primitive conversion of
 //               the next stage input (fvm_equation.py:35-44) and, on the last stage, the FP64
 //               reductions for the adaptive step size (integrators.py:42-62), the CFL time step and
 //               the conservation sums.
 //
-// All four are memory-bound gathers: one thread per cell / facet, slot-major tables so warps read
-// coalesced, AoS [row][C] state so each gathered neighbour is one or two 32-byte sectors.
+// All kernels are memory-bound gathers with one thread per cell or facet.  Every per-cell and
+// per-facet table is one contiguous record read with 16-byte loads, and every gathered row
+// (primitives, limited gradients, fluxes) is padded to a 16-byte multiple, so a gather is one or
+// two aligned vector loads and never straddles more 32-byte sectors than it must.  Rebuilding the
+// facet values in k_face removes the reference's [F, 2, C] facet table (a scattered write plus a
+// read per facet side).
 #include <math.h>
 
 #include "fvm_common.cuh"
@@ -46,6 +52,50 @@ struct StageArgs {
     float coef_lo[FVM_MAX_STAGES];
     int adaptive, cfl, cons;
 };
+
+// Compile-time layout of one dimension.
+template <int DIM>
+struct L {
+    static constexpr int C = DIM + 2, K = DIM + 1, KG = DIM + 2;
+    static constexpr int RS = FVM_ROW(DIM), GS = FVM_GROW(DIM);
+    static constexpr int CR = FVM_CELL_REC(DIM), FR = FVM_FACE_REC(DIM), DR = FVM_DIV_REC;
+    // cell record offsets
+    static constexpr int GV = 0, GC = DIM * KG, DISP = GC + KG, EPS = DISP + K * DIM, META = EPS + 1;
+    // face record offsets
+    static constexpr int FA = 0, FB = 1, INVD = 2, SIZE = 3, NRM = 4, XO = 4 + DIM, RA = 4 + 2 * DIM,
+                         RB = 4 + 3 * DIM;
+    // limited-gradient row index of (spatial direction d, component comp)
+    static __host__ __device__ __forceinline__ constexpr int gi(int d, int comp) {
+        return comp == DIM ? DIM * (DIM + 1) + d : d * (DIM + 1) + (comp < DIM ? comp : DIM);
+    }
+    static_assert(META + 1 <= CR && RB + DIM <= FR && 2 * K <= DR, "record layout");
+};
+
+// N consecutive floats (N % 4 == 0, 16-byte aligned) -> registers.
+template <int N>
+__device__ __forceinline__ void ld_vec(const float* __restrict__ p, float (&v)[N]) {
+#pragma unroll
+    for (int q = 0; q < N / 4; ++q) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(p) + q);
+        v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+    }
+}
+// Same, for data written by an earlier kernel of the same sequence (no read-only cache).
+template <int N>
+__device__ __forceinline__ void ld_vec_cg(const float* p, float (&v)[N]) {
+#pragma unroll
+    for (int q = 0; q < N / 4; ++q) {
+        const float4 t = __ldcg(reinterpret_cast<const float4*>(p) + q);
+        v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+    }
+}
+template <int N>
+__device__ __forceinline__ void st_vec(float* p, const float (&v)[N]) {
+#pragma unroll
+    for (int q = 0; q < N / 4; ++q)
+        reinterpret_cast<float4*>(p)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+}
+__device__ __forceinline__ int as_int(float x) { return __float_as_int(x); }
 
 // ------------------------------------------------------------------------------------------
 // Slope limiters (limiter.py:29-77).  delta: allowed range, dU: unlimited increment.
@@ -86,14 +136,13 @@ __device__ __forceinline__ float limiter_phi(int p, float delta, float dU, float
 // ------------------------------------------------------------------------------------------
 // Sum of the interior sound speed over characteristic facets [lo, hi): every caller uses the same
 // thread -> element mapping and reduction tree, so batched and single-mesh runs agree bitwise.
-template <int C>
+template <int DIM>
 __device__ __forceinline__ double char_c_sum(const fvm_mesh_t& m, const Phys& p, const float* prims, int lo,
                                              int hi, double* red) {
-    constexpr int DIM = C - 2;
     double acc = 0.0;
     for (int t = lo + threadIdx.x; t < hi; t += blockDim.x) {
         const int cell = __ldg(m.ch_cell + t);
-        acc += (double)sqrtf(p.gR * __ldg(prims + (int64_t)cell * C + DIM + 1));
+        acc += (double)sqrtf(p.gR * __ldg(prims + (int64_t)cell * L<DIM>::RS + DIM + 1));
     }
     double v[1] = {acc};
     block_sum<1>(v, red);
@@ -104,27 +153,27 @@ __device__ __forceinline__ double char_c_sum(const fvm_mesh_t& m, const Phys& p,
 template <int DIM>
 __global__ void __launch_bounds__(kBlock) k_char_scale(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
                                                         double* __restrict__ red_out) {
-    constexpr int C = DIM + 2;
     __shared__ double red[32];
     const int c = blockIdx.x;
     const int lo = __ldg(m.ch_off + c), hi = __ldg(m.ch_off + c + 1);
-    const double sum = char_c_sum<C>(m, p, prims, lo, hi, red);
-    if (threadIdx.x == 0) red_out[FVM_RED_DOUBLES + 8 * c + 6] = hi > lo ? (double)(10.0f / (float)(sum / (double)(hi - lo))) : 0.0;
+    const double sum = char_c_sum<DIM>(m, p, prims, lo, hi, red);
+    if (threadIdx.x == 0)
+        red_out[FVM_RED_DOUBLES + 8 * c + 6] = hi > lo ? (double)(10.0f / (float)(sum / (double)(hi - lo))) : 0.0;
 }
 
 template <int DIM>
 __global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
                                                 const float* __restrict__ grads,
                                                 const int32_t* __restrict__ has_grads,
-                                                float* __restrict__ bcv, float* __restrict__ face_vals,
-                                                const double* __restrict__ wred) {
-    constexpr int C = DIM + 2;
+                                                float* __restrict__ bcv, const double* __restrict__ wred) {
+    using Ly = L<DIM>;
+    constexpr int C = Ly::C;
     __shared__ double red[32];
     float scale = 0.f;
     if (m.n_char > 0 && m.n_cases == 0) {
         // Group mean of the interior sound speed c = sqrt(gamma R T) (facet_boundary.py:427),
         // recomputed identically by every block.
-        const double sum = char_c_sum<C>(m, p, prims, 0, m.n_char, red);
+        const double sum = char_c_sum<DIM>(m, p, prims, 0, m.n_char, red);
         __shared__ float s_scale;
         if (threadIdx.x == 0) s_scale = 10.0f / (float)(sum / (double)m.n_char);
         __syncthreads();
@@ -134,10 +183,12 @@ __global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float
     if (b >= m.n_bc) return;
     if (m.n_cases > 0) scale = (float)wred[FVM_RED_DOUBLES + 8 * __ldg(m.bc_case + b) + 6];
     const int cell = __ldg(m.bc_cell + b);
-    float U[C];
-    load_row<C>(prims + (int64_t)cell * C, U);
+    float U[Ly::RS];
+    ld_vec<Ly::RS>(prims + (int64_t)cell * Ly::RS, U);
     const bool prev = *has_grads != 0;
-    float out[C];
+    float out[Ly::RS];
+#pragma unroll
+    for (int c = 0; c < Ly::RS; ++c) out[c] = 0.f;
 #pragma unroll
     for (int c = 0; c < C; ++c) {
         const int kind = __ldg(m.bc_kind + b * C + c);
@@ -146,7 +197,7 @@ __global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float
             float corr = 0.f;
 #pragma unroll
             for (int d = 0; d < DIM; ++d)
-                corr = fmaf(__ldg(m.bc_l + b * DIM + d), grads[((int64_t)cell * DIM + d) * C + c], corr);
+                corr = fmaf(__ldg(m.bc_l + b * DIM + d), grads[(int64_t)cell * Ly::GS + Ly::gi(d, c)], corr);
             v += corr;
         }
         out[c] = v;
@@ -190,29 +241,27 @@ __global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float
         out[DIM] = rho_b;
         out[DIM + 1] = p_b / (p.R * rho_b);
     }
-    store_row<C>(bcv + (int64_t)b * C, out);
-    const int f = __ldg(m.bc_face + b), sd = __ldg(m.bc_side + b);
-    store_row<C>(face_vals + ((int64_t)f * 2 + sd) * C, out);
+    st_vec<Ly::RS>(bcv + (int64_t)b * Ly::RS, out);
 }
 
 // ------------------------------------------------------------------------------------------
-// k_cell: gradient, limiter, limited facet values, limited gradient.
+// k_cell: gradient, limiter, limited gradient.
 // ------------------------------------------------------------------------------------------
-template <int DIM, int KG>
+template <int DIM>
 __global__ void __launch_bounds__(kBlock) k_cell(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
-                                                  const float* __restrict__ bcv,
-                                                  float* __restrict__ face_vals,
-                                                  float* __restrict__ grads,
+                                                  const float* __restrict__ bcv, float* __restrict__ grads,
                                                   int32_t* __restrict__ has_grads) {
-    constexpr int C = DIM + 2, K = DIM + 1;
+    using Ly = L<DIM>;
+    constexpr int C = Ly::C, K = Ly::K, KG = Ly::KG, RS = Ly::RS;
     const int N = m.n_cells;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) *has_grads = 1;
     if (i >= N) return;
-    float U[C];
-    load_row<C>(prims + (int64_t)i * C, U);
-    const int meta = __ldg(m.nb_slot + i);
-    const int nvalid = (meta >> 24) & 31;
+    float rec[Ly::CR];
+    ld_vec<Ly::CR>(m.cell_rec + (int64_t)i * Ly::CR, rec);
+    float U[RS];
+    ld_vec<RS>(prims + (int64_t)i * RS, U);
+    const int nvalid = (as_int(rec[Ly::META]) >> 24) & 31;
     float g[DIM][C];
 #pragma unroll
     for (int d = 0; d < DIM; ++d)
@@ -223,13 +272,13 @@ __global__ void __launch_bounds__(kBlock) k_cell(fvm_mesh_t m, Phys p, const flo
     for (int c = 0; c < C; ++c) up[c] = lo[c] = U[c];
 #pragma unroll
     for (int k = 0; k < KG; ++k) {
-        const int col = __ldg(m.g_cols + (int64_t)k * N + i);
-        float X[C];
-        if (col < N) load_row<C>(prims + (int64_t)col * C, X);
-        else load_row_cg<C>(bcv + (int64_t)(col - N) * C, X);
+        const int col = as_int(rec[Ly::GC + k]);
+        float X[RS];
+        if (col < N) ld_vec<RS>(prims + (int64_t)col * RS, X);
+        else ld_vec_cg<RS>(bcv + (int64_t)(col - N) * RS, X);
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
-            const float w = __ldg(m.g_vals + ((int64_t)d * KG + k) * N + i);
+            const float w = rec[Ly::GV + d * KG + k];
 #pragma unroll
             for (int c = 0; c < C; ++c) g[d][c] = fmaf(w, X[c], g[d][c]);
         }
@@ -241,47 +290,33 @@ __global__ void __launch_bounds__(kBlock) k_cell(fvm_mesh_t m, Phys p, const flo
             }
         }
     }
+    const float eps = rec[Ly::EPS];
+    float phim[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) {
         up[c] -= U[c];
         lo[c] -= U[c];
+        phim[c] = INFINITY;
     }
-    const float eps = __ldg(m.eps + i);
-    float dU[K][C], phim[C];
-#pragma unroll
-    for (int c = 0; c < C; ++c) phim[c] = INFINITY;
 #pragma unroll
     for (int j = 0; j < K; ++j) {
-        float r[DIM];
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) r[d] = __ldg(m.disp + ((int64_t)j * DIM + d) * N + i);
 #pragma unroll
         for (int c = 0; c < C; ++c) {
-            float du = g[0][c] * r[0];
+            float du = g[0][c] * rec[Ly::DISP + j * DIM];
 #pragma unroll
-            for (int d = 1; d < DIM; ++d) du = fmaf(g[d][c], r[d], du);
-            dU[j][c] = du;
+            for (int d = 1; d < DIM; ++d) du = fmaf(g[d][c], rec[Ly::DISP + j * DIM + d], du);
             const float num = du > 0.f ? up[c] : lo[c];
             phim[c] = fminf(phim[c], limiter_phi(p.lim_p, num, du, eps));
         }
     }
-    const int sides = __ldg(m.side + i);
+    float go[Ly::GS];
 #pragma unroll
-    for (int j = 0; j < K; ++j) {
-        float fv[C];
+    for (int q = 0; q < Ly::GS; ++q) go[q] = 0.f;
 #pragma unroll
-        for (int c = 0; c < C; ++c) fv[c] = fmaf(dU[j][c], phim[c], U[c]);
-        const int f = __ldg(m.c2f + (int64_t)j * N + i);
-        store_row<C>(face_vals + ((int64_t)f * 2 + ((sides >> j) & 1)) * C, fv);
-    }
-    float* go = grads + (int64_t)i * DIM * C;
+    for (int d = 0; d < DIM; ++d)
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-        float gd[C];
-#pragma unroll
-        for (int c = 0; c < C; ++c) gd[c] = g[d][c] * phim[c];
-        store_row<C>(go + d * C, gd);
-    }
+        for (int c = 0; c < C; ++c) go[Ly::gi(d, c)] = g[d][c] * phim[c];
+    st_vec<Ly::GS>(grads + (int64_t)i * Ly::GS, go);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -289,64 +324,86 @@ __global__ void __launch_bounds__(kBlock) k_cell(fvm_mesh_t m, Phys p, const flo
 // ------------------------------------------------------------------------------------------
 template <int DIM>
 __global__ void __launch_bounds__(kBlock) k_face(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
-                                                  const float* __restrict__ face_vals,
-                                                  const float* __restrict__ grads,
-                                                  float* __restrict__ flux) {
-    constexpr int C = DIM + 2, NG = DIM + 1;
+                                                  const float* __restrict__ bcv,
+                                                  const float* __restrict__ grads, float* __restrict__ flux) {
+    using Ly = L<DIM>;
+    constexpr int C = Ly::C, NG = DIM + 1, RS = Ly::RS, GS = Ly::GS;
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.n_facets) return;
-    const int cL = __ldg(m.fcell + 2 * f), cR = __ldg(m.fcell + 2 * f + 1);
-    const int b = __ldg(m.fbc + f);
-    float n[DIM], nh[DIM], xo[DIM];
-    const float size = __ldg(m.fsize + f);
+    float rec[Ly::FR];
+    ld_vec<Ly::FR>(m.face_rec + (int64_t)f * Ly::FR, rec);
+    const int ca = as_int(rec[Ly::FA]), cb = as_int(rec[Ly::FB]);
+    const float size = rec[Ly::SIZE];
+    float n[DIM], nh[DIM];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
-        n[d] = __ldg(m.normals + f * DIM + d);
+        n[d] = rec[Ly::NRM + d];
         nh[d] = n[d] / size;
-        xo[d] = __ldg(m.xorth + f * DIM + d);
     }
-    float UL[C], UR[C];
-    load_row_cg<C>(face_vals + (int64_t)f * 2 * C, UL);
-    load_row_cg<C>(face_vals + ((int64_t)f * 2 + 1) * C, UR);
-
+    // Both sides: primitives and limited gradient of the cell(s); a boundary side (code < 0) takes
+    // the boundary value, and its gradient is the interior cell's (facet_process.py:364-368).
+    const int cell0 = ca >= 0 ? ca : cb;
+    const int cell1 = cb >= 0 ? cb : ca;
+    float P0[RS], P1[RS], G0[GS], G1[GS];
+    ld_vec<RS>(prims + (int64_t)cell0 * RS, P0);
+    ld_vec<RS>(prims + (int64_t)cell1 * RS, P1);
+    ld_vec_cg<GS>(grads + (int64_t)cell0 * GS, G0);
+    ld_vec_cg<GS>(grads + (int64_t)cell1 * GS, G1);
+    float UL[RS], UR[RS];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        const int code = s == 0 ? ca : cb;
+        float* Us = s == 0 ? UL : UR;
+        if (code >= 0) {
+            const float* P = s == 0 ? P0 : P1;
+            const float* G = s == 0 ? G0 : G1;
+            const int roff = s == 0 ? Ly::RA : Ly::RB;
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                float acc = G[Ly::gi(0, c)] * rec[roff];
+#pragma unroll
+                for (int d = 1; d < DIM; ++d) acc = fmaf(G[Ly::gi(d, c)], rec[roff + d], acc);
+                Us[c] = P[c] + acc;
+            }
+        } else {
+            float B[RS];
+            ld_vec_cg<RS>(bcv + (int64_t)(-1 - code) * RS, B);
+#pragma unroll
+            for (int c = 0; c < C; ++c) Us[c] = B[c];
+        }
+    }
     // Facet-averaged limited gradients of (V, T): gls[d][k] (facet_process.py:362-371).
     float gls[DIM][NG];
-    const float* gA = grads + (int64_t)cL * DIM * C;
-    const float* gB = grads + (int64_t)cR * DIM * C;
 #pragma unroll
     for (int d = 0; d < DIM; ++d)
 #pragma unroll
-        for (int k = 0; k < NG; ++k) {
-            const int comp = k < DIM ? k : DIM + 1;
-            gls[d][k] = (__ldcg(gA + d * C + comp) + __ldcg(gB + d * C + comp)) / 2.f;
-        }
+        for (int k = 0; k < NG; ++k) gls[d][k] = (G0[d * NG + k] + G1[d * NG + k]) / 2.f;
     // Normal gradient (A_face_grad row, facet_process.py:420-450).
     float dn[NG];
-    if (b < 0) {
-        const float w = __ldg(m.inv_d + f);
+    if (ca >= 0 && cb >= 0) {
+        const float w = rec[Ly::INVD];
 #pragma unroll
         for (int k = 0; k < NG; ++k) {
             const int comp = k < DIM ? k : DIM + 1;
-            const float x0 = __ldg(prims + (int64_t)cL * C + comp);
-            const float x1 = __ldg(prims + (int64_t)cR * C + comp);
-            dn[k] = cL < cR ? fmaf(w, x1, (-w) * x0) : fmaf(-w, x0, w * x1);
+            const float x0 = P0[comp], x1 = P1[comp];
+            dn[k] = ca < cb ? fmaf(w, x1, (-w) * x0) : fmaf(-w, x0, w * x1);
         }
     } else {
+        const int b = ca < 0 ? -1 - ca : -1 - cb;
 #pragma unroll
         for (int k = 0; k < NG; ++k) {
             const int comp = k < DIM ? k : DIM + 1;
-            const float x = __ldg(prims + (int64_t)cL * C + comp);
-            dn[k] = __ldg(m.bc_ga + b * C + comp) * x + __ldg(m.bc_gb + b * C + comp);
+            dn[k] = __ldg(m.bc_ga + b * C + comp) * P0[comp] + __ldg(m.bc_gb + b * C + comp);
         }
     }
     // Non-orthogonal correction (facet_process.py:377-385).
     float dFdn[NG], gF[DIM][NG];
 #pragma unroll
     for (int k = 0; k < NG; ++k) {
-        float sx = gls[0][k] * xo[0], sn = gls[0][k] * nh[0];
+        float sx = gls[0][k] * rec[Ly::XO], sn = gls[0][k] * nh[0];
 #pragma unroll
         for (int d = 1; d < DIM; ++d) {
-            sx = fmaf(gls[d][k], xo[d], sx);
+            sx = fmaf(gls[d][k], rec[Ly::XO + d], sx);
             sn = fmaf(gls[d][k], nh[d], sn);
         }
         dFdn[k] = dn[k] - sx;
@@ -400,7 +457,9 @@ __global__ void __launch_bounds__(kBlock) k_face(fvm_mesh_t m, Phys p, const flo
 #pragma unroll
         for (int c = 0; c < DIM; ++c) tau[a][c] = (a == c ? a0 : 0.f) + a1 * D[a][c];
 
-    float F[C];
+    float F[RS];
+#pragma unroll
+    for (int c = 0; c < RS; ++c) F[c] = 0.f;
     // Advection (fvm_equation.py:210-231)
 #pragma unroll
     for (int d = 0; d < DIM; ++d) F[d] = (mom[0][d] * phi[0] + mom[1][d] * phi[1]) / 2.f;
@@ -439,14 +498,14 @@ __global__ void __launch_bounds__(kBlock) k_face(fvm_mesh_t m, Phys p, const flo
     for (int d = 0; d < DIM; ++d) F[d] += 0.5f * (a_vel * (mom[0][d] - mom[1][d])) * size;
     F[DIM] += 0.5f * (a_oth * (rho[0] - rho[1])) * size;
     F[DIM + 1] += 0.5f * (a_oth * (Q[0] - Q[1])) * size;
-    store_row<C>(flux + (int64_t)f * C, F);
+    st_vec<RS>(flux + (int64_t)f * RS, F);
 }
 
 // ------------------------------------------------------------------------------------------
 // k_div_stage: divergence + stage combination.
 // ------------------------------------------------------------------------------------------
-template <int C>
-__device__ __forceinline__ void state_to_prim(const float (&U)[C], float inv_Cv, float (&P)[C]) {
+template <int C, int RS>
+__device__ __forceinline__ void state_to_prim(const float* U, float inv_Cv, float (&P)[RS]) {
     constexpr int DIM = C - 2;
     const float rho = U[DIM];
     float v2 = 0.f;
@@ -457,6 +516,19 @@ __device__ __forceinline__ void state_to_prim(const float (&U)[C], float inv_Cv,
     }
     P[DIM] = rho;
     P[DIM + 1] = inv_Cv * (U[DIM + 1] / rho - 0.5f * v2);
+#pragma unroll
+    for (int c = C; c < RS; ++c) P[c] = 0.f;
+}
+
+template <int C>
+__device__ __forceinline__ void load_state(const float* p, float (&v)[C]) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) v[c] = __ldcg(p + c);
+}
+template <int C>
+__device__ __forceinline__ void store_state(float* p, const float (&v)[C]) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) p[c] = v[c];
 }
 
 // Speed scale inv_h (|u| + c) of a conserved state, FP64 (CFL time step).
@@ -531,7 +603,8 @@ __global__ void __launch_bounds__(kBlock) k_div_stage(fvm_mesh_t m, Phys p, cons
                                                        const float* __restrict__ dt,
                                                        double* __restrict__ red,
                                                        float* __restrict__ dudt) {
-    constexpr int C = DIM + 2;
+    using Ly = L<DIM>;
+    constexpr int C = Ly::C, RS = Ly::RS;
     const int N = m.n_cells;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i < N;
@@ -539,16 +612,18 @@ __global__ void __launch_bounds__(kBlock) k_div_stage(fvm_mesh_t m, Phys p, cons
 #pragma unroll
     for (int c = 0; c < C; ++c) r[c] = 0.f;
     if (live) {
+        float rec[Ly::DR];
+        ld_vec<Ly::DR>(m.div_rec + (int64_t)i * Ly::DR, rec);
         for (int k = 0; k < m.kf; ++k) {
-            const float w = __ldg(m.f_vals + (int64_t)k * N + i);
-            float Fk[C];
-            load_row_cg<C>(flux + (int64_t)__ldg(m.f_cols + (int64_t)k * N + i) * C, Fk);
+            const float w = rec[k];
+            float Fk[RS];
+            ld_vec_cg<RS>(flux + (int64_t)as_int(rec[Ly::K + k]) * RS, Fk);
 #pragma unroll
             for (int c = 0; c < C; ++c) r[c] = fmaf(w, Fk[c], r[c]);
         }
     }
     if (dudt) {  // residual only
-        if (live) store_row<C>(dudt + (int64_t)i * C, r);
+        if (live) store_state<C>(dudt + (int64_t)i * C, r);
         return;
     }
     const int cse = (m.n_cases > 0 && live) ? __ldg(m.cell_case + i) : 0;
@@ -558,27 +633,28 @@ __global__ void __launch_bounds__(kBlock) k_div_stage(fvm_mesh_t m, Phys p, cons
     for (int c = 0; c < C; ++c) {
         kk[c] = h * r[c];
         inc[c] = 0.f;
+        U0[c] = U[c] = 0.f;
     }
     if (live) {
-        if (a.store_k) store_row<C>(kbuf + ((int64_t)a.s * N + i) * C, kk);
-        load_row_cg<C>(state + (int64_t)i * C, U0);
+        if (a.store_k) store_state<C>(kbuf + ((int64_t)a.s * N + i) * C, kk);
+        load_state<C>(state + (int64_t)i * C, U0);
         for (int t = 0; t < a.n_terms; ++t) {
             float kt[C];
             if (a.idx[t] == a.s) {
 #pragma unroll
                 for (int c = 0; c < C; ++c) kt[c] = kk[c];
             } else {
-                load_row_cg<C>(kbuf + ((int64_t)a.idx[t] * N + i) * C, kt);
+                load_state<C>(kbuf + ((int64_t)a.idx[t] * N + i) * C, kt);
             }
 #pragma unroll
             for (int c = 0; c < C; ++c) inc[c] = fmaf(a.coef[t], kt[c], inc[c]);
         }
 #pragma unroll
         for (int c = 0; c < C; ++c) U[c] = U0[c] + inc[c];
-        if (a.final_) store_row<C>(state + (int64_t)i * C, U);
-        float P[C];
-        state_to_prim<C>(U, p.inv_Cv, P);
-        store_row<C>(prims + (int64_t)i * C, P);
+        if (a.final_) store_state<C>(state + (int64_t)i * C, U);
+        float P[RS];
+        state_to_prim<C, RS>(U, p.inv_Cv, P);
+        st_vec<RS>(prims + (int64_t)i * RS, P);
     }
     if (!a.final_) return;
     __shared__ double smem[32 * 3 * C];
@@ -597,7 +673,7 @@ __global__ void __launch_bounds__(kBlock) k_div_stage(fvm_mesh_t m, Phys p, cons
 #pragma unroll
                     for (int c = 0; c < C; ++c) kt[c] = kk[c];
                 } else {
-                    load_row_cg<C>(kbuf + ((int64_t)a.idx_lo[t] * N + i) * C, kt);
+                    load_state<C>(kbuf + ((int64_t)a.idx_lo[t] * N + i) * C, kt);
                 }
 #pragma unroll
                 for (int c = 0; c < C; ++c) lo[c] = fmaf(a.coef_lo[t], kt[c], lo[c]);
@@ -667,15 +743,29 @@ __global__ void k_finalize(int C, int adaptive, float atol, float rtol, float mt
     }
 }
 
-template <int C>
+template <int DIM>
 __global__ void __launch_bounds__(kBlock) k_state_to_prims(int N, float inv_Cv, const float* __restrict__ state,
                                                             float* __restrict__ prims) {
+    using Ly = L<DIM>;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    float U[C], P[C];
-    load_row<C>(state + (int64_t)i * C, U);
-    state_to_prim<C>(U, inv_Cv, P);
-    store_row<C>(prims + (int64_t)i * C, P);
+    float U[Ly::C], P[Ly::RS];
+#pragma unroll
+    for (int c = 0; c < Ly::C; ++c) U[c] = __ldg(state + (int64_t)i * Ly::C + c);
+    state_to_prim<Ly::C, Ly::RS>(U, inv_Cv, P);
+    st_vec<Ly::RS>(prims + (int64_t)i * Ly::RS, P);
+}
+
+// [N][C] primitives -> padded [N][RS] rows (fvm_residual takes the reference's layout).
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_pad_prims(int N, const float* __restrict__ src, float* __restrict__ dst) {
+    using Ly = L<DIM>;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float P[Ly::RS];
+#pragma unroll
+    for (int c = 0; c < Ly::RS; ++c) P[c] = c < Ly::C ? __ldg(src + (int64_t)i * Ly::C + c) : 0.f;
+    st_vec<Ly::RS>(dst + (int64_t)i * Ly::RS, P);
 }
 
 template <int DIM>
@@ -688,7 +778,9 @@ __global__ void __launch_bounds__(kBlock) k_reduce_state(fvm_mesh_t m, Phys p, c
     float U[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) U[c] = 1.f;
-    if (live) load_row<C>(state + (int64_t)i * C, U);
+    if (live)
+#pragma unroll
+        for (int c = 0; c < C; ++c) U[c] = __ldg(state + (int64_t)i * C + c);
     const int cse = (m.n_cases > 0 && live) ? __ldg(m.cell_case + i) : 0;
     reduce_cons_cfl<DIM>(m, p, U, live, cse, want_cons, want_cfl, red, smem);
 }
@@ -717,16 +809,16 @@ static Phys make_phys(const fvm_physics_t* ph) {
     return p;
 }
 
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
 static bool mesh_ok(const fvm_mesh_t* m) {
     if (!m || (m->dim != 2 && m->dim != 3) || m->n_comp != m->dim + 2) return false;
     if (m->n_cells <= 0 || m->n_facets <= 0 || m->n_bc < 0 || m->n_char < 0) return false;
-    if (m->kg != m->dim + 2 || m->kf < 1 || m->kf > 8) return false;
-    if (!m->g_vals || !m->g_cols || !m->nb_slot || !m->disp || !m->eps || !m->c2f || !m->side ||
-        !m->f_vals || !m->f_cols || !m->fcell || !m->fbc || !m->normals || !m->fsize || !m->xorth ||
-        !m->inv_d || !m->inv_h || !m->volumes)
-        return false;
-    if (m->n_bc > 0 && (!m->bc_face || !m->bc_side || !m->bc_cell || !m->bc_kind || !m->bc_b ||
-                        !m->bc_l || !m->bc_ga || !m->bc_gb || !m->bc_char))
+    if (m->kg != m->dim + 2 || m->kf < 1 || m->kf > m->dim + 1) return false;
+    if (!m->cell_rec || !m->div_rec || !m->face_rec || !m->inv_h || !m->volumes) return false;
+    if (!aligned16(m->cell_rec) || !aligned16(m->div_rec) || !aligned16(m->face_rec)) return false;
+    if (m->n_bc > 0 && (!m->bc_cell || !m->bc_kind || !m->bc_b || !m->bc_l || !m->bc_ga || !m->bc_gb ||
+                        !m->bc_char))
         return false;
     if (m->n_char > 0 && (!m->ch_cell || !m->ch_normal || !m->ch_rho || !m->ch_vn || !m->ch_p || !m->ch_vt))
         return false;
@@ -738,13 +830,15 @@ static bool mesh_ok(const fvm_mesh_t* m) {
 }
 
 static bool work_ok(const fvm_mesh_t* m, const fvm_work_t* w) {
-    return w && w->face_vals && w->flux && w->red && (m->n_bc == 0 || w->bc_vals);
+    return w && w->flux && w->red && aligned16(w->flux) && (m->n_bc == 0 || (w->bc_vals && aligned16(w->bc_vals)));
 }
 
 static inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
-static inline unsigned fin_blocks(const fvm_mesh_t* m) { return m->n_cases > 0 ? (unsigned)((m->n_cases + 127) / 128) : 1u; }
+static inline unsigned fin_blocks(const fvm_mesh_t* m) {
+    return m->n_cases > 0 ? (unsigned)((m->n_cases + 127) / 128) : 1u;
+}
 
-// bc -> cell -> face for the primitives `prims`; leaves fluxes in work->flux.
+// bc -> cell -> face for the padded primitives `prims`; leaves fluxes in work->flux.
 template <int DIM>
 static int launch_fluxes(const fvm_mesh_t* m, const Phys& p, const float* prims, float* grads,
                          int32_t* has_grads, const fvm_work_t* w, cudaStream_t s) {
@@ -752,19 +846,21 @@ static int launch_fluxes(const fvm_mesh_t* m, const Phys& p, const float* prims,
         if (m->n_cases > 0 && m->n_char > 0)
             FVM_LAUNCH(KID_BC, s, k_char_scale<DIM><<<m->n_cases, kBlock, 0, s>>>(*m, p, prims, w->red));
         FVM_LAUNCH(KID_BC, s, k_bc<DIM><<<blocks_for(m->n_bc), kBlock, 0, s>>>(*m, p, prims, grads, has_grads,
-                                                                               w->bc_vals, w->face_vals, w->red));
+                                                                               w->bc_vals, w->red));
     }
-    FVM_LAUNCH(KID_CELL, s, k_cell<DIM, DIM + 2><<<blocks_for(m->n_cells), kBlock, 0, s>>>(
-                                *m, p, prims, w->bc_vals, w->face_vals, grads, has_grads));
-    FVM_LAUNCH(KID_FACE, s, k_face<DIM><<<blocks_for(m->n_facets), kBlock, 0, s>>>(*m, p, prims, w->face_vals,
+    FVM_LAUNCH(KID_CELL, s, k_cell<DIM><<<blocks_for(m->n_cells), kBlock, 0, s>>>(*m, p, prims, w->bc_vals,
+                                                                                   grads, has_grads));
+    FVM_LAUNCH(KID_FACE, s, k_face<DIM><<<blocks_for(m->n_facets), kBlock, 0, s>>>(*m, p, prims, w->bc_vals,
                                                                                    grads, w->flux));
     return launch_status();
 }
 
 template <int DIM>
-static int residual_impl(const fvm_mesh_t* m, const Phys& p, const float* prims, float* grads,
+static int residual_impl(const fvm_mesh_t* m, const Phys& p, const float* prims_user, float* grads,
                          int32_t* has_grads, float* dudt, const fvm_work_t* w, cudaStream_t s) {
-    int rc = launch_fluxes<DIM>(m, p, prims, grads, has_grads, w, s);
+    FVM_LAUNCH(KID_STATE_TO_PRIMS, s, k_pad_prims<DIM><<<blocks_for(m->n_cells), kBlock, 0, s>>>(
+                                          m->n_cells, prims_user, w->prims));
+    int rc = launch_fluxes<DIM>(m, p, w->prims, grads, has_grads, w, s);
     if (rc) return rc;
     StageArgs a{};
     FVM_LAUNCH(KID_DIV_STAGE, s, k_div_stage<DIM><<<blocks_for(m->n_cells), kBlock, 0, s>>>(
@@ -819,9 +915,10 @@ static int stage_impl(const fvm_mesh_t* m, const Phys& p, const fvm_tableau_t* t
     if (rc) return rc;
     if (a.final_ && (a.adaptive || a.cfl || a.cons)) {
         FVM_LAUNCH(KID_FINALIZE, st,
-                   k_finalize<<<fin_blocks(m), 128, 0, st>>>(m->n_comp, tab->adaptive, tab->atol, tab->rtol, tab->mtol,
-                                                tab->alpha_hi_err, tab->alpha_lo_err, tab->order, tab->cfl,
-                                                a.cons, w->red, b->dt, b->cons, m->n_cases));
+                   k_finalize<<<fin_blocks(m), 128, 0, st>>>(m->n_comp, tab->adaptive, tab->atol, tab->rtol,
+                                                             tab->mtol, tab->alpha_hi_err, tab->alpha_lo_err,
+                                                             tab->order, tab->cfl, a.cons, w->red, b->dt, b->cons,
+                                                             m->n_cases));
         rc = launch_status();
     }
     return rc;
@@ -848,8 +945,9 @@ static int multistep_impl(const fvm_mesh_t* m, const Phys& p, int store, int n_t
     rc = launch_status();
     if (rc) return rc;
     if (a.cons) {
-        FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(m), 128, 0, st>>>(m->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f,
-                                                                   0.f, 1, w->red, b->dt, b->cons, m->n_cases));
+        FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(m), 128, 0, st>>>(m->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f,
+                                                                              1.f, 0.f, 1, w->red, b->dt, b->cons,
+                                                                              m->n_cases));
         rc = launch_status();
     }
     return rc;
@@ -868,7 +966,9 @@ extern "C" int fvm_residual(const fvm_mesh_t* mesh, const fvm_physics_t* phys, c
                             float* grads, int32_t* has_grads, float* dudt, const fvm_work_t* work,
                             void* stream) {
     if (const int rc = check_common(mesh)) return rc;
-    if (!phys || !prims || !grads || !has_grads || !dudt || !work_ok(mesh, work)) return FVM_E_ARG;
+    if (!phys || !prims || !grads || !has_grads || !dudt || !work_ok(mesh, work) || !work->prims ||
+        !aligned16(work->prims) || !aligned16(grads))
+        return FVM_E_ARG;
     const Phys p = make_phys(phys);
     cudaStream_t s = (cudaStream_t)stream;
     return mesh->dim == 2 ? residual_impl<2>(mesh, p, prims, grads, has_grads, dudt, work, s)
@@ -881,8 +981,8 @@ extern "C" int fvm_residual(const fvm_mesh_t* mesh, const fvm_physics_t* phys, c
 // Some callers cannot allocate device memory where they call the residual: an application whose
 // own pool allocator has already reserved the GPU's memory, or a time-critical loop that forbids
 // allocation once it runs (cudaMalloc / cudaFree can also wait for the whole device to go idle,
-// stalling unrelated streams).  This variant takes its scratch -- boundary values, the facet-value
-// table and the fluxes (plus per-case slots of batched meshes) -- from one file-scope device array
+// stalling unrelated streams).  This variant takes its scratch -- boundary values, padded
+// primitives and fluxes (plus per-case slots of batched meshes) -- from one file-scope device array
 // of FVM_NOALLOC_SCRATCH_BYTES, which every GPU that loads this library keeps until the process
 // exits.  The residual overwrites every scratch element it reads before reading it, so nothing has
 // to be cleared between calls.  All calls on a device share the array: calls that overlap on the
@@ -910,11 +1010,11 @@ static float* noalloc_scratch_address() {
 static inline int64_t align64(int64_t n) { return (n + 63) / 64 * 64; }   // 256-byte units of floats
 
 static bool bufs_ok(const fvm_solver_bufs_t* b) {
-    return b && b->state && b->prims && b->grads && b->k && b->dt && b->has_grads;
+    return b && b->state && b->prims && b->grads && b->k && b->dt && b->has_grads && aligned16(b->prims) &&
+           aligned16(b->grads);
 }
 
 static bool tab_ok(const fvm_tableau_t* t) { return t && t->stages >= 1 && t->stages <= FVM_MAX_STAGES; }
-
 
 extern "C" int fvm_stage(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const fvm_tableau_t* tab,
                          int32_t s, const fvm_solver_bufs_t* bufs, const fvm_work_t* work, void* stream) {
@@ -958,14 +1058,14 @@ extern "C" int fvm_multistep(const fvm_mesh_t* mesh, const fvm_physics_t* phys, 
 
 extern "C" int fvm_state_to_prims(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const float* state,
                                   float* prims, void* stream) {
-    if (!mesh_ok(mesh) || !phys || !state || !prims) return FVM_E_ARG;
+    if (!mesh_ok(mesh) || !phys || !state || !prims || !aligned16(prims)) return FVM_E_ARG;
     const Phys p = make_phys(phys);
     cudaStream_t st = (cudaStream_t)stream;
     if (mesh->dim == 2)
-        FVM_LAUNCH(KID_STATE_TO_PRIMS, st, k_state_to_prims<4><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
+        FVM_LAUNCH(KID_STATE_TO_PRIMS, st, k_state_to_prims<2><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
                                                mesh->n_cells, p.inv_Cv, state, prims));
     else
-        FVM_LAUNCH(KID_STATE_TO_PRIMS, st, k_state_to_prims<5><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
+        FVM_LAUNCH(KID_STATE_TO_PRIMS, st, k_state_to_prims<3><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
                                                mesh->n_cells, p.inv_Cv, state, prims));
     return launch_status();
 }
@@ -983,8 +1083,9 @@ extern "C" int fvm_cfl_dt(const fvm_mesh_t* mesh, const fvm_physics_t* phys, con
                                              *mesh, p, state, 1, 0, work->red));
     int rc = launch_status();
     if (rc) return rc;
-    FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(mesh), 128, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, cfl,
-                                                               0, work->red, dt, nullptr, mesh->n_cases));
+    FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(mesh), 128, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f,
+                                                                             0.f, 1.f, cfl, 0, work->red, dt,
+                                                                             nullptr, mesh->n_cases));
     return launch_status();
 }
 
@@ -1001,21 +1102,22 @@ extern "C" int fvm_conservation(const fvm_mesh_t* mesh, const float* state, doub
                                              *mesh, p, state, 0, 1, work->red));
     int rc = launch_status();
     if (rc) return rc;
-    FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(mesh), 128, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f,
-                                                               1, work->red, nullptr, out, mesh->n_cases));
+    FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(mesh), 128, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f,
+                                                                             0.f, 1.f, 0.f, 1, work->red, nullptr,
+                                                                             out, mesh->n_cases));
     return launch_status();
 }
 
 extern "C" int fvm_residual_noalloc(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const float* prims,
                                     float* grads, int32_t* has_grads, float* dudt, void* stream) {
     if (const int rc = check_common(mesh)) return rc;
-    if (!phys || !prims || !grads || !has_grads || !dudt) return FVM_E_ARG;
-    const int64_t C = mesh->n_comp;
-    const int64_t n_bc = align64((int64_t)mesh->n_bc * C);
-    const int64_t n_face = align64((int64_t)mesh->n_facets * 2 * C);
-    const int64_t n_flux = align64((int64_t)mesh->n_facets * C);
+    if (!phys || !prims || !grads || !has_grads || !dudt || !aligned16(grads)) return FVM_E_ARG;
+    const int64_t R = FVM_ROW(mesh->dim);
+    const int64_t n_bc = align64((int64_t)mesh->n_bc * R);
+    const int64_t n_prims = align64((int64_t)mesh->n_cells * R);
+    const int64_t n_flux = align64((int64_t)mesh->n_facets * R);
     const int64_t n_red = align64(2 * ((int64_t)FVM_RED_DOUBLES + 8 * (int64_t)mesh->n_cases));
-    if (n_bc + n_face + n_flux + n_red > kNoAllocFloats) return FVM_E_CAPACITY;
+    if (n_bc + n_prims + n_flux + n_red > kNoAllocFloats) return FVM_E_CAPACITY;
     float* base = noalloc_scratch_address();
     if (!base) {
         launch_status();
@@ -1023,9 +1125,9 @@ extern "C" int fvm_residual_noalloc(const fvm_mesh_t* mesh, const fvm_physics_t*
     }
     fvm_work_t w;
     w.bc_vals = base;
-    w.face_vals = base + n_bc;
-    w.flux = base + n_bc + n_face;
-    w.red = reinterpret_cast<double*>(base + n_bc + n_face + n_flux);
+    w.prims = base + n_bc;
+    w.flux = base + n_bc + n_prims;
+    w.red = reinterpret_cast<double*>(base + n_bc + n_prims + n_flux);
     const Phys p = make_phys(phys);
     cudaStream_t s = (cudaStream_t)stream;
     return mesh->dim == 2 ? residual_impl<2>(mesh, p, prims, grads, has_grads, dudt, &w, s)

@@ -18,7 +18,9 @@ import torch
 from . import _lib
 from .config import ConfigFVM
 from .fvm_mesh import FVMMesh, FVMMesh2D, FVMMesh3D
-from .tables import FVMTables, KernelTables
+from types import SimpleNamespace
+
+from .tables import FVMTables, KernelTables, grad_index, row_sizes
 
 
 class FluidConstitution:
@@ -80,40 +82,52 @@ class FluidConstitution3D(FluidConstitution):
 
 
 class DeviceMesh:
-    """Kernel tables uploaded to one device, plus the ``fvm_mesh_t`` struct pointing at them."""
+    """Kernel tables uploaded to one device (record layout), plus the ``fvm_mesh_t`` struct."""
 
-    _ptr_fields = [f for f in _lib.MESH_PTR_FIELDS if f not in
-                   ("cell_case", "face_case", "bc_case", "ch_off", "case_mu", "case_mu_b", "case_kappa")]
+    _struct_fields = [f for f in _lib.MESH_PTR_FIELDS if f not in
+                      ("cell_rec", "div_rec", "face_rec", "cell_case", "face_case", "bc_case", "ch_off",
+                       "case_mu", "case_mu_b", "case_kappa")]
 
     def __init__(self, kt: KernelTables, device):
         self.device = torch.device(device)
-        self.t = kt.to(self.device)
         self.dim, self.n_comp, self.n_cells = kt.dim, kt.n_comp, kt.n_cells
-        self.n_facets, self.n_bc = kt.n_facets, kt.n_bc
+        self.n_facets, self.n_bc, self.kg, self.kf = kt.n_facets, kt.n_bc, kt.kg, kt.kf
+        self.row, self.grow = row_sizes(kt.dim)
+        up = {k: v.contiguous().to(self.device) for k, v in kt.records().items()}
+        for f in self._struct_fields:
+            up[f] = getattr(kt, f).contiguous().to(self.device)
+        self.t = SimpleNamespace(**up)
         m = _lib.Mesh(dim=kt.dim, n_comp=kt.n_comp, n_cells=kt.n_cells, n_facets=kt.n_facets,
                       n_bc=kt.n_bc, n_char=kt.n_char, kg=kt.kg, kf=kt.kf)
-        for f in self._ptr_fields:
-            setattr(m, f, _lib.ptr(getattr(self.t, f)))
+        for f, v in up.items():
+            setattr(m, f, _lib.ptr(v))
         self.struct = m
 
     def work(self) -> "Work":
         return Work(self)
 
     def bytes(self) -> int:
-        return sum(v.numel() * v.element_size() for v in self.t.__dict__.values() if isinstance(v, torch.Tensor))
+        return sum(v.numel() * v.element_size() for v in vars(self.t).values())
 
 
 class Work:
     """Caller-owned scratch of one mesh (``fvm_work_t``)."""
 
     def __init__(self, dm: DeviceMesh):
-        C, dev = dm.n_comp, dm.device
-        self.bc_vals = torch.zeros((max(dm.n_bc, 1), C), device=dev)
-        self.face_vals = torch.zeros((dm.n_facets, 2, C), device=dev)
-        self.flux = torch.zeros((dm.n_facets, C), device=dev)
+        R, dev = dm.row, dm.device
+        self.bc_vals = torch.zeros((max(dm.n_bc, 1), R), device=dev)
+        self.prims = torch.zeros((dm.n_cells, R), device=dev)
+        self.flux = torch.zeros((dm.n_facets, R), device=dev)
         self.red = torch.zeros(_lib.FVM_RED_DOUBLES, device=dev, dtype=torch.float64)
-        self.struct = _lib.Work(bc_vals=_lib.ptr(self.bc_vals), face_vals=_lib.ptr(self.face_vals),
+        self.struct = _lib.Work(bc_vals=_lib.ptr(self.bc_vals), prims=_lib.ptr(self.prims),
                                 flux=_lib.ptr(self.flux), red=_lib.ptr(self.red))
+
+
+def grads_to_reference(g: torch.Tensor, dim: int) -> torch.Tensor:
+    """Limited-gradient rows [N][FVM_GROW] -> the reference's cell_grads layout [N, dim, C]."""
+    C = dim + 2
+    idx = torch.tensor([[grad_index(dim, d, c) for c in range(C)] for d in range(dim)], device=g.device)
+    return g[:, idx]
 
 
 def _host_mesh(mesh, dim_hint=None) -> FVMMesh:
@@ -192,7 +206,7 @@ class FVMEquation:
         self.work = self.dev.work()
         self.phys = phy_setup.physics_struct(cfg)
         N, dim = self.mesh.n_cells, self.mesh.dim
-        self.grads = torch.zeros((N, dim, n_comp), device=self.device)
+        self.grads = torch.zeros((N, self.dev.grow), device=self.device)
         self.has_grads = torch.zeros(1, dtype=torch.int32, device=self.device)
         self._has_grads_host = False
         self.cells = FVMCells(N, n_comp, init_val=us_init, phys_setup=phy_setup, device=self.device)
@@ -215,7 +229,7 @@ class FVMEquation:
         self.dev = DeviceMesh(kt, self.device)
         self.work = self.dev.work()
         self.phys = phy_setup.physics_struct(cfg)
-        self.grads = torch.zeros((kt.n_cells, kt.dim, kt.n_comp), device=self.device)
+        self.grads = torch.zeros((kt.n_cells, self.dev.grow), device=self.device)
         self.has_grads = torch.zeros(1, dtype=torch.int32, device=self.device)
         self._has_grads_host = False
         self.cells = FVMCells(kt.n_cells, kt.n_comp, init_val=us_init, phys_setup=phy_setup, device=self.device)
@@ -228,7 +242,7 @@ class FVMEquation:
     @property
     def cell_grads(self):
         """Limited cell gradients of the last evaluation [N, dim, C], or None before the first."""
-        return self.grads if self._has_grads_host else None
+        return grads_to_reference(self.grads, self.mesh.dim) if self._has_grads_host else None
 
     def reset_gradients(self):
         """Forget the carried gradients (the next evaluation behaves like the reference's first)."""

@@ -1,33 +1,36 @@
 """Algorithmic (compulsory) bytes per kernel launch, for roofline accounting.
 
-Every array a kernel must touch is counted once (4 bytes per float / int32, 8 per double);
-gathers of an array already counted are not counted again.  N cells, F facets, Fb boundary
-facets, d = dim, C = d + 2 components, K = d + 1 facets per cell, KG = d + 2 gradient slots.
+Every array a kernel must touch is counted once at its stored width (4 bytes per float / int32,
+8 per double); gathers of an array already counted are not counted again.  N cells, F facets,
+Fb boundary facets, d = dim, C = d + 2 components, K = d + 1 facets per cell; R = FVM_ROW (4 in
+2D, 8 in 3D) floats per padded primitive / flux row, G = FVM_GROW (8 / 16) per limited-gradient
+row, CR / FR / DR = cell / facet / divergence record widths (20 / 12 / 8 in 2D, 36 / 16 / 8 in 3D).
 
-k_cell      reads  prims N C, G weights d KG N, G columns KG N, nb_slot N, disp K d N, eps N,
-                   c2f K N, side N, boundary values Fb C
-            writes facet values K N C, limited gradients N d C
-k_face      reads  fcell 2F, fbc F, normals d F, fsize F, xorth d F, inv_d F, facet values 2F C,
-                   limited gradients N d C, prims N C, boundary gradient rows 2 Fb C
-            writes fluxes F C
-k_div_stage reads  divergence weights + columns 2 K N, fluxes F C, state N C,
-                   stored increments (one N C each)
-            writes prims N C, stored increment N C (if kept), state N C (last stage)
-k_bc        reads  cell prims Fb C, tables (kind, b, ga, gb) 4 Fb C, l d Fb, characteristic data
-            writes boundary values 2 Fb C
+k_cell      reads  cell records CR N, primitives R N, boundary values R Fb
+            writes limited gradients G N
+k_face      reads  facet records FR F, primitives R N, limited gradients G N, boundary values R Fb,
+                   boundary gradient rows 2 C Fb
+            writes fluxes R F
+k_div_stage reads  divergence records DR N, fluxes R F, state C N, stored increments C N each
+            writes primitives R N, stored increment C N (if kept), state C N (last stage)
+k_bc        reads  cell primitives R Fb, tables (kind, b, ga, gb) 4 C Fb, lever arm d Fb,
+                   characteristic data (2 + 2d) Fb, gradients of Neumann cells G Fb
+            writes boundary values R Fb
 """
 from __future__ import annotations
 
+from .tables import record_sizes, row_sizes
+
 
 def kernel_bytes(dim: int, N: int, F: int, Fb: int, kf: int | None = None) -> dict:
-    C, K, KG = dim + 2, dim + 1, dim + 2
-    kf = kf or K
+    C = dim + 2
+    R, G = row_sizes(dim)
+    CR, FR, DR = record_sizes(dim)
     w = 4
-    cell = w * (N * C + dim * KG * N + KG * N + N + K * dim * N + N + K * N + N + Fb * C
-                + K * N * C + N * dim * C)
-    face = w * (2 * F + F + dim * F + F + dim * F + F + 2 * F * C + N * dim * C + N * C + 2 * Fb * C + F * C)
-    div_base = w * (2 * kf * N + F * C + N * C + N * C)
-    bc = w * (Fb * C + 4 * Fb * C + dim * Fb + 2 * Fb * C + 4 * Fb)
+    cell = w * (CR * N + R * N + R * Fb + G * N)
+    face = w * (FR * F + R * N + G * N + R * Fb + 2 * C * Fb + R * F)
+    div_base = w * (DR * N + R * F + C * N + R * N)
+    bc = w * (R * Fb + 4 * C * Fb + dim * Fb + (2 + 2 * dim) * Fb + G * Fb + R * Fb)
     return dict(cell=cell, face=face, div_base=div_base, bc=bc, row=w * N * C)
 
 
@@ -38,10 +41,7 @@ def div_stage_bytes(dim, N, F, Fb, stage_terms: list, kf=None) -> list:
     this stage's increment is stored, whether it writes the state.
     """
     kb = kernel_bytes(dim, N, F, Fb, kf)
-    out = []
-    for n_reads, store, final in stage_terms:
-        out.append(kb["div_base"] + kb["row"] * (n_reads + int(store) + int(final)))
-    return out
+    return [kb["div_base"] + kb["row"] * (n_reads + int(store) + int(final)) for n_reads, store, final in stage_terms]
 
 
 def tableau_terms(tab) -> list:

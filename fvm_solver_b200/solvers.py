@@ -115,7 +115,7 @@ class TSolver:
         self.end_t = cfg.end_t
         self.print_i = cfg.print_i
         N, C = eq.mesh.n_cells, eq.n_comp
-        self.prims = torch.zeros((N, C), device=dev)
+        self.prims = torch.zeros((N, eq.dev.row), device=dev)
         self.k = torch.zeros((max(self.n_k, 1), N, C), device=dev)
         self.n_cases = max(1, int(getattr(eq, "n_cases", 0) or 0))
         self.dt = torch.full((self.n_cases,), cfg.dt if cfg.dt is not None else 0.0, dtype=torch.float32,

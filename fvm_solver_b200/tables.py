@@ -211,6 +211,68 @@ class KernelTables:
             out[k] = v.contiguous().to(device) if isinstance(v, torch.Tensor) else v
         return KernelTables(**out)
 
+    def records(self) -> dict:
+        """The device record layout of ``include/fvm_b200.h`` (cell, divergence and facet records).
+
+        Cell record [N][CR]: G weights [dim][KG], G columns [KG] (int32 bits), centroid->facet
+        displacements [K][dim], limiter epsilon, meta (int32 bits), zero padding.
+        Divergence record [N][8]: weights [kf], facet indices [kf] (int32 bits), padding.
+        Facet record [F][FR]: side-0 cell, side-1 cell (int32 bits; a boundary side holds
+        -1 - boundary index), 1/d, |S|, normal [dim], non-orthogonal vector [dim], side-0 and
+        side-1 centroid->facet displacements [dim] each, padding.
+        """
+        dim, N, F, K, kg, kf = self.dim, self.n_cells, self.n_facets, self.dim + 1, self.kg, self.kf
+        CR, FR, DR = record_sizes(dim)
+        bits = lambda t: t.to(torch.int32).view(torch.float32)
+        cell = torch.zeros((N, CR), dtype=torch.float32)
+        o = 0
+        cell[:, o:o + dim * kg] = self.g_vals.permute(2, 0, 1).reshape(N, dim * kg)
+        o += dim * kg
+        cell[:, o:o + kg] = bits(self.g_cols.t().contiguous())
+        o += kg
+        cell[:, o:o + K * dim] = self.disp.permute(2, 0, 1).reshape(N, K * dim)
+        o += K * dim
+        cell[:, o] = self.eps
+        cell[:, o + 1] = bits(self.nb_slot)
+        div = torch.zeros((N, DR), dtype=torch.float32)
+        div[:, :kf] = self.f_vals.t()
+        div[:, K:K + kf] = bits(self.f_cols.t().contiguous())
+        # per facet side: centroid -> facet displacement of the cell on that side
+        fdisp = torch.zeros((F, 2, dim), dtype=torch.float32)
+        for j in range(K):
+            fdisp[self.c2f[j].long(), ((self.side >> j) & 1).long()] = self.disp[j].t()
+        codes = self.fcell.clone()
+        if self.n_bc:
+            b = torch.arange(self.n_bc, dtype=torch.int32)
+            codes[self.bc_face.long(), self.bc_side.long()] = -1 - b
+        face = torch.zeros((F, FR), dtype=torch.float32)
+        face[:, 0] = bits(codes[:, 0].contiguous())
+        face[:, 1] = bits(codes[:, 1].contiguous())
+        face[:, 2] = self.inv_d
+        face[:, 3] = self.fsize
+        face[:, 4:4 + dim] = self.normals
+        face[:, 4 + dim:4 + 2 * dim] = self.xorth
+        face[:, 4 + 2 * dim:4 + 3 * dim] = fdisp[:, 0]
+        face[:, 4 + 3 * dim:4 + 4 * dim] = fdisp[:, 1]
+        return dict(cell_rec=cell, div_rec=div, face_rec=face)
+
+
+def record_sizes(dim: int):
+    """(cell record, facet record, divergence record) widths in floats (FVM_CELL_REC etc.)."""
+    return (20, 12, 8) if dim == 2 else (36, 16, 8)
+
+
+def row_sizes(dim: int):
+    """(padded state row, limited-gradient row) widths in floats (FVM_ROW, FVM_GROW)."""
+    return (4, 8) if dim == 2 else (8, 16)
+
+
+def grad_index(dim: int, d: int, comp: int) -> int:
+    """Position of d(comp)/dx_d in a limited-gradient row (V_k and T per direction, rho last)."""
+    if comp == dim:
+        return dim * (dim + 1) + d
+    return d * (dim + 1) + (comp if comp < dim else dim)
+
 
 # ---------------------------------------------------------------------------------------------
 # Assembly

@@ -41,52 +41,59 @@ extern "C" {
 #define FVM_RED_DOUBLES 64
 #define FVM_NOALLOC_SCRATCH_BYTES (16 * 1024 * 1024)
 
-/* Mesh tables (see fvm_solver_b200/tables.py KernelTables for how they are built).
- * N cells, F facets, Fb boundary facets, Fc characteristic facets, K = dim + 1. */
+/* Row layouts.  Gathered per-cell / per-facet rows are padded to 16-byte multiples so every row
+ * is read and written with 16-byte vector accesses:
+ *   primitives, fluxes, boundary values: FVM_ROW(dim) floats per row (4 in 2D, 8 in 3D), the first
+ *     C = dim + 2 used (V..., rho, T for primitives; the conserved order for fluxes);
+ *   limited gradients: FVM_GROW(dim) floats per cell (8 / 16); entry (d, V_k) at d*(dim+1) + k,
+ *     (d, T) at d*(dim+1) + dim, (d, rho) at dim*(dim+1) + d;
+ *   state and stage increments keep the plain [N][C] layout. */
+#define FVM_ROW(dim) ((dim) == 2 ? 4 : 8)
+#define FVM_GROW(dim) ((dim) == 2 ? 8 : 16)
+#define FVM_CELL_REC(dim) ((dim) == 2 ? 20 : 36)
+#define FVM_FACE_REC(dim) ((dim) == 2 ? 12 : 16)
+#define FVM_DIV_REC 8
+
+/* Mesh tables (built by fvm_solver_b200/tables.py).  N cells, F facets, Fb boundary facets,
+ * Fc characteristic facets, K = dim + 1 facets per cell, KG = kg gradient slots (= dim + 2).
+ * Integer fields inside float records are stored bit-cast (int32 bits in a float slot). */
 typedef struct fvm_mesh {
     int32_t dim, n_comp, n_cells, n_facets, n_bc, n_char, kg, kf;
-    /* cells (slot-major: [slot][cell]) */
-    const float *g_vals;      /* [dim][kg][N]  LSQ gradient weights                       */
-    const int32_t *g_cols;    /* [kg][N]       columns into [prims ; boundary values]      */
-    const int32_t *nb_slot;   /* [N]           4 bits per local facet: slot of neighbour   */
-    const float *disp;        /* [K][dim][N]   centroid -> facet midpoint                  */
-    const float *eps;         /* [N]           limiter epsilon                             */
-    const int32_t *c2f;       /* [K][N]        cell -> facet                               */
-    const int32_t *side;      /* [N]           bit j: side of local facet j (0 left)       */
-    const float *f_vals;      /* [kf][N]       divergence weights +-1/vol                  */
-    const int32_t *f_cols;    /* [kf][N]       facet indices                               */
-    const double *inv_h;      /* [N]           max facet area / volume                     */
-    const double *volumes;    /* [N]                                                       */
-    /* facets */
-    const int32_t *fcell;     /* [F][2]        side-0 / side-1 cell (boundary: cell twice)  */
-    const int32_t *fbc;       /* [F]           boundary-local index or -1                  */
-    const float *normals;     /* [F][dim]      area-weighted normals                       */
-    const float *fsize;       /* [F]           |normal|                                    */
-    const float *xorth;       /* [F][dim]      non-orthogonal correction vector            */
-    const float *inv_d;       /* [F]           1 / projected centroid distance             */
+    /* [N][FVM_CELL_REC]: LSQ gradient weights [dim][KG], their columns [KG] (into
+     * [cells ; boundary facets]), centroid->facet displacements [K][dim], limiter epsilon, meta
+     * (bits 24..28: number of valid gradient slots), padding */
+    const float *cell_rec;
+    /* [N][FVM_DIV_REC]: divergence weights +-1/vol [K], facet indices [K] */
+    const float *div_rec;
+    const double *inv_h;      /* [N] max facet area / volume (CFL)                          */
+    const double *volumes;    /* [N]                                                        */
+    /* [F][FVM_FACE_REC]: side-0 cell, side-1 cell (a boundary side holds -1 - boundary index),
+     * 1/d, |S|, area normal [dim], non-orthogonal correction vector [dim], centroid->facet
+     * displacement of side 0 [dim] and of side 1 [dim] */
+    const float *face_rec;
     /* boundary facets */
-    const int32_t *bc_face, *bc_side, *bc_cell;   /* [Fb]                                  */
+    const int32_t *bc_cell;   /* [Fb] adjacent cell                                         */
     const int32_t *bc_kind;   /* [Fb][C] 1 Dirichlet, 2 Neumann, 0 other                    */
-    const float *bc_b;        /* [Fb][C] face-value offset                                 */
+    const float *bc_b;        /* [Fb][C] face-value offset                                  */
     const float *bc_l;        /* [Fb][dim] tangential lever arm (non-orthogonal correction) */
-    const float *bc_ga;       /* [Fb][C] face-gradient coefficient                         */
-    const float *bc_gb;       /* [Fb][C] face-gradient offset                              */
-    const int32_t *bc_char;   /* [Fb] index into the characteristic arrays or -1            */
-    const int32_t *ch_cell;   /* [Fc] cell adjacent to each characteristic facet            */
-    const float *ch_normal;   /* [Fc][dim] outward unit normals                            */
-    const float *ch_rho, *ch_vn, *ch_p;            /* [Fc]                                 */
-    const float *ch_vt;       /* [Fc][dim]                                                 */
+    const float *bc_ga;       /* [Fb][C] face-gradient coefficient                          */
+    const float *bc_gb;       /* [Fb][C] face-gradient offset                               */
+    const int32_t *bc_char;   /* [Fb] index into the characteristic arrays or -1             */
+    const int32_t *ch_cell;   /* [Fc] cell adjacent to each characteristic facet             */
+    const float *ch_normal;   /* [Fc][dim] outward unit normals                             */
+    const float *ch_rho, *ch_vn, *ch_p;            /* [Fc]                                  */
+    const float *ch_vt;       /* [Fc][dim]                                                  */
     /* Batched meshes: n_cases > 0 means the tables are several independent meshes
      * concatenated (cells, facets, boundary and characteristic facets each contiguous per
      * case, all indices global).  Each case has its own time step (dt[case]), gas transport
      * coefficients, characteristic-BC sound-speed mean, CFL and conservation reductions.
      * n_cases = 0 and NULL pointers: a single mesh. */
     int32_t n_cases;
-    const int32_t *cell_case; /* [N]  case of each cell                                    */
-    const int32_t *face_case; /* [F]  case of each facet                                   */
-    const int32_t *bc_case;   /* [Fb] case of each boundary facet                          */
-    const int32_t *ch_off;    /* [n_cases + 1] characteristic-facet offsets per case        */
-    const float *case_mu, *case_mu_b, *case_kappa;   /* [n_cases] transport coefficients   */
+    const int32_t *cell_case; /* [N]  case of each cell                                     */
+    const int32_t *face_case; /* [F]  case of each facet                                    */
+    const int32_t *bc_case;   /* [Fb] case of each boundary facet                           */
+    const int32_t *ch_off;    /* [n_cases + 1] characteristic-facet offsets per case         */
+    const float *case_mu, *case_mu_b, *case_kappa;   /* [n_cases] transport coefficients    */
 } fvm_mesh_t;
 
 /* Gas and scheme constants (ConfigFVM fields, time_fvm/config_fvm.py:52-63). */
@@ -97,9 +104,9 @@ typedef struct fvm_physics {
 
 /* Caller-owned scratch for one mesh. */
 typedef struct fvm_work {
-    float *bc_vals;     /* [Fb][C]                                   */
-    float *face_vals;   /* [F][2][C]                                 */
-    float *flux;        /* [F][C]                                    */
+    float *bc_vals;     /* [Fb][FVM_ROW] boundary facet values                          */
+    float *prims;       /* [N][FVM_ROW] padded primitives (used by fvm_residual only)   */
+    float *flux;        /* [F][FVM_ROW] facet fluxes                                    */
     double *red;        /* [FVM_RED_DOUBLES + 8 * n_cases], zero-initialised once */
 } fvm_work_t;
 
@@ -117,8 +124,8 @@ typedef struct fvm_tableau {
 /* Time-stepping buffers (caller-owned). */
 typedef struct fvm_solver_bufs {
     float *state;       /* [N][C] conserved state, updated in place                      */
-    float *prims;       /* [N][C] primitives of the current stage input                   */
-    float *grads;       /* [N][dim][C] limited gradients, carried across evaluations      */
+    float *prims;       /* [N][FVM_ROW] primitives of the current stage input             */
+    float *grads;       /* [N][FVM_GROW] limited gradients, carried across evaluations    */
     float *k;           /* [stages][N][C] stage increments dt * f                          */
     float *dt;          /* [max(1, n_cases)] time step per case (device)                  */
     int32_t *has_grads; /* [1] device flag: grads hold a previous evaluation              */
@@ -153,7 +160,7 @@ int fvm_ell_spmm(const float *vals, const int32_t *cols, int64_t M, int32_t K,
                  const float *X, int64_t ldx, int32_t B, const float *bias, float *Y, int64_t ldy,
                  void *stream);
 
-/* dU/dt [N][C] (conserved variables) of the primitives prims [N][C].  grads [N][dim][C] is
+/* dU/dt [N][C] (conserved variables) of the primitives prims [N][C].  grads [N][FVM_GROW] is
  * read as the previous limited gradient when the device flag *has_grads != 0 (the reference's
  * FacetCalc.cell_grads is not None) and overwritten with this evaluation's limited gradient;
  * the call sets *has_grads = 1.  Returns FVM_E_UNSUPPORTED if mesh->kg != dim + 2. */
@@ -166,11 +173,12 @@ int fvm_residual(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float 
  * allocator has already reserved the GPU's memory, or a time-critical loop that forbids
  * allocation once it runs (cudaMalloc / cudaFree can also wait for the device to go idle).
  * Same arguments and results as fvm_residual, minus `work`: the scratch (boundary values,
- * facet-value table, fluxes) lives in one static device array of FVM_NOALLOC_SCRATCH_BYTES
+ * padded primitives, fluxes) lives in one static device array of FVM_NOALLOC_SCRATCH_BYTES
  * (16 MiB) that every GPU loading the library keeps until the process exits.  A mesh whose
- * scratch does not fit -- 4 * (align64(Fb*C) + align64(2*F*C) + align64(F*C)
- * + align64(2*(64 + 8*n_cases))) bytes, i.e. up to about 280 000 facets in 3D or 350 000 in 2D --
- * is rejected with FVM_E_CAPACITY before anything is launched.  The function never allocates;
+ * scratch does not fit -- 4 * (align64(Fb*R) + align64(N*R) + align64(F*R)
+ * + align64(2*(64 + 8*n_cases))) bytes with R = FVM_ROW(dim), i.e. up to about 340 000 facets
+ * (170 000 tetrahedra) in 3D or 600 000 facets (400 000 triangles) in 2D -- is rejected with
+ * FVM_E_CAPACITY before anything is launched.  The function never allocates;
  * the first call on each device looks up the array's device address (with that device
  * current), so make that first call before any stream capture.  Every call overwrites the
  * scratch it reads, so no clearing is needed; all calls on a device share the array, so calls
@@ -196,7 +204,7 @@ int fvm_multistep(const fvm_mesh_t *mesh, const fvm_physics_t *phys, int32_t sto
                   int32_t n_terms, const int32_t *idx, const float *coef,
                   const fvm_solver_bufs_t *bufs, const fvm_work_t *work, void *stream);
 
-/* prims [N][C] <- primitives of state [N][C]. */
+/* prims [N][FVM_ROW] <- primitives of state [N][C]. */
 int fvm_state_to_prims(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *state,
                        float *prims, void *stream);
 

@@ -63,7 +63,7 @@ def test_batched_graph_and_conservation(cases):
     torch.cuda.synchronize()
     cons = batch.t_solver.cons.cpu().numpy()
     st = batch.cells.state.cpu().double().numpy()
-    vol = batch.dev.t.volumes.cpu().numpy()
+    vol = batch.dev.t.volumes.cpu().numpy()   # uploaded FP64 volumes
     for k in range(len(cases)):
         sl = batch.case_slice(k)
         want = (vol[sl, None] * st[sl]).sum(0)

@@ -208,5 +208,5 @@ def test_free_stream_preservation_periodic():
     m, r, Q = phy.primatives_to_state(V, rho, T)
     eq = E.FVMEquation(cfg, phy, spec, 5, {}, us_init=torch.cat([m, r, Q], 1))
     d = eq.forward(prim)
-    scale = float(eq.dev.t.f_vals.abs().max()) * 250.0   # |flux| ~ rho E u |S|
+    scale = float(eq.tables.kernel.f_vals.abs().max()) * 250.0   # |flux| ~ rho E u |S|
     assert float(d.abs().max()) < 1e-4 * scale

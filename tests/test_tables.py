@@ -43,3 +43,32 @@ def test_coo_to_ell_overflow():
     except ValueError:
         return
     raise AssertionError("expected ValueError")
+
+
+def test_device_records_encode_tables(golden):
+    """The packed device records hold the same operators as the semantic kernel tables."""
+    g, spec, T, cfg = golden
+    K = T.kernel
+    R = K.records()
+    dim, N, F, kg = K.dim, K.n_cells, K.n_facets, K.kg
+    cell, face, div = R["cell_rec"], R["face_rec"], R["div_rec"]
+    assert torch.equal(cell[:, :dim * kg].reshape(N, dim, kg), K.g_vals.permute(2, 0, 1))
+    assert torch.equal(cell[:, dim * kg:dim * kg + kg].contiguous().view(torch.int32), K.g_cols.t())
+    assert torch.equal(div[:, :K.kf], K.f_vals.t())
+    assert torch.equal(div[:, dim + 1:dim + 1 + K.kf].contiguous().view(torch.int32), K.f_cols.t())
+    codes = face[:, :2].contiguous().view(torch.int32)
+    bc = K.bc_face.long()
+    # interior facets: both cells; boundary facets: the cell on one side, -1 - b on the other
+    interior = torch.ones(F, dtype=torch.bool)
+    interior[bc] = False
+    assert torch.equal(codes[interior], K.fcell[interior])
+    side = K.bc_side.long()
+    assert torch.equal(codes[bc, side], -1 - torch.arange(K.n_bc, dtype=torch.int32))
+    assert torch.equal(codes[bc, 1 - side], K.bc_cell)
+    assert torch.equal(face[:, 2], K.inv_d) and torch.equal(face[:, 3], K.fsize)
+    # side displacements reproduce cent_to_facet_disp through cell_to_facet
+    for j in range(dim + 1):
+        f = K.c2f[j].long()
+        s_ = ((K.side >> j) & 1).long()
+        off = 4 + 2 * dim + s_[:, None] * dim + torch.arange(dim)[None, :]
+        assert torch.equal(face[f[:, None], off], K.disp[j].t())

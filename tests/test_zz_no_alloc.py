@@ -40,8 +40,8 @@ def test_noalloc_matches_residual(case):
     N, C, dim = eq.mesh.n_cells, eq.n_comp, eq.mesh.dim
     p1 = torch.from_numpy(g["prim0"]).cuda().contiguous()
     p2 = torch.from_numpy(g["prim2"]).cuda().contiguous()
-    ga = torch.zeros((N, dim, C), device="cuda")
-    gb = torch.zeros((N, dim, C), device="cuda")
+    ga = torch.zeros((N, eq.dev.grow), device="cuda")      # limited-gradient rows (FVM_GROW)
+    gb = torch.zeros((N, eq.dev.grow), device="cuda")
     fa = torch.zeros(1, dtype=torch.int32, device="cuda")
     fb = torch.zeros(1, dtype=torch.int32, device="cuda")
     for prims in (p1, p2):            # second call uses the gradients carried from the first
@@ -69,10 +69,10 @@ def test_noalloc_rejects_oversized_mesh():
     g, eq, T, cfg = make_equation("b3d")
     lib = _lib.load()
     big = _lib.Mesh.from_buffer_copy(eq.dev.struct)
-    big.n_facets = _lib.FVM_NOALLOC_SCRATCH_BYTES // (4 * 3 * big.n_comp) + 1   # 15 floats per 3D facet
+    big.n_facets = _lib.FVM_NOALLOC_SCRATCH_BYTES // (4 * 8) + 1   # 8 floats of flux per 3D facet alone
     N, C = eq.mesh.n_cells, eq.n_comp
     prims = torch.from_numpy(g["prim0"]).cuda()
-    grads = torch.zeros((N, 3, C), device="cuda")
+    grads = torch.zeros((N, eq.dev.grow), device="cuda")
     flag = torch.zeros(1, dtype=torch.int32, device="cuda")
     out = torch.full((N, C), 7.0, device="cuda")
     rc = lib.fvm_residual_noalloc(ct.byref(big), ct.byref(eq.phys), _lib.ptr(prims), _lib.ptr(grads),
