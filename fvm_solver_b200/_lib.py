@@ -76,6 +76,7 @@ _SIGS = [
     ("fvm_conservation", ct.c_int, [ct.POINTER(Mesh), _P, _P, ct.POINTER(Work), _P]),
     ("fvm_residual_noalloc", ct.c_int, [ct.POINTER(Mesh), ct.POINTER(Physics), _P, _P, _P, _P, _P]),
     ("fvm_profile_start", ct.c_int, [ct.c_int32]),
+    ("fvm_set_block_size", ct.c_int, [ct.c_int32, ct.c_int32]),
     ("fvm_profile_stop", ct.c_int, []),
     ("fvm_profile_read", ct.c_int, [ct.c_int32, _P, _P]),
 ]

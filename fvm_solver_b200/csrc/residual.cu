@@ -22,9 +22,9 @@
 //               the conservation sums.
 //
 // All kernels are memory-bound gathers with one thread per cell or facet.  Every per-cell and
-// per-facet table is one contiguous record read with 16-byte loads, and every gathered row
-// (primitives, limited gradients, fluxes) is padded to a 16-byte multiple, so a gather is one or
-// two aligned vector loads and never straddles more 32-byte sectors than it must.  Rebuilding the
+// per-facet table is one contiguous record, and every gathered row (primitives, limited gradients,
+// fluxes) is padded to a 32-byte multiple (16 bytes for the 4-float rows of 2D), so a record or a
+// gather is a few aligned 256-bit loads and never straddles more 32-byte sectors than it must.  Rebuilding the
 // facet values in k_face removes the reference's [F, 2, C] facet table (a scattered write plus a
 // read per facet side).
 #include <math.h>
@@ -32,6 +32,8 @@
 #include "fvm_common.cuh"
 
 namespace fvm {
+
+constexpr int kMaxBlock = 512;   // largest block size the autotuner may pick
 
 struct Phys {
     float T_0, mu, mu_b, S, C_v, gamma, kappa, v_factor;
@@ -71,29 +73,65 @@ struct L {
     static_assert(META + 1 <= CR && RB + DIM <= FR && 2 * K <= DR, "record layout");
 };
 
-// N consecutive floats (N % 4 == 0, 16-byte aligned) -> registers.
+// N consecutive floats -> registers.  Rows whose width is a multiple of 8 floats start on 32-byte
+// boundaries and move with 256-bit accesses (one L1 wavefront per lane-row instead of two); the
+// others (4-float rows) with 128-bit accesses.
+__device__ __forceinline__ void ld8_nc(const float* p, float* v) {
+    asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+                 : "l"(p));
+}
+__device__ __forceinline__ void ld8_cg(const float* p, float* v) {
+    asm volatile("ld.global.cg.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+                 : "l"(p));
+}
+__device__ __forceinline__ void st8(float* p, const float* v) {
+    asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(v[0]), "f"(v[1]), "f"(v[2]),
+                 "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+                 : "memory");
+}
+
 template <int N>
 __device__ __forceinline__ void ld_vec(const float* __restrict__ p, float (&v)[N]) {
+    static_assert(N % 4 == 0, "row width");
+    if constexpr (N % 8 == 0) {
 #pragma unroll
-    for (int q = 0; q < N / 4; ++q) {
-        const float4 t = __ldg(reinterpret_cast<const float4*>(p) + q);
-        v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+        for (int q = 0; q < N / 8; ++q) ld8_nc(p + 8 * q, v + 8 * q);
+    } else {
+#pragma unroll
+        for (int q = 0; q < N / 4; ++q) {
+            const float4 t = __ldg(reinterpret_cast<const float4*>(p) + q);
+            v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+        }
     }
 }
 // Same, for data written by an earlier kernel of the same sequence (no read-only cache).
 template <int N>
 __device__ __forceinline__ void ld_vec_cg(const float* p, float (&v)[N]) {
+    static_assert(N % 4 == 0, "row width");
+    if constexpr (N % 8 == 0) {
 #pragma unroll
-    for (int q = 0; q < N / 4; ++q) {
-        const float4 t = __ldcg(reinterpret_cast<const float4*>(p) + q);
-        v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+        for (int q = 0; q < N / 8; ++q) ld8_cg(p + 8 * q, v + 8 * q);
+    } else {
+#pragma unroll
+        for (int q = 0; q < N / 4; ++q) {
+            const float4 t = __ldcg(reinterpret_cast<const float4*>(p) + q);
+            v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+        }
     }
 }
 template <int N>
 __device__ __forceinline__ void st_vec(float* p, const float (&v)[N]) {
+    static_assert(N % 4 == 0, "row width");
+    if constexpr (N % 8 == 0) {
 #pragma unroll
-    for (int q = 0; q < N / 4; ++q)
-        reinterpret_cast<float4*>(p)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        for (int q = 0; q < N / 8; ++q) st8(p + 8 * q, v + 8 * q);
+    } else {
+#pragma unroll
+        for (int q = 0; q < N / 4; ++q)
+            reinterpret_cast<float4*>(p)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    }
 }
 __device__ __forceinline__ int as_int(float x) { return __float_as_int(x); }
 
@@ -248,7 +286,7 @@ __global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float
 // k_cell: gradient, limiter, limited gradient.
 // ------------------------------------------------------------------------------------------
 template <int DIM>
-__global__ void __launch_bounds__(kBlock) k_cell(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+__global__ void __launch_bounds__(kMaxBlock) k_cell(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
                                                   const float* __restrict__ bcv, float* __restrict__ grads,
                                                   int32_t* __restrict__ has_grads) {
     using Ly = L<DIM>;
@@ -323,7 +361,7 @@ __global__ void __launch_bounds__(kBlock) k_cell(fvm_mesh_t m, Phys p, const flo
 // k_face: facet fluxes.
 // ------------------------------------------------------------------------------------------
 template <int DIM>
-__global__ void __launch_bounds__(kBlock) k_face(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+__global__ void __launch_bounds__(kMaxBlock) k_face(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
                                                   const float* __restrict__ bcv,
                                                   const float* __restrict__ grads, float* __restrict__ flux) {
     using Ly = L<DIM>;
@@ -597,7 +635,7 @@ __device__ __forceinline__ void reduce_cons_cfl(const fvm_mesh_t& m, const Phys&
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(kBlock) k_div_stage(fvm_mesh_t m, Phys p, const float* __restrict__ flux,
+__global__ void __launch_bounds__(kMaxBlock) k_div_stage(fvm_mesh_t m, Phys p, const float* __restrict__ flux,
                                                        StageArgs a, float* __restrict__ state,
                                                        float* __restrict__ prims, float* __restrict__ kbuf,
                                                        const float* __restrict__ dt,
@@ -809,7 +847,7 @@ static Phys make_phys(const fvm_physics_t* ph) {
     return p;
 }
 
-static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+static bool aligned16(const void* p) { return ((uintptr_t)p & 31u) == 0; }   // rows use 256-bit accesses
 
 static bool mesh_ok(const fvm_mesh_t* m) {
     if (!m || (m->dim != 2 && m->dim != 3) || m->n_comp != m->dim + 2) return false;
@@ -834,6 +872,12 @@ static bool work_ok(const fvm_mesh_t* m, const fvm_work_t* w) {
 }
 
 static inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+// Threads per block of the cell, facet and divergence kernels (set by the autotuner through
+// fvm_set_block_size).  The boundary kernels keep kBlock: their per-block reduction order must not
+// change between single-mesh and batched runs.
+static int g_block_cell = kBlock, g_block_face = kBlock, g_block_div = kBlock;
+static inline unsigned blocks_of(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 static inline unsigned fin_blocks(const fvm_mesh_t* m) {
     return m->n_cases > 0 ? (unsigned)((m->n_cases + 127) / 128) : 1u;
 }
@@ -848,10 +892,10 @@ static int launch_fluxes(const fvm_mesh_t* m, const Phys& p, const float* prims,
         FVM_LAUNCH(KID_BC, s, k_bc<DIM><<<blocks_for(m->n_bc), kBlock, 0, s>>>(*m, p, prims, grads, has_grads,
                                                                                w->bc_vals, w->red));
     }
-    FVM_LAUNCH(KID_CELL, s, k_cell<DIM><<<blocks_for(m->n_cells), kBlock, 0, s>>>(*m, p, prims, w->bc_vals,
-                                                                                   grads, has_grads));
-    FVM_LAUNCH(KID_FACE, s, k_face<DIM><<<blocks_for(m->n_facets), kBlock, 0, s>>>(*m, p, prims, w->bc_vals,
-                                                                                   grads, w->flux));
+    FVM_LAUNCH(KID_CELL, s, k_cell<DIM><<<blocks_of(m->n_cells, g_block_cell), g_block_cell, 0, s>>>(
+                                *m, p, prims, w->bc_vals, grads, has_grads));
+    FVM_LAUNCH(KID_FACE, s, k_face<DIM><<<blocks_of(m->n_facets, g_block_face), g_block_face, 0, s>>>(
+                                *m, p, prims, w->bc_vals, grads, w->flux));
     return launch_status();
 }
 
@@ -863,7 +907,7 @@ static int residual_impl(const fvm_mesh_t* m, const Phys& p, const float* prims_
     int rc = launch_fluxes<DIM>(m, p, w->prims, grads, has_grads, w, s);
     if (rc) return rc;
     StageArgs a{};
-    FVM_LAUNCH(KID_DIV_STAGE, s, k_div_stage<DIM><<<blocks_for(m->n_cells), kBlock, 0, s>>>(
+    FVM_LAUNCH(KID_DIV_STAGE, s, k_div_stage<DIM><<<blocks_of(m->n_cells, g_block_div), g_block_div, 0, s>>>(
                                      *m, p, w->flux, a, nullptr, nullptr, nullptr, nullptr, nullptr, dudt));
     return launch_status();
 }
@@ -909,7 +953,7 @@ static int stage_impl(const fvm_mesh_t* m, const Phys& p, const fvm_tableau_t* t
     if (rc) return rc;
     StageArgs a = stage_args(tab, s);
     a.cons = a.final_ && b->cons != nullptr;
-    FVM_LAUNCH(KID_DIV_STAGE, st, k_div_stage<DIM><<<blocks_for(m->n_cells), kBlock, 0, st>>>(
+    FVM_LAUNCH(KID_DIV_STAGE, st, k_div_stage<DIM><<<blocks_of(m->n_cells, g_block_div), g_block_div, 0, st>>>(
                                       *m, p, w->flux, a, b->state, b->prims, b->k, b->dt, w->red, nullptr));
     rc = launch_status();
     if (rc) return rc;
@@ -940,7 +984,7 @@ static int multistep_impl(const fvm_mesh_t* m, const Phys& p, int store, int n_t
         a.coef[t] = coef[t];
     }
     a.cons = b->cons != nullptr;
-    FVM_LAUNCH(KID_DIV_STAGE, st, k_div_stage<DIM><<<blocks_for(m->n_cells), kBlock, 0, st>>>(
+    FVM_LAUNCH(KID_DIV_STAGE, st, k_div_stage<DIM><<<blocks_of(m->n_cells, g_block_div), g_block_div, 0, st>>>(
                                       *m, p, w->flux, a, b->state, b->prims, b->k, b->dt, w->red, nullptr));
     rc = launch_status();
     if (rc) return rc;
@@ -1132,4 +1176,14 @@ extern "C" int fvm_residual_noalloc(const fvm_mesh_t* mesh, const fvm_physics_t*
     cudaStream_t s = (cudaStream_t)stream;
     return mesh->dim == 2 ? residual_impl<2>(mesh, p, prims, grads, has_grads, dudt, &w, s)
                           : residual_impl<3>(mesh, p, prims, grads, has_grads, dudt, &w, s);
+}
+
+extern "C" int fvm_set_block_size(int32_t kernel_id, int32_t threads) {
+    if (threads < 64 || threads > kMaxBlock || threads % 32 != 0) return FVM_E_ARG;
+    switch (kernel_id) {
+        case KID_CELL: g_block_cell = threads; return FVM_OK;
+        case KID_FACE: g_block_face = threads; return FVM_OK;
+        case KID_DIV_STAGE: g_block_div = threads; return FVM_OK;
+        default: return FVM_E_ARG;
+    }
 }

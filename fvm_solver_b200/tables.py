@@ -259,7 +259,7 @@ class KernelTables:
 
 def record_sizes(dim: int):
     """(cell record, facet record, divergence record) widths in floats (FVM_CELL_REC etc.)."""
-    return (20, 12, 8) if dim == 2 else (36, 16, 8)
+    return (24, 16, 8) if dim == 2 else (40, 16, 8)
 
 
 def row_sizes(dim: int):

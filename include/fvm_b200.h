@@ -41,8 +41,8 @@ extern "C" {
 #define FVM_RED_DOUBLES 64
 #define FVM_NOALLOC_SCRATCH_BYTES (16 * 1024 * 1024)
 
-/* Row layouts.  Gathered per-cell / per-facet rows are padded to 16-byte multiples so every row
- * is read and written with 16-byte vector accesses:
+/* Row layouts.  Records and gathered rows are padded so every row is read and written with
+ * 32-byte (or, for 4-float rows, 16-byte) vector accesses; all row arrays must be 32-byte aligned:
  *   primitives, fluxes, boundary values: FVM_ROW(dim) floats per row (4 in 2D, 8 in 3D), the first
  *     C = dim + 2 used (V..., rho, T for primitives; the conserved order for fluxes);
  *   limited gradients: FVM_GROW(dim) floats per cell (8 / 16); entry (d, V_k) at d*(dim+1) + k,
@@ -50,8 +50,8 @@ extern "C" {
  *   state and stage increments keep the plain [N][C] layout. */
 #define FVM_ROW(dim) ((dim) == 2 ? 4 : 8)
 #define FVM_GROW(dim) ((dim) == 2 ? 8 : 16)
-#define FVM_CELL_REC(dim) ((dim) == 2 ? 20 : 36)
-#define FVM_FACE_REC(dim) ((dim) == 2 ? 12 : 16)
+#define FVM_CELL_REC(dim) ((dim) == 2 ? 24 : 40)
+#define FVM_FACE_REC(dim) ((dim) == 2 ? 16 : 16)
 #define FVM_DIV_REC 8
 
 /* Mesh tables (built by fvm_solver_b200/tables.py).  N cells, F facets, Fb boundary facets,
@@ -146,6 +146,11 @@ const char *fvm_version(void);
  * the events.  Kernel ids: 0 ell_spmv, 1 ell_spmm, 2 bc, 3 cell, 4 face, 5 div_stage,
  * 6 finalize, 7 state_to_prims, 8 reduce_state, 9 batched. */
 int fvm_profile_start(int32_t capacity);
+/* Launch configuration (no reference counterpart): threads per block of the cell (id 3), facet
+ * (id 4) and divergence/stage (id 5) kernels for all later launches of this process; a multiple
+ * of 32 in [64, 512].  Results do not depend on it (each thread's arithmetic is unchanged); the
+ * autotuner (fvm_solver_b200/autotune.py) picks it per mesh. */
+int fvm_set_block_size(int32_t kernel_id, int32_t threads);
 int fvm_profile_stop(void);
 int fvm_profile_read(int32_t n, int32_t *ids, float *ms);
 
