@@ -185,6 +185,8 @@ def secondary(args):
         case = W.channel_cylinder(device="cuda")
         eq = case.equation()
         sol = eq.t_solver
+        from fvm_solver_b200.autotune import autotune
+        autotune(eq)
         sol.step(args.warmup)
         with ClockSampler(0) as clk:
             ms = timed(sol, args.steps)
@@ -222,6 +224,8 @@ def secondary(args):
     cfg = W.ensemble_case(0, device="cuda", cfl=0.3).cfg
     batch = B.BatchedFVM(parts, cfg, device="cuda")
     Nt = batch.n_cells
+    from fvm_solver_b200.autotune import autotune
+    tuned = {k: v["threads"] for k, v in autotune(batch).items()}
     batch.t_solver.step(max(args.warmup, 3))
     with ClockSampler(0) as clk:
         ms_b = timed(batch.t_solver, args.steps)
@@ -232,6 +236,7 @@ def secondary(args):
     for k, p in enumerate(parts):
         c = W.ensemble_case(k, device="cuda", cfl=0.3).cfg
         eq = FVMEquation.from_kernel_tables(c, FluidConstitution2D(c), p.kt, p.state0)
+        autotune(eq)                       # per size bucket (cached), so small cases get their own
         eq.t_solver.step(max(args.warmup, 3))
         ms_p += timed(eq.t_solver, args.steps)
         cells_p += p.kt.n_cells
@@ -244,7 +249,8 @@ def secondary(args):
            "data": "synthetic",
            "config": {"workload": "ensemble_2d_ab3_batched", "cases": args.cases, "cells_total": Nt,
                       "cells_min": min(sizes), "cells_max": max(sizes), "integrator": "AB3 (SSP-RK3 start), CFL 0.3",
-                      "timing": "cuda graph replay", "table_build_s": t_build},
+                      "timing": "cuda graph replay", "table_build_s": t_build, "host_cpus": os.cpu_count(),
+                      "block_sizes": tuned},
            "plain": {"value": vp, "unit": "cell-steps/s", "ms_per_step_all_cases": ms_p / args.steps,
                      "how": "each case alone, own CUDA graph, sequential"},
            "batched_over_plain": vb / vp, "clocks": clk.summary()}
@@ -279,6 +285,8 @@ def main():
     sol = eq.t_solver
     N, F, Fb = eq.mesh.n_cells, eq.mesh.n_facets, eq.dev.n_bc
     lib = _lib.load()
+    from fvm_solver_b200.autotune import autotune
+    tuned = {k: v["threads"] for k, v in autotune(eq).items()}
 
     # warm-up
     sol.step(args.warmup)
@@ -382,7 +390,8 @@ def main():
             "config": {"workload": "taylor_green_periodic_box_rk4_cfl0.5", "points_per_axis": args.n,
                        "cells_per_gpu": N, "facets_per_gpu": F, "state": "fp32 [N,5]",
                        "l2": "inputs larger than L2 (>1 GB touched per stage), no flush",
-                       "parallelism": f"{world} independent boxes (one per rank)", "timing": "cuda graph replay"},
+                       "parallelism": f"{world} independent boxes (one per rank)", "timing": "cuda graph replay",
+                       "block_sizes": tuned},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": per_launch[dom]},

@@ -77,12 +77,14 @@ _SIGS = [
     ("fvm_residual_noalloc", ct.c_int, [ct.POINTER(Mesh), ct.POINTER(Physics), _P, _P, _P, _P, _P]),
     ("fvm_profile_start", ct.c_int, [ct.c_int32]),
     ("fvm_set_block_size", ct.c_int, [ct.c_int32, ct.c_int32]),
+    ("fvm_gemm_bf16", ct.c_int, [_P, ct.c_int64, _P, ct.c_int64, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32,
+                                 _P, _P, ct.c_int64, _P, _P, ct.c_int64, _P, ct.c_int32, _P, _P]),
     ("fvm_profile_stop", ct.c_int, []),
     ("fvm_profile_read", ct.c_int, [ct.c_int32, _P, _P]),
 ]
 
 KERNEL_NAMES = {0: "ell_spmv", 1: "ell_spmm", 2: "bc", 3: "cell", 4: "face", 5: "div_stage", 6: "finalize",
-                7: "state_to_prims", 8: "reduce_state", 9: "batched"}
+                7: "state_to_prims", 8: "reduce_state", 9: "batched", 10: "corrector"}
 
 EXPORTED = [s[0] for s in _SIGS]
 

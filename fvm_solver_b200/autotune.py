@@ -1,0 +1,88 @@
+"""Launch-configuration autotuner for the residual kernels.
+
+The cell, facet and divergence kernels (one thread per cell / facet) run at any block size; which
+one is fastest depends on the mesh (cell count, boundary fraction, batched or not) because it sets
+how many warps each SM keeps in flight against the gather latency.  ``autotune`` times each
+candidate block size on the caller's own mesh -- residual evaluations bracketed by the library's
+per-launch CUDA events -- keeps the fastest per kernel, and installs it with
+``fvm_set_block_size``.  Results do not change with the block size (every thread's arithmetic is
+the same), only the time does.  Choices are cached per (dim, cell-count bucket, batch size).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+
+CANDIDATES = (64, 128, 256, 512)
+KERNELS = {3: "cell", 4: "face", 5: "div_stage"}
+_cache: dict = {}
+
+
+def _key(eq) -> tuple:
+    n = eq.mesh.n_cells
+    return (eq.mesh.dim, int(round(math.log2(max(n, 1)) * 2)), int(getattr(eq, "n_cases", 0) or 0))
+
+
+def set_block_size(kernel: str, threads: int):
+    kid = {v: k for k, v in KERNELS.items()}[kernel]
+    _lib.check(_lib.load().fvm_set_block_size(kid, int(threads)), "fvm_set_block_size")
+
+
+def _time_residual(eq, prims, out, reps: int) -> dict:
+    """Mean device time per launch of each kernel over ``reps`` residual evaluations."""
+    lib = eq.lib
+    _lib.check(lib.fvm_profile_start(reps * 8 + 8), "fvm_profile_start")
+    for _ in range(reps):
+        _lib.check(lib.fvm_residual(ct.byref(eq.dev.struct), ct.byref(eq.phys), _lib.ptr(prims), _lib.ptr(eq.grads),
+                                    _lib.ptr(eq.has_grads), _lib.ptr(out), ct.byref(eq.work.struct),
+                                    _lib.stream_ptr()), "fvm_residual")
+    n = lib.fvm_profile_stop()
+    if n < 0:
+        raise RuntimeError("profiling buffer overflow")
+    ids = np.zeros(n, np.int32)
+    ms = np.zeros(n, np.float32)
+    if lib.fvm_profile_read(n, ids.ctypes.data, ms.ctypes.data) != n:
+        raise RuntimeError("fvm_profile_read failed")
+    return {KERNELS[k]: float(ms[ids == k].mean()) for k in KERNELS if np.any(ids == k)}
+
+
+def autotune(eq, reps: int = 5, candidates=CANDIDATES, use_cache: bool = True) -> dict:
+    """Pick and install the fastest block size per kernel for ``eq`` (FVMEquation or BatchedFVM).
+
+    The carried limited gradients are saved and restored, so the tuning runs leave the solver's
+    state untouched.  Returns ``{kernel: {"threads": best, "ms": {threads: mean ms}}}``.
+    """
+    key = _key(eq)
+    if use_cache and key in _cache:
+        for k, v in _cache[key].items():
+            set_block_size(k, v["threads"])
+        return _cache[key]
+    prims = eq.cells.get_values()[0].contiguous()
+    out = torch.empty_like(prims)
+    g_save, f_save = eq.grads.clone(), eq.has_grads.clone()
+    timings = {k: {} for k in KERNELS.values()}
+    for bs in candidates:
+        for k in KERNELS.values():
+            set_block_size(k, bs)
+        _time_residual(eq, prims, out, 1)               # warm-up at this configuration
+        for k, ms in _time_residual(eq, prims, out, reps).items():
+            timings[k][bs] = ms
+    best = {k: {"threads": min(t, key=t.get), "ms": t} for k, t in timings.items()}
+    for k, v in best.items():
+        set_block_size(k, v["threads"])
+    eq.grads.copy_(g_save)
+    eq.has_grads.copy_(f_save)
+    torch.cuda.synchronize()
+    _cache[key] = best
+    return best
+
+
+def reset():
+    """Back to the default block size (256) for every tunable kernel."""
+    for k in KERNELS.values():
+        set_block_size(k, 256)

@@ -52,12 +52,17 @@ def _ensemble_worker(args):
     return build_case_tables(ensemble_case(i, device="cpu", base_seed=base_seed))
 
 
+def _worker_init():
+    # one intra-op thread per worker process: the workers already run in parallel
+    torch.set_num_threads(1)
+
+
 def build_ensemble_tables(n_cases: int, base_seed: int = 1234, workers: int = 0) -> list:
     """Per-case tables of the seeded ensemble; ``workers > 0`` builds them in spawned processes."""
     jobs = [(i, base_seed) for i in range(n_cases)]
     if workers > 0:
         ctx = mp.get_context("spawn")
-        with cfut.ProcessPoolExecutor(max_workers=workers, mp_context=ctx) as ex:
+        with cfut.ProcessPoolExecutor(max_workers=workers, mp_context=ctx, initializer=_worker_init) as ex:
             return list(ex.map(_ensemble_worker, jobs, chunksize=4))
     return [_ensemble_worker(j) for j in jobs]
 

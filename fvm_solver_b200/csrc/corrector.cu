@@ -1,0 +1,535 @@
+// Learned k-step corrector: BF16 tcgen05 GEMMs (FP32 accumulation in TMEM), message passing over
+// the mesh adjacency, SiLU, MSE loss and Adam -- forward, backward and optimiser all hand-written.
+//
+// GEMM form used throughout:  D[M][N] = epilogue(A[M][K] . B[N][K]^T)
+//   A, B: bf16, row-major, K contiguous ("K-major" for both UMMA operands); M any (128-row tiles,
+//   rows past M read as zero and are not stored); N in {32, 64, 128, 256}; K a multiple of 64.
+// One CTA of 128 threads computes one 128 x N tile:
+//   * the K loop stages 64-wide slices of A and B in shared memory in the canonical no-swizzle
+//     K-major core-matrix layout (8 rows x 16 bytes per core matrix; the two 16-byte K halves of an
+//     MMA step LBO = 128 B apart; 8-row groups SBO = 256 B apart);
+//   * one elected thread issues tcgen05.mma.cta_group::1.kind::f16 (M = 128, N, K = 16) four times
+//     per slice and tcgen05.commit's completion to an mbarrier, which all threads wait on with an
+//     iteration limit (a timeout sets the error flag instead of hanging);
+//   * the accumulator lives in tensor memory (N fp32 columns x 128 lanes, allocated per CTA); the
+//     epilogue reads it back with tcgen05.ld (warp w owns lanes 32w..32w+31 = rows of the tile),
+//     adds the bias, stores the pre-activation if asked, applies SiLU, adds a residual, and writes
+//     fp32 and/or bf16.
+// Split-K (for weight gradients, K = number of cells): `k_splits` > 1 makes each CTA handle one
+// K range and atomically add its fp32 tile into D (no epilogue other than the add).
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "fvm_common.cuh"
+
+namespace fvm {
+namespace corr {
+
+constexpr int TM = 128;          // tile rows (UMMA M)
+constexpr int TK = 64;           // K slice staged per iteration
+constexpr int kGemmThreads = 128;
+constexpr long long kWaitLimit = 1LL << 22;   // mbarrier polls before a wait gives up
+
+struct GemmArgs {
+    const __nv_bfloat16* A;
+    int64_t lda;
+    const __nv_bfloat16* B;
+    int64_t ldb;
+    int M, N, K;
+    int k_splits;                 // > 1: split-K with atomic accumulation into Df
+    const float* bias;            // [N] or null
+    const float* resid;           // [M][ldr] fp32 added after the activation, or null
+    int64_t ldr;
+    float* Df;                    // [M][ldd] fp32 output (or accumulation target), or null
+    __nv_bfloat16* Db;            // [M][ldd] bf16 output, or null
+    int64_t ldd;
+    float* preact;                // [M][ldd] fp32 pre-activation, or null
+    int act;                      // 0 none, 1 SiLU
+    int* err;                     // device error flag (set to 1 on an mbarrier timeout)
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// UMMA shared-memory matrix descriptor: no swizzle, K-major, version 1 (sm100).
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;       // descriptor version for tcgen05
+    return d;                      // base offset 0, lbo mode 0, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor of kind::f16: D fp32, A and B bf16, both K-major, M = 128.
+__host__ __device__ constexpr uint32_t make_idesc(int N) {
+    return (1u << 4)                      // D format: F32
+           | (1u << 7)                    // A format: BF16
+           | (1u << 10)                   // B format: BF16
+           | ((uint32_t)(N >> 3) << 17)   // N / 8
+           | ((uint32_t)(TM >> 4) << 24); // M / 16
+}
+
+// Stage rows [r0, r0 + nrows) x K columns [k0, k0 + 64) of a row-major bf16 matrix into the
+// core-matrix layout: 16-byte unit (row r, unit u of 8 K elements) -> slice u/2, half u%2.
+__device__ __forceinline__ void stage_tile(uint8_t* smem, const __nv_bfloat16* src, int64_t ld, int r0, int rows_valid,
+                                           int nrows, int k0, int kmax) {
+    const int units = nrows * (TK / 8);
+    const int slice_bytes = (nrows / 8) * 256;
+    for (int t = threadIdx.x; t < units; t += blockDim.x) {
+        const int r = t >> 3, u = t & 7;
+        const int k = k0 + 8 * u;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (r < rows_valid && k < kmax) v = *reinterpret_cast<const uint4*>(src + (int64_t)(r0 + r) * ld + k);
+        const int off = (u >> 1) * slice_bytes + (r >> 3) * 256 + (u & 1) * 128 + (r & 7) * 16;
+        *reinterpret_cast<uint4*>(smem + off) = v;
+    }
+}
+
+__device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
+
+template <int N>
+__global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* sA = smem;                                  // TM * TK * 2 = 16 KB
+    uint8_t* sB = smem + TM * TK * 2;                    // N * TK * 2
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t s_taddr;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * TM;
+    const int split = blockIdx.y;
+    const int kchunks = g.K / TK;
+    const int per = (kchunks + g.k_splits - 1) / g.k_splits;
+    const int kc0 = split * per, kc1 = min(kchunks, kc0 + per);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_taddr)),
+                     "r"((uint32_t)(N < 32 ? 32 : N)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t taddr = s_taddr;
+    const uint32_t idesc = make_idesc(N);
+    const int rows_a = min(TM, g.M - m0);
+    bool ok = true;
+    uint32_t phase = 0;
+    for (int kc = kc0; kc < kc1; ++kc) {
+        stage_tile(sA, g.A, g.lda, m0, rows_a, TM, kc * TK, g.K);
+        stage_tile(sB, g.B, g.ldb, 0, g.N, N, kc * TK, g.K);
+        asm volatile("fence.proxy.async.shared::cta;");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+            for (int s = 0; s < TK / 16; ++s) {
+                const uint64_t ad = make_desc(smem_u32(sA) + s * (TM / 8) * 256, 128, 256);
+                const uint64_t bd = make_desc(smem_u32(sB) + s * (N / 8) * 256, 128, 256);
+                const uint32_t acc = (kc > kc0 || s > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(taddr),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&mbar))
+                         : "memory");
+        }
+        // Wait for the MMAs (they read shared memory asynchronously) before restaging.
+        uint32_t done = 0;
+        for (long long it = 0; it < kWaitLimit && !done; ++it) {
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}\n"
+                : "=r"(done)
+                : "r"(smem_u32(&mbar)), "r"(phase));
+        }
+        if (!done) {
+            // Give the MMAs in flight a second bounded chance to finish before the tensor memory
+            // they write is released, then report the timeout.
+            for (long long it = 0; it < kWaitLimit && !done; ++it) {
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                    "selp.u32 %0, 1, 0, p;\n\t}\n"
+                    : "=r"(done)
+                    : "r"(smem_u32(&mbar)), "r"(phase));
+            }
+            ok = false;
+            if (g.err) atomicExch(g.err, 1);
+            break;
+        }
+        phase ^= 1u;
+        __syncthreads();
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const bool have = ok && kc1 > kc0;
+    // Epilogue: warp w owns tile rows 32w .. 32w + 31 (TMEM lanes).
+    const int row = m0 + warp * 32 + lane;
+    if (have) {
+#pragma unroll 1
+        for (int c0 = 0; c0 < N; c0 += 32) {
+            uint32_t r[32];
+            const uint32_t a = taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(a));
+            asm volatile("tcgen05.wait::ld.sync.aligned;");
+            if (row < g.M) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int col = c0 + j;
+                    if (col >= g.N) break;
+                    float v = __uint_as_float(r[j]);
+                    if (g.k_splits > 1) {
+                        atomicAdd(g.Df + (int64_t)row * g.ldd + col, v);
+                        continue;
+                    }
+                    if (g.bias) v += g.bias[col];
+                    if (g.preact) g.preact[(int64_t)row * g.ldd + col] = v;
+                    if (g.act == 1) v = silu(v);
+                    if (g.resid) v += g.resid[(int64_t)row * g.ldr + col];
+                    if (g.Df) g.Df[(int64_t)row * g.ldd + col] = v;
+                    if (g.Db) g.Db[(int64_t)row * g.ldd + col] = __float2bfloat16(v);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr),
+                     "r"((uint32_t)(N < 32 ? 32 : N)));
+}
+
+template <int N>
+static int launch_gemm(const GemmArgs& g, cudaStream_t s) {
+    const size_t smem = (size_t)TM * TK * 2 + (size_t)N * TK * 2;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_gemm<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    dim3 grid((unsigned)((g.M + TM - 1) / TM), (unsigned)g.k_splits);
+    FVM_LAUNCH(KID_CORRECTOR, s, k_gemm<N><<<grid, kGemmThreads, smem, s>>>(g));
+    return launch_status();
+}
+
+}  // namespace corr
+}  // namespace fvm
+
+using namespace fvm;
+
+extern "C" int fvm_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int32_t M, int32_t N, int32_t K,
+                             int32_t k_splits, const float* bias, const float* resid, int64_t ldr, float* Df,
+                             void* Db, int64_t ldd, float* preact, int32_t act, int32_t* err, void* stream) {
+    if (!A || !B || M <= 0 || K <= 0 || K % corr::TK != 0 || k_splits < 1 || (!Df && !Db) || !err) return FVM_E_ARG;
+    if (N != 32 && N != 64 && N != 128 && N != 256) return FVM_E_UNSUPPORTED;
+    if ((uintptr_t)A % 16 || (uintptr_t)B % 16 || lda % 8 || ldb % 8) return FVM_E_ARG;
+    if (k_splits > 1 && (!Df || bias || resid || preact || Db || act)) return FVM_E_ARG;
+    corr::GemmArgs g{static_cast<const __nv_bfloat16*>(A), lda, static_cast<const __nv_bfloat16*>(B), ldb, M, N, K,
+                     k_splits, bias, resid, ldr, Df, static_cast<__nv_bfloat16*>(Db), ldd, preact, act, err};
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (N) {
+        case 32: return corr::launch_gemm<32>(g, s);
+        case 64: return corr::launch_gemm<64>(g, s);
+        case 128: return corr::launch_gemm<128>(g, s);
+        default: return corr::launch_gemm<256>(g, s);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Message passing, activations, loss and optimiser kernels of the corrector.
+// Activations h: bf16 [N][W] (W = 64); neighbour table nbr: int32 [N][KN] (-1 = none).
+// ------------------------------------------------------------------------------------------
+namespace fvm {
+namespace corr {
+
+// out[i] = [h_i, mean_{j in nbr(i)} h_j]  (bf16 [N][2W]); one thread per (cell, 8-channel group).
+__global__ void k_mp_gather(const __nv_bfloat16* __restrict__ h, const int32_t* __restrict__ nbr, int N, int W, int KN,
+                            __nv_bfloat16* __restrict__ out) {
+    const int groups = W / 8;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)N * groups) return;
+    const int i = (int)(t / groups), g = (int)(t % groups);
+    const uint4 self = *reinterpret_cast<const uint4*>(h + (int64_t)i * W + 8 * g);
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int cnt = 0;
+    for (int k = 0; k < KN; ++k) {
+        const int j = __ldg(nbr + (int64_t)i * KN + k);
+        if (j < 0) continue;
+        const uint4 v = *reinterpret_cast<const uint4*>(h + (int64_t)j * W + 8 * g);
+        const __nv_bfloat16* b = reinterpret_cast<const __nv_bfloat16*>(&v);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[q] += __bfloat162float(b[q]);
+        ++cnt;
+    }
+    const float inv = cnt > 0 ? 1.f / (float)cnt : 0.f;
+    __align__(16) __nv_bfloat16 m[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) m[q] = __float2bfloat16(acc[q] * inv);
+    *reinterpret_cast<uint4*>(out + (int64_t)i * 2 * W + 8 * g) = self;
+    *reinterpret_cast<uint4*>(out + (int64_t)i * 2 * W + W + 8 * g) = *reinterpret_cast<const uint4*>(m);
+}
+
+// dh_out[i] = dh_in[i] + dA[i][:W] + sum_{j in nbr(i)} dA[j][W:] / deg(j)   (adjacency symmetric).
+__global__ void k_mp_scatter_back(const float* __restrict__ dA, const int32_t* __restrict__ nbr, int N, int W, int KN,
+                                  const float* __restrict__ dh_in, float* __restrict__ dh_out) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)N * W) return;
+    const int i = (int)(t / W), c = (int)(t % W);
+    float v = dA[(int64_t)i * 2 * W + c] + (dh_in ? dh_in[t] : 0.f);
+    for (int k = 0; k < KN; ++k) {
+        const int j = __ldg(nbr + (int64_t)i * KN + k);
+        if (j < 0) continue;
+        int deg = 0;
+        for (int q = 0; q < KN; ++q) deg += __ldg(nbr + (int64_t)j * KN + q) >= 0;
+        v += dA[(int64_t)j * 2 * W + W + c] / (float)deg;
+    }
+    dh_out[t] = v;
+}
+
+// dZ = dh * silu'(Z); writes dZ as bf16 [N][W] and transposed bf16 [W][ldT] (columns >= N zero),
+// and accumulates the bias gradient sum_i dZ[i].
+__global__ void k_silu_back(const float* __restrict__ dh, const float* __restrict__ Z, int N, int W,
+                            __nv_bfloat16* __restrict__ dZ, __nv_bfloat16* __restrict__ dZT, int64_t ldT,
+                            float* __restrict__ db) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)N * W) return;
+    const int i = (int)(t / W), c = (int)(t % W);
+    const float z = Z[t];
+    const float s = 1.f / (1.f + __expf(-z));
+    const float g = dh[t] * s * (1.f + z * (1.f - s));
+    dZ[t] = __float2bfloat16(g);
+    if (dZT) dZT[(int64_t)c * ldT + i] = __float2bfloat16(g);
+    if (db) atomicAdd(db + c, g);
+}
+
+// dst[c][r] = src[r][c] for a bf16 [R][Cc] matrix (32 x 32 tiles through shared memory).
+__global__ void k_transpose_bf16(const __nv_bfloat16* __restrict__ src, int R, int Cc, int64_t lds,
+                                 __nv_bfloat16* __restrict__ dst, int64_t ldd) {
+    __shared__ __nv_bfloat16 tile[32][33];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = r0 + k, c = c0 + threadIdx.x;
+        tile[k][threadIdx.x] = (r < R && c < Cc) ? src[(int64_t)r * lds + c] : __float2bfloat16(0.f);
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int c = c0 + k, r = r0 + threadIdx.x;
+        if (c < Cc && r < R) dst[(int64_t)c * ldd + r] = tile[threadIdx.x][k];
+    }
+}
+
+// out[i][o] = sum_c h[i][c] Wo[o][c] + bo[o]  (decoder, CUDA cores; O <= 8 outputs).
+__global__ void k_decoder(const __nv_bfloat16* __restrict__ h, const float* __restrict__ Wo, const float* __restrict__ bo,
+                          int N, int W, int O, float* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float acc[8];
+    for (int o = 0; o < O; ++o) acc[o] = bo[o];
+    for (int c = 0; c < W; c += 8) {
+        const uint4 v = *reinterpret_cast<const uint4*>(h + (int64_t)i * W + c);
+        const __nv_bfloat16* b = reinterpret_cast<const __nv_bfloat16*>(&v);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float x = __bfloat162float(b[q]);
+            for (int o = 0; o < O; ++o) acc[o] = fmaf(x, Wo[o * W + c + q], acc[o]);
+        }
+    }
+    for (int o = 0; o < O; ++o) out[(int64_t)i * O + o] = acc[o];
+}
+
+// Decoder backward: dh[i][c] = sum_o dOut[i][o] Wo[o][c]; dWo[o][c] += sum_i dOut[i][o] h[i][c];
+// dbo[o] += sum_i dOut[i][o].  One thread per (cell, channel); weight gradients through atomics.
+__global__ void k_decoder_back(const __nv_bfloat16* __restrict__ h, const float* __restrict__ Wo,
+                               const float* __restrict__ dOut, int N, int W, int O, float* __restrict__ dh,
+                               float* __restrict__ dWo, float* __restrict__ dbo) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)N * W) return;
+    const int i = (int)(t / W), c = (int)(t % W);
+    const float x = __bfloat162float(h[t]);
+    float v = 0.f;
+    for (int o = 0; o < O; ++o) {
+        const float d = dOut[(int64_t)i * O + o];
+        v = fmaf(d, Wo[o * W + c], v);
+        atomicAdd(dWo + o * W + c, d * x);
+        if (c == 0) atomicAdd(dbo + o, d);
+    }
+    dh[t] = v;
+}
+
+// Masked mean-squared error: loss += sum (pred - tgt)^2 / n over rows with mask != 0 (mask may be
+// null); dpred = 2 (pred - tgt) / n.
+__global__ void k_mse(const float* __restrict__ pred, const float* __restrict__ tgt, int64_t n_elem, float inv_n,
+                      double* __restrict__ loss, float* __restrict__ dpred) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    __shared__ double red[32];
+    double v[1] = {0.0};
+    if (t < n_elem) {
+        const float d = pred[t] - tgt[t];
+        dpred[t] = 2.f * d * inv_n;
+        v[0] = (double)d * d * inv_n;
+    }
+    block_sum<1>(v, red);
+    if (threadIdx.x == 0) atomicAdd(loss, v[0]);
+}
+
+// Adam (decoupled bias correction) on fp32 master weights; refreshes the bf16 copy [rows][cols]
+// and, if requested, its transpose [cols][rows] used by the backward GEMMs.  Zeroes the gradient.
+__global__ void k_adam(float* __restrict__ p, float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                       int64_t n, float lr, float b1, float b2, float eps, float c1, float c2,
+                       __nv_bfloat16* __restrict__ pb, __nv_bfloat16* __restrict__ pbT, int rows, int cols) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const float gr = g[t];
+    const float mt = b1 * m[t] + (1.f - b1) * gr;
+    const float vt = b2 * v[t] + (1.f - b2) * gr * gr;
+    m[t] = mt;
+    v[t] = vt;
+    const float w = p[t] - lr * (mt / c1) / (sqrtf(vt / c2) + eps);
+    p[t] = w;
+    g[t] = 0.f;
+    if (pb) pb[t] = __float2bfloat16(w);
+    if (pbT) {
+        const int r = (int)(t / cols), c = (int)(t % cols);
+        pbT[(int64_t)c * rows + r] = __float2bfloat16(w);
+    }
+}
+
+// Network input: X[i] = [(U_i - mean) * inv_std (C values), geometry (G values), zeros] bf16 [N][64].
+__global__ void k_features(const float* __restrict__ state, int N, int C, const float* __restrict__ mean,
+                           const float* __restrict__ inv_std, const float* __restrict__ geo, int G,
+                           __nv_bfloat16* __restrict__ X, int XW) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)N * XW) return;
+    const int i = (int)(t / XW), c = (int)(t % XW);
+    float v = 0.f;
+    if (c < C) v = (state[(int64_t)i * C + c] - mean[c]) * inv_std[c];
+    else if (c < C + G) v = geo[(int64_t)i * G + (c - C)];
+    X[t] = __float2bfloat16(v);
+}
+
+// U_new = U + scale * out (out: normalised increment, fp32 [N][C]).
+__global__ void k_apply_increment(const float* __restrict__ state, const float* __restrict__ out,
+                                  const float* __restrict__ scale, int N, int C, float* __restrict__ new_state) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)N * C) return;
+    new_state[t] = state[t] + scale[t % C] * out[t];
+}
+
+static inline unsigned nblk(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+}  // namespace corr
+}  // namespace fvm
+
+extern "C" int fvm_mp_gather(const void* h, const int32_t* nbr, int32_t N, int32_t W, int32_t KN, void* out,
+                             void* stream) {
+    if (!h || !nbr || !out || N <= 0 || W % 8 || KN <= 0) return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_mp_gather<<<corr::nblk((int64_t)N * (W / 8), 256), 256, 0, s>>>(
+                                     static_cast<const __nv_bfloat16*>(h), nbr, N, W, KN,
+                                     static_cast<__nv_bfloat16*>(out)));
+    return launch_status();
+}
+
+extern "C" int fvm_mp_scatter_back(const float* dA, const int32_t* nbr, int32_t N, int32_t W, int32_t KN,
+                                   const float* dh_in, float* dh_out, void* stream) {
+    if (!dA || !nbr || !dh_out || N <= 0 || W <= 0 || KN <= 0) return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_mp_scatter_back<<<corr::nblk((int64_t)N * W, 256), 256, 0, s>>>(
+                                     dA, nbr, N, W, KN, dh_in, dh_out));
+    return launch_status();
+}
+
+extern "C" int fvm_silu_back(const float* dh, const float* Z, int32_t N, int32_t W, void* dZ, void* dZT, int64_t ldT,
+                             float* db, void* stream) {
+    if (!dh || !Z || !dZ || N <= 0 || W <= 0 || (dZT && ldT < N)) return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_silu_back<<<corr::nblk((int64_t)N * W, 256), 256, 0, s>>>(
+                                     dh, Z, N, W, static_cast<__nv_bfloat16*>(dZ), static_cast<__nv_bfloat16*>(dZT),
+                                     ldT, db));
+    return launch_status();
+}
+
+extern "C" int fvm_transpose_bf16(const void* src, int32_t R, int32_t Cc, int64_t lds, void* dst, int64_t ldd,
+                                  void* stream) {
+    if (!src || !dst || R <= 0 || Cc <= 0 || ldd < R || lds < Cc) return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    dim3 grid((unsigned)((Cc + 31) / 32), (unsigned)((R + 31) / 32));
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_transpose_bf16<<<grid, dim3(32, 8), 0, s>>>(
+                                     static_cast<const __nv_bfloat16*>(src), R, Cc, lds,
+                                     static_cast<__nv_bfloat16*>(dst), ldd));
+    return launch_status();
+}
+
+extern "C" int fvm_decoder(const void* h, const float* Wo, const float* bo, int32_t N, int32_t W, int32_t O,
+                           float* out, void* stream) {
+    if (!h || !Wo || !bo || !out || N <= 0 || W % 8 || O < 1 || O > 8) return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_decoder<<<corr::nblk(N, 256), 256, 0, s>>>(
+                                     static_cast<const __nv_bfloat16*>(h), Wo, bo, N, W, O, out));
+    return launch_status();
+}
+
+extern "C" int fvm_decoder_back(const void* h, const float* Wo, const float* dOut, int32_t N, int32_t W, int32_t O,
+                                float* dh, float* dWo, float* dbo, void* stream) {
+    if (!h || !Wo || !dOut || !dh || !dWo || !dbo || N <= 0 || W <= 0 || O < 1 || O > 8) return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_decoder_back<<<corr::nblk((int64_t)N * W, 256), 256, 0, s>>>(
+                                     static_cast<const __nv_bfloat16*>(h), Wo, dOut, N, W, O, dh, dWo, dbo));
+    return launch_status();
+}
+
+extern "C" int fvm_mse(const float* pred, const float* tgt, int64_t n_elem, double* loss, float* dpred,
+                       void* stream) {
+    if (!pred || !tgt || !loss || !dpred || n_elem <= 0) return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_mse<<<corr::nblk(n_elem, 256), 256, 0, s>>>(
+                                     pred, tgt, n_elem, 1.f / (float)n_elem, loss, dpred));
+    return launch_status();
+}
+
+extern "C" int fvm_adam(float* p, float* g, float* m, float* v, int64_t n, float lr, float beta1, float beta2,
+                        float eps, int32_t step, void* pb, void* pbT, int32_t rows, int32_t cols, void* stream) {
+    if (!p || !g || !m || !v || n <= 0 || step < 1 || (pbT && (int64_t)rows * cols != n)) return FVM_E_ARG;
+    const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
+    cudaStream_t s = (cudaStream_t)stream;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_adam<<<corr::nblk(n, 256), 256, 0, s>>>(
+                                     p, g, m, v, n, lr, beta1, beta2, eps, c1, c2, static_cast<__nv_bfloat16*>(pb),
+                                     static_cast<__nv_bfloat16*>(pbT), rows, cols));
+    return launch_status();
+}
+
+extern "C" int fvm_corrector_features(const float* state, int32_t N, int32_t C, const float* mean,
+                                      const float* inv_std, const float* geo, int32_t G, void* X, int32_t XW,
+                                      void* stream) {
+    if (!state || !mean || !inv_std || !X || N <= 0 || C + G > XW || (G > 0 && !geo)) return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_features<<<corr::nblk((int64_t)N * XW, 256), 256, 0, s>>>(
+                                     state, N, C, mean, inv_std, geo, G, static_cast<__nv_bfloat16*>(X), XW));
+    return launch_status();
+}
+
+extern "C" int fvm_apply_increment(const float* state, const float* out, const float* scale, int32_t N, int32_t C,
+                                   float* new_state, void* stream) {
+    if (!state || !out || !scale || !new_state || N <= 0 || C <= 0) return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_apply_increment<<<corr::nblk((int64_t)N * C, 256), 256, 0, s>>>(
+                                     state, out, scale, N, C, new_state));
+    return launch_status();
+}

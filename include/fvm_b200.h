@@ -144,7 +144,7 @@ const char *fvm_version(void);
  * the number of launches recorded (FVM_E_ARG if more than `capacity` were attempted);
  * fvm_profile_read fills host arrays with each launch's kernel id and duration in ms, waiting for
  * the events.  Kernel ids: 0 ell_spmv, 1 ell_spmm, 2 bc, 3 cell, 4 face, 5 div_stage,
- * 6 finalize, 7 state_to_prims, 8 reduce_state, 9 batched. */
+ * 6 finalize, 7 state_to_prims, 8 reduce_state, 9 batched, 10 corrector. */
 int fvm_profile_start(int32_t capacity);
 /* Launch configuration (no reference counterpart): threads per block of the cell (id 3), facet
  * (id 4) and divergence/stage (id 5) kernels for all later launches of this process; a multiple
@@ -220,6 +220,19 @@ int fvm_cfl_dt(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *s
 /* out[case][C] <- sum_i vol_i * state[i][c] over the case's cells, in FP64. */
 int fvm_conservation(const fvm_mesh_t *mesh, const float *state, double *out,
                      const fvm_work_t *work, void *stream);
+
+/* ---- learned corrector (no reference counterpart) ------------------------------------------
+ * D[M][N] = epilogue(A[M][K] . B[N][K]^T) on the 5th-generation tensor cores (tcgen05, BF16
+ * operands, FP32 accumulation in tensor memory).  A, B: bf16 row-major with leading dimensions
+ * lda, ldb (multiples of 8, 16-byte aligned); N in {32, 64, 128, 256}; K a multiple of 64; M any.
+ * Epilogue, in order: + bias[N] (may be NULL), store the pre-activation to `preact` (NULL = skip),
+ * act (0 identity, 1 SiLU), + resid[M][ldr] (NULL = skip), store fp32 to Df and/or bf16 to Db
+ * (leading dimension ldd).  k_splits > 1 splits K over that many CTAs per row tile, each
+ * atomically adding its FP32 partial into Df (no other epilogue allowed).  *err is set to 1 if
+ * a tensor-core completion wait times out (the kernel then returns without hanging). */
+int fvm_gemm_bf16(const void *A, int64_t lda, const void *B, int64_t ldb, int32_t M, int32_t N, int32_t K,
+                  int32_t k_splits, const float *bias, const float *resid, int64_t ldr, float *Df, void *Db,
+                  int64_t ldd, float *preact, int32_t act, int32_t *err, void *stream);
 
 #ifdef __cplusplus
 }

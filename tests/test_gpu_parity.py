@@ -210,3 +210,27 @@ def test_free_stream_preservation_periodic():
     d = eq.forward(prim)
     scale = float(eq.tables.kernel.f_vals.abs().max()) * 250.0   # |flux| ~ rho E u |S|
     assert float(d.abs().max()) < 1e-4 * scale
+
+
+def test_block_size_invariance_and_autotune():
+    """Residuals do not depend on the launch configuration; the autotuner installs a valid one."""
+    from fvm_solver_b200 import autotune
+    g, eq, T, cfg = make_equation("b3d")
+    p = torch.from_numpy(g["prim0"]).cuda()
+    outs = []
+    try:
+        for bs in (64, 128, 256, 512):
+            for k in ("cell", "face", "div_stage"):
+                autotune.set_block_size(k, bs)
+            eq.reset_gradients()
+            outs.append(eq.forward(p))
+        assert all(torch.equal(outs[0], o) for o in outs)
+        best = autotune.autotune(eq, reps=2, use_cache=False)
+        assert set(best) == {"cell", "face", "div_stage"}
+        assert all(v["threads"] in autotune.CANDIDATES for v in best.values())
+        eq.reset_gradients()
+        assert torch.equal(eq.forward(p), outs[0])
+    finally:
+        autotune.reset()
+    with pytest.raises(RuntimeError):
+        autotune.set_block_size("cell", 48)
