@@ -131,6 +131,29 @@ def cpu_baseline(sample_n: int, steps: int | None = None, budget_s: float = 15.0
             "sample": f"numpy oracle, periodic TGV box {sample_n}^3 points ({N} tets), {n} RK4 steps, {el:.1f} s"}
 
 
+def parity_check(sample_n: int, steps: int = 5) -> dict:
+    """The CUDA path vs the oracle on the sample box: rel-L2 of the state after ``steps`` RK4 + CFL
+    steps against the FP32 oracle (the reference's arithmetic) and the FP64 oracle."""
+    from fvm_solver_b200 import workloads as W
+    from oracle import fvm_oracle as O
+    case = W.taylor_green(n=sample_n, seed=0, device="cuda")
+    eq = case.equation()
+    eq.t_solver.step(steps)
+    got = eq.cells.state.double().cpu().numpy()
+    T = eq.tables
+    inv_h = T.kernel.inv_h.numpy()
+    out = {"steps": steps, "cells": case.spec.n_cells}
+    for name, dt in (("fp32", np.float32), ("fp64", np.float64)):
+        res = O.OracleResidual(T, case.cfg, dt)
+        s = O.OracleSolver(res, case.state0.numpy().astype(dt), 1.0)
+        for _ in range(steps):
+            s.dt = res.dt(O.cfl_dt(s.state, 3, case.cfg.C_v, case.cfg.gamma, inv_h, 0.5))
+            s.butcher_step("RK4")
+        ref = s.state.astype(np.float64)
+        out[f"rel_l2_vs_oracle_{name}"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -377,9 +400,10 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_value = cells_total * ke / (float(t.item()) / 1e3)
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.sample_n)
+        parity = parity_check(args.sample_n)
     launches_per_step = n_launch / args.steps
     if rank == 0:
         out = {
@@ -397,6 +421,7 @@ def main():
                          "algorithmic_bytes_per_launch": per_launch[dom]},
             "kernels": kern,
             "cpu_baseline": cpu,
+            "parity": parity,
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": N * 5 * 4,
                     "d2h_bytes_per_step": N * 5 * 4, "steps": ke},
             "gpu_launches": int(round(launches_per_step * args.steps)),

@@ -185,6 +185,41 @@ class TSolver:
         replay.graph = g
         return replay
 
+    # -- checkpoint / restart ------------------------------------------------------------------
+    def state_dict(self) -> dict:
+        """Everything a bitwise-identical restart needs: the conserved state, the carried limited
+        gradients and their flag (the reference keeps them in ``FacetCalc.cell_grads`` and never
+        saves them), the device time step, the stage / multistep history and the counters."""
+        d = {"state": self.cells.state.clone(), "grads": self.eq.grads.clone(), "has_grads": self.eq.has_grads.clone(),
+             "dt": self.dt.clone(), "k": self.k.clone(), "t": self.t, "steps_done": self.steps_done,
+             "solver": type(self).__name__}
+        d.update(self._extra_state())
+        return d
+
+    def load_state_dict(self, d: dict):
+        if d.get("solver") != type(self).__name__:
+            raise ValueError(f"checkpoint of a {d.get('solver')} solver, not {type(self).__name__}")
+        self.cells.state = d["state"].to(self.cells.state.device)
+        self.eq.grads.copy_(d["grads"])
+        self.eq.has_grads.copy_(d["has_grads"])
+        self.eq._has_grads_host = bool(int(d["has_grads"].item()))
+        self.dt.copy_(d["dt"])
+        self.k.copy_(d["k"])
+        self.t, self.steps_done = d["t"], d["steps_done"]
+        self._load_extra_state(d)
+
+    def save_checkpoint(self, path: str):
+        torch.save({k: (v.cpu() if isinstance(v, torch.Tensor) else v) for k, v in self.state_dict().items()}, path)
+
+    def load_checkpoint(self, path: str):
+        self.load_state_dict(torch.load(path, weights_only=False))
+
+    def _extra_state(self) -> dict:
+        return {}
+
+    def _load_extra_state(self, d: dict):
+        pass
+
     def solve(self):
         """Run ``n_iter`` steps (or until ``end_t`` with host-side time accounting)."""
         if self.n_steps is None and self.end_t is None:
@@ -246,6 +281,13 @@ class AB3(TSolver):
                                        cons=None)
         self._idx = (ct.c_int32 * 3)()
         self._coef = (ct.c_float * 3)()
+
+    def _extra_state(self) -> dict:
+        return {"n_hist": self.n_hist, "head": self.head, "rk_k": self.rk_k.clone()}
+
+    def _load_extra_state(self, d: dict):
+        self.n_hist, self.head = d["n_hist"], d["head"]
+        self.rk_k.copy_(d["rk_k"])
 
     def _multistep(self, n_terms, idx, coef):
         for t in range(n_terms):

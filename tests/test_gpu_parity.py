@@ -234,3 +234,19 @@ def test_block_size_invariance_and_autotune():
         autotune.reset()
     with pytest.raises(RuntimeError):
         autotune.set_block_size("cell", 48)
+
+
+@pytest.mark.parametrize("name,extra", [("Butcher", "RK4"), ("Butcher_adapt", "RK3_SSP4"), ("AB3", "")])
+def test_checkpoint_restart_bitwise(tmp_path, name, extra):
+    """Stop after 3 steps, checkpoint, restart in a fresh solver: identical to 6 uninterrupted steps."""
+    g, eq, T, cfg = make_equation("c2d", name, extra, cfl=0.5 if name != "Butcher_adapt" else None)
+    eq.t_solver.step(6)
+    g2, eq2, _, _ = make_equation("c2d", name, extra, cfl=0.5 if name != "Butcher_adapt" else None)
+    eq2.t_solver.step(3)
+    path = str(tmp_path / "ckpt.pt")
+    eq2.t_solver.save_checkpoint(path)
+    g3, eq3, _, _ = make_equation("c2d", name, extra, cfl=0.5 if name != "Butcher_adapt" else None)
+    eq3.t_solver.load_checkpoint(path)
+    eq3.t_solver.step(3)
+    assert torch.equal(eq3.cells.state, eq.cells.state)
+    assert torch.equal(eq3.t_solver.dt, eq.t_solver.dt)
