@@ -107,6 +107,7 @@ def concat_tables(parts: list) -> tuple:
         g_vals=cat("g_vals", 2), g_cols=torch.cat(gcols, 1).contiguous(), nb_slot=cat("nb_slot", 0),
         disp=cat("disp", 2), eps=cat("eps", 0), c2f=cat("c2f", 1, fo), side=cat("side", 0),
         f_vals=cat("f_vals", 1), f_cols=cat("f_cols", 1, fo), inv_h=cat("inv_h", 0), volumes=cat("volumes", 0),
+        centroids=cat("centroids", 0),
         fcell=cat("fcell", 0, co), fbc=cat("fbc", 0, bo, True), normals=cat("normals", 0), fsize=cat("fsize", 0),
         xorth=cat("xorth", 0), inv_d=cat("inv_d", 0),
         bc_face=cat("bc_face", 0, fo), bc_side=cat("bc_side", 0), bc_cell=cat("bc_cell", 0, co),
@@ -160,6 +161,7 @@ class BatchedFVM:
         if len(gas) != 1:
             raise ValueError("batched cases must share T_0, S_const, C_v, gamma, v_factor and lim_p")
         kt, ca, off = concat_tables(parts)
+        self.kt = kt
         self.offsets = off
         self.dev = BatchedDeviceMesh(kt, ca, self.device)
         T_0, S, C_v, gamma, v_factor, lim_p = next(iter(gas))

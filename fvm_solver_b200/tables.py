@@ -181,6 +181,7 @@ class KernelTables:
     f_cols: torch.Tensor      # [kf, N] i32 facet indices
     inv_h: torch.Tensor       # [N] f64 max facet area / volume (CFL length scale inverse)
     volumes: torch.Tensor     # [N] f64
+    centroids: torch.Tensor   # [N, dim] f32 (host only: corrector features)
     # facets
     fcell: torch.Tensor       # [F, 2] i32 (side 0 cell, side 1 cell); boundary: the cell twice
     fbc: torch.Tensor         # [F] i32 boundary-local index or -1
@@ -566,7 +567,7 @@ class FVMTables:
             g_vals=g_vals.float(), g_cols=g_cols, nb_slot=nb_slot.to(i32), disp=disp.float(),
             eps=eps.float(), c2f=c2f, side=side.to(i32),
             f_vals=fv.t().contiguous(), f_cols=fc.t().contiguous().to(i32),
-            inv_h=inv_h, volumes=vol,
+            inv_h=inv_h, volumes=vol, centroids=self.mesh.centroids.float().contiguous(),
             fcell=fcell.to(i32), fbc=fbc.to(i32), normals=self.normals.contiguous(),
             fsize=self.facet_size.reshape(-1).contiguous(), xorth=self.X_orthog.contiguous(),
             inv_d=inv_d,

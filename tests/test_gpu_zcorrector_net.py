@@ -1,0 +1,98 @@
+"""Corrector network: hand-written forward/backward vs torch autograd, training, checked rollout.
+
+The torch reference rounds to bf16 exactly where the CUDA path does (GEMM operands: features,
+activations, weights) and accumulates in fp32, so forward outputs agree to ~1e-3 relative and
+weight gradients to ~1e-2 relative (bf16 rounding of the backward operands dZ and A).
+Needs a B200.
+"""
+import copy
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small_batch():
+    if not torch.cuda.is_available():
+        pytest.skip("needs CUDA")
+    from fvm_solver_b200 import batched as B, workloads as W
+    cases, params = [], []
+    for i, n in enumerate([2100, 3300, 2600]):
+        p = W.ensemble_params(i)
+        p["n_cells"] = n
+        c = W.channel_cylinder(device="cuda", solver_name="Butcher", solver_extra="SSP_RK3", **p)
+        c.cfg.cfl = None
+        cases.append(c)
+        params.append([p["mach"], np.log10(p["reynolds"])])
+    parts = [B.build_case_tables(c) for c in cases]
+    batch = B.BatchedFVM(parts, cases[0].cfg, device="cuda")
+    batch.t_solver.update_cfl_dt(0.5)
+    return batch, torch.tensor(params, dtype=torch.float32)
+
+
+def _torch_reference(net, X, nbr, target, N):
+    """The network in torch with the CUDA path's bf16 rounding points; returns out, loss, grads."""
+    bf = lambda t: t.to(torch.bfloat16).float()
+    P = {k: v.detach().clone().requires_grad_(True) for k, v in net.params.items()}
+    x = X[:N].float()
+    z = x @ bf(P["W_in"]).t() + P["b_in"]
+    h = torch.nn.functional.silu(z)
+    nb = nbr.long()
+    valid = (nb >= 0)
+    for l in range(net.L):
+        hb = bf(h)
+        gathered = torch.where(valid.unsqueeze(-1), hb[nb.clamp(min=0)], torch.zeros(()).cuda())
+        mean = gathered.sum(1) / valid.sum(1, keepdim=True).clamp(min=1)
+        A = torch.cat([hb, bf(mean)], 1)
+        z = A @ bf(P[f"W{l}"]).t() + P[f"b{l}"]
+        h = h + torch.nn.functional.silu(z)
+    out = bf(h) @ P["W_out"].t() + P["b_out"]
+    loss = ((out - target) ** 2).mean()
+    loss.backward()
+    return out.detach(), loss.detach(), {k: v.grad for k, v in P.items()}
+
+
+def test_forward_backward_vs_autograd(small_batch):
+    from fvm_solver_b200.corrector import CorrectorModel
+    batch, params = small_batch
+    model = CorrectorModel(batch, params, seed=3, lr=0.0)          # lr 0: the step leaves weights unchanged
+    U = batch.cells.state.clone()
+    model.set_normalisation(U.unsqueeze(0), U.unsqueeze(0) * 1e-3 + 1e-3)
+    N = U.shape[0]
+    X = model.net.features(U, model.mean, model.inv_std, model.geo).clone()
+    target = torch.randn(N, 4, device="cuda", generator=torch.Generator(device="cuda").manual_seed(0))
+    ref_out, ref_loss, ref_g = _torch_reference(model.net, X, model.nbr, target, N)
+    out = model.net.forward(model.nbr).clone()
+    assert rel_l2(out.cpu().numpy(), ref_out.cpu().numpy()) < 2e-3
+    grads_before = {k: v.clone() for k, v in model.net.grads.items()}
+    assert all(float(v.abs().max()) == 0.0 for v in grads_before.values())
+    # capture the gradients: run the backward pass but stop Adam from zeroing them
+    net = model.net
+    saved_adam = net.adam
+    net.adam = lambda *a, **k: None
+    loss = net.train_step(model.nbr, target)
+    net.adam = saved_adam
+    assert abs(float(loss.item()) / float(ref_loss) - 1) < 2e-3
+    for k in ref_g:
+        assert rel_l2(net.grads[k].cpu().numpy(), ref_g[k].cpu().numpy()) < 3e-2, k
+    net.check_errors()
+
+
+def test_training_reduces_loss_and_rollout(small_batch):
+    from fvm_solver_b200.corrector import CheckedRollout, CorrectorModel, record_trajectory, train
+    batch, params = small_batch
+    traj = record_trajectory(batch, steps=60, spinup=10)
+    model = CorrectorModel(batch, params, k=8, seed=1, lr=2e-3)
+    hist = train(model, traj, iters=300, log_every=50)
+    assert hist[-1][1] < 0.5 * hist[0][1]
+    ro = CheckedRollout(model)
+    for _ in range(3):
+        ok = ro.window()
+        assert ok.shape == (batch.n_cases,)
+    assert torch.isfinite(batch.cells.state).all()
+    assert 0 <= ro.accepted <= ro.windows
