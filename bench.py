@@ -48,7 +48,12 @@ def parse():
     ap.add_argument("--sample-n", type=int, default=20, help="points per axis of the CPU sample box")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="taylor_green", choices=["taylor_green", "channel_cylinder", "ensemble"],
+    ap.add_argument("--train-cases", type=int, default=32)
+    ap.add_argument("--eval-cases", type=int, default=16)
+    ap.add_argument("--iters", type=int, default=2000, help="corrector training iterations")
+    ap.add_argument("--windows", type=int, default=50, help="corrector rollout windows of k = 8 steps")
+    ap.add_argument("--workload", default="taylor_green",
+                    choices=["taylor_green", "channel_cylinder", "ensemble", "corrector"],
                     help="taylor_green: the headline 3D box; channel_cylinder: the 2D cylinder case (11k cells); "
                          "ensemble: batched 2D ensemble vs the same cases run one by one")
     ap.add_argument("--cases", type=int, default=256, help="ensemble size")
@@ -204,6 +209,8 @@ def secondary(args):
         torch.cuda.synchronize()
         return a.elapsed_time(b)
 
+    if args.workload == "corrector":
+        return corrector_bench(args, timed)
     if args.workload == "channel_cylinder":
         case = W.channel_cylinder(device="cuda")
         eq = case.equation()
@@ -277,6 +284,79 @@ def secondary(args):
            "plain": {"value": vp, "unit": "cell-steps/s", "ms_per_step_all_cases": ms_p / args.steps,
                      "how": "each case alone, own CUDA graph, sequential"},
            "batched_over_plain": vb / vp, "clocks": clk.summary()}
+    print(json.dumps(out))
+
+
+def corrector_bench(args, timed):
+    """Learned k-step corrector (k = 8) + FVM fallback vs plain FVM on held-out 2D cases.
+
+    Training: 32 seeded channel-cylinder cases stepped together (SSP-RK3, fixed per-case dt from
+    CFL 0.5 at the start), spin-up then recorded; random 8-step windows.  Evaluation: held-out
+    cases (other seeds), same spin-up, then R windows advanced (a) by plain FVM and (b) by the
+    corrector with per-case checks and FVM fallback; both timed on the device.
+    """
+    import copy
+    from fvm_solver_b200 import batched as B, workloads as W
+    from fvm_solver_b200.corrector import CheckedRollout, CorrectorModel, record_trajectory, train
+    workers = min(16, os.cpu_count() or 1)
+
+    def make(n, seed):
+        parts = B.build_ensemble_tables(n, base_seed=seed, workers=workers)
+        cfg = copy.deepcopy(W.ensemble_case(0, device="cuda", base_seed=seed).cfg)
+        cfg.solver_name, cfg.solver_extra, cfg.cfl = "Butcher", "SSP_RK3", None
+        prm = torch.tensor([[W.ensemble_params(i, seed)["mach"], np.log10(W.ensemble_params(i, seed)["reynolds"])]
+                            for i in range(n)], dtype=torch.float32)
+        return parts, cfg, prm
+
+    t0 = time.time()
+    parts, cfg, prm = make(args.train_cases, 1234)
+    batch = B.BatchedFVM(parts, cfg, device="cuda")
+    batch.t_solver.update_cfl_dt(0.5)
+    traj = record_trajectory(batch, steps=400, spinup=200)
+    model = CorrectorModel(batch, prm, k=8, seed=0, lr=1e-3)
+    torch.cuda.synchronize()
+    t1 = time.time()
+    hist = train(model, traj, iters=args.iters, log_every=max(1, args.iters // 10))
+    torch.cuda.synchronize()
+    t_train = time.time() - t1
+    del traj
+    torch.cuda.empty_cache()
+
+    eparts, ecfg, eprm = make(args.eval_cases, 9000)
+    plain = B.BatchedFVM(eparts, ecfg, device="cuda")
+    corr = B.BatchedFVM(eparts, ecfg, device="cuda")
+    for b in (plain, corr):
+        b.t_solver.update_cfl_dt(0.5)
+        b.t_solver.step(200)
+    emodel = CorrectorModel(corr, eprm, like=model)
+    ro = CheckedRollout(emodel)
+    stream = torch.cuda.current_stream()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    e[0].record(stream)
+    plain.t_solver.step(8 * args.windows)
+    e[1].record(stream)
+    e[2].record(stream)
+    for _ in range(args.windows):
+        ro.window()
+    e[3].record(stream)
+    torch.cuda.synchronize()
+    ms_plain, ms_corr = e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3])
+    err = []
+    for c in range(args.eval_cases):
+        a = corr.case_state(c).double()
+        r = plain.case_state(c).double()
+        err.append(float(((a - r).norm() / r.norm()).item()))
+    out = {"metric": "sim-time/s corrector+fallback over plain FVM", "value": ms_plain / ms_corr, "unit": "x",
+           "higher_is_better": True, "n_gpus": 1, "dtype": "bf16 GEMM / f32 state", "data": "synthetic",
+           "config": {"workload": "corrector_2d_k8", "train_cases": args.train_cases, "eval_cases": args.eval_cases,
+                      "iters": args.iters, "windows": args.windows, "fvm": "SSP-RK3, fixed per-case dt (CFL 0.5)",
+                      "net": "4 message-passing layers, width 64, SiLU, tcgen05 BF16 GEMMs"},
+           "accept_rate": ro.accepted / max(ro.windows, 1),
+           "rel_l2_vs_plain": {"max": max(err), "mean": float(np.mean(err))},
+           "ms_plain": ms_plain, "ms_corrected": ms_corr,
+           "train": {"loss_first": hist[0][1], "loss_last": hist[-1][1], "seconds": t_train,
+                     "setup_seconds": t1 - t0}}
     print(json.dumps(out))
 
 

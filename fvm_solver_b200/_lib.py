@@ -79,6 +79,17 @@ _SIGS = [
     ("fvm_set_block_size", ct.c_int, [ct.c_int32, ct.c_int32]),
     ("fvm_gemm_bf16", ct.c_int, [_P, ct.c_int64, _P, ct.c_int64, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32,
                                  _P, _P, ct.c_int64, _P, _P, ct.c_int64, _P, ct.c_int32, _P, _P]),
+    ("fvm_mp_gather", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, ct.c_int32, _P, _P]),
+    ("fvm_mp_scatter_back", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, ct.c_int32, _P, _P, _P]),
+    ("fvm_silu_back", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, _P, _P, ct.c_int64, _P, _P]),
+    ("fvm_transpose_bf16", ct.c_int, [_P, ct.c_int32, ct.c_int32, ct.c_int64, _P, ct.c_int64, _P]),
+    ("fvm_decoder", ct.c_int, [_P, _P, _P, ct.c_int32, ct.c_int32, ct.c_int32, _P, _P]),
+    ("fvm_decoder_back", ct.c_int, [_P, _P, _P, ct.c_int32, ct.c_int32, ct.c_int32, _P, _P, _P, _P]),
+    ("fvm_mse", ct.c_int, [_P, _P, ct.c_int64, _P, _P, _P]),
+    ("fvm_adam", ct.c_int, [_P, _P, _P, _P, ct.c_int64, ct.c_float, ct.c_float, ct.c_float, ct.c_float,
+                            ct.c_int32, _P, _P, ct.c_int32, ct.c_int32, _P]),
+    ("fvm_corrector_features", ct.c_int, [_P, ct.c_int32, ct.c_int32, _P, _P, _P, ct.c_int32, _P, ct.c_int32, _P]),
+    ("fvm_apply_increment", ct.c_int, [_P, _P, _P, ct.c_int32, ct.c_int32, _P, _P]),
     ("fvm_profile_stop", ct.c_int, []),
     ("fvm_profile_read", ct.c_int, [ct.c_int32, _P, _P]),
 ]
@@ -98,12 +109,26 @@ def load(require_cuda: bool = True):
         if not os.path.exists(LIB_PATH):
             raise RuntimeError(f"CUDA library {LIB_PATH} is missing; run `python -m fvm_solver_b200.build`")
         lib = ct.CDLL(LIB_PATH)
+        fns = {}
         for name, res, args in _SIGS:
             fn = getattr(lib, name)
             fn.restype = res
             fn.argtypes = args
-        _lib = lib
+            fns[name] = fn
+        _lib = _Bound(fns)
     return _lib
+
+
+class _Bound:
+    """The library's functions, each with its declared signature.  Looking up a function that has
+    no signature here raises, so no call can fall back to ctypes' default int conversion (which
+    would truncate 64-bit device pointers)."""
+
+    def __init__(self, fns: dict):
+        self.__dict__.update(fns)
+
+    def __getattr__(self, name):
+        raise AttributeError(f"{name} has no declared signature in fvm_solver_b200._lib")
 
 
 def check(rc: int, what: str):

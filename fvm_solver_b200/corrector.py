@@ -207,12 +207,15 @@ class CorrectorNet:
 class CorrectorModel:
     """Network + the normalisation and geometry of one batch of meshes."""
 
-    def __init__(self, batch, case_params: torch.Tensor, k: int = 8, seed: int = 0, lr: float = 1e-3):
+    def __init__(self, batch, case_params: torch.Tensor, k: int = 8, seed: int = 0, lr: float = 1e-3,
+                 like: "CorrectorModel | None" = None):
+        """``like``: reuse another model's trained network and normalisation on this batch of meshes
+        (the weights are mesh-independent; neighbours and geometry are this batch's)."""
         self.batch = batch
-        self.k = k
+        self.k = k if like is None else like.k
         C = batch.n_comp
         kt = batch.kt
-        self.net = CorrectorNet(C, device=batch.device, seed=seed, lr=lr)
+        self.net = CorrectorNet(C, device=batch.device, seed=seed, lr=lr) if like is None else like.net
         self.nbr = neighbour_table(kt).to(batch.device)
         cp = case_params[batch.dev.case["cell_case"].long().cpu()]
         self.geo = geometry_features(kt, cp).to(batch.device)
@@ -221,6 +224,8 @@ class CorrectorModel:
         self.mean = torch.zeros(C, device=batch.device)
         self.inv_std = torch.ones(C, device=batch.device)
         self.scale = torch.ones(C, device=batch.device)
+        if like is not None:
+            self.mean, self.inv_std, self.scale = like.mean, like.inv_std, like.scale
 
     def set_normalisation(self, states: torch.Tensor, increments: torch.Tensor):
         self.mean = states.mean(dim=(0, 1)).float().contiguous()

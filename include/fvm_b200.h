@@ -234,6 +234,37 @@ int fvm_gemm_bf16(const void *A, int64_t lda, const void *B, int64_t ldb, int32_
                   int32_t k_splits, const float *bias, const float *resid, int64_t ldr, float *Df, void *Db,
                   int64_t ldd, float *preact, int32_t act, int32_t *err, void *stream);
 
+/* Corrector kernels (no reference counterpart).  Activations are bf16 [N][W] (W % 8 == 0, rows
+ * 16-byte aligned); nbr is an int32 [N][KN] neighbour table (-1 = none, adjacency symmetric). */
+/* out[i] = [h_i, mean_{j in nbr(i)} h_j]  (bf16 [N][2W]). */
+int fvm_mp_gather(const void *h, const int32_t *nbr, int32_t N, int32_t W, int32_t KN, void *out, void *stream);
+/* dh_out[i] = dh_in[i] + dA[i][:W] + sum_{j in nbr(i)} dA[j][W:] / deg(j)  (fp32; dh_in may be NULL). */
+int fvm_mp_scatter_back(const float *dA, const int32_t *nbr, int32_t N, int32_t W, int32_t KN, const float *dh_in,
+                        float *dh_out, void *stream);
+/* dZ = dh * SiLU'(Z) -> bf16 [N][W] and (if dZT) bf16 [W][ldT]; db[c] += sum_i dZ[i][c] (if db). */
+int fvm_silu_back(const float *dh, const float *Z, int32_t N, int32_t W, void *dZ, void *dZT, int64_t ldT, float *db,
+                  void *stream);
+/* dst[c][r] = src[r][c] for a bf16 [R][Cc] matrix (leading dimensions lds, ldd). */
+int fvm_transpose_bf16(const void *src, int32_t R, int32_t Cc, int64_t lds, void *dst, int64_t ldd, void *stream);
+/* out[i][o] = h[i] . Wo[o] + bo[o] for O <= 8 outputs (h bf16, Wo fp32 [O][W]). */
+int fvm_decoder(const void *h, const float *Wo, const float *bo, int32_t N, int32_t W, int32_t O, float *out,
+                void *stream);
+/* Decoder backward: dh = dOut Wo; dWo += dOut^T h; dbo += column sums of dOut. */
+int fvm_decoder_back(const void *h, const float *Wo, const float *dOut, int32_t N, int32_t W, int32_t O, float *dh,
+                     float *dWo, float *dbo, void *stream);
+/* loss[0] += mean((pred - tgt)^2) over n_elem values (FP64); dpred = 2 (pred - tgt) / n_elem. */
+int fvm_mse(const float *pred, const float *tgt, int64_t n_elem, double *loss, float *dpred, void *stream);
+/* Adam on fp32 master weights p with gradient g (zeroed afterwards), moments m, v; step >= 1.
+ * Refreshes the bf16 copy pb (if not NULL) and its [cols][rows] transpose pbT (if not NULL). */
+int fvm_adam(float *p, float *g, float *m, float *v, int64_t n, float lr, float beta1, float beta2, float eps,
+             int32_t step, void *pb, void *pbT, int32_t rows, int32_t cols, void *stream);
+/* X[i] = [(U_i - mean) * inv_std (C values), geo[i] (G values), zeros] as bf16 [N][XW]. */
+int fvm_corrector_features(const float *state, int32_t N, int32_t C, const float *mean, const float *inv_std,
+                           const float *geo, int32_t G, void *X, int32_t XW, void *stream);
+/* new_state = state + scale[c] * out (fp32 [N][C]). */
+int fvm_apply_increment(const float *state, const float *out, const float *scale, int32_t N, int32_t C,
+                        float *new_state, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
