@@ -186,8 +186,9 @@ class OracleResidual:
             self._bc_characteristic(Uf, U[g["cells"]], g)
         return Uf
 
-    def forward(self, U, grads_prev=None):
-        """Returns (dU/dt [N, C] in conserved variables, limited cell gradients [N, dim, C])."""
+    def forward(self, U, grads_prev=None, return_faces=False):
+        """Returns (dU/dt [N, C] in conserved variables, limited cell gradients [N, dim, C]); with
+        ``return_faces`` also the facet values of both sides [F, 2, C] (``U_face_all``)."""
         U = np.asarray(U, dtype=self.dt)
         d, C, N, F, K = self.dim, self.C, self.N, self.F, self.K
         # 1-2. boundary facet values; cell + boundary value table
@@ -259,6 +260,8 @@ class OracleResidual:
                                    a_oth * (Q[:, 0] - Q[:, 1])], axis=1) * self.fsize
         flux = flux + kt
         # divergence (fvm_equation.py:428-435)
+        if return_faces:
+            return ell_spmm(*self.Fm, flux), grads, Ufa
         return ell_spmm(*self.Fm, flux), grads
 
 

@@ -7,6 +7,8 @@ Tolerances (written per check):
 * ELL operators vs torch sparse (FP32): rel-L2 <= 1e-6.
 The FP64 error of every result is also checked to stay within the reference's own FP32 error x 10.
 """
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -250,3 +252,19 @@ def test_checkpoint_restart_bitwise(tmp_path, name, extra):
     eq3.t_solver.step(3)
     assert torch.equal(eq3.cells.state, eq.cells.state)
     assert torch.equal(eq3.t_solver.dt, eq.t_solver.dt)
+
+
+def test_saver_boundary_values_vs_oracle(tmp_path):
+    """Saved boundary-facet values = mean of the facet's two sides, as the oracle computes them."""
+    from fvm_solver_b200 import trajectory_io as tio
+    from oracle import fvm_oracle as O
+    g, eq, T, cfg = make_equation("c2d")
+    prims = torch.from_numpy(g["prim0"]).cuda()
+    got = tio.boundary_face_values(eq, prims).cpu().numpy()
+    _, _, faces = O.OracleResidual(T, cfg, np.float32).forward(g["prim0"], return_faces=True)
+    want = faces[T.bc_locations.numpy().astype(np.int64)].mean(axis=1)
+    assert rel_l2(got, want) < 1e-5
+    saver = tio.TrajectorySaver(eq, str(tmp_path))
+    path = saver.save(0.5)
+    t, cell, bc = tio.load_step(path)
+    assert bc.shape == (T.n_bc, 4) and os.path.exists(str(tmp_path / "mesh_props.npz"))
