@@ -77,6 +77,7 @@ _SIGS = [
     ("fvm_residual_noalloc", ct.c_int, [ct.POINTER(Mesh), ct.POINTER(Physics), _P, _P, _P, _P, _P]),
     ("fvm_profile_start", ct.c_int, [ct.c_int32]),
     ("fvm_set_block_size", ct.c_int, [ct.c_int32, ct.c_int32]),
+    ("fvm_set_prefetch", ct.c_int, [ct.c_int32, ct.c_int32]),
     ("fvm_gemm_bf16", ct.c_int, [_P, ct.c_int64, _P, ct.c_int64, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32,
                                  _P, _P, ct.c_int64, _P, _P, ct.c_int64, _P, ct.c_int32, _P, _P]),
     ("fvm_mp_gather", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, ct.c_int32, _P, _P]),

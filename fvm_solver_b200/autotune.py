@@ -1,12 +1,14 @@
 """Launch-configuration autotuner for the residual kernels.
 
-The cell, facet and divergence kernels (one thread per cell / facet) run at any block size; which
-one is fastest depends on the mesh (cell count, boundary fraction, batched or not) because it sets
-how many warps each SM keeps in flight against the gather latency.  ``autotune`` times each
-candidate block size on the caller's own mesh -- residual evaluations bracketed by the library's
-per-launch CUDA events -- keeps the fastest per kernel, and installs it with
-``fvm_set_block_size``.  Results do not change with the block size (every thread's arithmetic is
-the same), only the time does.  Choices are cached per (dim, cell-count bucket, batch size).
+The cell, facet and divergence kernels (one thread per cell / facet) run at any block size, with or
+without the L2 prefetch of their record streams one wave of blocks ahead; which configuration is
+fastest depends on the mesh (cell count, boundary fraction, batched or not) because it sets how
+many warps each SM keeps in flight against the gather latency and whether the records still come
+from DRAM when a block reads them.  ``autotune`` times each candidate (block size, prefetch) on the
+caller's own mesh -- residual evaluations bracketed by the library's per-launch CUDA events --
+keeps the fastest per kernel, and installs it with ``fvm_set_block_size`` / ``fvm_set_prefetch``.
+Results do not change with either (every thread's arithmetic is the same), only the time does.
+Choices are cached per (dim, cell-count bucket, batch size).
 """
 from __future__ import annotations
 
@@ -19,6 +21,7 @@ import torch
 from . import _lib
 
 CANDIDATES = (64, 128, 256, 512)
+PREFETCH = (0, 1)           # off, one wave of resident blocks ahead
 KERNELS = {3: "cell", 4: "face", 5: "div_stage"}
 _cache: dict = {}
 
@@ -31,6 +34,16 @@ def _key(eq) -> tuple:
 def set_block_size(kernel: str, threads: int):
     kid = {v: k for k, v in KERNELS.items()}[kernel]
     _lib.check(_lib.load().fvm_set_block_size(kid, int(threads)), "fvm_set_block_size")
+
+
+def set_prefetch(kernel: str, blocks_ahead: int):
+    kid = {v: k for k, v in KERNELS.items()}[kernel]
+    _lib.check(_lib.load().fvm_set_prefetch(kid, int(blocks_ahead)), "fvm_set_prefetch")
+
+
+def _install(kernel: str, cfg: tuple):
+    set_block_size(kernel, cfg[0])
+    set_prefetch(kernel, cfg[1])
 
 
 def _time_residual(eq, prims, out, reps: int) -> dict:
@@ -51,30 +64,34 @@ def _time_residual(eq, prims, out, reps: int) -> dict:
     return {KERNELS[k]: float(ms[ids == k].mean()) for k in KERNELS if np.any(ids == k)}
 
 
-def autotune(eq, reps: int = 5, candidates=CANDIDATES, use_cache: bool = True) -> dict:
-    """Pick and install the fastest block size per kernel for ``eq`` (FVMEquation or BatchedFVM).
+def autotune(eq, reps: int = 5, candidates=CANDIDATES, prefetch=PREFETCH, use_cache: bool = True) -> dict:
+    """Pick and install the fastest (block size, prefetch) per kernel for ``eq`` (FVMEquation or
+    BatchedFVM).
 
     The carried limited gradients are saved and restored, so the tuning runs leave the solver's
-    state untouched.  Returns ``{kernel: {"threads": best, "ms": {threads: mean ms}}}``.
+    state untouched.  Returns ``{kernel: {"threads": bs, "prefetch": pf, "ms": {(bs, pf): mean ms}}}``.
     """
     key = _key(eq)
     if use_cache and key in _cache:
         for k, v in _cache[key].items():
-            set_block_size(k, v["threads"])
+            _install(k, (v["threads"], v["prefetch"]))
         return _cache[key]
     prims = eq.cells.get_values()[0].contiguous()
     out = torch.empty_like(prims)
     g_save, f_save = eq.grads.clone(), eq.has_grads.clone()
     timings = {k: {} for k in KERNELS.values()}
     for bs in candidates:
-        for k in KERNELS.values():
-            set_block_size(k, bs)
-        _time_residual(eq, prims, out, 1)               # warm-up at this configuration
-        for k, ms in _time_residual(eq, prims, out, reps).items():
-            timings[k][bs] = ms
-    best = {k: {"threads": min(t, key=t.get), "ms": t} for k, t in timings.items()}
-    for k, v in best.items():
-        set_block_size(k, v["threads"])
+        for pf in prefetch:
+            for k in KERNELS.values():
+                _install(k, (bs, pf))
+            _time_residual(eq, prims, out, 1)               # warm-up at this configuration
+            for k, ms in _time_residual(eq, prims, out, reps).items():
+                timings[k][(bs, pf)] = ms
+    best = {}
+    for k, t in timings.items():
+        cfg = min(t, key=t.get)
+        best[k] = {"threads": cfg[0], "prefetch": cfg[1], "ms": t}
+        _install(k, cfg)
     eq.grads.copy_(g_save)
     eq.has_grads.copy_(f_save)
     torch.cuda.synchronize()
@@ -83,6 +100,6 @@ def autotune(eq, reps: int = 5, candidates=CANDIDATES, use_cache: bool = True) -
 
 
 def reset():
-    """Back to the default block size (256) for every tunable kernel."""
+    """Back to the defaults (256 threads, no prefetch) for every tunable kernel."""
     for k in KERNELS.values():
-        set_block_size(k, 256)
+        _install(k, (256, 0))

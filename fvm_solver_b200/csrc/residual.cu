@@ -21,10 +21,14 @@
 //               reductions for the adaptive step size (integrators.py:42-62), the CFL time step and
 //               the conservation sums.
 //
-// All kernels are memory-bound gathers with one thread per cell or facet.  Every per-cell and
-// per-facet table is one contiguous record, and every gathered row (primitives, limited gradients,
-// fluxes) is padded to a 32-byte multiple (16 bytes for the 4-float rows of 2D), so a record or a
-// gather is a few aligned 256-bit loads and never straddles more 32-byte sectors than it must.  Rebuilding the
+// All kernels are memory-bound gathers.  Every per-cell and per-facet table is one contiguous
+// record, and every gathered row (primitives, limited gradients, fluxes) is padded to a 32-byte
+// multiple (16 bytes for the 4-float rows of 2D), so a record or a gather is a few aligned 256-bit
+// loads and never straddles more 32-byte sectors than it must.  k_cell, k_face and k_div_stage are
+// persistent grid-stride loops over one wave of resident blocks that load the next item's gather
+// indices one iteration ahead: a cell's or facet's gathers then leave together with its record,
+// one dependent memory round trip per item instead of two.  Optionally (autotuned) each block also
+// has the bulk-copy unit prefetch the record tile it will read a wave later into L2.  Rebuilding the
 // facet values in k_face removes the reference's [F, 2, C] facet table (a scattered write plus a
 // read per facet side).
 #include <math.h>
@@ -134,6 +138,36 @@ __device__ __forceinline__ void st_vec(float* p, const float (&v)[N]) {
     }
 }
 __device__ __forceinline__ int as_int(float x) { return __float_as_int(x); }
+
+// L2 prefetch of a contiguous byte range by the bulk-copy (TMA) unit: no shared memory, no
+// completion to wait for.  Address and size must be multiples of 16 bytes.
+__device__ __forceinline__ void l2_prefetch(const void* p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Thread 0 asks for the rows [tile * blockDim, (tile + 1) * blockDim) of a row-major array of
+// `n_rows` rows of `row_floats` floats: the rows a block will read when it reaches `tile`.
+// Issued one wave of blocks ahead, the record streams arrive in L2 while the current wave computes,
+// and the blocks' own loads see L2 latency instead of DRAM latency.  The range is clamped to the
+// array and rounded inward to 16-byte boundaries.
+__device__ __forceinline__ void prefetch_tile(const float* base, int64_t n_rows, int row_floats, int64_t tile) {
+    if (threadIdx.x != 0 || base == nullptr) return;
+    const int64_t first = tile * blockDim.x;
+    if (first >= n_rows) return;
+    const int64_t last = min(first + (int64_t)blockDim.x, n_rows);
+    int64_t b0 = first * row_floats * 4, b1 = last * row_floats * 4;
+    b0 = (b0 + 15) & ~(int64_t)15;
+    b1 &= ~(int64_t)15;
+    if (b1 > b0) l2_prefetch(reinterpret_cast<const char*>(base) + b0, (uint32_t)(b1 - b0));
+}
+
+// The two side codes (first two words) of a facet record.
+__device__ __forceinline__ int2 ld_codes(const float* rec) { return __ldg(reinterpret_cast<const int2*>(rec)); }
+
+// Non-persistent kernels: block b prefetches the rows of block b + ahead (0 = off).
+__device__ __forceinline__ void prefetch_rows(const float* base, int64_t n_rows, int row_floats, int ahead) {
+    if (ahead > 0) prefetch_tile(base, n_rows, row_floats, (int64_t)blockIdx.x + ahead);
+}
 
 // ------------------------------------------------------------------------------------------
 // Slope limiters (limiter.py:29-77).  delta: allowed range, dU: unlimited increment.
@@ -285,76 +319,91 @@ __global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float
 // ------------------------------------------------------------------------------------------
 // k_cell: gradient, limiter, limited gradient.
 // ------------------------------------------------------------------------------------------
+// Persistent grid-stride loop (one wave of resident blocks): each thread loads the next cell's
+// gradient-stencil columns one iteration ahead, so the neighbour gathers of a cell are issued at
+// the top of its iteration together with its record, one memory round trip instead of two.
 template <int DIM>
 __global__ void __launch_bounds__(kMaxBlock) k_cell(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
                                                   const float* __restrict__ bcv, float* __restrict__ grads,
-                                                  int32_t* __restrict__ has_grads) {
+                                                  int32_t* __restrict__ has_grads, int waves) {
     using Ly = L<DIM>;
     constexpr int C = Ly::C, K = Ly::K, KG = Ly::KG, RS = Ly::RS;
     const int N = m.n_cells;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stride = gridDim.x * blockDim.x;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) *has_grads = 1;
-    if (i >= N) return;
-    float rec[Ly::CR];
-    ld_vec<Ly::CR>(m.cell_rec + (int64_t)i * Ly::CR, rec);
-    float U[RS];
-    ld_vec<RS>(prims + (int64_t)i * RS, U);
-    const int nvalid = (as_int(rec[Ly::META]) >> 24) & 31;
-    float g[DIM][C];
+    int cols[KG];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d)
+    for (int k = 0; k < KG; ++k) cols[k] = i < N ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)i * Ly::CR + Ly::GC + k) : 0;
+    for (int64_t tile = blockIdx.x; i < N; i += stride, tile += gridDim.x) {
+        if (waves > 0) prefetch_tile(m.cell_rec, N, Ly::CR, tile + (int64_t)waves * gridDim.x);
+        float X[KG][RS];
 #pragma unroll
-        for (int c = 0; c < C; ++c) g[d][c] = 0.f;
-    float up[C], lo[C];
-#pragma unroll
-    for (int c = 0; c < C; ++c) up[c] = lo[c] = U[c];
-#pragma unroll
-    for (int k = 0; k < KG; ++k) {
-        const int col = as_int(rec[Ly::GC + k]);
-        float X[RS];
-        if (col < N) ld_vec<RS>(prims + (int64_t)col * RS, X);
-        else ld_vec_cg<RS>(bcv + (int64_t)(col - N) * RS, X);
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            const float w = rec[Ly::GV + d * KG + k];
-#pragma unroll
-            for (int c = 0; c < C; ++c) g[d][c] = fmaf(w, X[c], g[d][c]);
+        for (int k = 0; k < KG; ++k) {
+            if (cols[k] < N) ld_vec<RS>(prims + (int64_t)cols[k] * RS, X[k]);
+            else ld_vec_cg<RS>(bcv + (int64_t)(cols[k] - N) * RS, X[k]);
         }
-        if (k < nvalid) {
+        float U[RS];
+        ld_vec<RS>(prims + (int64_t)i * RS, U);
+        float rec[Ly::CR];
+        ld_vec<Ly::CR>(m.cell_rec + (int64_t)i * Ly::CR, rec);
+        const int inext = i + stride;
 #pragma unroll
-            for (int c = 0; c < C; ++c) {
-                up[c] = fmaxf(up[c], X[c]);
-                lo[c] = fminf(lo[c], X[c]);
+        for (int k = 0; k < KG; ++k)
+            cols[k] = inext < N ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)inext * Ly::CR + Ly::GC + k) : 0;
+        const int nvalid = (as_int(rec[Ly::META]) >> 24) & 31;
+        float g[DIM][C];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+#pragma unroll
+            for (int c = 0; c < C; ++c) g[d][c] = 0.f;
+        float up[C], lo[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) up[c] = lo[c] = U[c];
+#pragma unroll
+        for (int k = 0; k < KG; ++k) {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                const float w = rec[Ly::GV + d * KG + k];
+#pragma unroll
+                for (int c = 0; c < C; ++c) g[d][c] = fmaf(w, X[k][c], g[d][c]);
+            }
+            if (k < nvalid) {
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    up[c] = fmaxf(up[c], X[k][c]);
+                    lo[c] = fminf(lo[c], X[k][c]);
+                }
             }
         }
-    }
-    const float eps = rec[Ly::EPS];
-    float phim[C];
-#pragma unroll
-    for (int c = 0; c < C; ++c) {
-        up[c] -= U[c];
-        lo[c] -= U[c];
-        phim[c] = INFINITY;
-    }
-#pragma unroll
-    for (int j = 0; j < K; ++j) {
+        const float eps = rec[Ly::EPS];
+        float phim[C];
 #pragma unroll
         for (int c = 0; c < C; ++c) {
-            float du = g[0][c] * rec[Ly::DISP + j * DIM];
-#pragma unroll
-            for (int d = 1; d < DIM; ++d) du = fmaf(g[d][c], rec[Ly::DISP + j * DIM + d], du);
-            const float num = du > 0.f ? up[c] : lo[c];
-            phim[c] = fminf(phim[c], limiter_phi(p.lim_p, num, du, eps));
+            up[c] -= U[c];
+            lo[c] -= U[c];
+            phim[c] = INFINITY;
         }
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                float du = g[0][c] * rec[Ly::DISP + j * DIM];
+#pragma unroll
+                for (int d = 1; d < DIM; ++d) du = fmaf(g[d][c], rec[Ly::DISP + j * DIM + d], du);
+                const float num = du > 0.f ? up[c] : lo[c];
+                phim[c] = fminf(phim[c], limiter_phi(p.lim_p, num, du, eps));
+            }
+        }
+        float go[Ly::GS];
+#pragma unroll
+        for (int q = 0; q < Ly::GS; ++q) go[q] = 0.f;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+#pragma unroll
+            for (int c = 0; c < C; ++c) go[Ly::gi(d, c)] = g[d][c] * phim[c];
+        st_vec<Ly::GS>(grads + (int64_t)i * Ly::GS, go);
     }
-    float go[Ly::GS];
-#pragma unroll
-    for (int q = 0; q < Ly::GS; ++q) go[q] = 0.f;
-#pragma unroll
-    for (int d = 0; d < DIM; ++d)
-#pragma unroll
-        for (int c = 0; c < C; ++c) go[Ly::gi(d, c)] = g[d][c] * phim[c];
-    st_vec<Ly::GS>(grads + (int64_t)i * Ly::GS, go);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -363,21 +412,17 @@ __global__ void __launch_bounds__(kMaxBlock) k_cell(fvm_mesh_t m, Phys p, const 
 template <int DIM>
 __global__ void __launch_bounds__(kMaxBlock) k_face(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
                                                   const float* __restrict__ bcv,
-                                                  const float* __restrict__ grads, float* __restrict__ flux) {
+                                                  const float* __restrict__ grads, float* __restrict__ flux,
+                                                  int waves) {
     using Ly = L<DIM>;
     constexpr int C = Ly::C, NG = DIM + 1, RS = Ly::RS, GS = Ly::GS;
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= m.n_facets) return;
-    float rec[Ly::FR];
-    ld_vec<Ly::FR>(m.face_rec + (int64_t)f * Ly::FR, rec);
-    const int ca = as_int(rec[Ly::FA]), cb = as_int(rec[Ly::FB]);
-    const float size = rec[Ly::SIZE];
-    float n[DIM], nh[DIM];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-        n[d] = rec[Ly::NRM + d];
-        nh[d] = n[d] / size;
-    }
+    const int nF = m.n_facets;
+    const int stride = gridDim.x * blockDim.x;
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    int2 nxt = f < nF ? ld_codes(m.face_rec + (int64_t)f * Ly::FR) : make_int2(0, 0);
+    for (int64_t tile = blockIdx.x; f < nF; f += stride, tile += gridDim.x) {
+    if (waves > 0) prefetch_tile(m.face_rec, nF, Ly::FR, tile + (int64_t)waves * gridDim.x);
+    const int ca = nxt.x, cb = nxt.y;
     // Both sides: primitives and limited gradient of the cell(s); a boundary side (code < 0) takes
     // the boundary value, and its gradient is the interior cell's (facet_process.py:364-368).
     const int cell0 = ca >= 0 ? ca : cb;
@@ -387,6 +432,16 @@ __global__ void __launch_bounds__(kMaxBlock) k_face(fvm_mesh_t m, Phys p, const 
     ld_vec<RS>(prims + (int64_t)cell1 * RS, P1);
     ld_vec_cg<GS>(grads + (int64_t)cell0 * GS, G0);
     ld_vec_cg<GS>(grads + (int64_t)cell1 * GS, G1);
+    float rec[Ly::FR];
+    ld_vec<Ly::FR>(m.face_rec + (int64_t)f * Ly::FR, rec);
+    if (f + stride < nF) nxt = ld_codes(m.face_rec + (int64_t)(f + stride) * Ly::FR);
+    const float size = rec[Ly::SIZE];
+    float n[DIM], nh[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        n[d] = rec[Ly::NRM + d];
+        nh[d] = n[d] / size;
+    }
     float UL[RS], UR[RS];
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
@@ -537,6 +592,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_face(fvm_mesh_t m, Phys p, const 
     F[DIM] += 0.5f * (a_oth * (rho[0] - rho[1])) * size;
     F[DIM + 1] += 0.5f * (a_oth * (Q[0] - Q[1])) * size;
     st_vec<RS>(flux + (int64_t)f * RS, F);
+    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -634,74 +690,136 @@ __device__ __forceinline__ void reduce_cons_cfl(const fvm_mesh_t& m, const Phys&
     }
 }
 
+// Batched meshes: per-case reductions of one item per lane, warp-level when the warp's live lanes
+// share a case, per-lane atomics otherwise (all lanes of the warp must call it).
 template <int DIM>
+__device__ __forceinline__ void reduce_batched_item(const fvm_mesh_t& m, const Phys& p, const float* U, bool live,
+                                                    int i, int cse, bool want_cons, bool want_cfl, double* red) {
+    constexpr int C = DIM + 2;
+    const int lane = threadIdx.x & 31;
+    const int c0 = __shfl_sync(0xffffffffu, cse, 0);
+    const bool uniform = __all_sync(0xffffffffu, !live || cse == c0);
+    double* slot = red + FVM_RED_DOUBLES + 8 * cse;
+    if (want_cfl) {
+        double sp = live ? cfl_speed<DIM>(m, p, U, i) : 0.0;
+        if (uniform) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sp = fmax(sp, __shfl_down_sync(0xffffffffu, sp, o));
+            if (lane == 0 && sp > 0.0) atomic_max_pos(red + FVM_RED_DOUBLES + 8 * c0, sp);
+        } else if (live) {
+            atomic_max_pos(slot, sp);
+        }
+    }
+    if (want_cons) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            double v = live ? __ldg(m.volumes + i) * (double)U[c] : 0.0;
+            if (uniform) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                if (lane == 0) atomicAdd(red + FVM_RED_DOUBLES + 8 * c0 + 1 + c, v);
+            } else if (live) {
+                atomicAdd(slot + 1 + c, v);
+            }
+        }
+    }
+}
+
+// What one k_div_stage launch does after the divergence.
+enum DivMode { DIV_RESIDUAL = 0, DIV_STAGE = 1, DIV_FINAL = 2, DIV_FINAL_ADAPT = 3 };
+
+// Persistent grid-stride loop, warp-uniform (every lane of a warp runs the same iterations, so the
+// batched reductions may shuffle): each thread loads the next cell's divergence record one iteration
+// ahead, so the flux gathers of a cell start at the top of its iteration.  Single-mesh reductions
+// are accumulated per thread and combined once per block after the loop.
+template <int DIM, int MODE>
 __global__ void __launch_bounds__(kMaxBlock) k_div_stage(fvm_mesh_t m, Phys p, const float* __restrict__ flux,
                                                        StageArgs a, float* __restrict__ state,
                                                        float* __restrict__ prims, float* __restrict__ kbuf,
                                                        const float* __restrict__ dt,
                                                        double* __restrict__ red,
-                                                       float* __restrict__ dudt) {
+                                                       float* __restrict__ dudt, int waves) {
     using Ly = L<DIM>;
     constexpr int C = Ly::C, RS = Ly::RS;
+    constexpr bool FINAL = MODE >= DIV_FINAL, ADAPT = MODE == DIV_FINAL_ADAPT;
     const int N = m.n_cells;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i < N;
-    float r[C];
+    const int stride = gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const bool do_cons = FINAL && a.cons, do_cfl = FINAL && a.cfl;
+    double cons_acc[C], ad_acc[ADAPT ? 3 * C : 1], cfl_acc = 0.0;
 #pragma unroll
-    for (int c = 0; c < C; ++c) r[c] = 0.f;
-    if (live) {
-        float rec[Ly::DR];
-        ld_vec<Ly::DR>(m.div_rec + (int64_t)i * Ly::DR, rec);
-        for (int k = 0; k < m.kf; ++k) {
-            const float w = rec[k];
-            float Fk[RS];
-            ld_vec_cg<RS>(flux + (int64_t)as_int(rec[Ly::K + k]) * RS, Fk);
+    for (int c = 0; c < C; ++c) cons_acc[c] = 0.0;
 #pragma unroll
-            for (int c = 0; c < C; ++c) r[c] = fmaf(w, Fk[c], r[c]);
+    for (int c = 0; c < (ADAPT ? 3 * C : 1); ++c) ad_acc[c] = 0.0;
+    int i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+    float nxt[Ly::DR];
+    if (i0 + lane < N) ld_vec<Ly::DR>(m.div_rec + (int64_t)(i0 + lane) * Ly::DR, nxt);
+    else
+#pragma unroll
+        for (int q = 0; q < Ly::DR; ++q) nxt[q] = 0.f;
+    for (int64_t tile = blockIdx.x; i0 < N; i0 += stride, tile += gridDim.x) {
+        if (waves > 0) {
+            prefetch_tile(m.div_rec, N, Ly::DR, tile + (int64_t)waves * gridDim.x);
+            if (MODE != DIV_RESIDUAL) prefetch_tile(state, N, C, tile + (int64_t)waves * gridDim.x);
         }
-    }
-    if (dudt) {  // residual only
-        if (live) store_state<C>(dudt + (int64_t)i * C, r);
-        return;
-    }
-    const int cse = (m.n_cases > 0 && live) ? __ldg(m.cell_case + i) : 0;
-    const float h = dt[cse];
-    float kk[C], U0[C], inc[C], U[C];
+        const int i = i0 + lane;
+        const bool live = i < N;
+        float rec[Ly::DR];
 #pragma unroll
-    for (int c = 0; c < C; ++c) {
-        kk[c] = h * r[c];
-        inc[c] = 0.f;
-        U0[c] = U[c] = 0.f;
-    }
-    if (live) {
-        if (a.store_k) store_state<C>(kbuf + ((int64_t)a.s * N + i) * C, kk);
-        load_state<C>(state + (int64_t)i * C, U0);
-        for (int t = 0; t < a.n_terms; ++t) {
-            float kt[C];
-            if (a.idx[t] == a.s) {
+        for (int q = 0; q < Ly::DR; ++q) rec[q] = nxt[q];
+        float r[C];
 #pragma unroll
-                for (int c = 0; c < C; ++c) kt[c] = kk[c];
-            } else {
-                load_state<C>(kbuf + ((int64_t)a.idx[t] * N + i) * C, kt);
+        for (int c = 0; c < C; ++c) r[c] = 0.f;
+        if (live) {
+#pragma unroll
+            for (int k = 0; k < Ly::K; ++k) {
+                if (k < m.kf) {
+                    const float w = rec[k];
+                    float Fk[RS];
+                    ld_vec_cg<RS>(flux + (int64_t)as_int(rec[Ly::K + k]) * RS, Fk);
+#pragma unroll
+                    for (int c = 0; c < C; ++c) r[c] = fmaf(w, Fk[c], r[c]);
+                }
+            }
+        }
+        if (i + stride < N) ld_vec<Ly::DR>(m.div_rec + (int64_t)(i + stride) * Ly::DR, nxt);
+        if (MODE == DIV_RESIDUAL) {
+            if (live) store_state<C>(dudt + (int64_t)i * C, r);
+            continue;
+        }
+        const int cse = (m.n_cases > 0 && live) ? __ldg(m.cell_case + i) : 0;
+        const float h = dt[cse];
+        float kk[C], U0[C], inc[C], U[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            kk[c] = h * r[c];
+            inc[c] = 0.f;
+            U0[c] = U[c] = 0.f;
+        }
+        if (live) {
+            if (a.store_k) store_state<C>(kbuf + ((int64_t)a.s * N + i) * C, kk);
+            load_state<C>(state + (int64_t)i * C, U0);
+            for (int t = 0; t < a.n_terms; ++t) {
+                float kt[C];
+                if (a.idx[t] == a.s) {
+#pragma unroll
+                    for (int c = 0; c < C; ++c) kt[c] = kk[c];
+                } else {
+                    load_state<C>(kbuf + ((int64_t)a.idx[t] * N + i) * C, kt);
+                }
+#pragma unroll
+                for (int c = 0; c < C; ++c) inc[c] = fmaf(a.coef[t], kt[c], inc[c]);
             }
 #pragma unroll
-            for (int c = 0; c < C; ++c) inc[c] = fmaf(a.coef[t], kt[c], inc[c]);
+            for (int c = 0; c < C; ++c) U[c] = U0[c] + inc[c];
+            if (FINAL) store_state<C>(state + (int64_t)i * C, U);
+            float P[RS];
+            state_to_prim<C, RS>(U, p.inv_Cv, P);
+            st_vec<RS>(prims + (int64_t)i * RS, P);
         }
-#pragma unroll
-        for (int c = 0; c < C; ++c) U[c] = U0[c] + inc[c];
-        if (a.final_) store_state<C>(state + (int64_t)i * C, U);
-        float P[RS];
-        state_to_prim<C, RS>(U, p.inv_Cv, P);
-        st_vec<RS>(prims + (int64_t)i * RS, P);
-    }
-    if (!a.final_) return;
-    __shared__ double smem[32 * 3 * C];
-    if (a.adaptive) {
-        // Column norms of dU_high - dU_low, dU_high and U0 (integrators.py:54), in FP64.
-        double v[3 * C];
-#pragma unroll
-        for (int c = 0; c < 3 * C; ++c) v[c] = 0.0;
-        if (live) {
+        if (!FINAL) continue;
+        if (ADAPT && live) {
+            // Column norms of dU_high - dU_low, dU_high and U0 (integrators.py:54), in FP64.
             float lo[C];
 #pragma unroll
             for (int c = 0; c < C; ++c) lo[c] = 0.f;
@@ -717,19 +835,40 @@ __global__ void __launch_bounds__(kMaxBlock) k_div_stage(fvm_mesh_t m, Phys p, c
                 for (int c = 0; c < C; ++c) lo[c] = fmaf(a.coef_lo[t], kt[c], lo[c]);
             }
 #pragma unroll
-            for (int c = 0; c < C; ++c) {
+            for (int c = 0; c < (ADAPT ? C : 0); ++c) {
                 const double e = (double)inc[c] - (double)lo[c];
-                v[c] = e * e;
-                v[C + c] = (double)inc[c] * inc[c];
-                v[2 * C + c] = (double)U0[c] * U0[c];
+                ad_acc[c] += e * e;
+                ad_acc[C + c] += (double)inc[c] * inc[c];
+                ad_acc[2 * C + c] += (double)U0[c] * U0[c];
             }
         }
-        block_sum<3 * C>(v, smem);
+        if (m.n_cases > 0) {
+            reduce_batched_item<DIM>(m, p, U, live, i, cse, do_cons, do_cfl, red);
+        } else if (live) {
+            if (do_cons)
+#pragma unroll
+                for (int c = 0; c < C; ++c) cons_acc[c] += __ldg(m.volumes + i) * (double)U[c];
+            if (do_cfl) cfl_acc = fmax(cfl_acc, cfl_speed<DIM>(m, p, U, i));
+        }
+    }
+    if (!FINAL || m.n_cases > 0) return;
+    __shared__ double smem[32 * (ADAPT ? 3 * C : C)];
+    if (ADAPT) {
+        block_sum<ADAPT ? 3 * C : 1>(ad_acc, smem);
         if (threadIdx.x == 0)
-            for (int c = 0; c < 3 * C; ++c) atomicAdd(red + c, v[c]);
+            for (int c = 0; c < 3 * C; ++c) atomicAdd(red + c, ad_acc[c]);
         __syncthreads();
     }
-    reduce_cons_cfl<DIM>(m, p, U, live, cse, a.cons, a.cfl, red, smem);
+    if (do_cons) {
+        block_sum<C>(cons_acc, smem);
+        if (threadIdx.x == 0)
+            for (int c = 0; c < C; ++c) atomicAdd(red + 24 + c, cons_acc[c]);
+        __syncthreads();
+    }
+    if (do_cfl) {
+        const double sp = block_max(cfl_acc, smem);
+        if (threadIdx.x == 0) atomic_max_pos(red + 16, sp);
+    }
 }
 
 // Step-end bookkeeping: adaptive dt (integrators.py:42-62) or CFL dt, conservation sums.
@@ -877,7 +1016,36 @@ static inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kBlock - 1
 // fvm_set_block_size).  The boundary kernels keep kBlock: their per-block reduction order must not
 // change between single-mesh and batched runs.
 static int g_block_cell = kBlock, g_block_face = kBlock, g_block_div = kBlock;
+// Record prefetch distance in waves of resident blocks per kernel: -1 = default (off: with the
+// persistent kernels' index look-ahead it measured slower on the 2M-tet box), 0 = off.
+static int g_pf_cell = -1, g_pf_face = -1, g_pf_div = -1;
+static inline int waves_of(int setting) { return setting < 0 ? 0 : setting; }
+
+// Resident blocks of `kernel` at `threads` per block over the whole GPU (one wave), cached.
+template <typename Kern>
+static int wave_blocks(Kern kernel, int threads) {
+    struct Entry { const void* k; int threads, dev, blocks; };
+    static Entry cache[128];
+    static int n_cache = 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    for (int e = 0; e < n_cache; ++e)
+        if (cache[e].k == (const void*)kernel && cache[e].threads == threads && cache[e].dev == dev)
+            return cache[e].blocks;
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 0;
+    const int blocks = per_sm * sms;
+    if (n_cache < 128) cache[n_cache++] = Entry{(const void*)kernel, threads, dev, blocks};
+    return blocks;
+}
 static inline unsigned blocks_of(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+// Grid of a persistent grid-stride kernel: one wave of resident blocks, or fewer if n is small.
+static inline unsigned persistent_grid(int64_t n, int threads, int wave) {
+    const unsigned all = blocks_of(n, threads);
+    return wave > 0 && (unsigned)wave < all ? (unsigned)wave : all;
+}
 static inline unsigned fin_blocks(const fvm_mesh_t* m) {
     return m->n_cases > 0 ? (unsigned)((m->n_cases + 127) / 128) : 1u;
 }
@@ -892,10 +1060,35 @@ static int launch_fluxes(const fvm_mesh_t* m, const Phys& p, const float* prims,
         FVM_LAUNCH(KID_BC, s, k_bc<DIM><<<blocks_for(m->n_bc), kBlock, 0, s>>>(*m, p, prims, grads, has_grads,
                                                                                w->bc_vals, w->red));
     }
-    FVM_LAUNCH(KID_CELL, s, k_cell<DIM><<<blocks_of(m->n_cells, g_block_cell), g_block_cell, 0, s>>>(
-                                *m, p, prims, w->bc_vals, grads, has_grads));
-    FVM_LAUNCH(KID_FACE, s, k_face<DIM><<<blocks_of(m->n_facets, g_block_face), g_block_face, 0, s>>>(
-                                *m, p, prims, w->bc_vals, grads, w->flux));
+    const unsigned gc = persistent_grid(m->n_cells, g_block_cell, wave_blocks(k_cell<DIM>, g_block_cell));
+    const unsigned gf = persistent_grid(m->n_facets, g_block_face, wave_blocks(k_face<DIM>, g_block_face));
+    FVM_LAUNCH(KID_CELL, s, k_cell<DIM><<<gc, g_block_cell, 0, s>>>(*m, p, prims, w->bc_vals, grads, has_grads,
+                                                                    waves_of(g_pf_cell)));
+    FVM_LAUNCH(KID_FACE, s, k_face<DIM><<<gf, g_block_face, 0, s>>>(*m, p, prims, w->bc_vals, grads, w->flux,
+                                                                    waves_of(g_pf_face)));
+    return launch_status();
+}
+
+template <int DIM, int MODE>
+static void launch_div_mode(const fvm_mesh_t* m, const Phys& p, const float* flux, const StageArgs& a, float* state,
+                            float* prims, float* kbuf, const float* dt, double* red, float* dudt, cudaStream_t s) {
+    const unsigned grid = persistent_grid(m->n_cells, g_block_div, wave_blocks(k_div_stage<DIM, MODE>, g_block_div));
+    FVM_LAUNCH(KID_DIV_STAGE, s, k_div_stage<DIM, MODE><<<grid, g_block_div, 0, s>>>(
+                                     *m, p, flux, a, state, prims, kbuf, dt, red, dudt, waves_of(g_pf_div)));
+}
+
+// Divergence (+ stage combination): picks the kernel variant for what the launch must do.
+template <int DIM>
+static int launch_div(const fvm_mesh_t* m, const Phys& p, const float* flux, const StageArgs& a, float* state,
+                      float* prims, float* kbuf, const float* dt, double* red, float* dudt, cudaStream_t s) {
+    if (dudt)
+        launch_div_mode<DIM, DIV_RESIDUAL>(m, p, flux, a, state, prims, kbuf, dt, red, dudt, s);
+    else if (!a.final_)
+        launch_div_mode<DIM, DIV_STAGE>(m, p, flux, a, state, prims, kbuf, dt, red, dudt, s);
+    else if (a.adaptive)
+        launch_div_mode<DIM, DIV_FINAL_ADAPT>(m, p, flux, a, state, prims, kbuf, dt, red, dudt, s);
+    else
+        launch_div_mode<DIM, DIV_FINAL>(m, p, flux, a, state, prims, kbuf, dt, red, dudt, s);
     return launch_status();
 }
 
@@ -907,9 +1100,7 @@ static int residual_impl(const fvm_mesh_t* m, const Phys& p, const float* prims_
     int rc = launch_fluxes<DIM>(m, p, w->prims, grads, has_grads, w, s);
     if (rc) return rc;
     StageArgs a{};
-    FVM_LAUNCH(KID_DIV_STAGE, s, k_div_stage<DIM><<<blocks_of(m->n_cells, g_block_div), g_block_div, 0, s>>>(
-                                     *m, p, w->flux, a, nullptr, nullptr, nullptr, nullptr, nullptr, dudt));
-    return launch_status();
+    return launch_div<DIM>(m, p, w->flux, a, nullptr, nullptr, nullptr, nullptr, nullptr, dudt, s);
 }
 
 static StageArgs stage_args(const fvm_tableau_t* tab, int s) {
@@ -953,9 +1144,7 @@ static int stage_impl(const fvm_mesh_t* m, const Phys& p, const fvm_tableau_t* t
     if (rc) return rc;
     StageArgs a = stage_args(tab, s);
     a.cons = a.final_ && b->cons != nullptr;
-    FVM_LAUNCH(KID_DIV_STAGE, st, k_div_stage<DIM><<<blocks_of(m->n_cells, g_block_div), g_block_div, 0, st>>>(
-                                      *m, p, w->flux, a, b->state, b->prims, b->k, b->dt, w->red, nullptr));
-    rc = launch_status();
+    rc = launch_div<DIM>(m, p, w->flux, a, b->state, b->prims, b->k, b->dt, w->red, nullptr, st);
     if (rc) return rc;
     if (a.final_ && (a.adaptive || a.cfl || a.cons)) {
         FVM_LAUNCH(KID_FINALIZE, st,
@@ -984,9 +1173,7 @@ static int multistep_impl(const fvm_mesh_t* m, const Phys& p, int store, int n_t
         a.coef[t] = coef[t];
     }
     a.cons = b->cons != nullptr;
-    FVM_LAUNCH(KID_DIV_STAGE, st, k_div_stage<DIM><<<blocks_of(m->n_cells, g_block_div), g_block_div, 0, st>>>(
-                                      *m, p, w->flux, a, b->state, b->prims, b->k, b->dt, w->red, nullptr));
-    rc = launch_status();
+    rc = launch_div<DIM>(m, p, w->flux, a, b->state, b->prims, b->k, b->dt, w->red, nullptr, st);
     if (rc) return rc;
     if (a.cons) {
         FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(m), 128, 0, st>>>(m->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f,
@@ -1176,6 +1363,16 @@ extern "C" int fvm_residual_noalloc(const fvm_mesh_t* mesh, const fvm_physics_t*
     cudaStream_t s = (cudaStream_t)stream;
     return mesh->dim == 2 ? residual_impl<2>(mesh, p, prims, grads, has_grads, dudt, &w, s)
                           : residual_impl<3>(mesh, p, prims, grads, has_grads, dudt, &w, s);
+}
+
+extern "C" int fvm_set_prefetch(int32_t kernel_id, int32_t waves_ahead) {
+    if (waves_ahead < -1 || waves_ahead > 8) return FVM_E_ARG;
+    switch (kernel_id) {
+        case KID_CELL: g_pf_cell = waves_ahead; return FVM_OK;
+        case KID_FACE: g_pf_face = waves_ahead; return FVM_OK;
+        case KID_DIV_STAGE: g_pf_div = waves_ahead; return FVM_OK;
+        default: return FVM_E_ARG;
+    }
 }
 
 extern "C" int fvm_set_block_size(int32_t kernel_id, int32_t threads) {

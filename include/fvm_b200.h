@@ -151,6 +151,11 @@ int fvm_profile_start(int32_t capacity);
  * of 32 in [64, 512].  Results do not depend on it (each thread's arithmetic is unchanged); the
  * autotuner (fvm_solver_b200/autotune.py) picks it per mesh. */
 int fvm_set_block_size(int32_t kernel_id, int32_t threads);
+/* Record prefetch (no reference counterpart): for the same kernel ids, each block has the bulk-copy
+ * unit prefetch into L2 the records (and, for the stage kernel, the state rows) it or another block
+ * will read `waves_ahead` waves of resident blocks later; -1 = the default (0), 0 = off, at most 8.
+ * Results do not depend on it. */
+int fvm_set_prefetch(int32_t kernel_id, int32_t waves_ahead);
 int fvm_profile_stop(void);
 int fvm_profile_read(int32_t n, int32_t *ids, float *ms);
 

@@ -222,20 +222,25 @@ def test_block_size_invariance_and_autotune():
     outs = []
     try:
         for bs in (64, 128, 256, 512):
-            for k in ("cell", "face", "div_stage"):
-                autotune.set_block_size(k, bs)
-            eq.reset_gradients()
-            outs.append(eq.forward(p))
+            for pf in (0, 1, 3):
+                for k in ("cell", "face", "div_stage"):
+                    autotune.set_block_size(k, bs)
+                    autotune.set_prefetch(k, pf)
+                eq.reset_gradients()
+                outs.append(eq.forward(p))
         assert all(torch.equal(outs[0], o) for o in outs)
         best = autotune.autotune(eq, reps=2, use_cache=False)
         assert set(best) == {"cell", "face", "div_stage"}
         assert all(v["threads"] in autotune.CANDIDATES for v in best.values())
+        assert all(v["prefetch"] in autotune.PREFETCH for v in best.values())
         eq.reset_gradients()
         assert torch.equal(eq.forward(p), outs[0])
     finally:
         autotune.reset()
     with pytest.raises(RuntimeError):
         autotune.set_block_size("cell", 48)
+    with pytest.raises(RuntimeError):
+        autotune.set_prefetch("face", -2)
 
 
 @pytest.mark.parametrize("name,extra", [("Butcher", "RK4"), ("Butcher_adapt", "RK3_SSP4"), ("AB3", "")])
