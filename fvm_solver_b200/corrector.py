@@ -1,14 +1,22 @@
 """Learned k-step corrector with plain-FVM fallback.
 
-A small message-passing network over the mesh's face adjacency predicts the state change over
-k FVM steps; a proposal is accepted only if it passes two checks against the FVM itself, else the
-window is recomputed with k plain FVM steps.
+A small message-passing network over the mesh's face adjacency corrects a first-order estimate of
+the state change over k FVM steps; a proposal is accepted only if it passes two checks against the
+FVM itself, else the window is recomputed with k plain FVM steps.
+
+Proposal for a window starting at U (per case time step dt, R = the FVM residual dU/dt):
+    base = k dt R(U)                                     (k forward-Euler steps of the FVM residual)
+    U'   = U + base + P(scale * net([U, base], geometry))
+where P removes, per case, the volume-weighted mean of the mass and energy components of the
+learned part, so the proposal changes total mass and energy by exactly k dt sum(vol R(U)) -- the
+FVM boundary-flux integral over the window.  The network only has to learn the higher-order part of
+the k-step change, and the conservation check cannot be failed by the network.
 
 Network (width W = 64, L = 4 message-passing layers, SiLU):
-    X  = [normalised state, geometry, case parameters]            (bf16 [N][64])
+    X  = [normalised U, normalised base, geometry, case parameters]   (bf16 [N][64])
     h0 = SiLU(X Win^T + b_in)
     h_{l+1} = h_l + SiLU([h_l, mean_{j in nbr} h_l,j] W_l^T + b_l)  (l = 0..3)
-    out = h_L Wout^T + b_out                                        (normalised dU over k steps)
+    out = h_L Wout^T + b_out                                        (normalised U_{t+k} - U_t - base)
 All matrix products run on ``fvm_gemm_bf16`` (tcgen05, BF16 operands, FP32 accumulation in tensor
 memory, bias / SiLU / residual fused into the epilogue); the backward pass (SiLU derivative,
 transposed products, split-K weight gradients, the transpose of the neighbour mean) and Adam are
@@ -17,12 +25,13 @@ the library's own kernels as well.  Weights are kept in FP32 (master) with BF16 
 Training data are trajectories the batched FVM solver generates (``BatchedFVM``): every step of a
 spin-up-then-record run is stored on the device and random (U_t, U_{t+k}) windows are drawn.
 
-Fallback (per case, per window): the proposal U' = U + scale * net(U) is accepted when
-  * the relative mass / energy drift |M(U') - M(U) - k dt sum(vol dU/dt(U))| / |M(U)| <= 1e-4
-    (the expected change is the FVM boundary-flux integral over the window, so open channels are
-    judged correctly), and
-  * ||dU/dt(U')||_vol <= 3 ||dU/dt(U)||_vol;
-otherwise the window is advanced with k plain FVM steps.
+Fallback (per case, per window): the proposal U' is accepted when
+  * the relative mass / energy drift |M(U') - M(U) - k dt sum(vol dU/dt(U))| / |M(U)| <= 1e-4,
+  * ||dU/dt(U')||_vol <= 3 ||dU/dt(U)||_vol, and
+  * U' is admissible: positive density and internal energy in every cell;
+otherwise the window is advanced with k plain FVM steps.  The proposal and both checks are one CUDA
+graph; the host reads the per-case verdicts once per window and replays a graph of k FVM steps for
+the batch only when some case failed.
 """
 from __future__ import annotations
 
@@ -131,18 +140,20 @@ class CorrectorNet:
                                                    _lib.stream_ptr()), "fvm_corrector_features")
         return b["X"]
 
-    def forward(self, nbr: torch.Tensor) -> torch.Tensor:
-        """Network output for the features already in the X buffer (``features``)."""
+    def forward(self, nbr: torch.Tensor, store_pre: bool = True) -> torch.Tensor:
+        """Network output for the features already in the X buffer (``features``).  Inference
+        (``store_pre=False``) skips the pre-activation stores the backward pass needs."""
         b = self._bufs
         N, L = b["N"], self.L
         p, s = self.params, _lib.stream_ptr()
+        Z = b["Z"] if store_pre else [None] * (L + 1)
         self._gemm(b["X"], XW, self.bf["W_in"], XW, N, W, XW, Df=b["hf"][0], Db=b["hb"][0], ldd=W, bias=p["b_in"],
-                   pre=b["Z"][0], act=1)
+                   pre=Z[0], act=1)
         for l in range(L):
             _lib.check(self.lib.fvm_mp_gather(b["hb"][l].data_ptr(), nbr.data_ptr(), N, W, nbr.shape[1],
                                               b["A"][l].data_ptr(), s), "fvm_mp_gather")
             self._gemm(b["A"][l], 2 * W, self.bf[f"W{l}"], 2 * W, N, W, 2 * W, Df=b["hf"][l + 1], Db=b["hb"][l + 1],
-                       ldd=W, bias=p[f"b{l}"], resid=b["hf"][l], ldr=W, pre=b["Z"][l + 1], act=1)
+                       ldd=W, bias=p[f"b{l}"], resid=b["hf"][l], ldr=W, pre=Z[l + 1], act=1)
         _lib.check(self.lib.fvm_decoder(b["hb"][L].data_ptr(), p["W_out"].data_ptr(), p["b_out"].data_ptr(), N, W,
                                         self.O, b["out"].data_ptr(), s), "fvm_decoder")
         return b["out"]
@@ -204,8 +215,27 @@ class CorrectorNet:
 # ---------------------------------------------------------------------------------------------
 # Training on solver trajectories and corrected rollouts
 # ---------------------------------------------------------------------------------------------
+class ResidualEval:
+    """dU/dt of a batch for a given conserved state, on scratch gradients (the solver's carried
+    gradients are left alone), as the FVM residual of the first stage of a fresh run."""
+
+    def __init__(self, batch):
+        self.b = batch
+        self.lib = _lib.load()
+        self.grads = torch.zeros_like(batch.grads)
+        self.flag = torch.zeros(1, dtype=torch.int32, device=batch.device)
+
+    def __call__(self, state: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+        prims = self.b.cells.phys_setup.state_to_primative(state)[0].contiguous()
+        self.flag.zero_()
+        _lib.check(self.lib.fvm_residual(ct.byref(self.b.dev.struct), ct.byref(self.b.phys), prims.data_ptr(),
+                                         self.grads.data_ptr(), self.flag.data_ptr(), out.data_ptr(),
+                                         ct.byref(self.b.work.struct), _lib.stream_ptr()), "fvm_residual")
+        return out
+
+
 class CorrectorModel:
-    """Network + the normalisation and geometry of one batch of meshes."""
+    """Network + the normalisation, geometry and residual baseline of one batch of meshes."""
 
     def __init__(self, batch, case_params: torch.Tensor, k: int = 8, seed: int = 0, lr: float = 1e-3,
                  like: "CorrectorModel | None" = None):
@@ -214,31 +244,72 @@ class CorrectorModel:
         self.batch = batch
         self.k = k if like is None else like.k
         C = batch.n_comp
+        self.C = C
         kt = batch.kt
-        self.net = CorrectorNet(C, device=batch.device, seed=seed, lr=lr) if like is None else like.net
-        self.nbr = neighbour_table(kt).to(batch.device)
-        cp = case_params[batch.dev.case["cell_case"].long().cpu()]
-        self.geo = geometry_features(kt, cp).to(batch.device)
-        if C + self.geo.shape[1] > XW:
+        dev = batch.device
+        self.net = CorrectorNet(C, device=dev, seed=seed, lr=lr) if like is None else like.net
+        self.nbr = neighbour_table(kt).to(dev)
+        self.cell_case = batch.dev.case["cell_case"].long().to(dev)
+        cp = case_params[self.cell_case.cpu()]
+        self.geo = geometry_features(kt, cp).to(dev)
+        if 2 * C + self.geo.shape[1] > XW:
             raise ValueError("too many input features")
-        self.mean = torch.zeros(C, device=batch.device)
-        self.inv_std = torch.ones(C, device=batch.device)
-        self.scale = torch.ones(C, device=batch.device)
+        self.vol = kt.volumes.to(dev).double()
+        self.case_vol = torch.zeros(batch.n_cases, dtype=torch.float64, device=dev).index_add_(
+            0, self.cell_case, self.vol)
+        self.cons = slice(batch.mesh.dim, batch.mesh.dim + 2)          # mass and energy components
+        self.res = ResidualEval(batch)
+        N = batch.n_cells
+        self.cell_case32 = batch.dev.case["cell_case"]
+        self.kdt_case = torch.empty(batch.n_cases, device=dev)
+        self.S = torch.empty((batch.n_cases, C), dtype=torch.float64, device=dev)
+        self.shift = torch.zeros((batch.n_cases, C), device=dev)
+        self.base = torch.empty((N, C), device=dev)
+        self.fmean = torch.zeros(2 * C, device=dev)
+        self.finv = torch.ones(2 * C, device=dev)
+        self.scale = torch.ones(C, device=dev)
         if like is not None:
-            self.mean, self.inv_std, self.scale = like.mean, like.inv_std, like.scale
+            self.fmean, self.finv, self.scale = like.fmean, like.finv, like.scale
 
-    def set_normalisation(self, states: torch.Tensor, increments: torch.Tensor):
-        self.mean = states.mean(dim=(0, 1)).float().contiguous()
-        self.inv_std = (1.0 / (states.std(dim=(0, 1)) + 1e-6)).float().contiguous()
-        self.scale = (increments.std(dim=(0, 1)) + 1e-12).float().contiguous()
+    def kdt(self) -> torch.Tensor:
+        """k * dt of each cell's case, [N][1] (read from the solver's device time steps)."""
+        return (self.k * self.batch.t_solver.dt)[self.cell_case].unsqueeze(1)
 
-    def predict(self, state: torch.Tensor, out_state: torch.Tensor):
-        self.net.features(state, self.mean, self.inv_std, self.geo)
-        out = self.net.forward(self.nbr)
-        N, C = state.shape
-        lib = self.net.lib
-        _lib.check(lib.fvm_apply_increment(state.data_ptr(), out.data_ptr(), self.scale.data_ptr(), N, C,
-                                           out_state.data_ptr(), _lib.stream_ptr()), "fvm_apply_increment")
+    def set_normalisation(self, feats: torch.Tensor, targets: torch.Tensor):
+        """feats [S][N][2C] = [U, base]; targets [S][N][C] = U_{t+k} - U_t - base."""
+        self.fmean = feats.mean(dim=(0, 1)).float().contiguous()
+        self.finv = (1.0 / (feats.std(dim=(0, 1)) + 1e-12)).float().contiguous()
+        self.scale = (targets.std(dim=(0, 1)) + 1e-12).float().contiguous()
+
+    def inputs(self, state: torch.Tensor, r0: torch.Tensor):
+        """Writes base = k dt r0 and the network input features for (state, base); returns them."""
+        b = self.net._alloc(state.shape[0])
+        torch.mul(self.batch.t_solver.dt, float(self.k), out=self.kdt_case)
+        _lib.check(self.net.lib.fvm_corrector_inputs(
+            state.data_ptr(), r0.data_ptr(), self.kdt_case.data_ptr(), self.cell_case32.data_ptr(), state.shape[0],
+            self.C, self.fmean.data_ptr(), self.finv.data_ptr(), self.geo.data_ptr(), self.geo.shape[1],
+            self.base.data_ptr(), b["X"].data_ptr(), XW, _lib.stream_ptr()), "fvm_corrector_inputs")
+        return b["X"]
+
+    def _shift(self, out: torch.Tensor) -> torch.Tensor:
+        """Per-case offsets that remove the volume-weighted mean of the mass and energy parts of
+        scale * out (the other components get no offset)."""
+        b = self.batch
+        _lib.check(self.net.lib.fvm_conservation(ct.byref(b.dev.struct), out.data_ptr(), self.S.data_ptr(),
+                                                 ct.byref(b.work.struct), _lib.stream_ptr()), "fvm_conservation")
+        mean = self.S[:, self.cons] / self.case_vol.unsqueeze(1) * self.scale[self.cons].double()
+        self.shift[:, self.cons] = mean.float()
+        return self.shift
+
+    def predict(self, state: torch.Tensor, out_state: torch.Tensor, r0: torch.Tensor):
+        """out_state = proposal for U_{t+k} from state = U_t with residual r0 = dU/dt(U_t)."""
+        self.inputs(state, r0)
+        out = self.net.forward(self.nbr, store_pre=False)
+        shift = self._shift(out)
+        _lib.check(self.net.lib.fvm_corrector_combine(
+            state.data_ptr(), self.base.data_ptr(), out.data_ptr(), self.scale.data_ptr(), shift.data_ptr(),
+            self.cell_case32.data_ptr(), state.shape[0], self.C, out_state.data_ptr(), _lib.stream_ptr()),
+            "fvm_corrector_combine")
         return out_state
 
 
@@ -258,16 +329,25 @@ def train(model: CorrectorModel, traj: torch.Tensor, iters: int, seed: int = 0, 
     """Adam on random windows (U_t -> U_{t+k}) of a recorded trajectory; returns the loss history."""
     k = model.k
     T = traj.shape[0] - k
-    inc = traj[k:] - traj[:T]
-    model.set_normalisation(traj, inc)
+    r0 = torch.empty_like(traj[0])
+    feats, tg = [], []
+    for t in range(0, T, max(1, T // 40)):
+        model.res(traj[t], r0)
+        base = model.kdt() * r0
+        feats.append(torch.cat([traj[t], base], 1))
+        tg.append(traj[t + k] - traj[t] - base)
+    model.set_normalisation(torch.stack(feats), torch.stack(tg))
+    del feats, tg
     g = torch.Generator().manual_seed(seed)
     target = torch.empty_like(traj[0])
     losses = []
     model.net._alloc(traj.shape[1])
     for it in range(iters):
         t = int(torch.randint(0, T, (1,), generator=g))
-        torch.div(inc[t], model.scale, out=target)
-        model.net.features(traj[t], model.mean, model.inv_std, model.geo)
+        model.res(traj[t], r0)
+        model.inputs(traj[t], r0)
+        torch.sub(traj[t + k], traj[t], out=target)
+        target.sub_(model.base).div_(model.scale)
         loss = model.net.train_step(model.nbr, target)
         if log_every and (it % log_every == 0 or it == iters - 1):
             losses.append((it, float(loss.item())))
@@ -278,7 +358,8 @@ def train(model: CorrectorModel, traj: torch.Tensor, iters: int, seed: int = 0, 
 class CheckedRollout:
     """Corrector + fallback rollout on a batch, with per-case acceptance checks (see module doc)."""
 
-    def __init__(self, model: CorrectorModel, drift_tol: float = 1e-4, residual_ratio: float = 3.0):
+    def __init__(self, model: CorrectorModel, drift_tol: float = 1e-4, residual_ratio: float = 3.0,
+                 use_graphs: bool = True):
         self.m = model
         b = model.batch
         self.b = b
@@ -290,18 +371,13 @@ class CheckedRollout:
         self.r0 = torch.empty((N, C), device=d)
         self.r1 = torch.empty((N, C), device=d)
         self.sq = torch.empty((N, C), device=d)
-        self.grads = torch.zeros_like(b.grads)
-        self.flag = torch.zeros(1, dtype=torch.int32, device=d)
-        self.cons = torch.empty((b.n_cases, C), dtype=torch.float64, device=d)
+        self.ok = torch.zeros(b.n_cases, dtype=torch.bool, device=d)
+        self.use_graphs = use_graphs
+        self._g_propose = None
+        self._fallback = None
         self.accepted = 0
         self.windows = 0
-
-    def _residual(self, state, out):
-        prims = self.b.cells.phys_setup.state_to_primative(state)[0].contiguous()
-        self.flag.zero_()
-        _lib.check(self.lib.fvm_residual(ct.byref(self.b.dev.struct), ct.byref(self.b.phys), prims.data_ptr(),
-                                         self.grads.data_ptr(), self.flag.data_ptr(), out.data_ptr(),
-                                         ct.byref(self.b.work.struct), _lib.stream_ptr()), "fvm_residual")
+        self.full_windows = 0
 
     def _sums(self, x) -> torch.Tensor:
         out = torch.empty((self.b.n_cases, x.shape[1]), dtype=torch.float64, device=x.device)
@@ -309,32 +385,72 @@ class CheckedRollout:
                                              ct.byref(self.b.work.struct), _lib.stream_ptr()), "fvm_conservation")
         return out
 
-    def window(self) -> torch.Tensor:
-        """Advance one window of k steps; returns the per-case acceptance mask (device)."""
+    def _propose(self):
+        """Proposal and both checks; leaves the per-case verdicts in ``self.ok`` (device)."""
         b, k = self.b, self.m.k
         U = b.cells.state
         dim = b.mesh.dim
-        self._residual(U, self.r0)
-        self.m.predict(U, self.prop)
-        self._residual(self.prop, self.r1)
+        self.m.res(U, self.r0)
+        self.m.predict(U, self.prop, self.r0)
+        self.m.res(self.prop, self.r1)
         M0, Mp, R0 = self._sums(U), self._sums(self.prop), self._sums(self.r0)
         dt = b.t_solver.dt.double()
-        cons = [dim, dim + 1]                                # mass and energy
+        cons = slice(dim, dim + 2)                           # mass and energy
         expected = M0[:, cons] + k * dt[:, None] * R0[:, cons]
         drift = ((Mp[:, cons] - expected).abs() / M0[:, cons].abs()).max(dim=1).values
         torch.mul(self.r0, self.r0, out=self.sq)
         n0 = self._sums(self.sq).sum(dim=1)
         torch.mul(self.r1, self.r1, out=self.sq)
         n1 = self._sums(self.sq).sum(dim=1)
-        ok = (drift <= self.drift_tol) & (n1 <= self.ratio ** 2 * n0) & torch.isfinite(drift)
+        # admissibility: density and internal energy positive in every cell of the case
+        P = self.prop
+        rho = P[:, dim]
+        e_int = P[:, dim + 1] - 0.5 * P[:, :dim].square().sum(dim=1) / rho
+        self.sq.zero_()
+        self.sq[:, 0] = ((rho <= 0) | (e_int <= 0) | ~torch.isfinite(e_int)).float()
+        bad = self._sums(self.sq)[:, 0]
+        self.ok.copy_((drift <= self.drift_tol) & (n1 <= self.ratio ** 2 * n0) & torch.isfinite(drift) & (bad == 0))
+
+    def _run_propose(self):
+        if not self.use_graphs:
+            self._propose()
+            return
+        if self._g_propose is None:
+            self._propose()                                  # eager once: allocates the network buffers
+            s = torch.cuda.Stream(device=self.b.device)
+            s.wait_stream(torch.cuda.current_stream())
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(s):
+                with torch.cuda.graph(g, stream=s):
+                    self._propose()
+            torch.cuda.current_stream().wait_stream(s)
+            self._g_propose = g
+        self._g_propose.replay()
+
+    def _run_fallback(self):
+        sol, k = self.b.t_solver, self.m.k
+        if not self.use_graphs:
+            sol.step(k)
+            return
+        sol._sync_prims()
+        if self._fallback is None:
+            self._fallback = sol.graph_steps(k)
+        self._fallback()
+
+    def window(self) -> torch.Tensor:
+        """Advance one window of k steps; returns the per-case acceptance mask (host)."""
+        b = self.b
+        self._run_propose()
+        ok = self.ok.cpu()
         self.windows += b.n_cases
         if bool(ok.all()):
             b.cells.state = self.prop
             self.accepted += b.n_cases
+            self.full_windows += 1
             return ok
         # fallback: k plain FVM steps for the batch, then keep the accepted proposals
-        keep = ok[b.dev.case["cell_case"].long()].unsqueeze(1)
-        b.t_solver.step(k)
+        keep = self.ok[self.m.cell_case].unsqueeze(1)
+        self._run_fallback()
         b.cells.state = torch.where(keep, self.prop, b.cells.state)
         self.accepted += int(ok.sum())
         return ok

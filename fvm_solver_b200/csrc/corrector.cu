@@ -46,6 +46,7 @@ struct GemmArgs {
     float* preact;                // [M][ldd] fp32 pre-activation, or null
     int act;                      // 0 none, 1 SiLU
     int* err;                     // device error flag (set to 1 on an mbarrier timeout)
+    int vec;                      // every epilogue row chunk is 32-byte aligned: 256-bit accesses
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -88,6 +89,60 @@ __device__ __forceinline__ void stage_tile(uint8_t* smem, const __nv_bfloat16* s
 }
 
 __device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
+
+// 8 consecutive floats (32-byte aligned) with one 256-bit access.
+__device__ __forceinline__ void ld8(const float* p, float* v) {
+    asm volatile("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+                 : "l"(p));
+}
+__device__ __forceinline__ void st8(float* p, const float* v) {
+    asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(v[0]), "f"(v[1]), "f"(v[2]),
+                 "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+                 : "memory");
+}
+
+// Epilogue of 32 consecutive accumulator columns [c0, c0 + 32) of one row with 256-bit accesses:
+// each thread reads and writes whole 32-byte sectors of its own row (no partial-sector traffic).
+__device__ __forceinline__ void epilogue_vec(const GemmArgs& g, int64_t row, int c0, const uint32_t (&r)[32]) {
+    float v[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+    if (g.bias) {
+        float b[32];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ld8(g.bias + c0 + 8 * q, b + 8 * q);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] += b[j];
+    }
+    if (g.preact)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) st8(g.preact + row * g.ldd + c0 + 8 * q, v + 8 * q);
+    if (g.act == 1)
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = silu(v[j]);
+    if (g.resid) {
+        float x[32];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ld8(g.resid + row * g.ldr + c0 + 8 * q, x + 8 * q);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] += x[j];
+    }
+    if (g.Df)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) st8(g.Df + row * g.ldd + c0 + 8 * q, v + 8 * q);
+    if (g.Db) {
+        float pk[16];   // bf16 pairs, bit patterns carried in float registers
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+            pk[j] = __uint_as_float(*reinterpret_cast<const uint32_t*>(&h));
+        }
+        float* dst = reinterpret_cast<float*>(g.Db + row * g.ldd + c0);
+        st8(dst, pk);
+        st8(dst + 8, pk + 8);
+    }
+}
 
 template <int N>
 __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
@@ -189,7 +244,9 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
                   "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
                 : "r"(a));
             asm volatile("tcgen05.wait::ld.sync.aligned;");
-            if (row < g.M) {
+            if (row < g.M && g.vec && g.k_splits == 1) {
+                epilogue_vec(g, row, c0, r);
+            } else if (row < g.M) {
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const int col = c0 + j;
@@ -241,8 +298,12 @@ extern "C" int fvm_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t 
     if (N != 32 && N != 64 && N != 128 && N != 256) return FVM_E_UNSUPPORTED;
     if ((uintptr_t)A % 16 || (uintptr_t)B % 16 || lda % 8 || ldb % 8) return FVM_E_ARG;
     if (k_splits > 1 && (!Df || bias || resid || preact || Db || act)) return FVM_E_ARG;
+    // 256-bit epilogue when every row chunk of 32 columns starts on a 32-byte boundary.
+    auto a32 = [](const void* p) { return ((uintptr_t)p & 31u) == 0; };
+    const int vec = a32(bias) && a32(resid) && a32(Df) && a32(Db) && a32(preact) && (!resid || ldr % 8 == 0) &&
+                    ((!Df && !preact) || ldd % 8 == 0) && (!Db || ldd % 16 == 0);
     corr::GemmArgs g{static_cast<const __nv_bfloat16*>(A), lda, static_cast<const __nv_bfloat16*>(B), ldb, M, N, K,
-                     k_splits, bias, resid, ldr, Df, static_cast<__nv_bfloat16*>(Db), ldd, preact, act, err};
+                     k_splits, bias, resid, ldr, Df, static_cast<__nv_bfloat16*>(Db), ldd, preact, act, err, vec};
     cudaStream_t s = (cudaStream_t)stream;
     switch (N) {
         case 32: return corr::launch_gemm<32>(g, s);
@@ -432,6 +493,64 @@ __global__ void k_apply_increment(const float* __restrict__ state, const float* 
     new_state[t] = state[t] + scale[t % C] * out[t];
 }
 
+// Corrector inputs, one thread per cell: base = k dt(case) * r0 and the bf16 feature row
+// [(U - mean) * inv_std, (base - mean) * inv_std, geometry, zeros] (XW entries).
+template <int C>
+__global__ void k_corrector_inputs(const float* __restrict__ state, const float* __restrict__ r0,
+                                   const float* __restrict__ kdt_case, const int32_t* __restrict__ cell_case, int N,
+                                   const float* __restrict__ mean, const float* __restrict__ inv_std,
+                                   const float* __restrict__ geo, int G, float* __restrict__ base,
+                                   __nv_bfloat16* __restrict__ X, int XW) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const float h = kdt_case[cell_case ? __ldg(cell_case + i) : 0];
+    float u[C], b[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        u[c] = __ldg(state + (int64_t)i * C + c);
+        b[c] = h * __ldg(r0 + (int64_t)i * C + c);
+        base[(int64_t)i * C + c] = b[c];
+    }
+    __nv_bfloat16* row = X + (int64_t)i * XW;
+    // entries 0..15 hold the 2C <= 10 state / baseline features (indices known at compile time)
+#pragma unroll
+    for (int q = 0; q < 16; q += 8) {
+        __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int c = q + e;
+            float x = 0.f;
+            if (c < C) x = (u[c < C ? c : 0] - __ldg(mean + c)) * __ldg(inv_std + c);
+            else if (c < 2 * C) x = (b[(c >= C && c < 2 * C) ? c - C : 0] - __ldg(mean + c)) * __ldg(inv_std + c);
+            else if (c < 2 * C + G) x = __ldg(geo + (int64_t)i * G + (c - 2 * C));
+            v[e] = __float2bfloat16(x);
+        }
+        *reinterpret_cast<uint4*>(row + q) = *reinterpret_cast<const uint4*>(v);
+    }
+    for (int q = 16; q < XW; q += 8) {
+        __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int c = q + e;
+            v[e] = __float2bfloat16(c < 2 * C + G ? __ldg(geo + (int64_t)i * G + (c - 2 * C)) : 0.f);
+        }
+        *reinterpret_cast<uint4*>(row + q) = *reinterpret_cast<const uint4*>(v);
+    }
+}
+
+// prop = state + base + scale * out - shift(case)  (shift: per-case [C] offsets, or null).
+__global__ void k_corrector_combine(const float* __restrict__ state, const float* __restrict__ base,
+                                    const float* __restrict__ out, const float* __restrict__ scale,
+                                    const float* __restrict__ shift, const int32_t* __restrict__ cell_case, int N,
+                                    int C, float* __restrict__ prop) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)N * C) return;
+    const int i = (int)(t / C), c = (int)(t % C);
+    float v = state[t] + base[t] + __ldg(scale + c) * out[t];
+    if (shift) v -= __ldg(shift + (int64_t)(cell_case ? __ldg(cell_case + i) : 0) * C + c);
+    prop[t] = v;
+}
+
 static inline unsigned nblk(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
 }  // namespace corr
@@ -531,5 +650,36 @@ extern "C" int fvm_apply_increment(const float* state, const float* out, const f
     cudaStream_t s = (cudaStream_t)stream;
     FVM_LAUNCH(KID_CORRECTOR, s, corr::k_apply_increment<<<corr::nblk((int64_t)N * C, 256), 256, 0, s>>>(
                                      state, out, scale, N, C, new_state));
+    return launch_status();
+}
+
+extern "C" int fvm_corrector_inputs(const float* state, const float* r0, const float* kdt_case,
+                                    const int32_t* cell_case, int32_t N, int32_t C, const float* mean,
+                                    const float* inv_std, const float* geo, int32_t G, float* base, void* X,
+                                    int32_t XW, void* stream) {
+    if (!state || !r0 || !kdt_case || !mean || !inv_std || (G > 0 && !geo) || !base || !X || N <= 0 || G < 0 ||
+        XW % 8 != 0 || XW < 16 || 2 * C + G > XW || ((uintptr_t)X & 15u) != 0)
+        return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (C == 4)
+        FVM_LAUNCH(KID_CORRECTOR, s, corr::k_corrector_inputs<4><<<corr::nblk(N, 128), 128, 0, s>>>(
+                                         state, r0, kdt_case, cell_case, N, mean, inv_std, geo, G, base,
+                                         static_cast<__nv_bfloat16*>(X), XW));
+    else if (C == 5)
+        FVM_LAUNCH(KID_CORRECTOR, s, corr::k_corrector_inputs<5><<<corr::nblk(N, 128), 128, 0, s>>>(
+                                         state, r0, kdt_case, cell_case, N, mean, inv_std, geo, G, base,
+                                         static_cast<__nv_bfloat16*>(X), XW));
+    else
+        return FVM_E_UNSUPPORTED;
+    return launch_status();
+}
+
+extern "C" int fvm_corrector_combine(const float* state, const float* base, const float* out, const float* scale,
+                                     const float* shift, const int32_t* cell_case, int32_t N, int32_t C, float* prop,
+                                     void* stream) {
+    if (!state || !base || !out || !scale || !prop || N <= 0 || C <= 0) return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_corrector_combine<<<corr::nblk((int64_t)N * C, 256), 256, 0, s>>>(
+                                     state, base, out, scale, shift, cell_case, N, C, prop));
     return launch_status();
 }

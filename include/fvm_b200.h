@@ -269,6 +269,17 @@ int fvm_corrector_features(const float *state, int32_t N, int32_t C, const float
 /* new_state = state + scale[c] * out (fp32 [N][C]). */
 int fvm_apply_increment(const float *state, const float *out, const float *scale, int32_t N, int32_t C,
                         float *new_state, void *stream);
+/* Corrector inputs with the residual baseline (C = 4 or 5): base[i] = kdt_case[case(i)] * r0[i]
+ * (fp32 [N][C]) and the bf16 feature rows X[i] = [(state_i - mean[:C]) * inv_std[:C],
+ * (base_i - mean[C:]) * inv_std[C:], geo_i, 0...] (XW entries, 2C + G <= XW, X 16-byte aligned).
+ * cell_case (int32 [N]) may be NULL for one mesh (case 0). */
+int fvm_corrector_inputs(const float *state, const float *r0, const float *kdt_case, const int32_t *cell_case,
+                         int32_t N, int32_t C, const float *mean, const float *inv_std, const float *geo, int32_t G,
+                         float *base, void *X, int32_t XW, void *stream);
+/* prop = state + base + scale[c] * out - shift[case(i)][c]  (fp32 [N][C]; shift [cases][C] or NULL). */
+int fvm_corrector_combine(const float *state, const float *base, const float *out, const float *scale,
+                          const float *shift, const int32_t *cell_case, int32_t N, int32_t C, float *prop,
+                          void *stream);
 
 #ifdef __cplusplus
 }

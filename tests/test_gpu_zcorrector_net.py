@@ -62,9 +62,10 @@ def test_forward_backward_vs_autograd(small_batch):
     batch, params = small_batch
     model = CorrectorModel(batch, params, seed=3, lr=0.0)          # lr 0: the step leaves weights unchanged
     U = batch.cells.state.clone()
-    model.set_normalisation(U.unsqueeze(0), U.unsqueeze(0) * 1e-3 + 1e-3)
+    r0 = model.res(U, torch.empty_like(U))
+    model.set_normalisation(torch.cat([U, U * 1e-3], 1).unsqueeze(0), (U * 1e-3 + 1e-3).unsqueeze(0))
     N = U.shape[0]
-    X = model.net.features(U, model.mean, model.inv_std, model.geo).clone()
+    X = model.inputs(U, r0).clone()
     target = torch.randn(N, 4, device="cuda", generator=torch.Generator(device="cuda").manual_seed(0))
     ref_out, ref_loss, ref_g = _torch_reference(model.net, X, model.nbr, target, N)
     out = model.net.forward(model.nbr).clone()
@@ -90,9 +91,34 @@ def test_training_reduces_loss_and_rollout(small_batch):
     model = CorrectorModel(batch, params, k=8, seed=1, lr=2e-3)
     hist = train(model, traj, iters=300, log_every=50)
     assert hist[-1][1] < 0.5 * hist[0][1]
+    # the proposal changes each case's mass and energy by exactly k dt sum(vol dU/dt)
+    U = batch.cells.state.clone()
+    r0 = model.res(U, torch.empty_like(U))
+    prop = model.predict(U, torch.empty_like(U), r0)
+    vol = model.vol.unsqueeze(1)
+    cc = model.cell_case
+    dM = torch.zeros(batch.n_cases, 4, dtype=torch.float64, device="cuda").index_add_(0, cc, (prop - U).double() * vol)
+    want = torch.zeros_like(dM).index_add_(0, cc, r0.double() * vol) * (model.k * batch.t_solver.dt.double())[:, None]
+    M = torch.zeros_like(dM).index_add_(0, cc, U.double() * vol)
+    assert float(((dM - want)[:, 2:].abs() / M[:, 2:].abs()).max()) < 1e-5
+    # graph-replayed and eager rollouts agree
+    start = batch.cells.state.clone()
+    g_start, f_start = batch.grads.clone(), batch.has_grads.clone()
     ro = CheckedRollout(model)
+    oks = []
     for _ in range(3):
         ok = ro.window()
         assert ok.shape == (batch.n_cases,)
+        oks.append(ok)
     assert torch.isfinite(batch.cells.state).all()
     assert 0 <= ro.accepted <= ro.windows
+    end_graph = batch.cells.state.clone()
+    batch.cells.state = start
+    batch.grads.copy_(g_start)
+    batch.has_grads.copy_(f_start)
+    ro2 = CheckedRollout(model, use_graphs=False)
+    for w in range(3):
+        ok = ro2.window()
+        assert torch.equal(ok, oks[w])
+    rel = float((batch.cells.state - end_graph).norm() / end_graph.norm())
+    assert rel < 1e-5
