@@ -27,7 +27,8 @@ class Mesh(ct.Structure):
                           "bc_cell", "bc_kind", "bc_b", "bc_l", "bc_ga", "bc_gb",
                           "bc_char", "ch_cell", "ch_normal", "ch_rho", "ch_vn", "ch_p", "ch_vt")] + [
         ("n_cases", ct.c_int32)] + [
-        (n, _P) for n in ("cell_case", "face_case", "bc_case", "ch_off", "case_mu", "case_mu_b", "case_kappa")]
+        (n, _P) for n in ("cell_case", "face_case", "bc_case", "ch_off", "case_mu", "case_mu_b", "case_kappa")] + [
+        ("n_owned", ct.c_int32), ("char_scale_given", ct.c_int32)]
 
 MESH_PTR_FIELDS = [f for f, t in Mesh._fields_ if t is _P]
 
@@ -76,6 +77,10 @@ _SIGS = [
     ("fvm_conservation", ct.c_int, [ct.POINTER(Mesh), _P, _P, ct.POINTER(Work), _P]),
     ("fvm_residual_noalloc", ct.c_int, [ct.POINTER(Mesh), ct.POINTER(Physics), _P, _P, _P, _P, _P]),
     ("fvm_profile_start", ct.c_int, [ct.c_int32]),
+    ("fvm_stage_begin", ct.c_int, [_P, _P, _P, _P, _P]),
+    ("fvm_stage_end", ct.c_int, [_P, _P, _P, ct.c_int32, _P, _P, ct.c_int32, _P]),
+    ("fvm_stage_finalize", ct.c_int, [_P, _P, _P, _P, _P]),
+    ("fvm_char_partial", ct.c_int, [_P, _P, _P, _P, _P]),
     ("fvm_set_block_size", ct.c_int, [ct.c_int32, ct.c_int32]),
     ("fvm_set_prefetch", ct.c_int, [ct.c_int32, ct.c_int32]),
     ("fvm_gemm_bf16", ct.c_int, [_P, ct.c_int64, _P, ct.c_int64, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32,

@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float
     constexpr int C = Ly::C;
     __shared__ double red[32];
     float scale = 0.f;
-    if (m.n_char > 0 && m.n_cases == 0) {
+    if (m.n_char > 0 && m.n_cases == 0 && !m.char_scale_given) {
         // Group mean of the interior sound speed c = sqrt(gamma R T) (facet_boundary.py:427),
         // recomputed identically by every block.
         const double sum = char_c_sum<DIM>(m, p, prims, 0, m.n_char, red);
@@ -254,6 +254,7 @@ __global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= m.n_bc) return;
     if (m.n_cases > 0) scale = (float)wred[FVM_RED_DOUBLES + 8 * __ldg(m.bc_case + b) + 6];
+    else if (m.char_scale_given) scale = (float)wred[FVM_RED_DOUBLES + 6];
     const int cell = __ldg(m.bc_cell + b);
     float U[Ly::RS];
     ld_vec<Ly::RS>(prims + (int64_t)cell * Ly::RS, U);
@@ -328,15 +329,16 @@ __global__ void __launch_bounds__(kMaxBlock) k_cell(fvm_mesh_t m, Phys p, const 
                                                   int32_t* __restrict__ has_grads, int waves) {
     using Ly = L<DIM>;
     constexpr int C = Ly::C, K = Ly::K, KG = Ly::KG, RS = Ly::RS;
-    const int N = m.n_cells;
+    const int N = m.n_cells;                              // columns < N are cells (halo included)
+    const int NA = m.n_owned > 0 ? m.n_owned : N;         // cells this launch updates
     const int stride = gridDim.x * blockDim.x;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) *has_grads = 1;
     int cols[KG];
 #pragma unroll
-    for (int k = 0; k < KG; ++k) cols[k] = i < N ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)i * Ly::CR + Ly::GC + k) : 0;
-    for (int64_t tile = blockIdx.x; i < N; i += stride, tile += gridDim.x) {
-        if (waves > 0) prefetch_tile(m.cell_rec, N, Ly::CR, tile + (int64_t)waves * gridDim.x);
+    for (int k = 0; k < KG; ++k) cols[k] = i < NA ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)i * Ly::CR + Ly::GC + k) : 0;
+    for (int64_t tile = blockIdx.x; i < NA; i += stride, tile += gridDim.x) {
+        if (waves > 0) prefetch_tile(m.cell_rec, NA, Ly::CR, tile + (int64_t)waves * gridDim.x);
         float X[KG][RS];
 #pragma unroll
         for (int k = 0; k < KG; ++k) {
@@ -350,7 +352,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_cell(fvm_mesh_t m, Phys p, const 
         const int inext = i + stride;
 #pragma unroll
         for (int k = 0; k < KG; ++k)
-            cols[k] = inext < N ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)inext * Ly::CR + Ly::GC + k) : 0;
+            cols[k] = inext < NA ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)inext * Ly::CR + Ly::GC + k) : 0;
         const int nvalid = (as_int(rec[Ly::META]) >> 24) & 31;
         float g[DIM][C];
 #pragma unroll
@@ -742,7 +744,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_div_stage(fvm_mesh_t m, Phys p, c
     using Ly = L<DIM>;
     constexpr int C = Ly::C, RS = Ly::RS;
     constexpr bool FINAL = MODE >= DIV_FINAL, ADAPT = MODE == DIV_FINAL_ADAPT;
-    const int N = m.n_cells;
+    const int N = m.n_cells;                              // row stride of the increment buffer
+    const int NA = m.n_owned > 0 ? m.n_owned : N;         // cells this launch updates
     const int stride = gridDim.x * blockDim.x;
     const int lane = threadIdx.x & 31;
     const bool do_cons = FINAL && a.cons, do_cfl = FINAL && a.cfl;
@@ -753,17 +756,17 @@ __global__ void __launch_bounds__(kMaxBlock) k_div_stage(fvm_mesh_t m, Phys p, c
     for (int c = 0; c < (ADAPT ? 3 * C : 1); ++c) ad_acc[c] = 0.0;
     int i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
     float nxt[Ly::DR];
-    if (i0 + lane < N) ld_vec<Ly::DR>(m.div_rec + (int64_t)(i0 + lane) * Ly::DR, nxt);
+    if (i0 + lane < NA) ld_vec<Ly::DR>(m.div_rec + (int64_t)(i0 + lane) * Ly::DR, nxt);
     else
 #pragma unroll
         for (int q = 0; q < Ly::DR; ++q) nxt[q] = 0.f;
-    for (int64_t tile = blockIdx.x; i0 < N; i0 += stride, tile += gridDim.x) {
+    for (int64_t tile = blockIdx.x; i0 < NA; i0 += stride, tile += gridDim.x) {
         if (waves > 0) {
-            prefetch_tile(m.div_rec, N, Ly::DR, tile + (int64_t)waves * gridDim.x);
-            if (MODE != DIV_RESIDUAL) prefetch_tile(state, N, C, tile + (int64_t)waves * gridDim.x);
+            prefetch_tile(m.div_rec, NA, Ly::DR, tile + (int64_t)waves * gridDim.x);
+            if (MODE != DIV_RESIDUAL) prefetch_tile(state, NA, C, tile + (int64_t)waves * gridDim.x);
         }
         const int i = i0 + lane;
-        const bool live = i < N;
+        const bool live = i < NA;
         float rec[Ly::DR];
 #pragma unroll
         for (int q = 0; q < Ly::DR; ++q) rec[q] = nxt[q];
@@ -782,7 +785,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_div_stage(fvm_mesh_t m, Phys p, c
                 }
             }
         }
-        if (i + stride < N) ld_vec<Ly::DR>(m.div_rec + (int64_t)(i + stride) * Ly::DR, nxt);
+        if (i + stride < NA) ld_vec<Ly::DR>(m.div_rec + (int64_t)(i + stride) * Ly::DR, nxt);
         if (MODE == DIV_RESIDUAL) {
             if (live) store_state<C>(dudt + (int64_t)i * C, r);
             continue;
@@ -951,7 +954,7 @@ __global__ void __launch_bounds__(kBlock) k_reduce_state(fvm_mesh_t m, Phys p, c
     constexpr int C = DIM + 2;
     __shared__ double smem[32 * C];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i < m.n_cells;
+    const bool live = i < (m.n_owned > 0 ? m.n_owned : m.n_cells);
     float U[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) U[c] = 1.f;
@@ -1000,6 +1003,8 @@ static bool mesh_ok(const fvm_mesh_t* m) {
     if (m->n_char > 0 && (!m->ch_cell || !m->ch_normal || !m->ch_rho || !m->ch_vn || !m->ch_p || !m->ch_vt))
         return false;
     if (m->n_cases < 0) return false;
+    if (m->n_owned < 0 || m->n_owned > m->n_cells || m->char_scale_given < 0 || m->char_scale_given > 1) return false;
+    if (m->n_cases > 0 && (m->n_owned > 0 || m->char_scale_given)) return false;
     if (m->n_cases > 0 && (!m->cell_case || !m->face_case || !m->ch_off || !m->case_mu || !m->case_mu_b ||
                            !m->case_kappa || (m->n_bc > 0 && !m->bc_case)))
         return false;
@@ -1011,6 +1016,7 @@ static bool work_ok(const fvm_mesh_t* m, const fvm_work_t* w) {
 }
 
 static inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+static inline int owned_cells(const fvm_mesh_t* m) { return m->n_owned > 0 ? m->n_owned : m->n_cells; }
 
 // Threads per block of the cell, facet and divergence kernels (set by the autotuner through
 // fvm_set_block_size).  The boundary kernels keep kBlock: their per-block reduction order must not
@@ -1050,29 +1056,44 @@ static inline unsigned fin_blocks(const fvm_mesh_t* m) {
     return m->n_cases > 0 ? (unsigned)((m->n_cases + 127) / 128) : 1u;
 }
 
-// bc -> cell -> face for the padded primitives `prims`; leaves fluxes in work->flux.
+// Boundary values and limited cell gradients for the padded primitives `prims`.
 template <int DIM>
-static int launch_fluxes(const fvm_mesh_t* m, const Phys& p, const float* prims, float* grads,
-                         int32_t* has_grads, const fvm_work_t* w, cudaStream_t s) {
+static int launch_begin(const fvm_mesh_t* m, const Phys& p, const float* prims, float* grads,
+                        int32_t* has_grads, const fvm_work_t* w, cudaStream_t s) {
     if (m->n_bc > 0) {
         if (m->n_cases > 0 && m->n_char > 0)
             FVM_LAUNCH(KID_BC, s, k_char_scale<DIM><<<m->n_cases, kBlock, 0, s>>>(*m, p, prims, w->red));
         FVM_LAUNCH(KID_BC, s, k_bc<DIM><<<blocks_for(m->n_bc), kBlock, 0, s>>>(*m, p, prims, grads, has_grads,
                                                                                w->bc_vals, w->red));
     }
-    const unsigned gc = persistent_grid(m->n_cells, g_block_cell, wave_blocks(k_cell<DIM>, g_block_cell));
-    const unsigned gf = persistent_grid(m->n_facets, g_block_face, wave_blocks(k_face<DIM>, g_block_face));
+    const unsigned gc = persistent_grid(owned_cells(m), g_block_cell, wave_blocks(k_cell<DIM>, g_block_cell));
     FVM_LAUNCH(KID_CELL, s, k_cell<DIM><<<gc, g_block_cell, 0, s>>>(*m, p, prims, w->bc_vals, grads, has_grads,
                                                                     waves_of(g_pf_cell)));
+    return launch_status();
+}
+
+template <int DIM>
+static int launch_face(const fvm_mesh_t* m, const Phys& p, const float* prims, const float* grads,
+                       const fvm_work_t* w, cudaStream_t s) {
+    const unsigned gf = persistent_grid(m->n_facets, g_block_face, wave_blocks(k_face<DIM>, g_block_face));
     FVM_LAUNCH(KID_FACE, s, k_face<DIM><<<gf, g_block_face, 0, s>>>(*m, p, prims, w->bc_vals, grads, w->flux,
                                                                     waves_of(g_pf_face)));
     return launch_status();
 }
 
+// bc -> cell -> face for the padded primitives `prims`; leaves fluxes in work->flux.
+template <int DIM>
+static int launch_fluxes(const fvm_mesh_t* m, const Phys& p, const float* prims, float* grads,
+                         int32_t* has_grads, const fvm_work_t* w, cudaStream_t s) {
+    const int rc = launch_begin<DIM>(m, p, prims, grads, has_grads, w, s);
+    return rc ? rc : launch_face<DIM>(m, p, prims, grads, w, s);
+}
+
 template <int DIM, int MODE>
 static void launch_div_mode(const fvm_mesh_t* m, const Phys& p, const float* flux, const StageArgs& a, float* state,
                             float* prims, float* kbuf, const float* dt, double* red, float* dudt, cudaStream_t s) {
-    const unsigned grid = persistent_grid(m->n_cells, g_block_div, wave_blocks(k_div_stage<DIM, MODE>, g_block_div));
+    const unsigned grid =
+        persistent_grid(owned_cells(m), g_block_div, wave_blocks(k_div_stage<DIM, MODE>, g_block_div));
     FVM_LAUNCH(KID_DIV_STAGE, s, k_div_stage<DIM, MODE><<<grid, g_block_div, 0, s>>>(
                                      *m, p, flux, a, state, prims, kbuf, dt, red, dudt, waves_of(g_pf_div)));
 }
@@ -1137,24 +1158,48 @@ static StageArgs stage_args(const fvm_tableau_t* tab, int s) {
     return a;
 }
 
+static int finalize_impl(const fvm_mesh_t* m, const fvm_tableau_t* tab, const fvm_solver_bufs_t* b,
+                         const fvm_work_t* w, int cons, cudaStream_t st) {
+    FVM_LAUNCH(KID_FINALIZE, st,
+               k_finalize<<<fin_blocks(m), 128, 0, st>>>(m->n_comp, tab->adaptive, tab->atol, tab->rtol, tab->mtol,
+                                                         tab->alpha_hi_err, tab->alpha_lo_err, tab->order, tab->cfl,
+                                                         cons, w->red, b->dt, b->cons, m->n_cases));
+    return launch_status();
+}
+
+// Facet fluxes, divergence and stage combination of stage s (the cell gradients are in b->grads);
+// on the last stage also the dt / conservation bookkeeping unless the caller defers it.
 template <int DIM>
-static int stage_impl(const fvm_mesh_t* m, const Phys& p, const fvm_tableau_t* tab, int s,
-                      const fvm_solver_bufs_t* b, const fvm_work_t* w, cudaStream_t st) {
-    int rc = launch_fluxes<DIM>(m, p, b->prims, b->grads, b->has_grads, w, st);
+static int stage_finish(const fvm_mesh_t* m, const Phys& p, const fvm_tableau_t* tab, int s,
+                        const fvm_solver_bufs_t* b, const fvm_work_t* w, int finalize, cudaStream_t st) {
+    int rc = launch_face<DIM>(m, p, b->prims, b->grads, w, st);
     if (rc) return rc;
     StageArgs a = stage_args(tab, s);
     a.cons = a.final_ && b->cons != nullptr;
     rc = launch_div<DIM>(m, p, w->flux, a, b->state, b->prims, b->k, b->dt, w->red, nullptr, st);
     if (rc) return rc;
-    if (a.final_ && (a.adaptive || a.cfl || a.cons)) {
-        FVM_LAUNCH(KID_FINALIZE, st,
-                   k_finalize<<<fin_blocks(m), 128, 0, st>>>(m->n_comp, tab->adaptive, tab->atol, tab->rtol,
-                                                             tab->mtol, tab->alpha_hi_err, tab->alpha_lo_err,
-                                                             tab->order, tab->cfl, a.cons, w->red, b->dt, b->cons,
-                                                             m->n_cases));
-        rc = launch_status();
-    }
+    if (finalize && a.final_ && (a.adaptive || a.cfl || a.cons)) rc = finalize_impl(m, tab, b, w, a.cons, st);
     return rc;
+}
+
+template <int DIM>
+static int stage_impl(const fvm_mesh_t* m, const Phys& p, const fvm_tableau_t* tab, int s,
+                      const fvm_solver_bufs_t* b, const fvm_work_t* w, cudaStream_t st) {
+    const int rc = launch_begin<DIM>(m, p, b->prims, b->grads, b->has_grads, w, st);
+    return rc ? rc : stage_finish<DIM>(m, p, tab, s, b, w, 1, st);
+}
+
+// Partitioned meshes: sum of the interior sound speed over this part's characteristic facets and
+// their count -> red[FVM_RED_DOUBLES + 6], red[FVM_RED_DOUBLES + 7].
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_char_partial(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+                                                          double* __restrict__ red_out) {
+    __shared__ double red[32];
+    const double sum = char_c_sum<DIM>(m, p, prims, 0, m.n_char, red);
+    if (threadIdx.x == 0) {
+        red_out[FVM_RED_DOUBLES + 6] = sum;
+        red_out[FVM_RED_DOUBLES + 7] = (double)m.n_char;
+    }
 }
 
 template <int DIM>
@@ -1274,6 +1319,48 @@ extern "C" int fvm_step(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const
     return FVM_OK;
 }
 
+extern "C" int fvm_char_partial(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const float* prims,
+                                const fvm_work_t* work, void* stream) {
+    if (const int rc = check_common(mesh)) return rc;
+    if (!phys || !prims || !work || !work->red || mesh->n_cases > 0) return FVM_E_ARG;
+    const Phys p = make_phys(phys);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (mesh->dim == 2)
+        FVM_LAUNCH(KID_BC, st, k_char_partial<2><<<1, kBlock, 0, st>>>(*mesh, p, prims, work->red));
+    else
+        FVM_LAUNCH(KID_BC, st, k_char_partial<3><<<1, kBlock, 0, st>>>(*mesh, p, prims, work->red));
+    return launch_status();
+}
+
+extern "C" int fvm_stage_begin(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const fvm_solver_bufs_t* bufs,
+                               const fvm_work_t* work, void* stream) {
+    if (const int rc = check_common(mesh)) return rc;
+    if (!phys || !bufs_ok(bufs) || !work_ok(mesh, work)) return FVM_E_ARG;
+    const Phys p = make_phys(phys);
+    cudaStream_t st = (cudaStream_t)stream;
+    return mesh->dim == 2 ? launch_begin<2>(mesh, p, bufs->prims, bufs->grads, bufs->has_grads, work, st)
+                          : launch_begin<3>(mesh, p, bufs->prims, bufs->grads, bufs->has_grads, work, st);
+}
+
+extern "C" int fvm_stage_end(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const fvm_tableau_t* tab, int32_t s,
+                             const fvm_solver_bufs_t* bufs, const fvm_work_t* work, int32_t finalize, void* stream) {
+    if (const int rc = check_common(mesh)) return rc;
+    if (!phys || !tab_ok(tab) || s < 0 || s >= tab->stages || !bufs_ok(bufs) || !work_ok(mesh, work))
+        return FVM_E_ARG;
+    if (mesh->n_cases > 0 && tab->adaptive) return FVM_E_UNSUPPORTED;
+    const Phys p = make_phys(phys);
+    cudaStream_t st = (cudaStream_t)stream;
+    return mesh->dim == 2 ? stage_finish<2>(mesh, p, tab, s, bufs, work, finalize != 0, st)
+                          : stage_finish<3>(mesh, p, tab, s, bufs, work, finalize != 0, st);
+}
+
+extern "C" int fvm_stage_finalize(const fvm_mesh_t* mesh, const fvm_tableau_t* tab, const fvm_solver_bufs_t* bufs,
+                                  const fvm_work_t* work, void* stream) {
+    if (!mesh_ok(mesh) || !tab_ok(tab) || !bufs_ok(bufs) || !work || !work->red) return FVM_E_ARG;
+    if (!(tab->adaptive || tab->cfl > 0.f || bufs->cons)) return FVM_OK;
+    return finalize_impl(mesh, tab, bufs, work, bufs->cons != nullptr, (cudaStream_t)stream);
+}
+
 extern "C" int fvm_multistep(const fvm_mesh_t* mesh, const fvm_physics_t* phys, int32_t store,
                              int32_t n_terms, const int32_t* idx, const float* coef,
                              const fvm_solver_bufs_t* bufs, const fvm_work_t* work, void* stream) {
@@ -1293,11 +1380,11 @@ extern "C" int fvm_state_to_prims(const fvm_mesh_t* mesh, const fvm_physics_t* p
     const Phys p = make_phys(phys);
     cudaStream_t st = (cudaStream_t)stream;
     if (mesh->dim == 2)
-        FVM_LAUNCH(KID_STATE_TO_PRIMS, st, k_state_to_prims<2><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
-                                               mesh->n_cells, p.inv_Cv, state, prims));
+        FVM_LAUNCH(KID_STATE_TO_PRIMS, st, k_state_to_prims<2><<<blocks_for(owned_cells(mesh)), kBlock, 0, st>>>(
+                                               owned_cells(mesh), p.inv_Cv, state, prims));
     else
-        FVM_LAUNCH(KID_STATE_TO_PRIMS, st, k_state_to_prims<3><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
-                                               mesh->n_cells, p.inv_Cv, state, prims));
+        FVM_LAUNCH(KID_STATE_TO_PRIMS, st, k_state_to_prims<3><<<blocks_for(owned_cells(mesh)), kBlock, 0, st>>>(
+                                               owned_cells(mesh), p.inv_Cv, state, prims));
     return launch_status();
 }
 

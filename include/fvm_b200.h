@@ -94,6 +94,15 @@ typedef struct fvm_mesh {
     const int32_t *bc_case;   /* [Fb] case of each boundary facet                           */
     const int32_t *ch_off;    /* [n_cases + 1] characteristic-facet offsets per case         */
     const float *case_mu, *case_mu_b, *case_kappa;   /* [n_cases] transport coefficients    */
+    /* Partitioned meshes (one part of a mesh split across ranks, single mesh only): cells
+     * [0, n_owned) are this part's own cells, [n_owned, n_cells) a one-cell-deep halo of copies
+     * of other parts' cells.  Gradients, divergences, stage updates and the CFL / conservation
+     * reductions cover owned cells only; the halo's primitives and limited gradients are written
+     * by the caller's exchange.  0 = every cell owned.  char_scale_given = 1: the
+     * characteristic-BC scale 10 / mean(c) is read from work->red[FVM_RED_DOUBLES + 6] (the
+     * caller forms it from every part's fvm_char_partial) instead of being computed here. */
+    int32_t n_owned;
+    int32_t char_scale_given;
 } fvm_mesh_t;
 
 /* Gas and scheme constants (ConfigFVM fields, time_fvm/config_fvm.py:52-63). */
@@ -195,6 +204,27 @@ int fvm_residual(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float 
  * that overlap on the GPU race and must be serialised by the caller. */
 int fvm_residual_noalloc(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *prims,
                          float *grads, int32_t *has_grads, float *dudt, void *stream);
+
+/* Split stage for partitioned meshes (no reference counterpart): a stage is fvm_stage_begin
+ * (boundary values + limited cell gradients of the owned cells from bufs->prims), then the
+ * caller's exchange of the halo cells' limited gradients, then fvm_stage_end (facet fluxes,
+ * divergence, stage combination and the next stage's primitives of the owned cells).  With
+ * finalize = 0 the last stage leaves its reductions in work->red (adaptive sums [0, 3C), CFL max
+ * at [16], conservation sums at [24, 24 + C)) for the caller to combine across parts, then
+ * fvm_stage_finalize turns them into dt / conservation output.  fvm_stage_begin + fvm_stage_end
+ * with finalize = 1 launch exactly what fvm_stage launches. */
+int fvm_stage_begin(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const fvm_solver_bufs_t *bufs,
+                    const fvm_work_t *work, void *stream);
+int fvm_stage_end(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const fvm_tableau_t *tab, int32_t s,
+                  const fvm_solver_bufs_t *bufs, const fvm_work_t *work, int32_t finalize, void *stream);
+int fvm_stage_finalize(const fvm_mesh_t *mesh, const fvm_tableau_t *tab, const fvm_solver_bufs_t *bufs,
+                       const fvm_work_t *work, void *stream);
+/* Partitioned meshes: this part's sum of the interior sound speed over its characteristic
+ * facets and their count into work->red[FVM_RED_DOUBLES + 6] and [+ 7] (padded primitives
+ * `prims`).  The caller sums both over the parts and stores 10 / (float)(sum / count) at [+ 6]
+ * before fvm_stage_begin when mesh->char_scale_given = 1 (facet_boundary.py:427). */
+int fvm_char_partial(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *prims,
+                     const fvm_work_t *work, void *stream);
 
 /* One explicit stage s of `tab` (residual of bufs->prims, then the stage combination); the
  * last stage writes the new state and, per `tab`, updates dt.  Adaptive tableaus are
