@@ -1430,6 +1430,7 @@ extern "C" int fvm_residual_noalloc(const fvm_mesh_t* mesh, const fvm_physics_t*
                                     float* grads, int32_t* has_grads, float* dudt, void* stream) {
     if (const int rc = check_common(mesh)) return rc;
     if (!phys || !prims || !grads || !has_grads || !dudt || !aligned16(grads)) return FVM_E_ARG;
+    if (mesh->char_scale_given) return FVM_E_ARG;   // its scratch holds no per-part slots
     const int64_t R = FVM_ROW(mesh->dim);
     const int64_t n_bc = align64((int64_t)mesh->n_bc * R);
     const int64_t n_prims = align64((int64_t)mesh->n_cells * R);

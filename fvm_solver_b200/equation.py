@@ -88,12 +88,13 @@ class DeviceMesh:
                       ("cell_rec", "div_rec", "face_rec", "cell_case", "face_case", "bc_case", "ch_off",
                        "case_mu", "case_mu_b", "case_kappa")]
 
-    def __init__(self, kt: KernelTables, device):
+    def __init__(self, kt: KernelTables, device, records: dict | None = None):
+        """``records``: precomputed device records (default ``kt.records()``)."""
         self.device = torch.device(device)
         self.dim, self.n_comp, self.n_cells = kt.dim, kt.n_comp, kt.n_cells
         self.n_facets, self.n_bc, self.kg, self.kf = kt.n_facets, kt.n_bc, kt.kg, kt.kf
         self.row, self.grow = row_sizes(kt.dim)
-        up = {k: v.contiguous().to(self.device) for k, v in kt.records().items()}
+        up = {k: v.contiguous().to(self.device) for k, v in (records or kt.records()).items()}
         for f in self._struct_fields:
             up[f] = getattr(kt, f).contiguous().to(self.device)
         self.t = SimpleNamespace(**up)
@@ -118,7 +119,8 @@ class Work:
         self.bc_vals = torch.zeros((max(dm.n_bc, 1), R), device=dev)
         self.prims = torch.zeros((dm.n_cells, R), device=dev)
         self.flux = torch.zeros((dm.n_facets, R), device=dev)
-        self.red = torch.zeros(_lib.FVM_RED_DOUBLES, device=dev, dtype=torch.float64)
+        # + 8: the per-part slots of partitioned meshes (fvm_char_partial / char_scale_given)
+        self.red = torch.zeros(_lib.FVM_RED_DOUBLES + 8, device=dev, dtype=torch.float64)
         self.struct = _lib.Work(bc_vals=_lib.ptr(self.bc_vals), prims=_lib.ptr(self.prims),
                                 flux=_lib.ptr(self.flux), red=_lib.ptr(self.red))
 

@@ -66,12 +66,21 @@ class MeshPart:
     facets: torch.Tensor           # [F_local] global facet ids
     bcs: torch.Tensor              # [Fb_local] global boundary-facet indices
     tables: KernelTables           # the part's tables, renumbered
+    face_rec: torch.Tensor | None = None       # [F_local][FVM_FACE_REC] facet records (see below)
     recv: dict = field(default_factory=dict)   # q -> (start, stop): halo rows owned by part q
     send: dict = field(default_factory=dict)   # q -> local ids of own cells part q keeps in its halo
 
     @property
     def n_local(self) -> int:
         return int(self.cells.numel())
+
+    def records(self) -> dict:
+        """Device records of the part: cell and divergence records from its tables, facet records
+        from the global ones (a facet record carries both sides' centroid -> facet displacements,
+        which for a halo side come from a cell whose own tables the part does not keep)."""
+        rec = self.tables.records()
+        rec["face_rec"] = self.face_rec
+        return rec
 
 
 def _remap(values: torch.Tensor, table: torch.Tensor, weights: torch.Tensor | None = None) -> torch.Tensor:
@@ -94,6 +103,7 @@ def split_tables(kt: KernelTables, parts: int, owner: torch.Tensor | None = None
     owner = partition_cells(N, parts) if owner is None else owner.long()
     fcell = kt.fcell.long()
     g_cols = kt.g_cols.long()                                 # [kg][N]
+    face_rec = kt.records()["face_rec"]
     out = []
     for p in range(parts):
         own = torch.nonzero(owner == p).flatten()
@@ -157,7 +167,16 @@ def split_tables(kt: KernelTables, parts: int, owner: torch.Tensor | None = None
             ch_cell=_remap(kt.ch_cell[chs], g2l) if chs.numel() else kt.ch_cell[:0].clone(),
             ch_normal=kt.ch_normal[chs].clone(), ch_rho=kt.ch_rho[chs].clone(), ch_vn=kt.ch_vn[chs].clone(),
             ch_vt=kt.ch_vt[chs].clone(), ch_p=kt.ch_p[chs].clone())
-        part = MeshPart(rank=p, parts=parts, n_owned=n_own, cells=cells, facets=facets, bcs=bcs, tables=t)
+        # facet records: the global rows with the side codes renumbered (cell -> local cell,
+        # boundary code -1 - b -> -1 - local b)
+        fr = face_rec[facets].clone()
+        codes = fr[:, :2].view(torch.int32).long()
+        loc = torch.where(codes >= 0, g2l[codes.clamp(min=0)], -1 - b2l[(-1 - codes).clamp(min=0)])
+        if bool((loc[codes >= 0] < 0).any()) or bool((loc[codes < 0] >= 0).any()):
+            raise RuntimeError("partition: a facet side points outside the part")
+        fr[:, :2] = loc.to(torch.int32).view(torch.float32)
+        part = MeshPart(rank=p, parts=parts, n_owned=n_own, cells=cells, facets=facets, bcs=bcs, tables=t,
+                        face_rec=fr)
         ho = owner[halo]
         for q in range(parts):
             sel = torch.nonzero(ho == q).flatten()
@@ -247,7 +266,7 @@ class _PartState:
     def __init__(self, part: MeshPart, n_k: int, device):
         from .equation import DeviceMesh
         self.part = part
-        self.dev = DeviceMesh(part.tables, device)
+        self.dev = DeviceMesh(part.tables, device, records=part.records())
         self.dev.struct.n_owned = part.n_owned
         # the characteristic-BC scale is the mean over all parts, formed by PartitionedSolver
         self.dev.struct.char_scale_given = 1

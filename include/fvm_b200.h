@@ -116,7 +116,8 @@ typedef struct fvm_work {
     float *bc_vals;     /* [Fb][FVM_ROW] boundary facet values                          */
     float *prims;       /* [N][FVM_ROW] padded primitives (used by fvm_residual only)   */
     float *flux;        /* [F][FVM_ROW] facet fluxes                                    */
-    double *red;        /* [FVM_RED_DOUBLES + 8 * n_cases], zero-initialised once */
+    double *red;        /* [FVM_RED_DOUBLES + 8 * n_cases], zero-initialised once; a partitioned
+                         * mesh (char_scale_given, fvm_char_partial) needs FVM_RED_DOUBLES + 8 */
 } fvm_work_t;
 
 /* Explicit Runge-Kutta tableau (optionally with an embedded low-order row). */
@@ -197,7 +198,8 @@ int fvm_residual(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float 
  * scratch does not fit -- 4 * (align64(Fb*R) + align64(N*R) + align64(F*R)
  * + align64(2*(64 + 8*n_cases))) bytes with R = FVM_ROW(dim), i.e. up to about 340 000 facets
  * (170 000 tetrahedra) in 3D or 600 000 facets (400 000 triangles) in 2D -- is rejected with
- * FVM_E_CAPACITY before anything is launched.  The function never allocates;
+ * FVM_E_CAPACITY before anything is launched; a partitioned mesh with char_scale_given = 1 is
+ * rejected with FVM_E_ARG (the scratch has no per-part slots).  The function never allocates;
  * the first call on each device looks up the array's device address (with that device
  * current), so make that first call before any stream capture.  Every call overwrites the
  * scratch it reads, so no clearing is needed; all calls on a device share the array, so calls

@@ -43,8 +43,18 @@ def test_partition_invariants(case, P):
             assert int(t.bc_cell.max()) < n_own
             assert torch.equal(p.cells[t.bc_cell.long()], kt.bc_cell[p.bcs].long())
             assert torch.equal(p.facets[t.bc_face.long()], kt.bc_face[p.bcs].long())
-        rec = t.records()                                                      # packs without error
+        rec = p.records()
         assert rec["cell_rec"].shape[0] == n_loc
+        # facet records: geometry and both sides' displacements as in the global records
+        grec = kt.records()["face_rec"][p.facets]
+        assert torch.equal(rec["face_rec"][:, 2:], grec[:, 2:])
+        codes, gcodes = rec["face_rec"][:, :2].view(torch.int32).long(), grec[:, :2].view(torch.int32).long()
+        cell_side = codes >= 0
+        assert torch.equal(p.cells[codes[cell_side]], gcodes[cell_side])
+        assert torch.equal(p.bcs[-1 - codes[~cell_side]], -1 - gcodes[~cell_side])
+        # the part's own cell and divergence records equal the global rows
+        grec_all = kt.records()
+        assert torch.equal(rec["cell_rec"][:n_own, t.kg * t.dim + t.kg:], grec_all["cell_rec"][p.cells[:n_own], t.kg * t.dim + t.kg:])
         # halo rows grouped by owner, matching the owner's send list
         for q, (a, b) in p.recv.items():
             assert torch.equal(parts[q].cells[parts[q].send[p.rank]], p.cells[a:b])
