@@ -51,9 +51,11 @@ def parse():
     ap.add_argument("--train-cases", type=int, default=32)
     ap.add_argument("--eval-cases", type=int, default=16)
     ap.add_argument("--iters", type=int, default=6000, help="corrector training iterations")
+    ap.add_argument("--parts", type=int, default=4,
+                    help="partitioned workload on one GPU: parts the box is split into")
     ap.add_argument("--windows", type=int, default=50, help="corrector rollout windows of k = 8 steps")
     ap.add_argument("--workload", default="taylor_green",
-                    choices=["taylor_green", "channel_cylinder", "ensemble", "corrector"],
+                    choices=["taylor_green", "channel_cylinder", "ensemble", "corrector", "partitioned"],
                     help="taylor_green: the headline 3D box; channel_cylinder: the 2D cylinder case (11k cells); "
                          "ensemble: batched 2D ensemble vs the same cases run one by one")
     ap.add_argument("--cases", type=int, default=256, help="ensemble size")
@@ -193,6 +195,103 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def partitioned_bench(args):
+    """One Taylor-Green box split into parts with one-cell halos (``fvm_solver_b200.partition``).
+
+    One process (no torchrun): ``--parts`` parts stepped on one GPU, exchanges as device copies;
+    reports the partitioned throughput next to the unpartitioned one on the same box and checks the
+    two final states for bitwise equality.  Under torchrun (N > 1): one part per rank, halo rows over
+    NCCL point-to-point, FP64 reductions over NCCL all-reduce; strong scaling (the box is fixed).
+    """
+    import torch.distributed as dist
+    from fvm_solver_b200 import workloads as W
+    from fvm_solver_b200.autotune import autotune
+    from fvm_solver_b200.partition import DistComm, LocalComm, PartitionedSolver, split_tables
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    case = W.taylor_green(n=args.n, device=f"cuda:{local}")
+    eq = case.equation()
+    autotune(eq)
+    N = eq.mesh.n_cells
+    state0 = eq.cells.state.clone()
+    t0 = time.time()
+    P = world if world > 1 else args.parts
+    parts = split_tables(eq.tables.kernel, P)
+    t_split = time.time() - t0
+    R, G = eq.dev.row, eq.dev.grow
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        ps = PartitionedSolver([parts[rank]], DistComm(parts[rank], f"cuda:{local}"), eq.phys, eq.t_solver.tab,
+                               device=f"cuda:{local}")
+        ps.set_state(state0)
+        ps.cfl_dt(case.cfg.cfl)
+        ps.step(args.warmup)
+        torch.cuda.synchronize()
+        dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ps.step(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        halo = torch.tensor([ps.halo_rows()], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(halo)
+        dist.barrier()
+        dist.destroy_process_group()
+        if rank == 0:
+            ms = float(t.item())
+            print(json.dumps({"metric": "cell-steps/s", "value": N * args.steps / (ms / 1e3), "unit": "cell-steps/s",
+                              "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                              "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+                              "dtype": "f32", "data": "synthetic",
+                              "config": {"workload": "taylor_green_partitioned", "cells": N, "parts": world,
+                                         "halo_rows_total": int(halo.item()),
+                                         "exchange": "NCCL point-to-point halo rows, NCCL all-reduce"}}))
+        return
+    # one GPU: single mesh, then the same box in P parts, both from state0 for K graph-replayed steps
+    sol = eq.t_solver
+    replay = sol.graph_steps(args.steps)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    replay()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms_single = a.elapsed_time(b)
+    want = eq.cells.state.clone()
+    del replay
+    ps = PartitionedSolver(parts, LocalComm(parts, "cuda"), eq.phys, sol.tab)
+    ps.set_state(state0)
+    ps.cfl_dt(case.cfg.cfl)
+    preplay = ps.graph_steps(args.steps)
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clk:
+        a.record(stream)
+        preplay()
+        b.record(stream)
+        torch.cuda.synchronize()
+    ms_part = a.elapsed_time(b)
+    got = torch.empty_like(want)
+    ps.gather_state(got)
+    halo = ps.halo_rows()
+    stages = sol.tab.stages
+    print(json.dumps({"metric": "cell-steps/s", "value": N * args.steps / (ms_part / 1e3), "unit": "cell-steps/s",
+                      "n_gpus": 1, "steps": args.steps, "warmup": 0, "ms_per_step": ms_part / args.steps,
+                      "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+                      "config": {"workload": "taylor_green_partitioned_on_one_gpu", "cells": N, "parts": P,
+                                 "timing": "cuda graph replay", "split_seconds": t_split},
+                      "unpartitioned": {"value": N * args.steps / (ms_single / 1e3), "ms_per_step": ms_single / args.steps},
+                      "halo_rows_total": halo, "halo_fraction": halo / N,
+                      "exchange_bytes_per_step": halo * 4 * (R + G) * stages,
+                      "bitwise_equal_to_unpartitioned": bool(torch.equal(got, want)),
+                      "clocks": clk.summary()}))
+
+
 def secondary(args):
     """Secondary workloads (single GPU): the 2D channel-cylinder case and the batched ensemble."""
     from fvm_solver_b200 import _lib, workloads as W
@@ -211,6 +310,8 @@ def secondary(args):
 
     if args.workload == "corrector":
         return corrector_bench(args, timed)
+    if args.workload == "partitioned":
+        return partitioned_bench(args)
     if args.workload == "channel_cylinder":
         case = W.channel_cylinder(device="cuda")
         eq = case.equation()

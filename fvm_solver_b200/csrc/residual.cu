@@ -476,12 +476,17 @@ __global__ void __launch_bounds__(kMaxBlock) k_face(fvm_mesh_t m, Phys p, const 
     // Normal gradient (A_face_grad row, facet_process.py:420-450).
     float dn[NG];
     if (ca >= 0 && cb >= 0) {
-        const float w = rec[Ly::INVD];
+        // The row's two products are summed in the order of the mesh's cell numbering (ascending
+        // ELL columns); the record's sign of 1/d says whether side 0 comes first, so a renumbered
+        // part of the mesh sums them in the same order as the whole mesh.
+        const float ws = rec[Ly::INVD];
+        const float w = fabsf(ws);
+        const bool side0_first = ws > 0.f;
 #pragma unroll
         for (int k = 0; k < NG; ++k) {
             const int comp = k < DIM ? k : DIM + 1;
             const float x0 = P0[comp], x1 = P1[comp];
-            dn[k] = ca < cb ? fmaf(w, x1, (-w) * x0) : fmaf(-w, x0, w * x1);
+            dn[k] = side0_first ? fmaf(w, x1, (-w) * x0) : fmaf(-w, x0, w * x1);
         }
     } else {
         const int b = ca < 0 ? -1 - ca : -1 - cb;

@@ -340,8 +340,30 @@ class PartitionedSolver:
         self.comm.allreduce([ps.work.red[sl] for ps in self.parts], "sum")
         for ps in self.parts:
             r = ps.work.red
-            mean = (r[sl][0] / r[sl][1]).float()
-            r[_lib.FVM_RED_DOUBLES + 6] = (torch.tensor(10.0, device=r.device) / mean).double()
+            mean = (r[sl][:1] / r[sl][1:]).float()          # (float)(sum / count), as in k_bc
+            r[sl][:1] = (torch.full_like(mean, 10.0) / mean).double()
+
+    def graph_steps(self, n: int):
+        """Capture ``n`` steps (kernels, exchanges and reductions) in a CUDA graph; returns a
+        callable that replays them.  The state must already be set (``set_state``)."""
+        dev = self.parts[0].state.device
+        st = torch.cuda.Stream(device=dev)
+        st.wait_stream(torch.cuda.current_stream())
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(st):
+            with torch.cuda.graph(g, stream=st):
+                self.step(n)
+        torch.cuda.current_stream().wait_stream(st)
+
+        def replay():
+            g.replay()
+
+        replay.graph = g
+        return replay
+
+    def halo_rows(self) -> int:
+        """Rows received per exchange, summed over this process's parts."""
+        return sum(ps.part.n_local - ps.part.n_owned for ps in self.parts)
 
     def step(self, n: int = 1):
         S = self.tab.stages

@@ -219,7 +219,8 @@ class KernelTables:
         displacements [K][dim], limiter epsilon, meta (int32 bits), zero padding.
         Divergence record [N][8]: weights [kf], facet indices [kf] (int32 bits), padding.
         Facet record [F][FR]: side-0 cell, side-1 cell (int32 bits; a boundary side holds
-        -1 - boundary index), 1/d, |S|, normal [dim], non-orthogonal vector [dim], side-0 and
+        -1 - boundary index), +-1/d (negative: side 1's cell has the lower index), |S|, normal [dim],
+        non-orthogonal vector [dim], side-0 and
         side-1 centroid->facet displacements [dim] each, padding.
         """
         dim, N, F, K, kg, kf = self.dim, self.n_cells, self.n_facets, self.dim + 1, self.kg, self.kf
@@ -249,7 +250,10 @@ class KernelTables:
         face = torch.zeros((F, FR), dtype=torch.float32)
         face[:, 0] = bits(codes[:, 0].contiguous())
         face[:, 1] = bits(codes[:, 1].contiguous())
-        face[:, 2] = self.inv_d
+        # 1/d, negative when the side-1 cell precedes the side-0 cell in the cell numbering (the
+        # order in which the facet's normal-gradient row sums its two terms)
+        order = torch.where(self.fcell[:, 0] < self.fcell[:, 1], 1.0, -1.0).to(torch.float32)
+        face[:, 2] = self.inv_d * order
         face[:, 3] = self.fsize
         face[:, 4:4 + dim] = self.normals
         face[:, 4 + dim:4 + 2 * dim] = self.xorth

@@ -68,7 +68,9 @@ typedef struct fvm_mesh {
     const double *inv_h;      /* [N] max facet area / volume (CFL)                          */
     const double *volumes;    /* [N]                                                        */
     /* [F][FVM_FACE_REC]: side-0 cell, side-1 cell (a boundary side holds -1 - boundary index),
-     * 1/d, |S|, area normal [dim], non-orthogonal correction vector [dim], centroid->facet
+     * +-1/d (negative when the side-1 cell has the lower index: the order in which the facet's
+     * normal-gradient row sums its two terms), |S|, area normal [dim], non-orthogonal correction
+     * vector [dim], centroid->facet
      * displacement of side 0 [dim] and of side 1 [dim] */
     const float *face_rec;
     /* boundary facets */

@@ -65,7 +65,10 @@ def test_device_records_encode_tables(golden):
     side = K.bc_side.long()
     assert torch.equal(codes[bc, side], -1 - torch.arange(K.n_bc, dtype=torch.int32))
     assert torch.equal(codes[bc, 1 - side], K.bc_cell)
-    assert torch.equal(face[:, 2], K.inv_d) and torch.equal(face[:, 3], K.fsize)
+    assert torch.equal(face[:, 2].abs(), K.inv_d.abs()) and torch.equal(face[:, 3], K.fsize)
+    inner = K.fbc < 0
+    first = K.fcell[:, 0] < K.fcell[:, 1]
+    assert torch.equal(face[inner, 2] > 0, first[inner])      # sign: order of the row's two terms
     # side displacements reproduce cent_to_facet_disp through cell_to_facet
     for j in range(dim + 1):
         f = K.c2f[j].long()
