@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--train-cases", type=int, default=32)
     ap.add_argument("--eval-cases", type=int, default=16)
     ap.add_argument("--iters", type=int, default=6000, help="corrector training iterations")
+    ap.add_argument("--drift-steps", type=int, default=500,
+                    help="channel_cylinder: steps of the trajectory compared with the FP32/FP64 oracle (0: skip)")
     ap.add_argument("--parts", type=int, default=4,
                     help="partitioned workload on one GPU: parts the box is split into")
     ap.add_argument("--windows", type=int, default=50, help="corrector rollout windows of k = 8 steps")
@@ -113,6 +115,51 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def _oracle_channel_trajectory(job):
+    """The oracle's SSP-RK3 + CFL 0.5 run of the channel-cylinder case from its initial condition,
+    in float32 or float64; returns the conserved state every ``every`` steps."""
+    dtype_name, n_steps, every = job
+    torch.set_num_threads(1)
+    from fvm_solver_b200 import workloads as W
+    from oracle import fvm_oracle as O
+    dt_ = np.float32 if dtype_name == "f32" else np.float64
+    case = W.channel_cylinder(device="cpu")
+    T = case.tables()
+    res = O.OracleResidual(T, case.cfg, dt_)
+    inv_h = T.kernel.inv_h.numpy()
+    s = O.OracleSolver(res, case.state0.numpy().astype(dt_), 1e-4)
+    out = []
+    for k in range(1, n_steps + 1):
+        s.dt = res.dt(O.cfl_dt(s.state, 2, case.cfg.C_v, case.cfg.gamma, inv_h, 0.5))
+        s.butcher_step("SSP_RK3")
+        if k % every == 0:
+            out.append(np.asarray(s.state, dtype=np.float64).copy())
+    return out
+
+
+def channel_drift(n_steps: int, every: int = 100) -> dict:
+    """Config-1 trajectory agreement: the CUDA path's state after 100, 200, ... SSP-RK3 steps
+    against the FP32 oracle (the reference's arithmetic) and the FP64 oracle, as rel-L2 over the
+    whole state (a drift curve; the flow is unsteady, so differences grow with time)."""
+    import multiprocessing as mp
+    from fvm_solver_b200 import workloads as W
+    with mp.get_context("spawn").Pool(2) as pool:
+        pending = pool.map_async(_oracle_channel_trajectory, [("f32", n_steps, every), ("f64", n_steps, every)])
+        case = W.channel_cylinder(device="cuda")
+        eq = case.equation()
+        gpu = []
+        for k in range(1, n_steps + 1):
+            eq.t_solver.step(1)
+            if k % every == 0:
+                gpu.append(eq.cells.state.double().cpu().numpy())
+        o32, o64 = pending.get()
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    return {"steps": list(range(every, n_steps + 1, every)),
+            "gpu_vs_oracle_fp32": [rel(g, o) for g, o in zip(gpu, o32)],
+            "gpu_vs_oracle_fp64": [rel(g, o) for g, o in zip(gpu, o64)],
+            "oracle_fp32_vs_fp64": [rel(a, b) for a, b in zip(o32, o64)]}
 
 
 def _oracle_worker(job):
@@ -359,12 +406,15 @@ def secondary(args):
             el = time.perf_counter() - t0
             cpu = {"value": N * n / el, "unit": "cell-steps/s", "cores": 1, "kind": "port",
                    "sample": f"numpy oracle, same mesh ({N} cells), {n} SSP-RK3 steps, {el:.1f} s"}
+        drift = None
+        if args.drift_steps:
+            drift = channel_drift(args.drift_steps)
         out = {"metric": "cell-steps/s", "value": N * args.steps / (ms / 1e3), "unit": "cell-steps/s", "n_gpus": 1,
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                "dtype": "f32", "data": "synthetic",
                "config": {"workload": "channel_cylinder_2d_ssprk3_cfl0.5", "cells": N, "facets": eq.dev.n_facets,
                           "l2": "working set fits in L2 (launch/latency bound case)", "timing": "cuda graph replay"},
-               "cpu_baseline": cpu, "clocks": clk.summary()}
+               "cpu_baseline": cpu, "drift_vs_oracle": drift, "clocks": clk.summary()}
         print(json.dumps(out))
         return
 
