@@ -48,16 +48,17 @@ def parse():
     ap.add_argument("--sample-n", type=int, default=20, help="points per axis of the CPU sample box")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--train-cases", type=int, default=32)
+    ap.add_argument("--train-cases", type=int, default=None, help="corrector: 32 (2D) / 4 (3D)")
     ap.add_argument("--eval-cases", type=int, default=16)
-    ap.add_argument("--iters", type=int, default=6000, help="corrector training iterations")
+    ap.add_argument("--iters", type=int, default=None, help="corrector training iterations: 6000 (2D) / 2000 (3D)")
     ap.add_argument("--drift-steps", type=int, default=500,
                     help="channel_cylinder: steps of the trajectory compared with the FP32/FP64 oracle (0: skip)")
     ap.add_argument("--parts", type=int, default=4,
                     help="partitioned workload on one GPU: parts the box is split into")
     ap.add_argument("--windows", type=int, default=50, help="corrector rollout windows of k = 8 steps")
     ap.add_argument("--workload", default="taylor_green",
-                    choices=["taylor_green", "channel_cylinder", "ensemble", "corrector", "partitioned"],
+                    choices=["taylor_green", "channel_cylinder", "ensemble", "corrector", "corrector3d",
+                             "partitioned"],
                     help="taylor_green: the headline 3D box; channel_cylinder: the 2D cylinder case (11k cells); "
                          "ensemble: batched 2D ensemble vs the same cases run one by one")
     ap.add_argument("--cases", type=int, default=256, help="ensemble size")
@@ -377,7 +378,7 @@ def secondary(args):
         torch.cuda.synchronize()
         return a.elapsed_time(b)
 
-    if args.workload == "corrector":
+    if args.workload in ("corrector", "corrector3d"):
         return corrector_bench(args, timed)
     if args.workload == "partitioned":
         return partitioned_bench(args)
@@ -474,21 +475,32 @@ def corrector_bench(args, timed):
     from fvm_solver_b200 import batched as B, workloads as W
     from fvm_solver_b200.corrector import CheckedRollout, CorrectorModel, record_trajectory, train
     workers = min(16, os.cpu_count() or 1)
+    three_d = args.workload == "corrector3d"
+    if args.train_cases is None:
+        args.train_cases = 4 if three_d else 32
+    if args.iters is None:
+        args.iters = 2000 if three_d else 6000
+    family = "sphere" if three_d else "channel"
+    params = (lambda i, seed: W.sphere_params(i, seed)) if three_d else W.ensemble_params
+    seeds = (5678, 9100) if three_d else (1234, 9000)
 
     def make(n, seed):
-        parts = B.build_ensemble_tables(n, base_seed=seed, workers=workers)
-        cfg = copy.deepcopy(W.ensemble_case(0, device="cuda", base_seed=seed).cfg)
+        parts = B.build_ensemble_tables(n, base_seed=seed, workers=workers, family=family)
+        case0 = W.sphere_case(0, device="cuda", base_seed=seed, cells=(20_000, 20_000)) if three_d else \
+            W.ensemble_case(0, device="cuda", base_seed=seed)
+        cfg = copy.deepcopy(case0.cfg)
         cfg.solver_name, cfg.solver_extra, cfg.cfl = "Butcher", "SSP_RK3", None
-        prm = torch.tensor([[W.ensemble_params(i, seed)["mach"], np.log10(W.ensemble_params(i, seed)["reynolds"])]
+        prm = torch.tensor([[params(i, seed)["mach"], np.log10(params(i, seed)["reynolds"])]
                             for i in range(n)], dtype=torch.float32)
         return parts, cfg, prm
 
     t0 = time.time()
-    parts, cfg, prm = make(args.train_cases, 1234)
+    parts, cfg, prm = make(args.train_cases, seeds[0])
     batch = B.BatchedFVM(parts, cfg, device="cuda")
     batch.t_solver.update_cfl_dt(0.5)
-    traj = record_trajectory(batch, steps=400, spinup=200)
+    traj = record_trajectory(batch, steps=200 if three_d else 400, spinup=200)
     model = CorrectorModel(batch, prm, k=8, seed=0, lr=1e-3)
+    batch_cells = batch.n_cells
     torch.cuda.synchronize()
     t1 = time.time()
     hist = train(model, traj, iters=args.iters, log_every=max(1, args.iters // 10))
@@ -497,7 +509,7 @@ def corrector_bench(args, timed):
     del traj
     torch.cuda.empty_cache()
 
-    eparts, ecfg, eprm = make(args.eval_cases, 9000)
+    eparts, ecfg, eprm = make(args.eval_cases, seeds[1])
     plain = B.BatchedFVM(eparts, ecfg, device="cuda")
     plain.t_solver.update_cfl_dt(0.5)
     plain.t_solver.step(200)
@@ -551,7 +563,9 @@ def corrector_bench(args, timed):
     strict = rollout(1.2)
     out = {"metric": "sim-time/s corrector+fallback over plain FVM", "value": spec["speedup"], "unit": "x",
            "higher_is_better": True, "n_gpus": 1, "dtype": "bf16 GEMM / f32 state", "data": "synthetic",
-           "config": {"workload": "corrector_2d_k8", "train_cases": args.train_cases, "eval_cases": args.eval_cases,
+           "config": {"workload": "corrector_3d_sphere_k8" if three_d else "corrector_2d_k8",
+                      "train_cases": args.train_cases, "eval_cases": args.eval_cases,
+                      "train_cells": int(batch_cells), "eval_cells": int(plain.n_cells),
                       "iters": args.iters, "windows": args.windows, "fvm": "SSP-RK3, fixed per-case dt (CFL 0.5)",
                       "net": "4 message-passing layers, width 64, SiLU, tcgen05 BF16 GEMMs",
                       "checks": "drift <= 1e-4, residual norm <= 3x, admissible state"},

@@ -47,8 +47,10 @@ def build_case_tables(case) -> CaseTables:
 
 
 def _ensemble_worker(args):
-    from .workloads import ensemble_case
-    i, base_seed = args
+    from .workloads import ensemble_case, sphere_case
+    i, base_seed, family, cells = args
+    if family == "sphere":
+        return build_case_tables(sphere_case(i, device="cpu", base_seed=base_seed, cells=cells))
     return build_case_tables(ensemble_case(i, device="cpu", base_seed=base_seed))
 
 
@@ -57,9 +59,12 @@ def _worker_init():
     torch.set_num_threads(1)
 
 
-def build_ensemble_tables(n_cases: int, base_seed: int = 1234, workers: int = 0) -> list:
-    """Per-case tables of the seeded ensemble; ``workers > 0`` builds them in spawned processes."""
-    jobs = [(i, base_seed) for i in range(n_cases)]
+def build_ensemble_tables(n_cases: int, base_seed: int = 1234, workers: int = 0, family: str = "channel",
+                          cells=(300_000, 800_000)) -> list:
+    """Per-case tables of a seeded ensemble -- ``family`` "channel" (2D channel-cylinder cases) or
+    "sphere" (3D flow over a sphere, ``cells`` the tet-count range); ``workers > 0`` builds them in
+    spawned processes."""
+    jobs = [(i, base_seed, family, tuple(cells)) for i in range(n_cases)]
     if workers > 0:
         ctx = mp.get_context("spawn")
         with cfut.ProcessPoolExecutor(max_workers=workers, mp_context=ctx, initializer=_worker_init) as ex:

@@ -185,6 +185,44 @@ class ChannelCylinderConfig(ConfigFVM):
 
 
 @dataclass
+class SphereConfig(ConfigFVM):
+    """3D flow over a sphere of radius 0.5 in [-5, 15] x [-5, 5]^2; freestream along +x, Mach /
+    Reynolds on the diameter.  Gas and transport as ``ChannelCylinderConfig``; the box faces are
+    characteristic boundaries with the freestream velocity vector, the sphere is a no-slip wall.
+    """
+    problem_setup: str | None = "sphere"
+    N_comp: int = 5
+    solver_name: str = "Butcher"
+    solver_extra: str = "SSP_RK3"
+    cfl: float | None = 0.5
+    dt: float | None = 1e-4
+    n_iter: int | None = 500
+    mach: float = 0.3
+    reynolds: float = 200.0
+    prandtl: float = 0.72
+    radius: float = 0.5
+    rho_inf: float = 1.0
+    T_inf: float = 100.0
+    T_0: float | None = 100.0
+    S_const: float | None = 110.4
+    gamma: float | None = 1.4
+    C_v: float | None = 2.0
+    noise: float = 1e-3
+
+    def __post_init__(self):
+        self.T_0 = self.T_inf
+        U = self.mach * _gas(self.gamma, self.C_v, self.T_inf)
+        self.u_inf = U
+        mu0 = self.rho_inf * U * (2.0 * self.radius) / self.reynolds
+        self.viscosity = mu0
+        self.visc_bulk = mu0
+        self.thermal_cond = self.gamma * self.C_v * mu0 / self.prandtl
+        v = (U, 0.0, 0.0)
+        self.inlet_cfg = CharacteristicBC(v_inf=v, rho_inf=self.rho_inf, T_inf=self.T_inf)
+        self.exit_cfg = CharacteristicBC(v_inf=v, rho_inf=self.rho_inf, T_inf=self.T_inf)
+
+
+@dataclass
 class TaylorGreenConfig(ConfigFVM):
     """3D periodic box [0, 2 pi L]^3, Taylor-Green vortex at Mach / Reynolds on V0 and L = 1."""
     problem_setup: str | None = "taylor_green"

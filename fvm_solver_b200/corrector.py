@@ -251,7 +251,8 @@ class CorrectorModel:
         self.nbr = neighbour_table(kt).to(dev)
         self.cell_case = batch.dev.case["cell_case"].long().to(dev)
         cp = case_params[self.cell_case.cpu()]
-        self.geo = geometry_features(kt, cp).to(dev)
+        lengths = (2.0, 1.0) if kt.dim == 2 else (20.0, 10.0, 10.0)   # channel / sphere box extents
+        self.geo = geometry_features(kt, cp, lengths).to(dev)
         if 2 * C + self.geo.shape[1] > XW:
             raise ValueError("too many input features")
         self.vol = kt.volumes.to(dev).double()

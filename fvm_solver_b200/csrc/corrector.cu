@@ -384,7 +384,7 @@ __global__ void k_silu_back(const float* __restrict__ dh, const float* __restric
 __global__ void k_transpose_bf16(const __nv_bfloat16* __restrict__ src, int R, int Cc, int64_t lds,
                                  __nv_bfloat16* __restrict__ dst, int64_t ldd) {
     __shared__ __nv_bfloat16 tile[32][33];
-    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;   // rows on x: R may exceed 65535 * 32
     for (int k = threadIdx.y; k < 32; k += blockDim.y) {
         const int r = r0 + k, c = c0 + threadIdx.x;
         tile[k][threadIdx.x] = (r < R && c < Cc) ? src[(int64_t)r * lds + c] : __float2bfloat16(0.f);
@@ -587,9 +587,9 @@ extern "C" int fvm_silu_back(const float* dh, const float* Z, int32_t N, int32_t
 
 extern "C" int fvm_transpose_bf16(const void* src, int32_t R, int32_t Cc, int64_t lds, void* dst, int64_t ldd,
                                   void* stream) {
-    if (!src || !dst || R <= 0 || Cc <= 0 || ldd < R || lds < Cc) return FVM_E_ARG;
+    if (!src || !dst || R <= 0 || Cc <= 0 || ldd < R || lds < Cc || (Cc + 31) / 32 > 65535) return FVM_E_ARG;
     cudaStream_t s = (cudaStream_t)stream;
-    dim3 grid((unsigned)((Cc + 31) / 32), (unsigned)((R + 31) / 32));
+    dim3 grid((unsigned)((R + 31) / 32), (unsigned)((Cc + 31) / 32));
     FVM_LAUNCH(KID_CORRECTOR, s, corr::k_transpose_bf16<<<grid, dim3(32, 8), 0, s>>>(
                                      static_cast<const __nv_bfloat16*>(src), R, Cc, lds,
                                      static_cast<__nv_bfloat16*>(dst), ldd));

@@ -187,6 +187,91 @@ def channel_cylinder_cells(n_cells: int, **kw) -> MeshSpec:
 
 
 # ---------------------------------------------------------------------------------------------
+# 3D flow over a sphere
+# ---------------------------------------------------------------------------------------------
+def sphere_box(n_cells: int = 500_000, radius: float = 0.5, box=((-5.0, 15.0), (-5.0, 5.0), (-5.0, 5.0)),
+               seed: int = 0, jitter: float = 0.2, levels: int = 4) -> MeshSpec:
+    """Tetrahedral mesh of a box around a sphere at the origin, with about ``n_cells`` tets.
+
+    Points are nested jittered grids: spacing H over the whole box and H / 2^l inside boxes around
+    the sphere that shrink with the level l (finest next to the sphere), each level's grid cut out
+    of the coarser ones; grid points on the box faces stay on their planes, and a Fibonacci lattice
+    at the finest spacing lies on the sphere.  After the Delaunay tetrahedralisation, tets whose
+    centroid lies inside the sphere are removed.  Boundary tags: the sphere "NavierWall", the
+    x-min face "Left" (inlet), the x-max face "Right" (exit), the four side faces "Farfield".
+    """
+    rng = np.random.default_rng(seed)
+    lo = np.array([b[0] for b in box], dtype=np.float64)
+    hi = np.array([b[1] for b in box], dtype=np.float64)
+    ext = hi - lo
+
+    def grid(a, b, h, on_faces):
+        n = np.maximum(1, np.round((b - a) / h).astype(int))
+        axes = [np.linspace(a[d], b[d], n[d] + 1) for d in range(3)]
+        P = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
+        hh = (b - a) / n
+        on = np.zeros_like(P, dtype=bool)
+        if on_faces:
+            on = (np.abs(P - lo) < 1e-9) | (np.abs(P - hi) < 1e-9)
+        return P + np.where(on, 0.0, rng.uniform(-jitter, jitter, P.shape) * hh), hh.min()
+
+    # level boxes: level l covers [-w_l, w_l]^3 around the sphere (clipped to the domain), w_l shrinking
+    def level_box(l):
+        w = radius * 2.5 * 2.0 ** (levels - 1 - l)
+        return np.maximum(lo, -w), np.minimum(hi, w)
+
+    def count(H):
+        tot = np.prod(ext / H)
+        for l in range(1, levels):
+            a, b = level_box(l)
+            tot += np.prod((b - a) / (H / 2 ** l)) * (1 - 1 / 8)
+        return tot * 7.0                      # ~7 tets per grid point (measured)
+
+    H = float(ext.min() / 8)
+    for _ in range(60):                       # spacing for the requested cell count
+        H *= (count(H) / n_cells) ** (1 / 3)
+    pts, _ = grid(lo, hi, H, True)
+    for l in range(1, levels):
+        a, b = level_box(l)
+        h = H / 2 ** l
+        inside = np.all((pts > a + 1e-9) & (pts < b - 1e-9), axis=1)
+        pts = pts[~inside]
+        fine, _ = grid(a, b, h, True)
+        keep = np.all((fine > a - 1e-9) & (fine < b + 1e-9), axis=1)
+        pts = np.concatenate([pts, fine[keep]])
+    h_min = H / 2 ** (levels - 1)
+    # points near the sphere: remove those inside or too close, add a surface lattice
+    r = np.linalg.norm(pts, axis=1)
+    pts = pts[r > radius + 0.45 * h_min]
+    n_s = max(60, int(round(4 * np.pi * radius ** 2 / (h_min ** 2 * np.sqrt(3) / 2))))
+    k = np.arange(n_s) + 0.5
+    phi = np.arccos(1 - 2 * k / n_s)
+    th = np.pi * (1 + 5 ** 0.5) * k
+    surf = radius * np.stack([np.cos(th) * np.sin(phi), np.sin(th) * np.sin(phi), np.cos(phi)], 1)
+    pts = np.unique(np.round(np.concatenate([pts, surf]), 12), axis=0)
+    pts = pts[morton_order(pts)]
+    tet = Delaunay(pts).simplices.astype(np.int64)
+    c = pts[tet].mean(axis=1)
+    tet = tet[np.linalg.norm(c, axis=1) > radius]
+    tet = _drop_degenerate(pts, tet, 1e-14 * float(np.prod(ext)) / len(pts))
+
+    def tag(fp):
+        if np.all(np.abs(np.linalg.norm(fp, axis=1) - radius) < 1e-6):
+            return "NavierWall"
+        if np.all(np.abs(fp[:, 0] - lo[0]) < 1e-9):
+            return "Left"
+        if np.all(np.abs(fp[:, 0] - hi[0]) < 1e-9):
+            return "Right"
+        on_side = any(np.all(np.abs(fp[:, d] - v) < 1e-9) for d in (1, 2) for v in (lo[d], hi[d]))
+        assert on_side, f"stray boundary facet {fp}"
+        return "Farfield"
+
+    spec = _finish_mesh(pts, tet, tag)
+    spec.info = dict(kind="sphere_box", radius=radius, seed=seed, spacing=H, spacing_min=h_min)
+    return spec
+
+
+# ---------------------------------------------------------------------------------------------
 # 3D boxes
 # ---------------------------------------------------------------------------------------------
 def box3d(n: int = 12, size: float = 1.0, seed: int = 0, jitter: float = 0.2,

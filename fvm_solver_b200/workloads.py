@@ -113,3 +113,35 @@ def ensemble_case(case_index: int, device: str = "cuda", base_seed: int = 1234, 
     c = channel_cylinder(device=device, solver_name="AB3", solver_extra="SSP_RK3", **p, **cfg_kw)
     c.name = f"ensemble_{case_index}"
     return c
+
+
+def sphere(n_cells: int = 500_000, seed: int = 0, device: str = "cuda", mach: float = 0.3, reynolds: float = 200.0,
+           **cfg_kw) -> Case:
+    """3D flow over a sphere (radius 0.5, box [-5, 15] x [-5, 5]^2): uniform freestream along +x with
+    seeded Gaussian density noise of amplitude 1e-3."""
+    spec = mg.sphere_box(n_cells, seed=seed)
+    cfg = cf.SphereConfig(device=device, mach=mach, reynolds=reynolds, **cfg_kw)
+    N = spec.n_cells
+    g = torch.Generator().manual_seed(seed)
+    noise = torch.randn(N, generator=g, dtype=torch.float64).numpy()
+    prim = np.zeros((N, 5))
+    prim[:, 0] = cfg.u_inf
+    prim[:, 3] = cfg.rho_inf * (1.0 + cfg.noise * noise)
+    prim[:, 4] = cfg.T_inf
+    st = torch.from_numpy(conserved(prim, 3, cfg.C_v).astype(np.float32))
+    return Case(spec, cfg, default_bc_tags(spec.bc_tags, 3), st, f"sphere_{N}")
+
+
+def sphere_params(case_index: int, base_seed: int = 5678, cells=(300_000, 800_000)) -> dict:
+    """Per-case parameters of the 3D sphere family (seeded): cells uniform in ``cells``, Mach
+    0.2-0.4, Reynolds 100-400."""
+    rng = np.random.default_rng(base_seed + case_index)
+    return dict(n_cells=int(rng.uniform(*cells)), mach=float(rng.uniform(0.2, 0.4)),
+                reynolds=float(rng.uniform(100, 400)), seed=int(base_seed + case_index))
+
+
+def sphere_case(case_index: int, device: str = "cuda", base_seed: int = 5678, cells=(300_000, 800_000),
+                **cfg_kw) -> Case:
+    c = sphere(device=device, **sphere_params(case_index, base_seed, cells), **cfg_kw)
+    c.name = f"sphere_{case_index}"
+    return c

@@ -122,3 +122,36 @@ def test_training_reduces_loss_and_rollout(small_batch):
         assert torch.equal(ok, oks[w])
     rel = float((batch.cells.state - end_graph).norm() / end_graph.norm())
     assert rel < 1e-5
+
+
+def test_corrector_3d_sphere_batch():
+    """The corrector on a batch of two small 3D sphere cases (C = 5): training lowers the loss, the
+    proposal keeps each case's mass and energy change at k dt sum(vol dU/dt), rollouts stay finite."""
+    import copy
+    import numpy as np
+    from fvm_solver_b200 import batched as B, workloads as W
+    from fvm_solver_b200.corrector import CheckedRollout, CorrectorModel, record_trajectory, train
+    parts = B.build_ensemble_tables(2, base_seed=77, family="sphere", cells=(15_000, 25_000))
+    cfg = copy.deepcopy(W.sphere_case(0, device="cuda", base_seed=77, cells=(15_000, 15_000)).cfg)
+    cfg.solver_name, cfg.solver_extra, cfg.cfl = "Butcher", "SSP_RK3", None
+    prm = torch.tensor([[W.sphere_params(i, 77)["mach"], np.log10(W.sphere_params(i, 77)["reynolds"])]
+                        for i in range(2)], dtype=torch.float32)
+    batch = B.BatchedFVM(parts, cfg, device="cuda")
+    batch.t_solver.update_cfl_dt(0.5)
+    traj = record_trajectory(batch, steps=40, spinup=5)
+    model = CorrectorModel(batch, prm, k=8, seed=2, lr=2e-3)
+    hist = train(model, traj, iters=200, log_every=50)
+    assert hist[-1][1] < hist[0][1]
+    U = batch.cells.state.clone()
+    r0 = model.res(U, torch.empty_like(U))
+    prop = model.predict(U, torch.empty_like(U), r0)
+    vol = model.vol.unsqueeze(1)
+    cc = model.cell_case
+    dM = torch.zeros(2, 5, dtype=torch.float64, device="cuda").index_add_(0, cc, (prop - U).double() * vol)
+    want = torch.zeros_like(dM).index_add_(0, cc, r0.double() * vol) * (model.k * batch.t_solver.dt.double())[:, None]
+    M = torch.zeros_like(dM).index_add_(0, cc, U.double() * vol)
+    assert float(((dM - want)[:, 3:].abs() / M[:, 3:].abs()).max()) < 1e-5
+    ro = CheckedRollout(model)
+    for _ in range(2):
+        assert ro.window().shape == (2,)
+    assert torch.isfinite(batch.cells.state).all()

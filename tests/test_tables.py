@@ -75,3 +75,20 @@ def test_device_records_encode_tables(golden):
         s_ = ((K.side >> j) & 1).long()
         off = 4 + 2 * dim + s_[:, None] * dim + torch.arange(dim)[None, :]
         assert torch.equal(face[f[:, None], off], K.disp[j].t())
+
+
+def test_sphere_box_mesh():
+    """The 3D sphere-in-box generator: requested size, tags, cells outside the sphere, valid tables."""
+    import collections
+    import numpy as np
+    from fvm_solver_b200 import meshgen as mg, workloads as W
+    spec = mg.sphere_box(20000, seed=3)
+    assert 0.6 * 20000 < spec.n_cells < 1.6 * 20000
+    tags = collections.Counter(spec.bc_tags)
+    assert set(tags) == {"NavierWall", "Left", "Right", "Farfield"}
+    P = spec.vertices.double().numpy()[spec.cells.long().numpy()]
+    assert np.all(np.linalg.norm(P.mean(axis=1), axis=1) > 0.5)
+    case = W.sphere(20000, seed=3, device="cpu")
+    kt = case.tables().kernel
+    assert kt.dim == 3 and kt.n_char > 0 and kt.n_bc == len(spec.bc_tags)
+    assert bool((kt.volumes > 0).all())
