@@ -28,7 +28,7 @@ class Mesh(ct.Structure):
                           "bc_char", "ch_cell", "ch_normal", "ch_rho", "ch_vn", "ch_p", "ch_vt")] + [
         ("n_cases", ct.c_int32)] + [
         (n, _P) for n in ("cell_case", "face_case", "bc_case", "ch_off", "case_mu", "case_mu_b", "case_kappa")] + [
-        ("n_owned", ct.c_int32), ("char_scale_given", ct.c_int32)]
+        ("n_owned", ct.c_int32), ("char_scale_given", ct.c_int32), ("case_active", _P)]
 
 MESH_PTR_FIELDS = [f for f, t in Mesh._fields_ if t is _P]
 

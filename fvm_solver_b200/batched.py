@@ -186,6 +186,14 @@ class BatchedFVM:
         from .solvers import get_solver
         self.t_solver = get_solver(self.cells, self, cfg)
 
+        self.active = torch.ones(self.n_cases, dtype=torch.uint8, device=self.device)
+
+    def use_case_mask(self, on: bool = True):
+        """Let ``self.active`` (device bytes, one per case) freeze cases: every kernel launched for
+        this batch afterwards -- also from CUDA graphs captured afterwards, which read the mask at
+        replay -- skips the cases whose byte is 0."""
+        self.dev.struct.case_active = _lib.ptr(self.active) if on else None
+
     def case_slice(self, c: int) -> slice:
         return slice(int(self.offsets["cells"][c]), int(self.offsets["cells"][c + 1]))
 

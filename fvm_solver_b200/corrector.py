@@ -29,9 +29,10 @@ Fallback (per case, per window): the proposal U' is accepted when
   * the relative mass / energy drift |M(U') - M(U) - k dt sum(vol dU/dt(U))| / |M(U)| <= 1e-4,
   * ||dU/dt(U')||_vol <= 3 ||dU/dt(U)||_vol, and
   * U' is admissible: positive density and internal energy in every cell;
-otherwise the window is advanced with k plain FVM steps.  The proposal and both checks are one CUDA
-graph; the host reads the per-case verdicts once per window and replays a graph of k FVM steps for
-the batch only when some case failed.
+otherwise the case is advanced with k plain FVM steps.  The proposal and the checks are one CUDA
+graph; the host reads the per-case verdicts once per window and, when some case failed, replays a
+graph of k FVM steps with the accepted cases frozen (``BatchedFVM.use_case_mask``: the kernels skip
+their cells, facets and boundary facets), so the fallback costs in proportion to the failed cases.
 """
 from __future__ import annotations
 
@@ -376,6 +377,7 @@ class CheckedRollout:
         self.use_graphs = use_graphs
         self._g_propose = None
         self._fallback = None
+        b.use_case_mask(True)             # the fallback advances only the cases that failed
         self.accepted = 0
         self.windows = 0
         self.full_windows = 0
@@ -449,9 +451,12 @@ class CheckedRollout:
             self.accepted += b.n_cases
             self.full_windows += 1
             return ok
-        # fallback: k plain FVM steps for the batch, then keep the accepted proposals
+        # fallback: k plain FVM steps for the cases that failed (the others are frozen), then the
+        # accepted proposals replace the frozen cases' states
         keep = self.ok[self.m.cell_case].unsqueeze(1)
+        b.active.copy_(~self.ok)
         self._run_fallback()
+        b.active.fill_(1)
         b.cells.state = torch.where(keep, self.prop, b.cells.state)
         self.accepted += int(ok.sum())
         return ok

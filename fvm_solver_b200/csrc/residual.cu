@@ -161,6 +161,11 @@ __device__ __forceinline__ void prefetch_tile(const float* base, int64_t n_rows,
     if (b1 > b0) l2_prefetch(reinterpret_cast<const char*>(base) + b0, (uint32_t)(b1 - b0));
 }
 
+// Batched meshes with a case mask: is the case of item `idx` (looked up in `case_of`) active?
+__device__ __forceinline__ bool case_on(const fvm_mesh_t& m, const int32_t* case_of, int idx) {
+    return m.case_active == nullptr || m.case_active[__ldg(case_of + idx)] != 0;
+}
+
 // The two side codes (first two words) of a facet record.
 __device__ __forceinline__ int2 ld_codes(const float* rec) { return __ldg(reinterpret_cast<const int2*>(rec)); }
 
@@ -227,6 +232,7 @@ __global__ void __launch_bounds__(kBlock) k_char_scale(fvm_mesh_t m, Phys p, con
                                                         double* __restrict__ red_out) {
     __shared__ double red[32];
     const int c = blockIdx.x;
+    if (m.case_active && !m.case_active[c]) return;
     const int lo = __ldg(m.ch_off + c), hi = __ldg(m.ch_off + c + 1);
     const double sum = char_c_sum<DIM>(m, p, prims, lo, hi, red);
     if (threadIdx.x == 0)
@@ -253,6 +259,7 @@ __global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float
     }
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= m.n_bc) return;
+    if (m.n_cases > 0 && !case_on(m, m.bc_case, b)) return;
     if (m.n_cases > 0) scale = (float)wred[FVM_RED_DOUBLES + 8 * __ldg(m.bc_case + b) + 6];
     else if (m.char_scale_given) scale = (float)wred[FVM_RED_DOUBLES + 6];
     const int cell = __ldg(m.bc_cell + b);
@@ -339,6 +346,13 @@ __global__ void __launch_bounds__(kMaxBlock) k_cell(fvm_mesh_t m, Phys p, const 
     for (int k = 0; k < KG; ++k) cols[k] = i < NA ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)i * Ly::CR + Ly::GC + k) : 0;
     for (int64_t tile = blockIdx.x; i < NA; i += stride, tile += gridDim.x) {
         if (waves > 0) prefetch_tile(m.cell_rec, NA, Ly::CR, tile + (int64_t)waves * gridDim.x);
+        if (m.case_active && !case_on(m, m.cell_case, i)) {
+            const int inext = i + stride;
+#pragma unroll
+            for (int k = 0; k < KG; ++k)
+                cols[k] = inext < NA ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)inext * Ly::CR + Ly::GC + k) : 0;
+            continue;
+        }
         float X[KG][RS];
 #pragma unroll
         for (int k = 0; k < KG; ++k) {
@@ -425,6 +439,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_face(fvm_mesh_t m, Phys p, const 
     for (int64_t tile = blockIdx.x; f < nF; f += stride, tile += gridDim.x) {
     if (waves > 0) prefetch_tile(m.face_rec, nF, Ly::FR, tile + (int64_t)waves * gridDim.x);
     const int ca = nxt.x, cb = nxt.y;
+    if (m.case_active && !case_on(m, m.face_case, f)) {
+        if (f + stride < nF) nxt = ld_codes(m.face_rec + (int64_t)(f + stride) * Ly::FR);
+        continue;
+    }
     // Both sides: primitives and limited gradient of the cell(s); a boundary side (code < 0) takes
     // the boundary value, and its gradient is the interior cell's (facet_process.py:364-368).
     const int cell0 = ca >= 0 ? ca : cb;
@@ -771,7 +789,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_div_stage(fvm_mesh_t m, Phys p, c
             if (MODE != DIV_RESIDUAL) prefetch_tile(state, NA, C, tile + (int64_t)waves * gridDim.x);
         }
         const int i = i0 + lane;
-        const bool live = i < NA;
+        const bool live = i < NA && (m.case_active == nullptr || case_on(m, m.cell_case, i));
         float rec[Ly::DR];
 #pragma unroll
         for (int q = 0; q < Ly::DR; ++q) rec[q] = nxt[q];
@@ -883,9 +901,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_div_stage(fvm_mesh_t m, Phys p, c
 // Batched meshes (n_cases > 0): one thread per case handles its CFL dt and sums.
 __global__ void k_finalize(int C, int adaptive, float atol, float rtol, float mtol, float alpha_hi,
                            float alpha_lo, float order, float cfl, int cons, double* red, float* dt,
-                           double* cons_out, int n_cases) {
+                           double* cons_out, int n_cases, const uint8_t* __restrict__ active) {
     if (n_cases > 0) {
         for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cases; c += gridDim.x * blockDim.x) {
+            if (active && !active[c]) continue;
             double* slot = red + FVM_RED_DOUBLES + 8 * c;
             if (cfl > 0.f) {
                 if (slot[0] > 0.0) dt[c] = (float)((double)cfl / slot[0]);
@@ -1010,6 +1029,7 @@ static bool mesh_ok(const fvm_mesh_t* m) {
     if (m->n_cases < 0) return false;
     if (m->n_owned < 0 || m->n_owned > m->n_cells || m->char_scale_given < 0 || m->char_scale_given > 1) return false;
     if (m->n_cases > 0 && (m->n_owned > 0 || m->char_scale_given)) return false;
+    if (m->n_cases == 0 && m->case_active) return false;
     if (m->n_cases > 0 && (!m->cell_case || !m->face_case || !m->ch_off || !m->case_mu || !m->case_mu_b ||
                            !m->case_kappa || (m->n_bc > 0 && !m->bc_case)))
         return false;
@@ -1168,7 +1188,7 @@ static int finalize_impl(const fvm_mesh_t* m, const fvm_tableau_t* tab, const fv
     FVM_LAUNCH(KID_FINALIZE, st,
                k_finalize<<<fin_blocks(m), 128, 0, st>>>(m->n_comp, tab->adaptive, tab->atol, tab->rtol, tab->mtol,
                                                          tab->alpha_hi_err, tab->alpha_lo_err, tab->order, tab->cfl,
-                                                         cons, w->red, b->dt, b->cons, m->n_cases));
+                                                         cons, w->red, b->dt, b->cons, m->n_cases, m->case_active));
     return launch_status();
 }
 
@@ -1228,7 +1248,7 @@ static int multistep_impl(const fvm_mesh_t* m, const Phys& p, int store, int n_t
     if (a.cons) {
         FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(m), 128, 0, st>>>(m->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f,
                                                                               1.f, 0.f, 1, w->red, b->dt, b->cons,
-                                                                              m->n_cases));
+                                                                              m->n_cases, m->case_active));
         rc = launch_status();
     }
     return rc;
@@ -1408,7 +1428,7 @@ extern "C" int fvm_cfl_dt(const fvm_mesh_t* mesh, const fvm_physics_t* phys, con
     if (rc) return rc;
     FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(mesh), 128, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f,
                                                                              0.f, 1.f, cfl, 0, work->red, dt,
-                                                                             nullptr, mesh->n_cases));
+                                                                             nullptr, mesh->n_cases, nullptr));
     return launch_status();
 }
 
@@ -1427,7 +1447,7 @@ extern "C" int fvm_conservation(const fvm_mesh_t* mesh, const float* state, doub
     if (rc) return rc;
     FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(mesh), 128, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f,
                                                                              0.f, 1.f, 0.f, 1, work->red, nullptr,
-                                                                             out, mesh->n_cases));
+                                                                             out, mesh->n_cases, nullptr));
     return launch_status();
 }
 

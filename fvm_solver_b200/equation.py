@@ -86,7 +86,7 @@ class DeviceMesh:
 
     _struct_fields = [f for f in _lib.MESH_PTR_FIELDS if f not in
                       ("cell_rec", "div_rec", "face_rec", "cell_case", "face_case", "bc_case", "ch_off",
-                       "case_mu", "case_mu_b", "case_kappa")]
+                       "case_mu", "case_mu_b", "case_kappa", "case_active")]
 
     def __init__(self, kt: KernelTables, device, records: dict | None = None):
         """``records``: precomputed device records (default ``kt.records()``)."""

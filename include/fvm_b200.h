@@ -105,6 +105,10 @@ typedef struct fvm_mesh {
      * caller forms it from every part's fvm_char_partial) instead of being computed here. */
     int32_t n_owned;
     int32_t char_scale_given;
+    /* Batched meshes only: [n_cases] bytes, 0 = the case is frozen -- its boundary facets, cells and
+     * facets are skipped by every kernel and its dt / conservation slots are left alone (a
+     * corrector's fallback advances only the cases whose proposal failed).  NULL = all active. */
+    const uint8_t *case_active;
 } fvm_mesh_t;
 
 /* Gas and scheme constants (ConfigFVM fields, time_fvm/config_fvm.py:52-63). */

@@ -69,3 +69,29 @@ def test_batched_graph_and_conservation(cases):
         want = (vol[sl, None] * st[sl]).sum(0)
         assert np.allclose(cons[k], want, rtol=1e-10, atol=1e-8)
     assert torch.isfinite(batch.cells.state).all()
+
+
+def test_case_mask_freezes_cases(cases):
+    """With the case mask, frozen cases keep their state and dt bitwise, and the active ones step
+    exactly as without a mask (eager and graph-replayed steps)."""
+    from fvm_solver_b200 import batched as B
+    parts = [B.build_case_tables(c) for c in cases]
+    cfg = copy.deepcopy(cases[0].cfg)
+    cfg.solver_name, cfg.solver_extra = "Butcher", "SSP_RK3"
+    free = B.BatchedFVM(parts, cfg, device="cuda")
+    masked = B.BatchedFVM(parts, cfg, device="cuda")
+    start = masked.cells.state.clone()
+    dt0 = masked.t_solver.dt.clone()
+    masked.use_case_mask(True)
+    masked.active.copy_(torch.tensor([1, 0, 1, 0], dtype=torch.uint8))
+    free.t_solver.step(2)
+    masked.t_solver.step(1)
+    masked.t_solver.graph_steps(1)()
+    torch.cuda.synchronize()
+    for k in range(len(cases)):
+        if k in (0, 2):
+            assert torch.equal(masked.case_state(k), free.case_state(k)), k
+            assert torch.equal(masked.t_solver.dt[k], free.t_solver.dt[k])
+        else:
+            assert torch.equal(masked.case_state(k), start[masked.case_slice(k)]), k
+            assert torch.equal(masked.t_solver.dt[k], dt0[k])

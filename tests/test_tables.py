@@ -92,3 +92,17 @@ def test_sphere_box_mesh():
     kt = case.tables().kernel
     assert kt.dim == 3 and kt.n_char > 0 and kt.n_bc == len(spec.bc_tags)
     assert bool((kt.volumes > 0).all())
+
+
+def test_device_mesh_struct_on_host():
+    """The fvm_mesh_t struct fills every pointer field from the tables (built on the CPU here)."""
+    from conftest import golden_setup
+    from fvm_solver_b200 import _lib
+    from fvm_solver_b200.equation import DeviceMesh
+    g, spec, tables, cfg = golden_setup("c2d")
+    dm = DeviceMesh(tables.kernel, "cpu")
+    m = dm.struct
+    for f in ("cell_rec", "div_rec", "face_rec", "inv_h", "volumes", "bc_cell", "bc_kind", "ch_cell"):
+        assert getattr(m, f), f
+    assert m.n_cases == 0 and not m.case_active and m.n_owned == 0 and m.char_scale_given == 0
+    assert m.n_cells == tables.kernel.n_cells and m.kg == tables.kernel.kg
