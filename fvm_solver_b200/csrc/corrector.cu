@@ -88,6 +88,40 @@ __device__ __forceinline__ void stage_tile(uint8_t* smem, const __nv_bfloat16* s
     }
 }
 
+// Same layout as stage_tile, copied global -> shared by cp.async (no registers; rows past
+// rows_valid and columns past kmax are zero-filled).  Thread -> (row, unit) mapping: the 32 lanes
+// of a warp take 8 consecutive rows x 4 units, so their 16-byte stores cover all 32 banks once per
+// 8 lanes (conflict-free) and each row's 4 units are 64 contiguous global bytes.
+__device__ __forceinline__ void stage_tile_async(uint8_t* smem, const __nv_bfloat16* src, int64_t ld, int r0,
+                                                 int rows_valid, int nrows, int k0, int kmax) {
+    const int units = nrows * (TK / 8);
+    const int slice_bytes = (nrows / 8) * 256;
+    const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    for (int t = threadIdx.x; t < units; t += blockDim.x) {
+        const int r = (t & 7) + 8 * (t >> 6), u = (t >> 3) & 7;
+        const int k = k0 + 8 * u;
+        const bool valid = r < rows_valid && k < kmax;
+        const __nv_bfloat16* gp = valid ? src + (int64_t)(r0 + r) * ld + k : src;
+        const uint32_t off = (uint32_t)((u >> 1) * slice_bytes + (r >> 3) * 256 + (u & 1) * 128 + (r & 7) * 16);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(base + off), "l"(gp),
+                     "r"(valid ? 16 : 0)
+                     : "memory");
+    }
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done = 0;
+    for (long long it = 0; it < kWaitLimit && !done; ++it) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(static_cast<uint32_t>(__cvta_generic_to_shared(bar))), "r"(parity));
+    }
+    return done != 0;
+}
+
 __device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
 
 // 8 consecutive floats (32-byte aligned) with one 256-bit access.
@@ -146,10 +180,12 @@ __device__ __forceinline__ void epilogue_vec(const GemmArgs& g, int64_t row, int
 
 template <int N>
 __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
+    // Two staging buffers of one K slice each (A: TM x TK, B: N x TK, bf16): slice j + 1 is copied
+    // (cp.async) while the tensor cores work on slice j; a buffer is refilled only after the MMAs
+    // that read it have completed (their commit's mbarrier).
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* sA = smem;                                  // TM * TK * 2 = 16 KB
-    uint8_t* sB = smem + TM * TK * 2;                    // N * TK * 2
-    __shared__ __align__(8) uint64_t mbar;
+    constexpr int kStageBytes = TM * TK * 2 + N * TK * 2;
+    __shared__ __align__(8) uint64_t mbar[2];
     __shared__ uint32_t s_taddr;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * TM;
@@ -157,6 +193,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
     const int kchunks = g.K / TK;
     const int per = (kchunks + g.k_splits - 1) / g.k_splits;
     const int kc0 = split * per, kc1 = min(kchunks, kc0 + per);
+    const int nk = max(0, kc1 - kc0);
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_taddr)),
@@ -164,7 +201,8 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -173,20 +211,28 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
     const uint32_t taddr = s_taddr;
     const uint32_t idesc = make_idesc(N);
     const int rows_a = min(TM, g.M - m0);
+    auto stage = [&](int buf, int kc) {
+        uint8_t* sA = smem + buf * kStageBytes;
+        stage_tile_async(sA, g.A, g.lda, m0, rows_a, TM, kc * TK, g.K);
+        stage_tile_async(sA + TM * TK * 2, g.B, g.ldb, 0, g.N, N, kc * TK, g.K);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
     bool ok = true;
-    uint32_t phase = 0;
-    for (int kc = kc0; kc < kc1; ++kc) {
-        stage_tile(sA, g.A, g.lda, m0, rows_a, TM, kc * TK, g.K);
-        stage_tile(sB, g.B, g.ldb, 0, g.N, N, kc * TK, g.K);
-        asm volatile("fence.proxy.async.shared::cta;");
+    for (int j = 0; j < min(2, nk); ++j) stage(j, kc0 + j);
+    for (int j = 0; j < nk && ok; ++j) {
+        const int buf = j & 1;
+        if (j + 1 < nk) asm volatile("cp.async.wait_group 1;" ::: "memory");
+        else asm volatile("cp.async.wait_group 0;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (threadIdx.x == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t sa = smem_u32(smem + buf * kStageBytes), sb = sa + TM * TK * 2;
 #pragma unroll
             for (int s = 0; s < TK / 16; ++s) {
-                const uint64_t ad = make_desc(smem_u32(sA) + s * (TM / 8) * 256, 128, 256);
-                const uint64_t bd = make_desc(smem_u32(sB) + s * (N / 8) * 256, 128, 256);
-                const uint32_t acc = (kc > kc0 || s > 0) ? 1u : 0u;
+                const uint64_t ad = make_desc(sa + s * (TM / 8) * 256, 128, 256);
+                const uint64_t bd = make_desc(sb + s * (N / 8) * 256, 128, 256);
+                const uint32_t acc = (j > 0 || s > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n\t.reg .pred p;\n\t"
                     "setp.ne.b32 p, %4, 0;\n\t"
@@ -194,37 +240,29 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
                     "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(&mbar))
+                             smem_u32(&mbar[buf]))
                          : "memory");
         }
-        // Wait for the MMAs (they read shared memory asynchronously) before restaging.
-        uint32_t done = 0;
-        for (long long it = 0; it < kWaitLimit && !done; ++it) {
-            asm volatile(
-                "{\n\t.reg .pred p;\n\t"
-                "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                "selp.u32 %0, 1, 0, p;\n\t}\n"
-                : "=r"(done)
-                : "r"(smem_u32(&mbar)), "r"(phase));
-        }
-        if (!done) {
-            // Give the MMAs in flight a second bounded chance to finish before the tensor memory
-            // they write is released, then report the timeout.
-            for (long long it = 0; it < kWaitLimit && !done; ++it) {
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                    "selp.u32 %0, 1, 0, p;\n\t}\n"
-                    : "=r"(done)
-                    : "r"(smem_u32(&mbar)), "r"(phase));
+        // Refill this buffer with slice j + 2 once its MMAs are done; after the last slice, wait
+        // for the last commit (the MMAs of one thread complete in order).
+        const bool refill = j + 2 < nk, last = j + 1 == nk;
+        if (refill || last) {                              // uniform across the block
+            bool done = mbar_wait(&mbar[buf], (uint32_t)((j >> 1) & 1));
+            if (!done) {
+                // Give the MMAs in flight a second bounded chance to finish before the tensor memory
+                // they write is released; the timeout is reported below.
+                done = mbar_wait(&mbar[buf], (uint32_t)((j >> 1) & 1)) && false;
             }
-            ok = false;
-            if (g.err) atomicExch(g.err, 1);
-            break;
+            // one verdict for the whole block (also the barrier before the buffer is refilled)
+            ok = __syncthreads_and(done) != 0;
+            if (!ok) {
+                if (threadIdx.x == 0 && g.err) atomicExch(g.err, 1);
+            } else if (refill) {
+                stage(buf, kc0 + j + 2);
+            }
         }
-        phase ^= 1u;
-        __syncthreads();
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     asm volatile("tcgen05.fence::after_thread_sync;");
     const bool have = ok && kc1 > kc0;
     // Epilogue: warp w owns tile rows 32w .. 32w + 31 (TMEM lanes).
@@ -275,7 +313,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
 
 template <int N>
 static int launch_gemm(const GemmArgs& g, cudaStream_t s) {
-    const size_t smem = (size_t)TM * TK * 2 + (size_t)N * TK * 2;
+    const size_t smem = 2 * ((size_t)TM * TK * 2 + (size_t)N * TK * 2);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_gemm<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
