@@ -7,8 +7,9 @@ FP32 5-variable state, classic RK4 with a CFL 0.5 time step recomputed on the de
 A "step" is one full RK4 step (4 residual evaluations + stage updates + FP64 CFL reduction).
 
 * ``value``  -- cell-steps/s of the whole job: sum over ranks of cells x K / max over ranks of
-  the device time of K steps replayed from a CUDA graph (inputs resident in HBM; the per-stage
-  working set, >1 GB, is larger than L2, so no L2 flush is needed).
+  the device time of K steps replayed from a CUDA graph (W eager warm-up steps and one untimed
+  replay of the graph first; inputs resident in HBM; the per-stage working set, >1 GB, is larger
+  than L2, so no L2 flush is needed).
 * ``e2e``    -- the same metric through the public API with host buffers: every step copies the
   state host->device from pinned memory, steps, and copies the new state back.
 * ``roofline`` -- the dominant kernel's algorithmic bytes per launch / its mean CUDA-event
@@ -270,7 +271,7 @@ def partitioned_bench(args):
 
     One process (no torchrun): ``--parts`` parts stepped on one GPU, exchanges as device copies;
     reports the partitioned throughput next to the unpartitioned one on the same box and checks the
-    two final states for bitwise equality.  Under torchrun (N > 1): one part per rank, halo rows over
+    two final states (after a warm-up replay and a timed replay of K steps each) for bitwise equality.  Under torchrun (N > 1): one part per rank, halo rows over
     NCCL point-to-point, FP64 reductions over NCCL all-reduce; strong scaling (the box is fixed).
     """
     import torch.distributed as dist
@@ -326,6 +327,7 @@ def partitioned_bench(args):
     # one GPU: single mesh, then the same box in P parts, both from state0 for K graph-replayed steps
     sol = eq.t_solver
     replay = sol.graph_steps(args.steps)
+    replay()                                 # untimed warm-up replay (uploads the graph)
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
@@ -339,6 +341,7 @@ def partitioned_bench(args):
     ps.set_state(state0)
     ps.cfl_dt(case.cfg.cfl)
     preplay = ps.graph_steps(args.steps)
+    preplay()                                # untimed warm-up replay: both runs end after 2 K steps
     torch.cuda.synchronize()
     with ClockSampler(0) as clk:
         a.record(stream)
@@ -370,6 +373,7 @@ def secondary(args):
 
     def timed(sol, steps):
         replay = sol.graph_steps(steps)
+        replay()                             # untimed: the first replay also uploads the graph
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
@@ -386,8 +390,9 @@ def secondary(args):
         case = W.channel_cylinder(device="cuda")
         eq = case.equation()
         sol = eq.t_solver
-        from fvm_solver_b200.autotune import autotune
+        from fvm_solver_b200.autotune import autotune, tune_fused
         autotune(eq)
+        fused = tune_fused(eq)
         sol.step(args.warmup)
         with ClockSampler(0) as clk:
             ms = timed(sol, args.steps)
@@ -414,7 +419,9 @@ def secondary(args):
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                "dtype": "f32", "data": "synthetic",
                "config": {"workload": "channel_cylinder_2d_ssprk3_cfl0.5", "cells": N, "facets": eq.dev.n_facets,
-                          "l2": "working set fits in L2 (launch/latency bound case)", "timing": "cuda graph replay"},
+                          "l2": "working set fits in L2 (launch/latency bound case)", "timing": "cuda graph replay",
+                          "step": "fused (one cooperative launch per step)" if fused["fused"] else "separate launches",
+                          "ms_per_step_by_variant": fused["ms_per_step"]},
                "cpu_baseline": cpu, "drift_vs_oracle": drift, "clocks": clk.summary()}
         print(json.dumps(out))
         return
@@ -428,20 +435,22 @@ def secondary(args):
     cfg = W.ensemble_case(0, device="cuda", cfl=0.3).cfg
     batch = B.BatchedFVM(parts, cfg, device="cuda")
     Nt = batch.n_cells
-    from fvm_solver_b200.autotune import autotune
+    from fvm_solver_b200.autotune import autotune, tune_fused
     tuned = {k: v["threads"] for k, v in autotune(batch).items()}
     batch.t_solver.step(max(args.warmup, 3))
+    fused_b = tune_fused(batch)
     with ClockSampler(0) as clk:
         ms_b = timed(batch.t_solver, args.steps)
     del batch
     torch.cuda.empty_cache()
     # plain: every case alone, each with its own captured graph of the same number of steps
-    ms_p, cells_p = 0.0, 0
+    ms_p, cells_p, n_fused = 0.0, 0, 0
     for k, p in enumerate(parts):
         c = W.ensemble_case(k, device="cuda", cfl=0.3).cfg
         eq = FVMEquation.from_kernel_tables(c, FluidConstitution2D(c), p.kt, p.state0)
         autotune(eq)                       # per size bucket (cached), so small cases get their own
         eq.t_solver.step(max(args.warmup, 3))
+        n_fused += tune_fused(eq)["fused"]  # each case alone also gets its faster step form
         ms_p += timed(eq.t_solver, args.steps)
         cells_p += p.kt.n_cells
         del eq
@@ -454,9 +463,10 @@ def secondary(args):
            "config": {"workload": "ensemble_2d_ab3_batched", "cases": args.cases, "cells_total": Nt,
                       "cells_min": min(sizes), "cells_max": max(sizes), "integrator": "AB3 (SSP-RK3 start), CFL 0.3",
                       "timing": "cuda graph replay", "table_build_s": t_build, "host_cpus": os.cpu_count(),
-                      "block_sizes": tuned},
+                      "block_sizes": tuned, "fused_step": fused_b},
            "plain": {"value": vp, "unit": "cell-steps/s", "ms_per_step_all_cases": ms_p / args.steps,
-                     "how": "each case alone, own CUDA graph, sequential"},
+                     "how": "each case alone, own CUDA graph, sequential",
+                     "cases_with_fused_step": n_fused},
            "batched_over_plain": vb / vp, "clocks": clk.summary()}
     print(json.dumps(out))
 
@@ -618,6 +628,7 @@ def main():
 
     # timed region 1: K steps replayed from one CUDA graph
     replay = sol.graph_steps(args.steps)
+    replay()                                 # untimed warm-up replay (the first one uploads the graph)
     barrier()
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()

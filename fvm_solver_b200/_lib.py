@@ -77,6 +77,9 @@ _SIGS = [
     ("fvm_conservation", ct.c_int, [ct.POINTER(Mesh), _P, _P, ct.POINTER(Work), _P]),
     ("fvm_residual_noalloc", ct.c_int, [ct.POINTER(Mesh), ct.POINTER(Physics), _P, _P, _P, _P, _P]),
     ("fvm_profile_start", ct.c_int, [ct.c_int32]),
+    ("fvm_step_fused", ct.c_int, [_P, _P, _P, _P, _P, _P]),
+    ("fvm_multistep_fused", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, _P, _P, _P, _P, _P]),
+    ("fvm_fused_status", ct.c_int, [_P, _P]),
     ("fvm_stage_begin", ct.c_int, [_P, _P, _P, _P, _P]),
     ("fvm_stage_end", ct.c_int, [_P, _P, _P, ct.c_int32, _P, _P, ct.c_int32, _P]),
     ("fvm_stage_finalize", ct.c_int, [_P, _P, _P, _P, _P]),
@@ -104,7 +107,7 @@ _SIGS = [
 ]
 
 KERNEL_NAMES = {0: "ell_spmv", 1: "ell_spmm", 2: "bc", 3: "cell", 4: "face", 5: "div_stage", 6: "finalize",
-                7: "state_to_prims", 8: "reduce_state", 9: "batched", 10: "corrector"}
+                7: "state_to_prims", 8: "reduce_state", 9: "batched", 10: "corrector", 11: "fused_step"}
 
 EXPORTED = [s[0] for s in _SIGS]
 

@@ -103,3 +103,31 @@ def reset():
     """Back to the defaults (256 threads, no prefetch) for every tunable kernel."""
     for k in KERNELS.values():
         _install(k, (256, 0))
+
+
+def tune_fused(eq, steps: int = 10, reps: int = 3) -> dict:
+    """Choose between separate launches per phase and the fused cooperative step for ``eq``'s
+    time stepper: each variant's CUDA graph of ``steps`` steps is replayed ``reps`` times on a copy
+    of the state, timed with CUDA events; the faster is kept (``t_solver.fused``).  The solver's
+    state, carried gradients, dt and history are restored.  Returns {"fused": bool, "ms": {...}}."""
+    sol = eq.t_solver
+    saved = sol.state_dict()
+    times = {}
+    for fused in (False, True):
+        sol.fused = fused
+        replay = sol.graph_steps(steps)
+        replay()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            replay()
+        e1.record()
+        torch.cuda.synchronize()
+        times[fused] = e0.elapsed_time(e1) / (reps * steps)
+        del replay
+        sol.load_state_dict(saved)
+    sol.fused = times[True] < times[False]
+    if sol.fused_status():
+        raise RuntimeError("fused step: a grid barrier wait gave up")
+    return {"fused": sol.fused, "ms_per_step": {"separate": times[False], "fused": times[True]}}

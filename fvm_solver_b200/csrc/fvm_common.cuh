@@ -17,6 +17,7 @@ int launch_status();
 enum KernelId {
     KID_ELL_SPMV = 0, KID_ELL_SPMM = 1, KID_BC = 2, KID_CELL = 3, KID_FACE = 4, KID_DIV_STAGE = 5,
     KID_FINALIZE = 6, KID_STATE_TO_PRIMS = 7, KID_REDUCE_STATE = 8, KID_BATCH = 9, KID_CORRECTOR = 10,
+    KID_FUSED = 11,
 };
 
 // When profiling is on, prof_begin/prof_end bracket a launch with CUDA events on its stream.

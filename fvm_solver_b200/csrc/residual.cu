@@ -33,6 +33,8 @@
 // read per facet side).
 #include <math.h>
 
+#include <algorithm>
+
 #include "fvm_common.cuh"
 
 namespace fvm {
@@ -125,6 +127,19 @@ __device__ __forceinline__ void ld_vec_cg(const float* p, float (&v)[N]) {
         }
     }
 }
+// Loads of arrays the same launch may have written (COH = true: the fused step kernel, whose
+// phases read what other blocks wrote before a grid barrier) go through L2 (.cg); in the one-phase
+// kernels those arrays are read-only for the launch and use the read-only path.
+template <bool COH, int N>
+__device__ __forceinline__ void ld_mut(const float* p, float (&v)[N]) {
+    if constexpr (COH) ld_vec_cg<N>(p, v);
+    else ld_vec<N>(p, v);
+}
+template <bool COH>
+__device__ __forceinline__ float ld1_mut(const float* p) {
+    if constexpr (COH) return __ldcg(p);
+    else return __ldg(p);
+}
 template <int N>
 __device__ __forceinline__ void st_vec(float* p, const float (&v)[N]) {
     static_assert(N % 4 == 0, "row width");
@@ -213,13 +228,13 @@ __device__ __forceinline__ float limiter_phi(int p, float delta, float dU, float
 // ------------------------------------------------------------------------------------------
 // Sum of the interior sound speed over characteristic facets [lo, hi): every caller uses the same
 // thread -> element mapping and reduction tree, so batched and single-mesh runs agree bitwise.
-template <int DIM>
+template <int DIM, bool COH = false>
 __device__ __forceinline__ double char_c_sum(const fvm_mesh_t& m, const Phys& p, const float* prims, int lo,
                                              int hi, double* red) {
     double acc = 0.0;
     for (int t = lo + threadIdx.x; t < hi; t += blockDim.x) {
         const int cell = __ldg(m.ch_cell + t);
-        acc += (double)sqrtf(p.gR * __ldg(prims + (int64_t)cell * L<DIM>::RS + DIM + 1));
+        acc += (double)sqrtf(p.gR * ld1_mut<COH>(prims + (int64_t)cell * L<DIM>::RS + DIM + 1));
     }
     double v[1] = {acc};
     block_sum<1>(v, red);
@@ -227,45 +242,56 @@ __device__ __forceinline__ double char_c_sum(const fvm_mesh_t& m, const Phys& p,
 }
 
 // Batched meshes: per-case characteristic gating scale 10 / mean(c), one block per case.
-template <int DIM>
-__global__ void __launch_bounds__(kBlock) k_char_scale(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
-                                                        double* __restrict__ red_out) {
+template <int DIM, bool COH>
+__device__ __forceinline__ void char_scale_case(const fvm_mesh_t& m, const Phys& p, const float* prims,
+                                                double* red_out, int c) {
     __shared__ double red[32];
-    const int c = blockIdx.x;
     if (m.case_active && !m.case_active[c]) return;
     const int lo = __ldg(m.ch_off + c), hi = __ldg(m.ch_off + c + 1);
-    const double sum = char_c_sum<DIM>(m, p, prims, lo, hi, red);
+    const double sum = char_c_sum<DIM, COH>(m, p, prims, lo, hi, red);
     if (threadIdx.x == 0)
         red_out[FVM_RED_DOUBLES + 8 * c + 6] = hi > lo ? (double)(10.0f / (float)(sum / (double)(hi - lo))) : 0.0;
+    __syncthreads();
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
-                                                const float* __restrict__ grads,
-                                                const int32_t* __restrict__ has_grads,
-                                                float* __restrict__ bcv, const double* __restrict__ wred) {
-    using Ly = L<DIM>;
-    constexpr int C = Ly::C;
+__global__ void __launch_bounds__(kBlock) k_char_scale(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+                                                        double* __restrict__ red_out) {
+    char_scale_case<DIM, false>(m, p, prims, red_out, blockIdx.x);
+}
+
+// Single mesh: the characteristic-BC scale 10 / mean(c) over the group (facet_boundary.py:427),
+// recomputed identically by every block (block-wide; 0 when not needed).
+template <int DIM, bool COH>
+__device__ __forceinline__ float bc_block_scale(const fvm_mesh_t& m, const Phys& p, const float* prims) {
     __shared__ double red[32];
+    __shared__ float s_scale;
     float scale = 0.f;
     if (m.n_char > 0 && m.n_cases == 0 && !m.char_scale_given) {
-        // Group mean of the interior sound speed c = sqrt(gamma R T) (facet_boundary.py:427),
-        // recomputed identically by every block.
-        const double sum = char_c_sum<DIM>(m, p, prims, 0, m.n_char, red);
-        __shared__ float s_scale;
+        const double sum = char_c_sum<DIM, COH>(m, p, prims, 0, m.n_char, red);
         if (threadIdx.x == 0) s_scale = 10.0f / (float)(sum / (double)m.n_char);
         __syncthreads();
         scale = s_scale;
+        __syncthreads();
     }
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= m.n_bc) return;
+    return scale;
+}
+
+// Boundary facet b's value (A_bc U + b_bc + A_corr grads_prev, then the characteristic BC).
+template <int DIM, bool COH>
+__device__ __forceinline__ void bc_item(const fvm_mesh_t& m, const Phys& p, const float* __restrict__ prims,
+                                        const float* __restrict__ grads, const int32_t* __restrict__ has_grads,
+                                        float* __restrict__ bcv, const double* __restrict__ wred, int b,
+                                        float scale) {
+    using Ly = L<DIM>;
+    constexpr int C = Ly::C;
     if (m.n_cases > 0 && !case_on(m, m.bc_case, b)) return;
-    if (m.n_cases > 0) scale = (float)wred[FVM_RED_DOUBLES + 8 * __ldg(m.bc_case + b) + 6];
-    else if (m.char_scale_given) scale = (float)wred[FVM_RED_DOUBLES + 6];
+    if (m.n_cases > 0) scale = (float)__ldcg(wred + FVM_RED_DOUBLES + 8 * __ldg(m.bc_case + b) + 6);
+    else if (m.char_scale_given) scale = (float)__ldcg(wred + FVM_RED_DOUBLES + 6);
     const int cell = __ldg(m.bc_cell + b);
     float U[Ly::RS];
-    ld_vec<Ly::RS>(prims + (int64_t)cell * Ly::RS, U);
-    const bool prev = *has_grads != 0;
+    ld_mut<COH, Ly::RS>(prims + (int64_t)cell * Ly::RS, U);
+    const bool prev = (COH ? __ldcg(has_grads) : *has_grads) != 0;
     float out[Ly::RS];
 #pragma unroll
     for (int c = 0; c < Ly::RS; ++c) out[c] = 0.f;
@@ -277,7 +303,8 @@ __global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float
             float corr = 0.f;
 #pragma unroll
             for (int d = 0; d < DIM; ++d)
-                corr = fmaf(__ldg(m.bc_l + b * DIM + d), grads[(int64_t)cell * Ly::GS + Ly::gi(d, c)], corr);
+                corr = fmaf(__ldg(m.bc_l + b * DIM + d), ld1_mut<COH>(grads + (int64_t)cell * Ly::GS + Ly::gi(d, c)),
+                            corr);
             v += corr;
         }
         out[c] = v;
@@ -324,16 +351,26 @@ __global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float
     st_vec<Ly::RS>(bcv + (int64_t)b * Ly::RS, out);
 }
 
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+                                                const float* __restrict__ grads,
+                                                const int32_t* __restrict__ has_grads,
+                                                float* __restrict__ bcv, const double* __restrict__ wred) {
+    const float scale = bc_block_scale<DIM, false>(m, p, prims);
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < m.n_bc) bc_item<DIM, false>(m, p, prims, grads, has_grads, bcv, wred, b, scale);
+}
+
 // ------------------------------------------------------------------------------------------
 // k_cell: gradient, limiter, limited gradient.
 // ------------------------------------------------------------------------------------------
 // Persistent grid-stride loop (one wave of resident blocks): each thread loads the next cell's
 // gradient-stencil columns one iteration ahead, so the neighbour gathers of a cell are issued at
 // the top of its iteration together with its record, one memory round trip instead of two.
-template <int DIM>
-__global__ void __launch_bounds__(kMaxBlock) k_cell(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
-                                                  const float* __restrict__ bcv, float* __restrict__ grads,
-                                                  int32_t* __restrict__ has_grads, int waves) {
+template <int DIM, bool COH>
+__device__ __forceinline__ void cell_body(const fvm_mesh_t& m, const Phys& p, const float* __restrict__ prims,
+                                          const float* __restrict__ bcv, float* __restrict__ grads,
+                                          int32_t* __restrict__ has_grads, int waves) {
     using Ly = L<DIM>;
     constexpr int C = Ly::C, K = Ly::K, KG = Ly::KG, RS = Ly::RS;
     const int N = m.n_cells;                              // columns < N are cells (halo included)
@@ -356,11 +393,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_cell(fvm_mesh_t m, Phys p, const 
         float X[KG][RS];
 #pragma unroll
         for (int k = 0; k < KG; ++k) {
-            if (cols[k] < N) ld_vec<RS>(prims + (int64_t)cols[k] * RS, X[k]);
+            if (cols[k] < N) ld_mut<COH, RS>(prims + (int64_t)cols[k] * RS, X[k]);
             else ld_vec_cg<RS>(bcv + (int64_t)(cols[k] - N) * RS, X[k]);
         }
         float U[RS];
-        ld_vec<RS>(prims + (int64_t)i * RS, U);
+        ld_mut<COH, RS>(prims + (int64_t)i * RS, U);
         float rec[Ly::CR];
         ld_vec<Ly::CR>(m.cell_rec + (int64_t)i * Ly::CR, rec);
         const int inext = i + stride;
@@ -422,14 +459,20 @@ __global__ void __launch_bounds__(kMaxBlock) k_cell(fvm_mesh_t m, Phys p, const 
     }
 }
 
+template <int DIM>
+__global__ void __launch_bounds__(kMaxBlock) k_cell(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+                                                  const float* __restrict__ bcv, float* __restrict__ grads,
+                                                  int32_t* __restrict__ has_grads, int waves) {
+    cell_body<DIM, false>(m, p, prims, bcv, grads, has_grads, waves);
+}
+
 // ------------------------------------------------------------------------------------------
 // k_face: facet fluxes.
 // ------------------------------------------------------------------------------------------
-template <int DIM>
-__global__ void __launch_bounds__(kMaxBlock) k_face(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
-                                                  const float* __restrict__ bcv,
-                                                  const float* __restrict__ grads, float* __restrict__ flux,
-                                                  int waves) {
+template <int DIM, bool COH>
+__device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, const float* __restrict__ prims,
+                                          const float* __restrict__ bcv, const float* __restrict__ grads,
+                                          float* __restrict__ flux, int waves) {
     using Ly = L<DIM>;
     constexpr int C = Ly::C, NG = DIM + 1, RS = Ly::RS, GS = Ly::GS;
     const int nF = m.n_facets;
@@ -448,8 +491,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_face(fvm_mesh_t m, Phys p, const 
     const int cell0 = ca >= 0 ? ca : cb;
     const int cell1 = cb >= 0 ? cb : ca;
     float P0[RS], P1[RS], G0[GS], G1[GS];
-    ld_vec<RS>(prims + (int64_t)cell0 * RS, P0);
-    ld_vec<RS>(prims + (int64_t)cell1 * RS, P1);
+    ld_mut<COH, RS>(prims + (int64_t)cell0 * RS, P0);
+    ld_mut<COH, RS>(prims + (int64_t)cell1 * RS, P1);
     ld_vec_cg<GS>(grads + (int64_t)cell0 * GS, G0);
     ld_vec_cg<GS>(grads + (int64_t)cell1 * GS, G1);
     float rec[Ly::FR];
@@ -620,6 +663,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_face(fvm_mesh_t m, Phys p, const 
     }
 }
 
+template <int DIM>
+__global__ void __launch_bounds__(kMaxBlock) k_face(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+                                                  const float* __restrict__ bcv,
+                                                  const float* __restrict__ grads, float* __restrict__ flux,
+                                                  int waves) {
+    face_body<DIM, false>(m, p, prims, bcv, grads, flux, waves);
+}
+
 // ------------------------------------------------------------------------------------------
 // k_div_stage: divergence + stage combination.
 // ------------------------------------------------------------------------------------------
@@ -757,13 +808,11 @@ enum DivMode { DIV_RESIDUAL = 0, DIV_STAGE = 1, DIV_FINAL = 2, DIV_FINAL_ADAPT =
 // batched reductions may shuffle): each thread loads the next cell's divergence record one iteration
 // ahead, so the flux gathers of a cell start at the top of its iteration.  Single-mesh reductions
 // are accumulated per thread and combined once per block after the loop.
-template <int DIM, int MODE>
-__global__ void __launch_bounds__(kMaxBlock) k_div_stage(fvm_mesh_t m, Phys p, const float* __restrict__ flux,
-                                                       StageArgs a, float* __restrict__ state,
-                                                       float* __restrict__ prims, float* __restrict__ kbuf,
-                                                       const float* __restrict__ dt,
-                                                       double* __restrict__ red,
-                                                       float* __restrict__ dudt, int waves) {
+template <int DIM, int MODE, bool COH>
+__device__ __forceinline__ void div_body(const fvm_mesh_t& m, const Phys& p, const float* __restrict__ flux,
+                                         const StageArgs& a, float* __restrict__ state, float* __restrict__ prims,
+                                         float* __restrict__ kbuf, const float* __restrict__ dt,
+                                         double* __restrict__ red, float* __restrict__ dudt, int waves) {
     using Ly = L<DIM>;
     constexpr int C = Ly::C, RS = Ly::RS;
     constexpr bool FINAL = MODE >= DIV_FINAL, ADAPT = MODE == DIV_FINAL_ADAPT;
@@ -814,7 +863,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_div_stage(fvm_mesh_t m, Phys p, c
             continue;
         }
         const int cse = (m.n_cases > 0 && live) ? __ldg(m.cell_case + i) : 0;
-        const float h = dt[cse];
+        const float h = COH ? __ldcg(dt + cse) : dt[cse];
         float kk[C], U0[C], inc[C], U[C];
 #pragma unroll
         for (int c = 0; c < C; ++c) {
@@ -897,22 +946,36 @@ __global__ void __launch_bounds__(kMaxBlock) k_div_stage(fvm_mesh_t m, Phys p, c
     }
 }
 
+template <int DIM, int MODE>
+__global__ void __launch_bounds__(kMaxBlock) k_div_stage(fvm_mesh_t m, Phys p, const float* __restrict__ flux,
+                                                       StageArgs a, float* __restrict__ state,
+                                                       float* __restrict__ prims, float* __restrict__ kbuf,
+                                                       const float* __restrict__ dt,
+                                                       double* __restrict__ red,
+                                                       float* __restrict__ dudt, int waves) {
+    div_body<DIM, MODE, false>(m, p, flux, a, state, prims, kbuf, dt, red, dudt, waves);
+}
+
 // Step-end bookkeeping: adaptive dt (integrators.py:42-62) or CFL dt, conservation sums.
 // Batched meshes (n_cases > 0): one thread per case handles its CFL dt and sums.
-__global__ void k_finalize(int C, int adaptive, float atol, float rtol, float mtol, float alpha_hi,
-                           float alpha_lo, float order, float cfl, int cons, double* red, float* dt,
-                           double* cons_out, int n_cases, const uint8_t* __restrict__ active) {
+// The sums were accumulated by atomics of other blocks (in the fused step, of the same launch):
+// read them through L2.
+__device__ __forceinline__ void finalize_body(int C, int adaptive, float atol, float rtol, float mtol,
+                                              float alpha_hi, float alpha_lo, float order, float cfl, int cons,
+                                              double* red, float* dt, double* cons_out, int n_cases,
+                                              const uint8_t* __restrict__ active) {
     if (n_cases > 0) {
         for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cases; c += gridDim.x * blockDim.x) {
             if (active && !active[c]) continue;
             double* slot = red + FVM_RED_DOUBLES + 8 * c;
             if (cfl > 0.f) {
-                if (slot[0] > 0.0) dt[c] = (float)((double)cfl / slot[0]);
+                const double smax = __ldcg(slot);
+                if (smax > 0.0) dt[c] = (float)((double)cfl / smax);
                 slot[0] = 0.0;
             }
             if (cons) {
                 for (int k = 0; k < C; ++k) {
-                    if (cons_out) cons_out[c * C + k] = slot[1 + k];
+                    if (cons_out) cons_out[c * C + k] = __ldcg(slot + 1 + k);
                     slot[1 + k] = 0.0;
                 }
             }
@@ -923,7 +986,7 @@ __global__ void k_finalize(int C, int adaptive, float atol, float rtol, float mt
     if (adaptive) {
         double E = 0.0;
         for (int c = 0; c < C; ++c) {
-            const double nd = sqrt(red[c]), nh = sqrt(red[C + c]), nu = sqrt(red[2 * C + c]);
+            const double nd = sqrt(__ldcg(red + c)), nh = sqrt(__ldcg(red + C + c)), nu = sqrt(__ldcg(red + 2 * C + c));
             E += nd / ((double)atol + (double)rtol * nh + (double)mtol * nu);
             red[c] = red[C + c] = red[2 * C + c] = 0.0;
         }
@@ -935,14 +998,115 @@ __global__ void k_finalize(int C, int adaptive, float atol, float rtol, float mt
         red[40] = E;
     }
     if (cfl > 0.f) {
-        const double smax = red[16];
+        const double smax = __ldcg(red + 16);
         if (smax > 0.0) dt[0] = (float)((double)cfl / smax);
         red[16] = 0.0;
     }
     if (cons) {
         for (int c = 0; c < C; ++c) {
-            if (cons_out) cons_out[c] = red[24 + c];
+            if (cons_out) cons_out[c] = __ldcg(red + 24 + c);
             red[24 + c] = 0.0;
+        }
+    }
+}
+
+__global__ void k_finalize(int C, int adaptive, float atol, float rtol, float mtol, float alpha_hi,
+                           float alpha_lo, float order, float cfl, int cons, double* red, float* dt,
+                           double* cons_out, int n_cases, const uint8_t* __restrict__ active) {
+    finalize_body(C, adaptive, atol, rtol, mtol, alpha_hi, alpha_lo, order, cfl, cons, red, dt, cons_out, n_cases,
+                  active);
+}
+
+// ------------------------------------------------------------------------------------------
+// Fused step: every phase of every stage of one step in one cooperative launch.
+//
+// For small meshes a step is latency bound: 3-4 dependent launches per stage, each too short to
+// fill the GPU.  k_step_fused runs the same phase bodies (boundary values, cell gradients, facet
+// fluxes, divergence + stage update, step-end bookkeeping) back to back in one persistent grid of
+// co-resident blocks (cooperative launch), separated by grid-wide barriers.  Loads of arrays written
+// earlier in the launch use the coherent (.cg) path.  Every per-item computation and every
+// block-level reduction order is the one of the separate kernels, so the result is bitwise the
+// same.  Barrier waits are bounded: a wait that gives up sets the status word and the launch runs
+// to its end (with wrong results) instead of hanging; the host checks it (fvm_fused_status).
+// ------------------------------------------------------------------------------------------
+constexpr long long kBarrierSpinLimit = 1LL << 22;
+
+struct FusedArgs {
+    int stages;
+    StageArgs st[FVM_MAX_STAGES];
+    int need_final;                       // last stage: adaptive / CFL / conservation bookkeeping
+    int adaptive;
+    float atol, rtol, mtol, alpha_hi, alpha_lo, order, cfl;
+    float* state;
+    float* prims;
+    float* grads;
+    int32_t* has_grads;
+    float* k;
+    float* dt;
+    double* cons;
+    float* bcv;
+    float* flux;
+    double* red;
+    unsigned* bar;                        // [0] arrivals, [1] generation
+    int* status;                          // set to 1 when a barrier wait gave up
+};
+
+__device__ __forceinline__ void grid_barrier(unsigned* bar, int* status) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) + 1u == gridDim.x) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long it = 0;
+            while (*gen == g) {
+                if (++it > kBarrierSpinLimit) {
+                    atomicExch(status, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_step_fused(fvm_mesh_t m, Phys p, FusedArgs f) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    for (int s = 0; s < f.stages; ++s) {
+        const StageArgs& a = f.st[s];
+        if (m.n_bc > 0) {
+            if (m.n_cases > 0 && m.n_char > 0) {
+                for (int c = blockIdx.x; c < m.n_cases; c += gridDim.x)
+                    char_scale_case<DIM, true>(m, p, f.prims, f.red, c);
+                grid_barrier(f.bar, f.status);
+            }
+            const float scale = bc_block_scale<DIM, true>(m, p, f.prims);
+            for (int b = tid; b < m.n_bc; b += nth)
+                bc_item<DIM, true>(m, p, f.prims, f.grads, f.has_grads, f.bcv, f.red, b, scale);
+            grid_barrier(f.bar, f.status);
+        }
+        cell_body<DIM, true>(m, p, f.prims, f.bcv, f.grads, f.has_grads, 0);
+        grid_barrier(f.bar, f.status);
+        face_body<DIM, true>(m, p, f.prims, f.bcv, f.grads, f.flux, 0);
+        grid_barrier(f.bar, f.status);
+        if (!a.final_)
+            div_body<DIM, DIV_STAGE, true>(m, p, f.flux, a, f.state, f.prims, f.k, f.dt, f.red, nullptr, 0);
+        else if (a.adaptive)
+            div_body<DIM, DIV_FINAL_ADAPT, true>(m, p, f.flux, a, f.state, f.prims, f.k, f.dt, f.red, nullptr, 0);
+        else
+            div_body<DIM, DIV_FINAL, true>(m, p, f.flux, a, f.state, f.prims, f.k, f.dt, f.red, nullptr, 0);
+        grid_barrier(f.bar, f.status);
+        if (a.final_ && f.need_final) {
+            finalize_body(DIM + 2, f.adaptive, f.atol, f.rtol, f.mtol, f.alpha_hi, f.alpha_lo, f.order, f.cfl, a.cons,
+                          f.red, f.dt, f.cons, m.n_cases, m.case_active);
+            grid_barrier(f.bar, f.status);
         }
     }
 }
@@ -1397,6 +1561,111 @@ extern "C" int fvm_multistep(const fvm_mesh_t* mesh, const fvm_physics_t* phys, 
     cudaStream_t st = (cudaStream_t)stream;
     return mesh->dim == 2 ? multistep_impl<2>(mesh, p, store, n_terms, idx, coef, bufs, work, st)
                           : multistep_impl<3>(mesh, p, store, n_terms, idx, coef, bufs, work, st);
+}
+
+// Barrier words and status of the fused step live in work->red[60], [61] (slots no reduction uses).
+static unsigned* fused_bar(const fvm_work_t* w) { return reinterpret_cast<unsigned*>(w->red + 60); }
+static int* fused_status(const fvm_work_t* w) { return reinterpret_cast<int*>(w->red + 61); }
+
+template <int DIM>
+static int fused_impl(const fvm_mesh_t* m, const Phys& p, FusedArgs& f, cudaStream_t st) {
+    static int blocks_per_sm[2] = {-1, -1}, sms = 0;
+    int& bps = blocks_per_sm[DIM - 2];
+    if (bps < 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_step_fused<DIM>, kBlock, 0) != cudaSuccess) {
+            bps = -1;
+            launch_status();
+            return FVM_E_CUDA;
+        }
+    }
+    if (bps < 1) return FVM_E_UNSUPPORTED;
+    // enough blocks for the largest phase, at most all co-resident ones
+    const int64_t items = std::max<int64_t>({(int64_t)owned_cells(m), (int64_t)m->n_facets, (int64_t)m->n_bc});
+    const unsigned grid = (unsigned)std::min<int64_t>((int64_t)bps * sms, std::max<int64_t>(1, (items + kBlock - 1) / kBlock));
+    fvm_mesh_t mc = *m;
+    void* args[] = {&mc, const_cast<Phys*>(&p), &f};
+    if (cudaMemsetAsync(f.bar, 0, sizeof(unsigned), st) != cudaSuccess) {   // arrivals start at zero
+        launch_status();
+        return FVM_E_CUDA;
+    }
+    prof_begin(KID_FUSED, st);
+    const cudaError_t e =
+        cudaLaunchCooperativeKernel((const void*)k_step_fused<DIM>, dim3(grid), dim3(kBlock), args, 0, st);
+    prof_end(st);
+    if (e != cudaSuccess) {
+        launch_status();
+        return FVM_E_CUDA;
+    }
+    return launch_status();
+}
+
+static void fill_fused(FusedArgs& f, const fvm_tableau_t* tab, const fvm_solver_bufs_t* b, const fvm_work_t* w) {
+    f.need_final = tab->adaptive || tab->cfl > 0.f || b->cons != nullptr;
+    f.adaptive = tab->adaptive;
+    f.atol = tab->atol; f.rtol = tab->rtol; f.mtol = tab->mtol;
+    f.alpha_hi = tab->alpha_hi_err; f.alpha_lo = tab->alpha_lo_err; f.order = tab->order; f.cfl = tab->cfl;
+    f.state = b->state; f.prims = b->prims; f.grads = b->grads; f.has_grads = b->has_grads; f.k = b->k;
+    f.dt = b->dt; f.cons = b->cons; f.bcv = w->bc_vals; f.flux = w->flux; f.red = w->red;
+    f.bar = fused_bar(w); f.status = fused_status(w);
+}
+
+extern "C" int fvm_step_fused(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const fvm_tableau_t* tab,
+                              const fvm_solver_bufs_t* bufs, const fvm_work_t* work, void* stream) {
+    if (const int rc = check_common(mesh)) return rc;
+    if (!phys || !tab_ok(tab) || !bufs_ok(bufs) || !work_ok(mesh, work)) return FVM_E_ARG;
+    if (mesh->n_cases > 0 && tab->adaptive) return FVM_E_UNSUPPORTED;
+    if (mesh->n_owned > 0 || mesh->char_scale_given) return FVM_E_UNSUPPORTED;   // partitions use the split stages
+    FusedArgs f{};
+    f.stages = tab->stages;
+    for (int s = 0; s < tab->stages; ++s) {
+        f.st[s] = stage_args(tab, s);
+        f.st[s].cons = f.st[s].final_ && bufs->cons != nullptr;
+    }
+    fill_fused(f, tab, bufs, work);
+    const Phys p = make_phys(phys);
+    cudaStream_t st = (cudaStream_t)stream;
+    return mesh->dim == 2 ? fused_impl<2>(mesh, p, f, st) : fused_impl<3>(mesh, p, f, st);
+}
+
+extern "C" int fvm_multistep_fused(const fvm_mesh_t* mesh, const fvm_physics_t* phys, int32_t store, int32_t n_terms,
+                                   const int32_t* idx, const float* coef, const fvm_solver_bufs_t* bufs,
+                                   const fvm_work_t* work, void* stream) {
+    if (const int rc = check_common(mesh)) return rc;
+    if (!phys || !bufs_ok(bufs) || !work_ok(mesh, work) || n_terms < 0 || n_terms > FVM_MAX_STAGES ||
+        (n_terms > 0 && (!idx || !coef)) || store < 0)
+        return FVM_E_ARG;
+    if (mesh->n_owned > 0 || mesh->char_scale_given) return FVM_E_UNSUPPORTED;
+    FusedArgs f{};
+    f.stages = 1;
+    StageArgs& a = f.st[0];
+    a.s = store;
+    a.store_k = 1;
+    a.final_ = 1;
+    a.n_terms = n_terms;
+    for (int t = 0; t < n_terms; ++t) {
+        a.idx[t] = idx[t];
+        a.coef[t] = coef[t];
+    }
+    a.cons = bufs->cons != nullptr;
+    fvm_tableau_t tab{};
+    tab.stages = 1;
+    tab.order = 1.f;
+    fill_fused(f, &tab, bufs, work);
+    const Phys p = make_phys(phys);
+    cudaStream_t st = (cudaStream_t)stream;
+    return mesh->dim == 2 ? fused_impl<2>(mesh, p, f, st) : fused_impl<3>(mesh, p, f, st);
+}
+
+extern "C" int fvm_fused_status(const fvm_work_t* work, int32_t* status) {
+    if (!work || !work->red || !status) return FVM_E_ARG;
+    if (cudaMemcpy(status, fused_status(work), sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        launch_status();
+        return FVM_E_CUDA;
+    }
+    return FVM_OK;
 }
 
 extern "C" int fvm_state_to_prims(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const float* state,

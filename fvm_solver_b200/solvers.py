@@ -132,6 +132,17 @@ class TSolver:
             self.update_cfl_dt()
 
     # -- helpers ------------------------------------------------------------------------------
+    fused = False     # True: whole steps as one cooperative launch (fvm_step_fused); see autotune
+
+    def _step_fn(self):
+        return self.lib.fvm_step_fused if self.fused else self.lib.fvm_step
+
+    def fused_status(self) -> int:
+        """1 if a grid-barrier wait of a fused step ever gave up (results invalid), else 0."""
+        out = ct.c_int32(0)
+        _lib.check(self.lib.fvm_fused_status(ct.byref(self.eq.work.struct), ct.byref(out)), "fvm_fused_status")
+        return int(out.value)
+
     def track_conservation(self, on: bool = True):
         """Record the FP64 totals sum vol * U after every step in ``self.cons`` (device)."""
         if on and self.cons is None:
@@ -248,8 +259,8 @@ class Butcher(TSolver):
         super().__init__(cells, eq, cfg)
 
     def _step(self):
-        _lib.check(self.lib.fvm_step(ct.byref(self.eq.dev.struct), ct.byref(self.eq.phys), ct.byref(self.tab),
-                                     ct.byref(self.bufs), ct.byref(self.eq.work.struct), _lib.stream_ptr()),
+        _lib.check(self._step_fn()(ct.byref(self.eq.dev.struct), ct.byref(self.eq.phys), ct.byref(self.tab),
+                                   ct.byref(self.bufs), ct.byref(self.eq.work.struct), _lib.stream_ptr()),
                    "fvm_step")
 
 
@@ -293,17 +304,18 @@ class AB3(TSolver):
         for t in range(n_terms):
             self._idx[t] = idx[t]
             self._coef[t] = coef[t]
-        _lib.check(self.lib.fvm_multistep(ct.byref(self.eq.dev.struct), ct.byref(self.eq.phys), idx[0], n_terms,
-                                          ct.cast(self._idx, ct.c_void_p), ct.cast(self._coef, ct.c_void_p),
-                                          ct.byref(self.bufs), ct.byref(self.eq.work.struct), _lib.stream_ptr()),
+        fn = self.lib.fvm_multistep_fused if self.fused else self.lib.fvm_multistep
+        _lib.check(fn(ct.byref(self.eq.dev.struct), ct.byref(self.eq.phys), idx[0], n_terms,
+                      ct.cast(self._idx, ct.c_void_p), ct.cast(self._coef, ct.c_void_p),
+                      ct.byref(self.bufs), ct.byref(self.eq.work.struct), _lib.stream_ptr()),
                    "fvm_multistep")
 
     def _step(self):
         h = self.head
         if self.n_hist < 2:
             # Start-up: an SSP-RK3 step from U_n; its first increment dt * f(U_n) joins the history.
-            _lib.check(self.lib.fvm_step(ct.byref(self.eq.dev.struct), ct.byref(self.eq.phys), ct.byref(self.rk),
-                                         ct.byref(self.rk_bufs), ct.byref(self.eq.work.struct), _lib.stream_ptr()),
+            _lib.check(self._step_fn()(ct.byref(self.eq.dev.struct), ct.byref(self.eq.phys), ct.byref(self.rk),
+                                       ct.byref(self.rk_bufs), ct.byref(self.eq.work.struct), _lib.stream_ptr()),
                        "fvm_step")
             self.k[h].copy_(self.rk_k[0])
         else:

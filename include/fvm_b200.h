@@ -160,7 +160,7 @@ const char *fvm_version(void);
  * the number of launches recorded (FVM_E_ARG if more than `capacity` were attempted);
  * fvm_profile_read fills host arrays with each launch's kernel id and duration in ms, waiting for
  * the events.  Kernel ids: 0 ell_spmv, 1 ell_spmm, 2 bc, 3 cell, 4 face, 5 div_stage,
- * 6 finalize, 7 state_to_prims, 8 reduce_state, 9 batched, 10 corrector. */
+ * 6 finalize, 7 state_to_prims, 8 reduce_state, 9 batched, 10 corrector, 11 fused step. */
 int fvm_profile_start(int32_t capacity);
 /* Launch configuration (no reference counterpart): threads per block of the cell (id 3), facet
  * (id 4) and divergence/stage (id 5) kernels for all later launches of this process; a multiple
@@ -212,6 +212,20 @@ int fvm_residual(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float 
  * that overlap on the GPU race and must be serialised by the caller. */
 int fvm_residual_noalloc(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *prims,
                          float *grads, int32_t *has_grads, float *dudt, void *stream);
+
+/* Fused step (no reference counterpart): the whole of fvm_step (all stages) -- or of
+ * fvm_multistep -- in one cooperative launch of co-resident blocks, phases separated by grid-wide
+ * barriers; bitwise the same results.  Meant for small meshes, where a step is launch-latency
+ * bound (the autotuner times both).  Its barrier words live in work->red[60..61]; a barrier wait
+ * that gives up (iteration limit) sets a status word instead of hanging, read back with
+ * fvm_fused_status (1 = a wait gave up and the results are invalid; the word stays set).
+ * Partitioned meshes are FVM_E_UNSUPPORTED. */
+int fvm_step_fused(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const fvm_tableau_t *tab,
+                   const fvm_solver_bufs_t *bufs, const fvm_work_t *work, void *stream);
+int fvm_multistep_fused(const fvm_mesh_t *mesh, const fvm_physics_t *phys, int32_t store, int32_t n_terms,
+                        const int32_t *idx, const float *coef, const fvm_solver_bufs_t *bufs,
+                        const fvm_work_t *work, void *stream);
+int fvm_fused_status(const fvm_work_t *work, int32_t *status);
 
 /* Split stage for partitioned meshes (no reference counterpart): a stage is fvm_stage_begin
  * (boundary values + limited cell gradients of the owned cells from bufs->prims), then the
