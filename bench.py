@@ -215,9 +215,15 @@ def cpu_replicas(sample_n: int, steps: int | None = None, warmup: int = 1, budge
     value = sum(n_ * k / el for n_, k, el in out)
     el_max = max(el for _, _, el in out)
     k_min = min(k for _, k, _ in out)
+    cpu_model = "unknown CPU"
+    try:
+        with open("/proc/cpuinfo") as fh:
+            cpu_model = next((ln.split(":", 1)[1].strip() for ln in fh if ln.startswith("model name")), cpu_model)
+    except OSError:
+        pass
     return {"value": value, "unit": "cell-steps/s", "cores": workers, "kind": "port",
-            "sample": f"{workers} single-threaded numpy oracle replicas, periodic TGV box {sample_n}^3 points "
-                      f"({N} tets) each, >= {k_min} RK4 steps each in {el_max:.1f} s",
+            "sample": f"{workers} single-threaded numpy oracle replicas ({cpu_model}), periodic TGV box "
+                      f"{sample_n}^3 points ({N} tets) each, >= {k_min} RK4 steps each in {el_max:.1f} s",
             "ms_per_step": 1e3 * el_max / max(k_min, 1)}
 
 
@@ -441,6 +447,7 @@ def secondary(args):
     fused_b = tune_fused(batch)
     with ClockSampler(0) as clk:
         ms_b = timed(batch.t_solver, args.steps)
+    roof = batched_roofline(batch, steps=10)
     del batch
     torch.cuda.empty_cache()
     # plain: every case alone, each with its own captured graph of the same number of steps
@@ -464,11 +471,45 @@ def secondary(args):
                       "cells_min": min(sizes), "cells_max": max(sizes), "integrator": "AB3 (SSP-RK3 start), CFL 0.3",
                       "timing": "cuda graph replay", "table_build_s": t_build, "host_cpus": os.cpu_count(),
                       "block_sizes": tuned, "fused_step": fused_b},
+           "roofline": roof,
            "plain": {"value": vp, "unit": "cell-steps/s", "ms_per_step_all_cases": ms_p / args.steps,
                      "how": "each case alone, own CUDA graph, sequential",
                      "cases_with_fused_step": n_fused},
            "batched_over_plain": vb / vp, "clocks": clk.summary()}
     print(json.dumps(out))
+
+
+def batched_roofline(batch, steps: int = 10) -> dict:
+    """Per-kernel achieved bandwidth of the batched AB3 step (an eager pass of ``steps`` steps with
+    every launch bracketed by CUDA events): algorithmic bytes (``roofline.kernel_bytes``; the
+    Adams step's divergence kernel reads two stored increments and writes one plus the state) over
+    the mean launch time, against the measured HBM copy bandwidth."""
+    from fvm_solver_b200 import _lib
+    from fvm_solver_b200.roofline import kernel_bytes
+    lib = _lib.load()
+    kt = batch.kt
+    _lib.check(lib.fvm_profile_start(steps * 16 + 16), "fvm_profile_start")
+    batch.t_solver.step(steps)
+    n = lib.fvm_profile_stop()
+    torch.cuda.synchronize()
+    ids = np.zeros(max(n, 1), np.int32)
+    ms = np.zeros(max(n, 1), np.float32)
+    if n <= 0 or lib.fvm_profile_read(n, ids.ctypes.data, ms.ctypes.data) != n:
+        return None
+    kb = kernel_bytes(kt.dim, kt.n_cells, kt.n_facets, kt.n_bc)
+    byts = {"bc": kb["bc"], "cell": kb["cell"], "face": kb["face"], "div_stage": kb["div_base"] + 4 * kb["row"]}
+    peak, peak_kind = measured_peaks()
+    kern = {}
+    for kid, name in ((2, "bc"), (3, "cell"), (4, "face"), (5, "div_stage")):
+        sel = ids == kid
+        if not np.any(sel):
+            continue
+        m = float(ms[sel].mean())
+        kern[name] = {"ms_mean": m, "share": float(ms[sel].sum() / ms[:n].sum()),
+                      "algorithmic_bytes_per_launch": byts[name], "achieved_gbs": byts[name] / (m / 1e3) / 1e9}
+    dom = max(kern, key=lambda k: kern[k]["share"])
+    return {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
+            "frac": kern[dom]["achieved_gbs"] / peak, "peak_source": peak_kind, "kernels": kern}
 
 
 def corrector_bench(args, timed):

@@ -4,7 +4,7 @@ Every array a kernel must touch is counted once at its stored width (4 bytes per
 8 per double); gathers of an array already counted are not counted again.  N cells, F facets,
 Fb boundary facets, d = dim, C = d + 2 components, K = d + 1 facets per cell; R = FVM_ROW (4 in
 2D, 8 in 3D) floats per padded primitive / flux row, G = FVM_GROW (8 / 16) per limited-gradient
-row, CR / FR / DR = cell / facet / divergence record widths (20 / 12 / 8 in 2D, 36 / 16 / 8 in 3D).
+row, CR / FR / DR = cell / facet / divergence record widths (24 / 16 / 8 in 2D, 40 / 16 / 8 in 3D).
 
 k_cell      reads  cell records CR N, primitives R N, boundary values R Fb
             writes limited gradients G N
