@@ -650,6 +650,8 @@ def main():
         if world > 1:
             dist.barrier()
 
+    if world > 1:
+        torch.set_num_threads(max(1, (os.cpu_count() or 1) // world))   # ranks build their meshes at once
     case = W.taylor_green(n=args.n, seed=rank, device=f"cuda:{local}")
     eq = case.equation()
     sol = eq.t_solver
@@ -754,8 +756,9 @@ def main():
     e2e_value = cells_total * ke / (float(t.item()) / 1e3)
 
     cpu = parity = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.sample_n)                 # on the host cores, at N = 1 only
     if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.sample_n)
         parity = parity_check(args.sample_n)
     launches_per_step = n_launch / args.steps
     if rank == 0:
