@@ -80,6 +80,7 @@ _SIGS = [
     ("fvm_step_fused", ct.c_int, [_P, _P, _P, _P, _P, _P]),
     ("fvm_multistep_fused", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, _P, _P, _P, _P, _P]),
     ("fvm_fused_status", ct.c_int, [_P, _P]),
+    ("fvm_barrier_selftest", ct.c_int, [ct.c_int32, ct.c_int32, _P]),
     ("fvm_stage_begin", ct.c_int, [_P, _P, _P, _P, _P]),
     ("fvm_stage_end", ct.c_int, [_P, _P, _P, ct.c_int32, _P, _P, ct.c_int32, _P]),
     ("fvm_stage_finalize", ct.c_int, [_P, _P, _P, _P, _P]),

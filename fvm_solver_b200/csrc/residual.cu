@@ -1076,6 +1076,33 @@ __device__ __forceinline__ void grid_barrier(unsigned* bar, int* status) {
     __syncthreads();
 }
 
+// Barrier self-test: every block but `skip` meets at grid_barrier twice; with skip >= 0 that block
+// never arrives, so the others' bounded waits give up and set the status word.
+__global__ void __launch_bounds__(64) k_barrier_selftest(unsigned* bar, int* status, int skip, long long limit) {
+    if ((int)blockIdx.x == skip) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) + 1u == gridDim.x) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long it = 0;
+            while (*gen == g) {
+                if (++it > limit) {
+                    atomicExch(status, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+    }
+    __syncthreads();
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(kBlock) k_step_fused(fvm_mesh_t m, Phys p, FusedArgs f) {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
@@ -1657,6 +1684,29 @@ extern "C" int fvm_multistep_fused(const fvm_mesh_t* mesh, const fvm_physics_t* 
     const Phys p = make_phys(phys);
     cudaStream_t st = (cudaStream_t)stream;
     return mesh->dim == 2 ? fused_impl<2>(mesh, p, f, st) : fused_impl<3>(mesh, p, f, st);
+}
+
+extern "C" int fvm_barrier_selftest(int32_t blocks, int32_t skip_block, int32_t* status) {
+    if (blocks < 2 || blocks > 64 || skip_block >= blocks || !status) return FVM_E_ARG;
+    unsigned* d = nullptr;   // [0] arrivals, [1] generation, [2] status
+    if (cudaMalloc(&d, 3 * sizeof(unsigned)) != cudaSuccess || cudaMemset(d, 0, 3 * sizeof(unsigned)) != cudaSuccess) {
+        launch_status();
+        if (d) cudaFree(d);
+        return FVM_E_CUDA;
+    }
+    unsigned* bar = d;
+    int* st = reinterpret_cast<int*>(d + 2);
+    int skip = skip_block;
+    long long limit = 1LL << 16;            // ~5 ms of polling: the test's waits run out quickly
+    void* args[] = {&bar, &st, &skip, &limit};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_barrier_selftest, dim3(blocks), dim3(64), args, 0, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(status, st, sizeof(int32_t), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+        launch_status();
+        return FVM_E_CUDA;
+    }
+    return FVM_OK;
 }
 
 extern "C" int fvm_fused_status(const fvm_work_t* work, int32_t* status) {

@@ -226,6 +226,11 @@ int fvm_multistep_fused(const fvm_mesh_t *mesh, const fvm_physics_t *phys, int32
                         const int32_t *idx, const float *coef, const fvm_solver_bufs_t *bufs,
                         const fvm_work_t *work, void *stream);
 int fvm_fused_status(const fvm_work_t *work, int32_t *status);
+/* Self-test of the fused step's bounded grid barrier (no reference counterpart): a cooperative
+ * launch of `blocks` blocks (2..64) meets at one barrier; with skip_block >= 0 that block never
+ * arrives, the others' waits give up after a short iteration limit and *status becomes 1 (0 when
+ * every block arrives).  Allocates and frees a few bytes of device memory; synchronous. */
+int fvm_barrier_selftest(int32_t blocks, int32_t skip_block, int32_t *status);
 
 /* Split stage for partitioned meshes (no reference counterpart): a stage is fvm_stage_begin
  * (boundary values + limited cell gradients of the owned cells from bufs->prims), then the

@@ -70,3 +70,21 @@ def test_tune_fused_picks_and_restores():
     assert set(res["ms_per_step"]) == {"separate", "fused"}
     assert eq.t_solver.fused == res["fused"]
     assert torch.equal(eq.cells.state, before)
+
+
+def test_grid_barrier_gives_up_and_context_survives():
+    """A block that never reaches the barrier: the others' bounded waits end, the status says so,
+    and the GPU context keeps working (a fused step runs correctly afterwards)."""
+    import ctypes as ct
+    from fvm_solver_b200 import _lib
+    lib = _lib.load()
+    st = ct.c_int32(-1)
+    assert lib.fvm_barrier_selftest(8, -1, ct.byref(st)) == 0 and st.value == 0
+    st = ct.c_int32(-1)
+    assert lib.fvm_barrier_selftest(8, 3, ct.byref(st)) == 0 and st.value == 1
+    from gpu_helpers import make_equation
+    a, b = _pair(lambda: make_equation("c2d", "Butcher", "RK4", cfl=0.5)[1])
+    a.t_solver.step(2)
+    b.t_solver.step(2)
+    torch.cuda.synchronize()
+    assert torch.equal(a.cells.state, b.cells.state) and b.t_solver.fused_status() == 0
