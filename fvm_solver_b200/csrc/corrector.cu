@@ -211,6 +211,14 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
     const uint32_t taddr = s_taddr;
     const uint32_t idesc = make_idesc(N);
     const int rows_a = min(TM, g.M - m0);
+    // The epilogue's residual rows (one contiguous block of the tile's rows) go to L2 while the
+    // tile is loaded and multiplied: the bulk-copy unit prefetches them, so the epilogue's loads
+    // see L2 latency instead of DRAM latency.
+    if (threadIdx.x == 0 && g.resid && g.k_splits == 1 && g.vec && rows_a > 0) {
+        const uint32_t bytes = (uint32_t)((int64_t)rows_a * g.ldr * 4) & ~15u;
+        if (bytes) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g.resid + (int64_t)m0 * g.ldr),
+                                "r"(bytes) : "memory");
+    }
     auto stage = [&](int buf, int kc) {
         uint8_t* sA = smem + buf * kStageBytes;
         stage_tile_async(sA, g.A, g.lda, m0, rows_a, TM, kc * TK, g.K);
@@ -313,10 +321,13 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
 
 template <int N>
 static int launch_gemm(const GemmArgs& g, cudaStream_t s) {
-    const size_t smem = 2 * ((size_t)TM * TK * 2 + (size_t)N * TK * 2);
+    // one staging buffer per K slice a CTA handles, at most two (fewer bytes: more CTAs per SM)
+    const int kchunks = g.K / TK, per = (kchunks + g.k_splits - 1) / g.k_splits;
+    const size_t smem = (size_t)(per >= 2 ? 2 : 1) * ((size_t)TM * TK * 2 + (size_t)N * TK * 2);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_gemm<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_gemm<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(2 * ((size_t)TM * TK * 2 + (size_t)N * TK * 2)));
         attr = true;
     }
     dim3 grid((unsigned)((g.M + TM - 1) / TM), (unsigned)g.k_splits);
