@@ -46,18 +46,6 @@ __device__ __forceinline__ void load_row(const float* __restrict__ p, float (&v)
     }
 }
 
-// Load from a buffer written earlier in the same kernel sequence but never in this kernel.
-template <int C>
-__device__ __forceinline__ void load_row_cg(const float* p, float (&v)[C]) {
-    if constexpr (C == 4) {
-        const float4 t = __ldcg(reinterpret_cast<const float4*>(p));
-        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-    } else {
-#pragma unroll
-        for (int c = 0; c < C; ++c) v[c] = __ldcg(p + c);
-    }
-}
-
 template <int C>
 __device__ __forceinline__ void store_row(float* p, const float (&v)[C]) {
     if constexpr (C == 4) {

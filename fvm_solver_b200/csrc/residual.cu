@@ -184,10 +184,6 @@ __device__ __forceinline__ bool case_on(const fvm_mesh_t& m, const int32_t* case
 // The two side codes (first two words) of a facet record.
 __device__ __forceinline__ int2 ld_codes(const float* rec) { return __ldg(reinterpret_cast<const int2*>(rec)); }
 
-// Non-persistent kernels: block b prefetches the rows of block b + ahead (0 = off).
-__device__ __forceinline__ void prefetch_rows(const float* base, int64_t n_rows, int row_floats, int ahead) {
-    if (ahead > 0) prefetch_tile(base, n_rows, row_floats, (int64_t)blockIdx.x + ahead);
-}
 
 // ------------------------------------------------------------------------------------------
 // Slope limiters (limiter.py:29-77).  delta: allowed range, dU: unlimited increment.
