@@ -100,6 +100,8 @@ _SIGS = [
                             ct.c_int32, _P, _P, ct.c_int32, ct.c_int32, _P]),
     ("fvm_corrector_features", ct.c_int, [_P, ct.c_int32, ct.c_int32, _P, _P, _P, ct.c_int32, _P, ct.c_int32, _P]),
     ("fvm_apply_increment", ct.c_int, [_P, _P, _P, ct.c_int32, ct.c_int32, _P, _P]),
+    ("fvm_mp_gemm", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, _P, _P, _P, ct.c_int64, _P, _P, ct.c_int64,
+                               ct.c_int32, _P, _P]),
     ("fvm_corrector_inputs", ct.c_int, [_P, _P, _P, _P, ct.c_int32, ct.c_int32, _P, _P, _P, ct.c_int32, _P, _P,
                                         ct.c_int32, _P]),
     ("fvm_corrector_combine", ct.c_int, [_P, _P, _P, _P, _P, _P, ct.c_int32, ct.c_int32, _P, _P]),

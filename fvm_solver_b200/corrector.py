@@ -151,6 +151,14 @@ class CorrectorNet:
         self._gemm(b["X"], XW, self.bf["W_in"], XW, N, W, XW, Df=b["hf"][0], Db=b["hb"][0], ldd=W, bias=p["b_in"],
                    pre=Z[0], act=1)
         for l in range(L):
+            if not store_pre:
+                # inference: the neighbour mean is built inside the layer's GEMM (bitwise the same)
+                _lib.check(self.lib.fvm_mp_gemm(b["hb"][l].data_ptr(), nbr.data_ptr(), N, nbr.shape[1],
+                                                self.bf[f"W{l}"].data_ptr(), p[f"b{l}"].data_ptr(),
+                                                b["hf"][l].data_ptr(), W, b["hf"][l + 1].data_ptr(),
+                                                b["hb"][l + 1].data_ptr(), W, 1, self.err.data_ptr(), s),
+                           "fvm_mp_gemm")
+                continue
             _lib.check(self.lib.fvm_mp_gather(b["hb"][l].data_ptr(), nbr.data_ptr(), N, W, nbr.shape[1],
                                               b["A"][l].data_ptr(), s), "fvm_mp_gather")
             self._gemm(b["A"][l], 2 * W, self.bf[f"W{l}"], 2 * W, N, W, 2 * W, Df=b["hf"][l + 1], Db=b["hb"][l + 1],

@@ -319,6 +319,147 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
                      "r"((uint32_t)(N < 32 ? 32 : N)));
 }
 
+// One message-passing layer with the neighbour mean built in shared memory (inference):
+//   D = epilogue([h_i, mean_{j in nbr(i)} h_j] . W^T),  h: bf16 [M][64], W: bf16 [64][128].
+// Thread r of the CTA stages row m0 + r of the A tile directly in the MMA's core-matrix layout:
+// K slice 0 = h_i, slice 1 = the neighbour mean, computed with the arithmetic of k_mp_gather
+// (fp32 sum over the valid neighbours in table order, times 1 / count, rounded to bf16), so the
+// result is bitwise that of fvm_mp_gather followed by fvm_gemm_bf16 -- without writing and reading
+// back the [M][128] gathered matrix.  Weights arrive by cp.async; MMA, bounded completion wait and
+// epilogue are those of k_gemm.
+constexpr int kMpW = 64;
+__global__ void __launch_bounds__(kGemmThreads) k_mp_gemm(GemmArgs g, const __nv_bfloat16* __restrict__ h,
+                                                          const int32_t* __restrict__ nbr, int KN) {
+    constexpr int N = kMpW;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    constexpr int kStageBytes = TM * TK * 2 + N * TK * 2;
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t s_taddr;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * TM;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_taddr)),
+                     "r"((uint32_t)N));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t taddr = s_taddr;
+    const uint32_t idesc = make_idesc(N);
+    const int rows_a = min(TM, g.M - m0);
+    if (threadIdx.x == 0 && g.resid && g.vec && rows_a > 0) {
+        const uint32_t bytes = (uint32_t)((int64_t)rows_a * g.ldr * 4) & ~15u;
+        if (bytes) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g.resid + (int64_t)m0 * g.ldr),
+                                "r"(bytes) : "memory");
+    }
+    // weights: both K slices
+    for (int c = 0; c < 2; ++c)
+        stage_tile_async(smem + c * kStageBytes + TM * TK * 2, g.B, g.ldb, 0, N, N, c * TK, 2 * kMpW);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    // A rows: slice 0 = own row, slice 1 = neighbour mean.  First each tile row's neighbour list
+    // and 1 / count go to shared memory; then the 128 x 8 (row, 8-channel unit) items are staged with
+    // the conflict-free lane mapping of stage_tile_async (a warp: 8 rows x 4 units), several items per
+    // thread in flight.
+    __shared__ int s_nb[TM * 8];
+    __shared__ float s_inv[TM];
+    {
+        const int r = threadIdx.x;
+        const bool valid = r < rows_a;
+        int cnt = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int j = (valid && k < KN) ? __ldg(nbr + ((int64_t)m0 + r) * KN + k) : -1;
+            s_nb[r * 8 + k] = j;
+            cnt += j >= 0;
+        }
+        s_inv[r] = cnt > 0 ? 1.f / (float)cnt : 0.f;
+    }
+    __syncthreads();
+    {
+        const int slice_bytes = (TM / 8) * 256;
+#pragma unroll 2
+        for (int t = threadIdx.x; t < TM * 8; t += kGemmThreads) {
+            const int r = (t & 7) + 8 * (t >> 6), u = (t >> 3) & 7;
+            const bool valid = r < rows_a;
+            const int64_t row = (int64_t)m0 + r;
+            const int off = (u >> 1) * slice_bytes + (r >> 3) * 256 + (u & 1) * 128 + (r & 7) * 16;
+            const uint4 self = valid ? *reinterpret_cast<const uint4*>(h + row * kMpW + 8 * u) : make_uint4(0, 0, 0, 0);
+            float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int j = s_nb[r * 8 + k];
+                if (j < 0) continue;
+                const uint4 v = *reinterpret_cast<const uint4*>(h + (int64_t)j * kMpW + 8 * u);
+                const __nv_bfloat16* bv = reinterpret_cast<const __nv_bfloat16*>(&v);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) acc[q] += __bfloat162float(bv[q]);
+            }
+            const float inv = s_inv[r];
+            __align__(16) __nv_bfloat16 mv[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) mv[q] = valid ? __float2bfloat16(acc[q] * inv) : __float2bfloat16(0.f);
+            *reinterpret_cast<uint4*>(smem + off) = self;
+            *reinterpret_cast<uint4*>(smem + kStageBytes + off) = *reinterpret_cast<const uint4*>(mv);
+        }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        for (int c = 0; c < 2; ++c) {
+            const uint32_t sa = smem_u32(smem + c * kStageBytes), sb = sa + TM * TK * 2;
+#pragma unroll
+            for (int s = 0; s < TK / 16; ++s) {
+                const uint64_t ad = make_desc(sa + s * (TM / 8) * 256, 128, 256);
+                const uint64_t bd = make_desc(sb + s * (N / 8) * 256, 128, 256);
+                const uint32_t acc = (c > 0 || s > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(taddr),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&mbar))
+                     : "memory");
+    }
+    bool done = mbar_wait(&mbar, 0u);
+    if (!done) done = mbar_wait(&mbar, 0u) && false;      // second bounded chance, then report
+    const bool ok = __syncthreads_and(done) != 0;
+    if (!ok && threadIdx.x == 0 && g.err) atomicExch(g.err, 1);
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const int row = m0 + warp * 32 + lane;
+    if (ok) {
+#pragma unroll 1
+        for (int c0 = 0; c0 < N; c0 += 32) {
+            uint32_t r[32];
+            const uint32_t a = taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(a));
+            asm volatile("tcgen05.wait::ld.sync.aligned;");
+            if (row < g.M) epilogue_vec(g, row, c0, r);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"((uint32_t)N));
+}
+
 template <int N>
 static int launch_gemm(const GemmArgs& g, cudaStream_t s) {
     // one staging buffer per K slice a CTA handles, at most two (fewer bytes: more CTAs per SM)
@@ -730,5 +871,29 @@ extern "C" int fvm_corrector_combine(const float* state, const float* base, cons
     cudaStream_t s = (cudaStream_t)stream;
     FVM_LAUNCH(KID_CORRECTOR, s, corr::k_corrector_combine<<<corr::nblk((int64_t)N * C, 256), 256, 0, s>>>(
                                      state, base, out, scale, shift, cell_case, N, C, prop));
+    return launch_status();
+}
+
+extern "C" int fvm_mp_gemm(const void* h, const int32_t* nbr, int32_t M, int32_t KN, const void* Wt,
+                           const float* bias, const float* resid, int64_t ldr, float* Df, void* Db, int64_t ldd,
+                           int32_t act, int32_t* err, void* stream) {
+    if (!h || !nbr || !Wt || M <= 0 || KN <= 0 || KN > 8 || (!Df && !Db) || !err) return FVM_E_ARG;
+    if ((uintptr_t)h % 16 || (uintptr_t)Wt % 16) return FVM_E_ARG;
+    auto a32 = [](const void* p) { return ((uintptr_t)p & 31u) == 0; };
+    const bool vec = a32(bias) && a32(resid) && a32(Df) && a32(Db) && (!resid || ldr % 8 == 0) &&
+                     (!Df || ldd % 8 == 0) && (!Db || ldd % 16 == 0);
+    if (!vec) return FVM_E_ARG;                              // the fused layer has only the 256-bit epilogue
+    corr::GemmArgs g{nullptr, 0, static_cast<const __nv_bfloat16*>(Wt), 2 * corr::kMpW, M, corr::kMpW,
+                     2 * corr::kMpW, 1, bias, resid, ldr, Df, static_cast<__nv_bfloat16*>(Db), ldd, nullptr, act,
+                     err, 1};
+    const size_t smem = 2 * ((size_t)corr::TM * corr::TK * 2 + (size_t)corr::kMpW * corr::TK * 2);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(corr::k_mp_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_mp_gemm<<<(unsigned)((M + corr::TM - 1) / corr::TM), corr::kGemmThreads,
+                                                   smem, s>>>(g, static_cast<const __nv_bfloat16*>(h), nbr, KN));
     return launch_status();
 }

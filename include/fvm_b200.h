@@ -298,6 +298,14 @@ int fvm_gemm_bf16(const void *A, int64_t lda, const void *B, int64_t ldb, int32_
 
 /* Corrector kernels (no reference counterpart).  Activations are bf16 [N][W] (W % 8 == 0, rows
  * 16-byte aligned); nbr is an int32 [N][KN] neighbour table (-1 = none, adjacency symmetric). */
+/* A message-passing layer in one kernel (W = 64): D = epilogue([h_i, mean_{j in nbr(i)} h_j] . Wt^T)
+ * with Wt bf16 [64][128] (K-major), epilogue as fvm_gemm_bf16 (bias, SiLU if act = 1, residual add,
+ * fp32 Df and/or bf16 Db [M][ldd]); the gathered [M][128] matrix is built in shared memory and never
+ * stored.  Bitwise equal to fvm_mp_gather + fvm_gemm_bf16.  KN <= 8; bias/resid/Df/Db 32-byte
+ * aligned with ldr, ldd multiples of 8 (16 for Db). */
+int fvm_mp_gemm(const void *h, const int32_t *nbr, int32_t M, int32_t KN, const void *Wt, const float *bias,
+                const float *resid, int64_t ldr, float *Df, void *Db, int64_t ldd, int32_t act, int32_t *err,
+                void *stream);
 /* out[i] = [h_i, mean_{j in nbr(i)} h_j]  (bf16 [N][2W]). */
 int fvm_mp_gather(const void *h, const int32_t *nbr, int32_t N, int32_t W, int32_t KN, void *out, void *stream);
 /* dh_out[i] = dh_in[i] + dA[i][:W] + sum_{j in nbr(i)} dA[j][W:] / deg(j)  (fp32; dh_in may be NULL). */

@@ -70,6 +70,8 @@ def test_forward_backward_vs_autograd(small_batch):
     ref_out, ref_loss, ref_g = _torch_reference(model.net, X, model.nbr, target, N)
     out = model.net.forward(model.nbr).clone()
     assert rel_l2(out.cpu().numpy(), ref_out.cpu().numpy()) < 2e-3
+    # inference builds the neighbour mean inside the GEMM: bitwise the same output
+    assert torch.equal(model.net.forward(model.nbr, store_pre=False), out)
     grads_before = {k: v.clone() for k, v in model.net.grads.items()}
     assert all(float(v.abs().max()) == 0.0 for v in grads_before.values())
     # capture the gradients: run the backward pass but stop Adam from zeroing them
