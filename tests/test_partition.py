@@ -15,7 +15,7 @@ def _parts(case, P):
     return tables.kernel, split_tables(tables.kernel, P)
 
 
-@pytest.mark.parametrize("case,P", [("c2d", 2), ("c2d", 3), ("b3d", 2), ("b3d", 4)])
+@pytest.mark.parametrize("case,P", [("c2d", 1), ("c2d", 2), ("c2d", 3), ("b3d", 2), ("b3d", 4)])
 def test_partition_invariants(case, P):
     kt, parts = _parts(case, P)
     N = kt.n_cells
