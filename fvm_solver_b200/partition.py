@@ -67,6 +67,7 @@ class MeshPart:
     bcs: torch.Tensor              # [Fb_local] global boundary-facet indices
     tables: KernelTables           # the part's tables, renumbered
     face_rec: torch.Tensor | None = None       # [F_local][FVM_FACE_REC] facet records (see below)
+    global_n_char: int = 0                     # characteristic facets of the whole mesh (same on every part)
     recv: dict = field(default_factory=dict)   # q -> (start, stop): halo rows owned by part q
     send: dict = field(default_factory=dict)   # q -> local ids of own cells part q keeps in its halo
 
@@ -176,7 +177,7 @@ def split_tables(kt: KernelTables, parts: int, owner: torch.Tensor | None = None
             raise RuntimeError("partition: a facet side points outside the part")
         fr[:, :2] = loc.to(torch.int32).view(torch.float32)
         part = MeshPart(rank=p, parts=parts, n_owned=n_own, cells=cells, facets=facets, bcs=bcs, tables=t,
-                        face_rec=fr)
+                        face_rec=fr, global_n_char=int(kt.n_char))
         ho = owner[halo]
         for q in range(parts):
             sel = torch.nonzero(ho == q).flatten()
@@ -300,7 +301,9 @@ class PartitionedSolver:
         self.phys = phys
         self.tab = tab
         self.C = parts[0].tables.n_comp
-        self.has_char = any(p.tables.n_char > 0 for p in parts)
+        # decided from the whole mesh, so that every rank takes the same collective steps even when
+        # its own part has no characteristic facet
+        self.has_char = parts[0].global_n_char > 0
 
     # -- state in and out ------------------------------------------------------------------------
     def set_state(self, global_state: torch.Tensor):

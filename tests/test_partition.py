@@ -23,6 +23,7 @@ def test_partition_invariants(case, P):
     assert torch.equal(torch.sort(owned).values, torch.arange(N))            # every cell owned once
     assert sum(p.tables.n_bc for p in parts) == kt.n_bc                      # every boundary facet once
     assert sum(p.tables.n_char for p in parts) == kt.n_char
+    assert all(p.global_n_char == kt.n_char for p in parts)     # same collective plan on every rank
     for p in parts:
         t, n_loc, n_own = p.tables, p.n_local, p.n_owned
         assert t.n_cells == n_loc and n_own > 0
