@@ -11,7 +11,9 @@ A "step" is one full RK4 step (4 residual evaluations + stage updates + FP64 CFL
   replay of the graph first; inputs resident in HBM; the per-stage working set, >1 GB, is larger
   than L2, so no L2 flush is needed).
 * ``e2e``    -- the same metric through the public API with host buffers: every step copies the
-  state host->device from pinned memory, steps, and copies the new state back.
+  state host->device from pinned memory, steps, and copies the new state back (all three queued
+  on one stream, so the host never waits between steps; each step's input is the previous
+  step's output read back to the host).
 * ``roofline`` -- the dominant kernel's algorithmic bytes per launch / its mean CUDA-event
   duration over a second timed pass of K steps (events bracket every launch), against the
   measured HBM copy bandwidth.
@@ -743,7 +745,7 @@ def main():
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for _ in range(ke):
-        eq.cells.state = host_in                 # H2D (pinned) into the device state
+        eq.cells.load(host_in, non_blocking=True)   # H2D (pinned), stream-ordered after the last D2H
         sol.step(1)
         host_out.copy_(eq.cells.state, non_blocking=True)   # D2H of the step's result
         host_in, host_out = host_out, host_in

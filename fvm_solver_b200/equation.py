@@ -171,6 +171,12 @@ class FVMCells:
         self._state.copy_(value)
         self.version += 1
 
+    def load(self, value: torch.Tensor, non_blocking: bool = False):
+        """Set the state from ``value`` (host or device); ``non_blocking`` with a pinned host
+        tensor enqueues the copy on the current stream without waiting for it."""
+        self._state.copy_(value, non_blocking=non_blocking)
+        self.version += 1
+
     def update_cells(self, state_new):
         self.state = state_new
 
