@@ -171,9 +171,10 @@ class FVMCells:
         self._state.copy_(value)
         self.version += 1
 
-    def load(self, value: torch.Tensor, non_blocking: bool = False):
+    def copy_from(self, value: torch.Tensor, non_blocking: bool = False):
         """Set the state from ``value`` (host or device); ``non_blocking`` with a pinned host
-        tensor enqueues the copy on the current stream without waiting for it."""
+        tensor enqueues the copy on the current stream without waiting for it.  (``load`` below
+        keeps the reference's meaning: read a saved state file.)"""
         self._state.copy_(value, non_blocking=non_blocking)
         self.version += 1
 

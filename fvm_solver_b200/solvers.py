@@ -196,6 +196,89 @@ class TSolver:
         replay.graph = g
         return replay
 
+    # -- host-resident states ------------------------------------------------------------------
+    def _restart(self, dt0: torch.Tensor):
+        """Make the next step behave as on a freshly built solver holding the current state: no
+        carried limiter gradients, no multistep history, the time step of ``dt0`` (or, with a CFL
+        number, recomputed from the state as the constructor does)."""
+        self.eq.has_grads.zero_()
+        self.eq._has_grads_host = False
+        self.dt.copy_(dt0)
+        if hasattr(self, "n_hist"):
+            self.n_hist, self.head = 0, 0
+        if self.cfl:
+            self.update_cfl_dt()
+
+    def step_host(self, inputs, outputs, steps: int = 1):
+        """Advance a stream of independent host states: ``outputs[i]`` <- ``inputs[i]`` after
+        ``steps`` steps, each state started afresh (see ``_restart``; the time step in force at
+        the call is every state's initial one).
+
+        ``inputs`` and ``outputs`` are sequences of contiguous float32 [N, C] host tensors, pinned
+        for the copies to run asynchronously (an output may appear twice; the later state wins).
+        The copies run on two copy streams through two device slots each way, so the host->device
+        copy of state i+1 and the device->host copy of state i-1 overlap the steps of state i on
+        the current stream; the host does not wait.  The call returns once everything is queued:
+        synchronise the current stream before reading ``outputs``.  The solver is left holding the
+        last state's result.
+        """
+        n = len(inputs)
+        if len(outputs) != n:
+            raise ValueError("step_host needs as many outputs as inputs")
+        if n == 0:
+            return outputs
+        N, C = self.cells.state.shape
+        for t in (*inputs, *outputs):
+            if t.is_cuda or t.dtype != torch.float32 or not t.is_contiguous() or tuple(t.shape) != (N, C):
+                raise ValueError(f"step_host needs contiguous float32 host tensors of shape [{N}, {C}]")
+        dev = self.eq.device
+        comp = torch.cuda.current_stream(dev)
+        st = getattr(self, "_host_stage", None)
+        if st is None:
+            st = self._host_stage = {
+                "h2d": torch.cuda.Stream(device=dev), "d2h": torch.cuda.Stream(device=dev),
+                "slot_in": [torch.empty((N, C), device=dev) for _ in range(2)],
+                "slot_out": [torch.empty((N, C), device=dev) for _ in range(2)]}
+        h2d, d2h, slot_in, slot_out = st["h2d"], st["d2h"], st["slot_in"], st["slot_out"]
+        in_ready = [torch.cuda.Event() for _ in range(2)]
+        in_free = [torch.cuda.Event() for _ in range(2)]
+        out_ready = [torch.cuda.Event() for _ in range(2)]
+        out_free = [torch.cuda.Event() for _ in range(2)]
+        dt0 = self.dt.clone()
+        h2d.wait_stream(comp)              # earlier work on the slots (and dt0) comes first
+        d2h.wait_stream(comp)
+
+        def fetch(i):
+            s = i % 2
+            if i >= 2:
+                h2d.wait_event(in_free[s])     # state i-2 has left slot s
+            with torch.cuda.stream(h2d):
+                slot_in[s].copy_(inputs[i], non_blocking=True)
+            in_ready[s].record(h2d)
+
+        fetch(0)
+        if n > 1:
+            fetch(1)
+        for i in range(n):
+            s = i % 2
+            comp.wait_event(in_ready[s])
+            self.cells.copy_from(slot_in[s])
+            in_free[s].record(comp)
+            if i + 2 < n:
+                fetch(i + 2)
+            self._restart(dt0)
+            self.step(steps)
+            if i >= 2:
+                comp.wait_event(out_free[s])   # state i-2 has left slot s
+            slot_out[s].copy_(self.cells.state)
+            out_ready[s].record(comp)
+            d2h.wait_event(out_ready[s])
+            with torch.cuda.stream(d2h):
+                outputs[i].copy_(slot_out[s], non_blocking=True)
+            out_free[s].record(d2h)
+        comp.wait_stream(d2h)
+        return outputs
+
     # -- checkpoint / restart ------------------------------------------------------------------
     def state_dict(self) -> dict:
         """Everything a bitwise-identical restart needs: the conserved state, the carried limited

@@ -9,7 +9,7 @@ import torch
 from conftest import golden_setup
 
 
-def make_equation(case, solver_name="Butcher", solver_extra="RK4", dt=None, cfl=None):
+def make_equation(case, solver_name="Butcher", solver_extra="RK4", dt=None, cfl=None, state0=None):
     from fvm_solver_b200 import equation as E, mesh_store as ms
     g, spec, tables, cfg = golden_setup(case)
     cfg = copy.deepcopy(cfg)
@@ -20,7 +20,7 @@ def make_equation(case, solver_name="Butcher", solver_extra="RK4", dt=None, cfl=
     dim = int(g["dim"])
     phy = E.FluidConstitution2D(cfg) if dim == 2 else E.FluidConstitution3D(cfg)
     eq = E.FVMEquation(cfg, phy, spec, dim + 2, ms.default_bc_tags(spec.bc_tags, dim),
-                       us_init=torch.from_numpy(g["state0"]))
+                       us_init=torch.from_numpy(g["state0"]) if state0 is None else state0)
     return g, eq, tables, cfg
 
 
