@@ -11,11 +11,14 @@ A "step" is one full RK4 step (4 residual evaluations + stage updates + FP64 CFL
   replay of the graph first; inputs resident in HBM; the per-stage working set, >1 GB, is larger
   than L2, so no L2 flush is needed).
 * ``e2e``    -- the same metric through the public API with host buffers: ``TSolver.step_host``
-  advances K independent pinned host states (a ring of 4 distinct snapshots) by one step each:
-  every step copies its state host->device, restarts the solver on it (CFL time step from the
-  state, no carried gradients), steps, and copies the result back; the copies run on two copy
-  streams and overlap the neighbouring steps.  ``chained_value`` is the serial case where each
+  advances max(K, 50) independent pinned host states (a ring of 4 distinct snapshots) by one
+  step each: every step copies its state host->device, restarts the solver on it (CFL time step
+  from the state, no carried gradients), steps, and copies the result back (the device part as
+  one CUDA-graph replay); the copies run on two copy streams and overlap the neighbouring steps.  ``chained_value`` is the serial case where each
   step's input is the previous step's output read back to the host (nothing can overlap).
+  ``bound`` sets the streamed step time against the slower of one state's device work (its
+  graph replayed alone: copy into the state, restart, step, copy out) and one state copied in
+  and one out at the same time (timed alone): ``frac`` = that bound / the step time.
 * ``roofline`` -- the dominant kernel's algorithmic bytes per launch / its mean CUDA-event
   duration over a second timed pass of K steps (events bracket every launch), against the
   measured HBM copy bandwidth.
@@ -738,14 +741,14 @@ def main():
             v["achieved_gbs"] = per_launch[k] / (v["ms_mean"] / 1e3) / 1e9
 
     # end-to-end through the public API with host buffers
-    ke = args.e2e_steps or args.steps
+    ke = args.e2e_steps or max(args.steps, 50)
     ring = 4                                          # distinct host states, cycled
     host_in = [torch.empty((N, 5), dtype=torch.float32).pin_memory() for _ in range(ring)]
     host_out = [torch.empty((N, 5), dtype=torch.float32).pin_memory() for _ in range(ring)]
     for h in host_in:
         sol.step(1)
         h.copy_(eq.cells.state.cpu())
-    sol.step_host(host_in[:2], host_out[:2])          # untimed: creates the copy streams and slots
+    sol.step_host(host_in[:2], host_out[:2])          # untimed: creates the copy streams, slots and graphs
     torch.cuda.synchronize()
 
     def e2e_time(run) -> float:
@@ -777,6 +780,44 @@ def main():
             a, b = b, a
     e2e_chained = e2e_time(chained)
 
+    # the transfer bound of (a): one state in and one state out at once, on two copy streams
+    # (what every streamed step has to move), timed alone
+    def copy_ms(h2d: bool, d2h: bool, reps: int = 5) -> float:
+        s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+        dev_in, dev_out = torch.empty((N, 5), device="cuda"), eq.cells.state.clone()
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        s_in.wait_stream(stream)
+        s_out.wait_stream(stream)
+        for _ in range(reps):
+            if h2d:
+                with torch.cuda.stream(s_in):
+                    dev_in.copy_(host_in[1], non_blocking=True)
+            if d2h:
+                with torch.cuda.stream(s_out):
+                    host_out[1].copy_(dev_out, non_blocking=True)
+        stream.wait_stream(s_in)
+        stream.wait_stream(s_out)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        return g0.elapsed_time(g1) / reps
+    copy_pair, copy_h2d, copy_d2h = copy_ms(True, True), copy_ms(True, False), copy_ms(False, True)
+
+    # the device bound of (a): one state's device work (copy into the state, restart, one step,
+    # copy out -- the graph step_host replays per state), replayed back to back without copies
+    per_state = sol._host_stage(1)["graphs"][0]
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for _ in range(10):
+        per_state.replay()
+    g1.record(stream)
+    torch.cuda.synchronize()
+    state_ms = g0.elapsed_time(g1) / 10
+    e2e_step_ms = cells_total * 1e3 / e2e_value
+    e2e_bound_ms = max(copy_pair, state_ms)
+
     cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.sample_n)                 # on the host cores, at N = 1 only
@@ -803,9 +844,14 @@ def main():
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": N * 5 * 4,
                     "d2h_bytes_per_step": N * 5 * 4, "steps": ke,
                     "mode": "TSolver.step_host: independent pinned host states, each copied in, stepped "
-                            "once (RK4, CFL dt from the state) and copied out; copies on two streams "
-                            "overlap the neighbouring steps",
+                            "once (RK4, CFL dt from the state; one CUDA-graph replay) and copied out; "
+                            "copies on two streams overlap the neighbouring steps",
                     "chained_value": e2e_chained,
+                    "bound": {"kind": "pcie" if copy_pair > state_ms else "device",
+                              "ms_per_step": e2e_step_ms, "copy_in_and_out_ms": copy_pair,
+                              "copy_in_ms": copy_h2d, "copy_out_ms": copy_d2h,
+                              "device_state_ms": state_ms, "device_step_ms": ms_max / args.steps,
+                              "frac": e2e_bound_ms / e2e_step_ms},
                     "chained_mode": "state round-trips through the host every step (no overlap possible)"},
             "gpu_launches": int(round(launches_per_step * args.steps)),
             "clocks": clocks,

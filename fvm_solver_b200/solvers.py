@@ -155,11 +155,14 @@ class TSolver:
                                        _lib.ptr(self.cells.state), float(cfl), _lib.ptr(self.dt),
                                        ct.byref(self.eq.work.struct), _lib.stream_ptr()), "fvm_cfl_dt")
 
+    def _state_to_prims(self):
+        _lib.check(self.lib.fvm_state_to_prims(ct.byref(self.eq.dev.struct), ct.byref(self.eq.phys),
+                                               _lib.ptr(self.cells.state), _lib.ptr(self.prims),
+                                               _lib.stream_ptr()), "fvm_state_to_prims")
+
     def _sync_prims(self):
         if self._prims_version != self.cells.version:
-            _lib.check(self.lib.fvm_state_to_prims(ct.byref(self.eq.dev.struct), ct.byref(self.eq.phys),
-                                                   _lib.ptr(self.cells.state), _lib.ptr(self.prims),
-                                                   _lib.stream_ptr()), "fvm_state_to_prims")
+            self._state_to_prims()
             self._prims_version = self.cells.version
 
     def _step(self):
@@ -209,6 +212,44 @@ class TSolver:
         if self.cfl:
             self.update_cfl_dt()
 
+    def _host_stage(self, steps: int) -> dict:
+        """Device slots, copy streams and the per-slot CUDA graphs of ``step_host``.  The graph of
+        slot s copies slot s into the state, restarts the solver (``_restart``), converts the
+        state to primitives, takes ``steps`` steps and copies the result to output slot s.  The
+        graphs are kept for the next call with the same ``steps`` and step form; block sizes set
+        later by the autotuner do not reach them (results do not depend on block sizes)."""
+        dev = self.eq.device
+        N, C = self.cells.state.shape
+        st = getattr(self, "_host_st", None)
+        if st is None:
+            st = self._host_st = {
+                "h2d": torch.cuda.Stream(device=dev), "d2h": torch.cuda.Stream(device=dev),
+                "slot_in": [torch.empty((N, C), device=dev) for _ in range(2)],
+                "slot_out": [torch.empty((N, C), device=dev) for _ in range(2)],
+                "dt0": torch.empty_like(self.dt), "key": None}
+        key = (steps, self.fused)
+        if st["key"] != key:
+            st["graphs"] = None
+            s = torch.cuda.Stream(device=dev)
+            s.wait_stream(torch.cuda.current_stream(dev))
+            graphs = []
+            for slot in range(2):
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.stream(s):
+                    with torch.cuda.graph(g, stream=s):
+                        self.cells.state.copy_(st["slot_in"][slot])
+                        self._restart(st["dt0"])
+                        self._state_to_prims()
+                        for _ in range(steps):
+                            self._step()
+                        st["slot_out"][slot].copy_(self.cells.state)
+                graphs.append(g)
+            torch.cuda.current_stream(dev).wait_stream(s)
+            # host-side multistep counters after the captured steps (set after every replay)
+            st["hist"] = (self.n_hist, self.head) if hasattr(self, "n_hist") else None
+            st["graphs"], st["key"] = graphs, key
+        return st
+
     def step_host(self, inputs, outputs, steps: int = 1):
         """Advance a stream of independent host states: ``outputs[i]`` <- ``inputs[i]`` after
         ``steps`` steps, each state started afresh (see ``_restart``; the time step in force at
@@ -216,11 +257,11 @@ class TSolver:
 
         ``inputs`` and ``outputs`` are sequences of contiguous float32 [N, C] host tensors, pinned
         for the copies to run asynchronously (an output may appear twice; the later state wins).
-        The copies run on two copy streams through two device slots each way, so the host->device
-        copy of state i+1 and the device->host copy of state i-1 overlap the steps of state i on
-        the current stream; the host does not wait.  The call returns once everything is queued:
-        synchronise the current stream before reading ``outputs``.  The solver is left holding the
-        last state's result.
+        Each state's device work is one CUDA-graph replay on the current stream, through two
+        device slots each way; the copies run on two copy streams, so the host->device copy of
+        state i+1 and the device->host copy of state i-1 overlap the steps of state i, and the
+        host does not wait.  The call returns once everything is queued: synchronise the current
+        stream before reading ``outputs``.  The solver is left holding the last state's result.
         """
         n = len(inputs)
         if len(outputs) != n:
@@ -233,25 +274,19 @@ class TSolver:
                 raise ValueError(f"step_host needs contiguous float32 host tensors of shape [{N}, {C}]")
         dev = self.eq.device
         comp = torch.cuda.current_stream(dev)
-        st = getattr(self, "_host_stage", None)
-        if st is None:
-            st = self._host_stage = {
-                "h2d": torch.cuda.Stream(device=dev), "d2h": torch.cuda.Stream(device=dev),
-                "slot_in": [torch.empty((N, C), device=dev) for _ in range(2)],
-                "slot_out": [torch.empty((N, C), device=dev) for _ in range(2)]}
-        h2d, d2h, slot_in, slot_out = st["h2d"], st["d2h"], st["slot_in"], st["slot_out"]
+        st = self._host_stage(steps)
+        h2d, d2h, slot_in, slot_out, graphs = st["h2d"], st["d2h"], st["slot_in"], st["slot_out"], st["graphs"]
         in_ready = [torch.cuda.Event() for _ in range(2)]
-        in_free = [torch.cuda.Event() for _ in range(2)]
-        out_ready = [torch.cuda.Event() for _ in range(2)]
+        slot_free = [torch.cuda.Event() for _ in range(2)]      # graph of the slot's last state done
         out_free = [torch.cuda.Event() for _ in range(2)]
-        dt0 = self.dt.clone()
-        h2d.wait_stream(comp)              # earlier work on the slots (and dt0) comes first
+        st["dt0"].copy_(self.dt)
+        h2d.wait_stream(comp)              # earlier work on the slots comes first
         d2h.wait_stream(comp)
 
         def fetch(i):
             s = i % 2
             if i >= 2:
-                h2d.wait_event(in_free[s])     # state i-2 has left slot s
+                h2d.wait_event(slot_free[s])   # state i-2's graph has read slot s
             with torch.cuda.stream(h2d):
                 slot_in[s].copy_(inputs[i], non_blocking=True)
             in_ready[s].record(h2d)
@@ -262,21 +297,24 @@ class TSolver:
         for i in range(n):
             s = i % 2
             comp.wait_event(in_ready[s])
-            self.cells.copy_from(slot_in[s])
-            in_free[s].record(comp)
+            if i >= 2:
+                comp.wait_event(out_free[s])   # state i-2's result has left output slot s
+            graphs[s].replay()
+            slot_free[s].record(comp)
             if i + 2 < n:
                 fetch(i + 2)
-            self._restart(dt0)
-            self.step(steps)
-            if i >= 2:
-                comp.wait_event(out_free[s])   # state i-2 has left slot s
-            slot_out[s].copy_(self.cells.state)
-            out_ready[s].record(comp)
-            d2h.wait_event(out_ready[s])
+            d2h.wait_event(slot_free[s])
             with torch.cuda.stream(d2h):
                 outputs[i].copy_(slot_out[s], non_blocking=True)
             out_free[s].record(d2h)
         comp.wait_stream(d2h)
+        # host bookkeeping as after eager steps: state and primitives agree, gradients carried
+        self.cells.version += 1
+        self._prims_version = self.cells.version
+        self.eq._has_grads_host = True
+        if st["hist"] is not None:
+            self.n_hist, self.head = st["hist"]
+        self.steps_done += n * steps
         return outputs
 
     # -- checkpoint / restart ------------------------------------------------------------------

@@ -1,6 +1,6 @@
 """``TSolver.step_host``: a stream of independent host states, each advanced as if by a freshly
-built solver holding it, with the copies overlapped on two copy streams -- bitwise equal to
-building one solver per state."""
+built solver holding it (one CUDA-graph replay per state, the copies overlapped on two copy
+streams) -- bitwise equal to building one solver per state."""
 import pytest
 import torch
 
@@ -44,6 +44,19 @@ def test_step_host_matches_fresh_solvers(case, solver, extra, cfl, steps):
     eq.t_solver.step(1)
     torch.cuda.synchronize()
     assert torch.equal(eq.cells.state, ref.cells.state)
+    # a second call reuses the captured graphs; another step count captures new ones
+    again = [torch.empty_like(x).pin_memory() for x in inputs[:3]]
+    eq.t_solver.step_host(inputs[:3][::-1], again, steps=steps)
+    torch.cuda.synchronize()
+    for y, z in zip(outputs[:3][::-1], again):
+        assert torch.equal(y, z)
+    one = [torch.empty_like(inputs[0]).pin_memory()]
+    eq.t_solver.step_host(inputs[:1], one, steps=steps + 1)
+    torch.cuda.synchronize()
+    ref = make(inputs[0].clone())
+    ref.t_solver.step(steps + 1)
+    torch.cuda.synchronize()
+    assert torch.equal(one[0], ref.cells.state.cpu())
 
 
 def test_step_host_rejects_bad_buffers():
