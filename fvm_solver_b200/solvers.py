@@ -216,8 +216,9 @@ class TSolver:
         """Device slots, copy streams and the per-slot CUDA graphs of ``step_host``.  The graph of
         slot s copies slot s into the state, restarts the solver (``_restart``), converts the
         state to primitives, takes ``steps`` steps and copies the result to output slot s.  The
-        graphs are kept for the next call with the same ``steps`` and step form; block sizes set
-        later by the autotuner do not reach them (results do not depend on block sizes)."""
+        graphs are kept for the next call with the same ``steps``, step form, CFL number and
+        conservation tracking (all baked into the captured launches); block sizes set later by
+        the autotuner do not reach them (results do not depend on block sizes)."""
         dev = self.eq.device
         N, C = self.cells.state.shape
         st = getattr(self, "_host_st", None)
@@ -227,7 +228,7 @@ class TSolver:
                 "slot_in": [torch.empty((N, C), device=dev) for _ in range(2)],
                 "slot_out": [torch.empty((N, C), device=dev) for _ in range(2)],
                 "dt0": torch.empty_like(self.dt), "key": None}
-        key = (steps, self.fused)
+        key = (steps, self.fused, self.cfl, self.bufs.cons)
         if st["key"] != key:
             st["graphs"] = None
             s = torch.cuda.Stream(device=dev)
