@@ -257,7 +257,8 @@ class TSolver:
         the call is every state's initial one).
 
         ``inputs`` and ``outputs`` are sequences of contiguous float32 [N, C] host tensors, pinned
-        for the copies to run asynchronously (an output may appear twice; the later state wins).
+        for the copies to run asynchronously (an output may appear twice; the later state wins;
+        an output must not also be an input, since the two copy streams are not ordered).
         Each state's device work is one CUDA-graph replay on the current stream, through two
         device slots each way; the copies run on two copy streams, so the host->device copy of
         state i+1 and the device->host copy of state i-1 overlap the steps of state i, and the
@@ -273,6 +274,8 @@ class TSolver:
         for t in (*inputs, *outputs):
             if t.is_cuda or t.dtype != torch.float32 or not t.is_contiguous() or tuple(t.shape) != (N, C):
                 raise ValueError(f"step_host needs contiguous float32 host tensors of shape [{N}, {C}]")
+        if {t.data_ptr() for t in inputs} & {t.data_ptr() for t in outputs}:
+            raise ValueError("step_host: an output buffer is also an input")
         dev = self.eq.device
         comp = torch.cuda.current_stream(dev)
         st = self._host_stage(steps)

@@ -70,4 +70,6 @@ def test_step_host_rejects_bad_buffers():
         eq.t_solver.step_host([torch.zeros((N + 1, C))], [good])
     with pytest.raises(ValueError):
         eq.t_solver.step_host([good], [torch.zeros((N, C), device="cuda")])
+    with pytest.raises(ValueError):
+        eq.t_solver.step_host([good], [good])
     assert eq.t_solver.step_host([], []) == []
