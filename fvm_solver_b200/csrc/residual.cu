@@ -707,61 +707,6 @@ __device__ __forceinline__ double cfl_speed(const fvm_mesh_t& m, const Phys& p, 
     return __ldg(m.inv_h + i) * (sqrt(v2) + sqrt((double)p.gamma * (double)p.R * fmax(T, 0.0)));
 }
 
-// Conservation sums sum vol U and CFL speed max of the block's cells into red (single mesh) or
-// into the per-case slots red[FVM_RED_DOUBLES + 8 case + {0: max speed, 1..C: sums}] (batched).
-// Batched: warps whose lanes all belong to one case reduce first; mixed warps use per-lane atomics.
-template <int DIM>
-__device__ __forceinline__ void reduce_cons_cfl(const fvm_mesh_t& m, const Phys& p, const float* U, bool live,
-                                                int cse, int want_cons, int want_cfl, double* red,
-                                                double* smem) {
-    constexpr int C = DIM + 2;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m.n_cases == 0) {
-        if (want_cons) {
-            double v[C];
-#pragma unroll
-            for (int c = 0; c < C; ++c) v[c] = live ? __ldg(m.volumes + i) * (double)U[c] : 0.0;
-            block_sum<C>(v, smem);
-            if (threadIdx.x == 0)
-                for (int c = 0; c < C; ++c) atomicAdd(red + 24 + c, v[c]);
-            __syncthreads();
-        }
-        if (want_cfl) {
-            double sp = live ? cfl_speed<DIM>(m, p, U, i) : 0.0;
-            sp = block_max(sp, smem);
-            if (threadIdx.x == 0) atomic_max_pos(red + 16, sp);
-        }
-        return;
-    }
-    const int lane = threadIdx.x & 31;
-    const int c0 = __shfl_sync(0xffffffffu, cse, 0);
-    const bool uniform = __all_sync(0xffffffffu, !live || cse == c0);
-    double* slot = red + FVM_RED_DOUBLES + 8 * cse;
-    if (want_cfl) {
-        double sp = live ? cfl_speed<DIM>(m, p, U, i) : 0.0;
-        if (uniform) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) sp = fmax(sp, __shfl_down_sync(0xffffffffu, sp, o));
-            if (lane == 0 && sp > 0.0) atomic_max_pos(red + FVM_RED_DOUBLES + 8 * c0, sp);
-        } else if (live) {
-            atomic_max_pos(slot, sp);
-        }
-    }
-    if (want_cons) {
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            double v = live ? __ldg(m.volumes + i) * (double)U[c] : 0.0;
-            if (uniform) {
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-                if (lane == 0) atomicAdd(red + FVM_RED_DOUBLES + 8 * c0 + 1 + c, v);
-            } else if (live) {
-                atomicAdd(slot + 1 + c, v);
-            }
-        }
-    }
-}
-
 // Batched meshes: per-case reductions of one item per lane, warp-level when the warp's live lanes
 // share a case, per-lane atomics otherwise (all lanes of the warp must call it).
 template <int DIM>
@@ -1159,21 +1104,53 @@ __global__ void __launch_bounds__(kBlock) k_pad_prims(int N, const float* __rest
     st_vec<Ly::RS>(dst + (int64_t)i * Ly::RS, P);
 }
 
+// Conservation sums sum vol U and the CFL speed maximum of a state: a persistent grid-stride loop.
+// Single mesh: each thread accumulates over its cells and the block combines once (one atomic
+// per block and quantity).  Batched meshes: warp-uniform iterations, per-item warp reductions
+// into the per-case slots (reduce_batched_item).
 template <int DIM>
 __global__ void __launch_bounds__(kBlock) k_reduce_state(fvm_mesh_t m, Phys p, const float* __restrict__ state,
                                                           int want_cfl, int want_cons, double* red) {
     constexpr int C = DIM + 2;
-    __shared__ double smem[32 * C];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i < (m.n_owned > 0 ? m.n_owned : m.n_cells);
-    float U[C];
+    const int NA = m.n_owned > 0 ? m.n_owned : m.n_cells;
+    const int stride = gridDim.x * blockDim.x;
+    if (m.n_cases == 0) {
+        __shared__ double smem[32 * C];
+        double cons[C], sp = 0.0;
 #pragma unroll
-    for (int c = 0; c < C; ++c) U[c] = 1.f;
-    if (live)
+        for (int c = 0; c < C; ++c) cons[c] = 0.0;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NA; i += stride) {
+            float U[C];
 #pragma unroll
-        for (int c = 0; c < C; ++c) U[c] = __ldg(state + (int64_t)i * C + c);
-    const int cse = (m.n_cases > 0 && live) ? __ldg(m.cell_case + i) : 0;
-    reduce_cons_cfl<DIM>(m, p, U, live, cse, want_cons, want_cfl, red, smem);
+            for (int c = 0; c < C; ++c) U[c] = __ldg(state + (int64_t)i * C + c);
+            if (want_cons) {
+                const double vol = __ldg(m.volumes + i);
+#pragma unroll
+                for (int c = 0; c < C; ++c) cons[c] += vol * (double)U[c];
+            }
+            if (want_cfl) sp = fmax(sp, cfl_speed<DIM>(m, p, U, i));
+        }
+        if (want_cons) {
+            block_sum<C>(cons, smem);
+            if (threadIdx.x == 0)
+                for (int c = 0; c < C; ++c) atomicAdd(red + 24 + c, cons[c]);
+            __syncthreads();
+        }
+        if (want_cfl) {
+            sp = block_max(sp, smem);
+            if (threadIdx.x == 0) atomic_max_pos(red + 16, sp);
+        }
+        return;
+    }
+    for (int i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < NA; i0 += stride) {
+        const int i = i0 + (threadIdx.x & 31);
+        const bool live = i < NA;
+        float U[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) U[c] = live ? __ldg(state + (int64_t)i * C + c) : 1.f;
+        const int cse = live ? __ldg(m.cell_case + i) : 0;
+        reduce_batched_item<DIM>(m, p, U, live, i, cse, want_cons, want_cfl, red);
+    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1263,6 +1240,10 @@ static inline unsigned blocks_of(int64_t n, int bs) { return (unsigned)((n + bs 
 static inline unsigned persistent_grid(int64_t n, int threads, int wave) {
     const unsigned all = blocks_of(n, threads);
     return wave > 0 && (unsigned)wave < all ? (unsigned)wave : all;
+}
+template <int DIM>
+static inline unsigned reduce_grid(const fvm_mesh_t* m) {
+    return persistent_grid(owned_cells(m), kBlock, wave_blocks(k_reduce_state<DIM>, kBlock));
 }
 static inline unsigned fin_blocks(const fvm_mesh_t* m) {
     return m->n_cases > 0 ? (unsigned)((m->n_cases + 127) / 128) : 1u;
@@ -1734,10 +1715,10 @@ extern "C" int fvm_cfl_dt(const fvm_mesh_t* mesh, const fvm_physics_t* phys, con
     const Phys p = make_phys(phys);
     cudaStream_t st = (cudaStream_t)stream;
     if (mesh->dim == 2)
-        FVM_LAUNCH(KID_REDUCE_STATE, st, k_reduce_state<2><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
+        FVM_LAUNCH(KID_REDUCE_STATE, st, k_reduce_state<2><<<reduce_grid<2>(mesh), kBlock, 0, st>>>(
                                              *mesh, p, state, 1, 0, work->red));
     else
-        FVM_LAUNCH(KID_REDUCE_STATE, st, k_reduce_state<3><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
+        FVM_LAUNCH(KID_REDUCE_STATE, st, k_reduce_state<3><<<reduce_grid<3>(mesh), kBlock, 0, st>>>(
                                              *mesh, p, state, 1, 0, work->red));
     int rc = launch_status();
     if (rc) return rc;
@@ -1753,10 +1734,10 @@ extern "C" int fvm_conservation(const fvm_mesh_t* mesh, const float* state, doub
     Phys p{};
     cudaStream_t st = (cudaStream_t)stream;
     if (mesh->dim == 2)
-        FVM_LAUNCH(KID_REDUCE_STATE, st, k_reduce_state<2><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
+        FVM_LAUNCH(KID_REDUCE_STATE, st, k_reduce_state<2><<<reduce_grid<2>(mesh), kBlock, 0, st>>>(
                                              *mesh, p, state, 0, 1, work->red));
     else
-        FVM_LAUNCH(KID_REDUCE_STATE, st, k_reduce_state<3><<<blocks_for(mesh->n_cells), kBlock, 0, st>>>(
+        FVM_LAUNCH(KID_REDUCE_STATE, st, k_reduce_state<3><<<reduce_grid<3>(mesh), kBlock, 0, st>>>(
                                              *mesh, p, state, 0, 1, work->red));
     int rc = launch_status();
     if (rc) return rc;
