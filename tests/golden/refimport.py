@@ -1,6 +1,7 @@
 """Import the reference implementation (Python, CPU path) for fixture generation and checks.
 
-Only this container has the reference sources; nothing that runs on a GPU box imports this.
+Only the machine that generates the fixtures has the reference sources; the GPU tests, the smoke
+test and the benchmark never import this.
 The stubs in ``refstubs/`` stand in for the reference's plotting / coloured-print dependencies,
 which are absent here.  ``fp64=True`` applies a dtype shim (default dtype float64 and
 ``torch.float32`` / ``Tensor.float`` redirected to float64) because the reference hard-codes
