@@ -184,6 +184,22 @@ __device__ __forceinline__ bool case_on(const fvm_mesh_t& m, const int32_t* case
 // The two side codes (first two words) of a facet record.
 __device__ __forceinline__ int2 ld_codes(const float* rec) { return __ldg(reinterpret_cast<const int2*>(rec)); }
 
+// One-ahead index loads of the persistent loops.  Nothing is read for an item past the end or of a
+// frozen case (case mask), so a masked-out case costs one case-id read per item.
+template <int DIM>
+__device__ __forceinline__ int2 next_codes(const fvm_mesh_t& m, int f, int nF) {
+    const bool on = f < nF && case_on(m, m.face_case, f);
+    return on ? ld_codes(m.face_rec + (int64_t)f * L<DIM>::FR) : make_int2(0, 0);
+}
+template <int DIM>
+__device__ __forceinline__ void next_cols(const fvm_mesh_t& m, int i, int NA, int* cols) {
+    using Ly = L<DIM>;
+    const bool on = i < NA && case_on(m, m.cell_case, i);
+#pragma unroll
+    for (int k = 0; k < Ly::KG; ++k)
+        cols[k] = on ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)i * Ly::CR + Ly::GC + k) : 0;
+}
+
 
 // ------------------------------------------------------------------------------------------
 // Slope limiters (limiter.py:29-77).  delta: allowed range, dU: unlimited increment.
@@ -375,15 +391,11 @@ __device__ __forceinline__ void cell_body(const fvm_mesh_t& m, const Phys& p, co
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) *has_grads = 1;
     int cols[KG];
-#pragma unroll
-    for (int k = 0; k < KG; ++k) cols[k] = i < NA ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)i * Ly::CR + Ly::GC + k) : 0;
+    next_cols<DIM>(m, i, NA, cols);
     for (int64_t tile = blockIdx.x; i < NA; i += stride, tile += gridDim.x) {
         if (waves > 0) prefetch_tile(m.cell_rec, NA, Ly::CR, tile + (int64_t)waves * gridDim.x);
         if (m.case_active && !case_on(m, m.cell_case, i)) {
-            const int inext = i + stride;
-#pragma unroll
-            for (int k = 0; k < KG; ++k)
-                cols[k] = inext < NA ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)inext * Ly::CR + Ly::GC + k) : 0;
+            next_cols<DIM>(m, i + stride, NA, cols);
             continue;
         }
         float X[KG][RS];
@@ -396,10 +408,7 @@ __device__ __forceinline__ void cell_body(const fvm_mesh_t& m, const Phys& p, co
         ld_mut<COH, RS>(prims + (int64_t)i * RS, U);
         float rec[Ly::CR];
         ld_vec<Ly::CR>(m.cell_rec + (int64_t)i * Ly::CR, rec);
-        const int inext = i + stride;
-#pragma unroll
-        for (int k = 0; k < KG; ++k)
-            cols[k] = inext < NA ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)inext * Ly::CR + Ly::GC + k) : 0;
+        next_cols<DIM>(m, i + stride, NA, cols);
         const int nvalid = (as_int(rec[Ly::META]) >> 24) & 31;
         float g[DIM][C];
 #pragma unroll
@@ -474,12 +483,12 @@ __device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, co
     const int nF = m.n_facets;
     const int stride = gridDim.x * blockDim.x;
     int f = blockIdx.x * blockDim.x + threadIdx.x;
-    int2 nxt = f < nF ? ld_codes(m.face_rec + (int64_t)f * Ly::FR) : make_int2(0, 0);
+    int2 nxt = next_codes<DIM>(m, f, nF);
     for (int64_t tile = blockIdx.x; f < nF; f += stride, tile += gridDim.x) {
     if (waves > 0) prefetch_tile(m.face_rec, nF, Ly::FR, tile + (int64_t)waves * gridDim.x);
     const int ca = nxt.x, cb = nxt.y;
     if (m.case_active && !case_on(m, m.face_case, f)) {
-        if (f + stride < nF) nxt = ld_codes(m.face_rec + (int64_t)(f + stride) * Ly::FR);
+        nxt = next_codes<DIM>(m, f + stride, nF);
         continue;
     }
     // Both sides: primitives and limited gradient of the cell(s); a boundary side (code < 0) takes
@@ -493,7 +502,7 @@ __device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, co
     ld_vec_cg<GS>(grads + (int64_t)cell1 * GS, G1);
     float rec[Ly::FR];
     ld_vec<Ly::FR>(m.face_rec + (int64_t)f * Ly::FR, rec);
-    if (f + stride < nF) nxt = ld_codes(m.face_rec + (int64_t)(f + stride) * Ly::FR);
+    nxt = next_codes<DIM>(m, f + stride, nF);
     const float size = rec[Ly::SIZE];
     float n[DIM], nh[DIM];
 #pragma unroll
@@ -769,7 +778,8 @@ __device__ __forceinline__ void div_body(const fvm_mesh_t& m, const Phys& p, con
     for (int c = 0; c < (ADAPT ? 3 * C : 1); ++c) ad_acc[c] = 0.0;
     int i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
     float nxt[Ly::DR];
-    if (i0 + lane < NA) ld_vec<Ly::DR>(m.div_rec + (int64_t)(i0 + lane) * Ly::DR, nxt);
+    if (i0 + lane < NA && case_on(m, m.cell_case, i0 + lane))
+        ld_vec<Ly::DR>(m.div_rec + (int64_t)(i0 + lane) * Ly::DR, nxt);
     else
 #pragma unroll
         for (int q = 0; q < Ly::DR; ++q) nxt[q] = 0.f;
@@ -798,7 +808,8 @@ __device__ __forceinline__ void div_body(const fvm_mesh_t& m, const Phys& p, con
                 }
             }
         }
-        if (i + stride < NA) ld_vec<Ly::DR>(m.div_rec + (int64_t)(i + stride) * Ly::DR, nxt);
+        if (i + stride < NA && case_on(m, m.cell_case, i + stride))
+            ld_vec<Ly::DR>(m.div_rec + (int64_t)(i + stride) * Ly::DR, nxt);
         if (MODE == DIV_RESIDUAL) {
             if (live) store_state<C>(dudt + (int64_t)i * C, r);
             continue;
@@ -1142,15 +1153,75 @@ __global__ void __launch_bounds__(kBlock) k_reduce_state(fvm_mesh_t m, Phys p, c
         }
         return;
     }
-    for (int i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < NA; i0 += stride) {
-        const int i = i0 + (threadIdx.x & 31);
-        const bool live = i < NA;
-        float U[C];
+    // Batched: each warp takes one contiguous chunk of cells and accumulates per lane while the
+    // case stays the same (a case's cells are contiguous); a change of case flushes the partial
+    // results with one warp reduction and one atomic per quantity into the old case's slots.
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = stride >> 5;
+    const int64_t w = (int64_t)(blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t chunk = (((int64_t)NA + warps - 1) / warps + 31) & ~(int64_t)31;
+    const int64_t beg = w * chunk, end = beg + chunk < NA ? beg + chunk : (int64_t)NA;
+    int cur = -1;                                      // case of the accumulators (warp-uniform)
+    double acc[C], amax = 0.0;
 #pragma unroll
-        for (int c = 0; c < C; ++c) U[c] = live ? __ldg(state + (int64_t)i * C + c) : 1.f;
-        const int cse = live ? __ldg(m.cell_case + i) : 0;
-        reduce_batched_item<DIM>(m, p, U, live, i, cse, want_cons, want_cfl, red);
+    for (int c = 0; c < C; ++c) acc[c] = 0.0;
+    auto flush = [&]() {
+        if (cur < 0) return;
+        double* slot = red + FVM_RED_DOUBLES + 8 * cur;
+        if (want_cfl) {
+            double v = amax;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(full, v, o));
+            if (lane == 0 && v > 0.0) atomic_max_pos(slot, v);
+        }
+        if (want_cons)
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                double v = acc[c];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(full, v, o);
+                if (lane == 0) atomicAdd(slot + 1 + c, v);
+            }
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[c] = 0.0;
+        amax = 0.0;
+    };
+    for (int64_t i0 = beg; i0 < end; i0 += 32) {
+        const int64_t i = i0 + lane;
+        const bool live = i < end;
+        const int cse = live ? __ldg(m.cell_case + i) : -1;
+        double v[C], sp = 0.0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) v[c] = 0.0;
+        if (live) {
+            float U[C];
+#pragma unroll
+            for (int c = 0; c < C; ++c) U[c] = __ldg(state + i * C + c);
+            if (want_cons) {
+                const double vol = __ldg(m.volumes + i);
+#pragma unroll
+                for (int c = 0; c < C; ++c) v[c] = vol * (double)U[c];
+            }
+            if (want_cfl) sp = cfl_speed<DIM>(m, p, U, (int)i);
+        }
+        unsigned pending = __ballot_sync(full, live);
+        while (pending) {                              // once per distinct case among the lanes
+            const int lc = __shfl_sync(full, cse, __ffs(pending) - 1);
+            if (lc != cur) {
+                flush();
+                cur = lc;
+            }
+            const bool mine = live && cse == lc;
+            if (mine) {
+#pragma unroll
+                for (int c = 0; c < C; ++c) acc[c] += v[c];
+                amax = fmax(amax, sp);
+            }
+            pending &= ~__ballot_sync(full, mine);
+        }
     }
+    flush();
 }
 
 // ------------------------------------------------------------------------------------------
