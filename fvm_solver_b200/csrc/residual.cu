@@ -184,17 +184,25 @@ __device__ __forceinline__ bool case_on(const fvm_mesh_t& m, const int32_t* case
 // The two side codes (first two words) of a facet record.
 __device__ __forceinline__ int2 ld_codes(const float* rec) { return __ldg(reinterpret_cast<const int2*>(rec)); }
 
-// One-ahead index loads of the persistent loops.  Nothing is read for an item past the end or of a
-// frozen case (case mask), so a masked-out case costs one case-id read per item.
+// Whether a persistent loop over n items with `stride` threads checks the case of each next item
+// before loading its record: only with a case mask and more than four items per thread.
+__device__ __forceinline__ bool frozen_skip(const fvm_mesh_t& m, int n, int stride) {
+    return m.case_active != nullptr && (int64_t)n > 4 * (int64_t)stride;
+}
+
+// One-ahead index loads of the persistent loops.  With `skip_frozen`, nothing is read for an item
+// of a frozen case (case mask), so a masked-out case costs one case-id read per item; the check
+// puts two dependent loads before the record load, so launches whose threads have only a few
+// items (latency-bound) leave it off (see frozen_skip).
 template <int DIM>
-__device__ __forceinline__ int2 next_codes(const fvm_mesh_t& m, int f, int nF) {
-    const bool on = f < nF && case_on(m, m.face_case, f);
+__device__ __forceinline__ int2 next_codes(const fvm_mesh_t& m, int f, int nF, bool skip_frozen) {
+    const bool on = f < nF && (!skip_frozen || case_on(m, m.face_case, f));
     return on ? ld_codes(m.face_rec + (int64_t)f * L<DIM>::FR) : make_int2(0, 0);
 }
 template <int DIM>
-__device__ __forceinline__ void next_cols(const fvm_mesh_t& m, int i, int NA, int* cols) {
+__device__ __forceinline__ void next_cols(const fvm_mesh_t& m, int i, int NA, int* cols, bool skip_frozen) {
     using Ly = L<DIM>;
-    const bool on = i < NA && case_on(m, m.cell_case, i);
+    const bool on = i < NA && (!skip_frozen || case_on(m, m.cell_case, i));
 #pragma unroll
     for (int k = 0; k < Ly::KG; ++k)
         cols[k] = on ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)i * Ly::CR + Ly::GC + k) : 0;
@@ -390,12 +398,13 @@ __device__ __forceinline__ void cell_body(const fvm_mesh_t& m, const Phys& p, co
     const int stride = gridDim.x * blockDim.x;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) *has_grads = 1;
+    const bool skip_frozen = frozen_skip(m, NA, stride);
     int cols[KG];
-    next_cols<DIM>(m, i, NA, cols);
+    next_cols<DIM>(m, i, NA, cols, skip_frozen);
     for (int64_t tile = blockIdx.x; i < NA; i += stride, tile += gridDim.x) {
         if (waves > 0) prefetch_tile(m.cell_rec, NA, Ly::CR, tile + (int64_t)waves * gridDim.x);
         if (m.case_active && !case_on(m, m.cell_case, i)) {
-            next_cols<DIM>(m, i + stride, NA, cols);
+            next_cols<DIM>(m, i + stride, NA, cols, skip_frozen);
             continue;
         }
         float X[KG][RS];
@@ -408,7 +417,7 @@ __device__ __forceinline__ void cell_body(const fvm_mesh_t& m, const Phys& p, co
         ld_mut<COH, RS>(prims + (int64_t)i * RS, U);
         float rec[Ly::CR];
         ld_vec<Ly::CR>(m.cell_rec + (int64_t)i * Ly::CR, rec);
-        next_cols<DIM>(m, i + stride, NA, cols);
+        next_cols<DIM>(m, i + stride, NA, cols, skip_frozen);
         const int nvalid = (as_int(rec[Ly::META]) >> 24) & 31;
         float g[DIM][C];
 #pragma unroll
@@ -483,12 +492,13 @@ __device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, co
     const int nF = m.n_facets;
     const int stride = gridDim.x * blockDim.x;
     int f = blockIdx.x * blockDim.x + threadIdx.x;
-    int2 nxt = next_codes<DIM>(m, f, nF);
+    const bool skip_frozen = frozen_skip(m, nF, stride);
+    int2 nxt = next_codes<DIM>(m, f, nF, skip_frozen);
     for (int64_t tile = blockIdx.x; f < nF; f += stride, tile += gridDim.x) {
     if (waves > 0) prefetch_tile(m.face_rec, nF, Ly::FR, tile + (int64_t)waves * gridDim.x);
     const int ca = nxt.x, cb = nxt.y;
     if (m.case_active && !case_on(m, m.face_case, f)) {
-        nxt = next_codes<DIM>(m, f + stride, nF);
+        nxt = next_codes<DIM>(m, f + stride, nF, skip_frozen);
         continue;
     }
     // Both sides: primitives and limited gradient of the cell(s); a boundary side (code < 0) takes
@@ -502,7 +512,7 @@ __device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, co
     ld_vec_cg<GS>(grads + (int64_t)cell1 * GS, G1);
     float rec[Ly::FR];
     ld_vec<Ly::FR>(m.face_rec + (int64_t)f * Ly::FR, rec);
-    nxt = next_codes<DIM>(m, f + stride, nF);
+    nxt = next_codes<DIM>(m, f + stride, nF, skip_frozen);
     const float size = rec[Ly::SIZE];
     float n[DIM], nh[DIM];
 #pragma unroll
@@ -778,7 +788,8 @@ __device__ __forceinline__ void div_body(const fvm_mesh_t& m, const Phys& p, con
     for (int c = 0; c < (ADAPT ? 3 * C : 1); ++c) ad_acc[c] = 0.0;
     int i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
     float nxt[Ly::DR];
-    if (i0 + lane < NA && case_on(m, m.cell_case, i0 + lane))
+    const bool skip_frozen = frozen_skip(m, NA, stride);
+    if (i0 + lane < NA && (!skip_frozen || case_on(m, m.cell_case, i0 + lane)))
         ld_vec<Ly::DR>(m.div_rec + (int64_t)(i0 + lane) * Ly::DR, nxt);
     else
 #pragma unroll
@@ -808,7 +819,7 @@ __device__ __forceinline__ void div_body(const fvm_mesh_t& m, const Phys& p, con
                 }
             }
         }
-        if (i + stride < NA && case_on(m, m.cell_case, i + stride))
+        if (i + stride < NA && (!skip_frozen || case_on(m, m.cell_case, i + stride)))
             ld_vec<Ly::DR>(m.div_rec + (int64_t)(i + stride) * Ly::DR, nxt);
         if (MODE == DIV_RESIDUAL) {
             if (live) store_state<C>(dudt + (int64_t)i * C, r);
