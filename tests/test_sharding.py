@@ -2,7 +2,6 @@
 import os
 import socket
 
-import pytest
 import torch
 import torch.multiprocessing as tmp
 

@@ -97,7 +97,6 @@ def test_sphere_box_mesh():
 def test_device_mesh_struct_on_host():
     """The fvm_mesh_t struct fills every pointer field from the tables (built on the CPU here)."""
     from conftest import golden_setup
-    from fvm_solver_b200 import _lib
     from fvm_solver_b200.equation import DeviceMesh
     g, spec, tables, cfg = golden_setup("c2d")
     dm = DeviceMesh(tables.kernel, "cpu")
