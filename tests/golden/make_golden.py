@@ -5,7 +5,9 @@ reference checkout)::
 
     python tests/golden/make_golden.py            # writes tests/golden/fvm_golden_<case>.npz
 
-For each case (2D channel-cylinder mesh, 3D box mesh) the script
+For each case (2D channel-cylinder mesh, 3D box mesh; ``--case c2d11k`` adds the 2D mesh at
+the channel-cylinder benchmark's size, stored light: the state, the first residual and the state
+after ten SSP-RK3 steps, FP32 and FP64) the script
 
 * builds the mesh with this package's generator and the reference's ``FVMMesh2D/3D``;
 * stores the reference's packed ELL operators (``csr_to_ell`` of G_mats, flux_mat,
@@ -43,9 +45,15 @@ def case_spec(case):
     from fvm_solver_b200 import meshgen as mg
     if case == "c2d":
         return mg.channel_cylinder(h=0.05, seed=3), 2
+    if case == "c2d11k":                    # the channel-cylinder benchmark's size (h = 0.02)
+        return mg.channel_cylinder(h=0.02, seed=3), 2
     if case == "b3d":
         return mg.box3d(6, seed=4), 3
     raise ValueError(case)
+
+
+# Cases stored without the ELL operators and with fewer results, to keep the fixture small.
+LIGHT = {"c2d11k": (("state0", "res1", "ssprk3_step10"), ("res1", "ssprk3_step10"))}
 
 
 def initial_prims(spec, dim, seed=11):
@@ -110,7 +118,7 @@ def run_reference(case, prim0, dt, fp64):
     out["state0"] = U0
     eq, _ = build_equation(R, spec, dim, cfg, U0, dtype)
 
-    if not fp64:
+    if not fp64 and case not in LIGHT:
         ek = R["ell_kernel"]
         M, BS = eq.E_props.mesh, eq.E_props.boundary_setter
         for name, spm in [("G", M.G_mats), ("flux", eq.flux_mat), ("Afg", M.A_face_grad),
@@ -150,7 +158,8 @@ def run_reference(case, prim0, dt, fp64):
         out["ssprk3_step10"] = eq.cells.state.clone()
 
     # ButcherAdapt RK3_SSP4 and the RK3_SSP4 class
-    for sname, sextra, key in [("Butcher_adapt", "RK3_SSP4", "adapt"), ("RK3_SSP4", "", "rk3ssp4")]:
+    for sname, sextra, key in ([] if case in LIGHT else
+                               [("Butcher_adapt", "RK3_SSP4", "adapt"), ("RK3_SSP4", "", "rk3ssp4")]):
         cfg2 = ref_config(R, dim, sname, sextra, dt)
         eq2, _ = build_equation(R, spec, dim, cfg2, U0, dtype)
         with torch.inference_mode():
@@ -199,6 +208,10 @@ def main():
                    cells=spec.cells.numpy(), facets=spec.facets.numpy(),
                    bc_facet_mask=spec.bc_facet_mask.numpy(), bc_tags=np.array(spec.bc_tags),
                    dim=np.int64(dim))
+        if case in LIGHT:
+            keep32, keep64 = LIGHT[case]
+            res32 = {k: res32[k] for k in keep32}
+            res64 = {k: res64[k] for k in keep64}
         out.update(res32)
         out.update({k + "_f64": v for k, v in res64.items()})
         path = os.path.join(HERE, f"fvm_golden_{case}.npz")
