@@ -124,6 +124,21 @@ def test_ten_steps(case):
     assert rel_l2(to_np(eq.cells.state), g["ssprk3_step10"]) < 1e-5
 
 
+def test_channel_benchmark_size_vs_reference():
+    """The 11 307-triangle channel mesh (the channel-cylinder benchmark's size): first residual and
+    ten SSP-RK3 steps against the reference, FP32 bar 1e-5; FP64 within 10x the reference's own
+    FP32 error."""
+    g, eq, T, cfg = make_equation("c2d11k", "Butcher", "SSP_RK3")
+    r1 = to_np(eq.forward(torch.from_numpy(g["prim0"])))
+    assert rel_l2(r1, g["res1"]) < 1e-5
+    assert rel_l2(r1, g["res1_f64"]) < max(10 * rel_l2(g["res1"], g["res1_f64"]), 1e-6)
+    eq.reset_gradients()
+    eq.t_solver.step(10)
+    st = to_np(eq.cells.state)
+    assert rel_l2(st, g["ssprk3_step10"]) < 1e-5
+    assert rel_l2(st, g["ssprk3_step10_f64"]) < 1e-5
+
+
 @pytest.mark.parametrize("case", CASES)
 @pytest.mark.parametrize("name,extra,key", [("Butcher_adapt", "RK3_SSP4", "adapt"), ("RK3_SSP4", "", "rk3ssp4")])
 def test_adaptive_step(case, name, extra, key):
