@@ -27,7 +27,8 @@ reference's FP32 path) or float64.
 Parity pinning: the oracle is checked against golden vectors produced by running the reference
 itself (``tests/golden/make_golden.py``) -- residuals, limited gradients and integrator steps on a
 2D channel-cylinder mesh and a 3D box mesh, in FP32 and FP64, and the first residual and ten
-SSP-RK3 steps on the 11 307-triangle channel mesh of the channel-cylinder benchmark.
+SSP-RK3 steps on two larger meshes (the 11 307-triangle channel mesh of the channel-cylinder
+benchmark, a 9 066-tet box).
 """
 from __future__ import annotations
 

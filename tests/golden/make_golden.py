@@ -5,9 +5,9 @@ reference checkout)::
 
     python tests/golden/make_golden.py            # writes tests/golden/fvm_golden_<case>.npz
 
-For each case (2D channel-cylinder mesh, 3D box mesh; ``--case c2d11k`` adds the 2D mesh at
-the channel-cylinder benchmark's size, stored light: the state, the first residual and the state
-after ten SSP-RK3 steps, FP32 and FP64) the script
+For each case (2D channel-cylinder mesh, 3D box mesh; ``--case c2d11k`` / ``--case b3d9k`` add
+the 2D mesh at the channel-cylinder benchmark's size and a 9 066-tet box, stored light: the
+state, the first residual and the state after ten SSP-RK3 steps, FP32 and FP64) the script
 
 * builds the mesh with this package's generator and the reference's ``FVMMesh2D/3D``;
 * stores the reference's packed ELL operators (``csr_to_ell`` of G_mats, flux_mat,
@@ -49,11 +49,14 @@ def case_spec(case):
         return mg.channel_cylinder(h=0.02, seed=3), 2
     if case == "b3d":
         return mg.box3d(6, seed=4), 3
+    if case == "b3d9k":
+        return mg.box3d(11, seed=4), 3
     raise ValueError(case)
 
 
 # Cases stored without the ELL operators and with fewer results, to keep the fixture small.
-LIGHT = {"c2d11k": (("state0", "res1", "ssprk3_step10"), ("res1", "ssprk3_step10"))}
+LIGHT = {"c2d11k": (("state0", "res1", "ssprk3_step10"), ("res1", "ssprk3_step10")),
+         "b3d9k": (("state0", "res1", "ssprk3_step10"), ("res1", "ssprk3_step10"))}
 
 
 def initial_prims(spec, dim, seed=11):

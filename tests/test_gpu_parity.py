@@ -124,11 +124,12 @@ def test_ten_steps(case):
     assert rel_l2(to_np(eq.cells.state), g["ssprk3_step10"]) < 1e-5
 
 
-def test_channel_benchmark_size_vs_reference():
-    """The 11 307-triangle channel mesh (the channel-cylinder benchmark's size): first residual and
-    ten SSP-RK3 steps against the reference, FP32 bar 1e-5; FP64 within 10x the reference's own
-    FP32 error."""
-    g, eq, T, cfg = make_equation("c2d11k", "Butcher", "SSP_RK3")
+@pytest.mark.parametrize("case", ["c2d11k", "b3d9k"])
+def test_larger_mesh_vs_reference(case):
+    """The larger light fixtures (the 11 307-triangle channel mesh of the channel-cylinder
+    benchmark, a 9 066-tet box): first residual and ten SSP-RK3 steps against the reference, FP32
+    bar 1e-5; FP64 within 10x the reference's own FP32 error."""
+    g, eq, T, cfg = make_equation(case, "Butcher", "SSP_RK3")
     r1 = to_np(eq.forward(torch.from_numpy(g["prim0"])))
     assert rel_l2(r1, g["res1"]) < 1e-5
     assert rel_l2(r1, g["res1_f64"]) < max(10 * rel_l2(g["res1"], g["res1_f64"]), 1e-6)

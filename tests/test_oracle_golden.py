@@ -63,24 +63,24 @@ def test_adaptive_steps(golden):
     assert abs(float(s.dt) / float(g["rk3ssp4_dt1"]) - 1) < 1e-5
 
 
-@pytest.fixture(scope="module")
-def golden_11k():
+@pytest.fixture(scope="module", params=["c2d11k", "b3d9k"])
+def golden_light(request):
     from conftest import golden_setup
-    return golden_setup("c2d11k")
+    return golden_setup(request.param)
 
 
-def test_channel_benchmark_size_residual(golden_11k):
-    """The oracle against the reference on the 11 307-triangle channel mesh (the channel-cylinder
-    benchmark's size): first residual in FP32 and FP64."""
-    g, spec, T, cfg = golden_11k
+def test_larger_mesh_residual(golden_light):
+    """The oracle against the reference on the larger light fixtures (the 11 307-triangle channel
+    mesh of the channel-cylinder benchmark, a 9 066-tet box): first residual in FP32 and FP64."""
+    g, spec, T, cfg = golden_light
     r1, _ = O.OracleResidual(T, cfg, np.float32).forward(g["prim0"])
     assert rel_l2(r1, g["res1"]) < 5e-6
     r64, _ = O.OracleResidual(T, cfg, np.float64).forward(g["prim0"].astype(np.float64))
     assert rel_l2(r64, g["res1_f64"]) < 1e-4
 
 
-def test_channel_benchmark_size_ten_steps(golden_11k):
-    g, spec, T, cfg = golden_11k
+def test_larger_mesh_ten_steps(golden_light):
+    g, spec, T, cfg = golden_light
     s = O.OracleSolver(O.OracleResidual(T, cfg, np.float32), g["state0"], float(g["dt"]))
     for _ in range(10):
         s.butcher_step("SSP_RK3")
