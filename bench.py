@@ -381,6 +381,9 @@ def partitioned_bench(args):
 def secondary(args):
     """Secondary workloads (single GPU): the 2D channel-cylinder case and the batched ensemble."""
     from fvm_solver_b200 import _lib, workloads as W
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and args.workload != "partitioned":
+        sys.exit(f"--workload {args.workload} runs on one GPU; several ranks run the default workload "
+                 f"(one box per rank) or --workload partitioned (one box split across the ranks)")
     torch.cuda.set_device(0)
     stream = torch.cuda.current_stream()
 

@@ -34,3 +34,10 @@ def test_reference_arm_other_ranks_do_nothing():
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
     assert r.stdout.strip() == ""
+
+
+def test_single_gpu_workloads_refuse_several_ranks():
+    env = dict(os.environ, RANK="0", WORLD_SIZE="2")
+    r = subprocess.run([sys.executable, "bench.py", "--workload", "ensemble"], cwd=ROOT, env=env,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode != 0 and "runs on one GPU" in r.stderr
