@@ -297,6 +297,40 @@ TABLEAUS = {
     "SSP_RK3": (np.array([[0, 0, 0], [1.0, 0, 0], [0.25, 0.25, 0]]),
                 np.array([1 / 6, 1 / 6, 2 / 3]), np.array([0.5, 0.5, 0.0])),
 }
+# The remaining tableaus of integrators.py, as lower-triangular rows (the coefficients are the
+# reference's constants and must be the same numbers).
+_SSP5_A = [[0.37726891511710], [0.37726891511710, 0.37726891511710],
+           [0.16352294089771] * 3, [0.14904059394856, 0.14831273384724, 0.14831273384724, 0.34217696850008]]
+_SSP6_A = [[0.28422], [0.28422] * 2, [0.23071] * 3, [0.13416] * 3 + [0.16528],
+           [0.13416] * 3 + [0.16528, 0.28422]]
+_RK4SSP5_A = [[0.39175222700392], [0.21766909633821, 0.36841059262959],
+              [0.08269208670950, 0.13995850206999, 0.25189177424738],
+              [0.06796628370320, 0.11503469844438, 0.20703489864929, 0.54497475021237]]
+_RK4SSP10_A = [[1 / 6] * k for k in range(1, 5)] + [[1 / 15] * 5 + [1 / 6] * k for k in range(0, 5)]
+
+
+def _lower(rows):
+    s = len(rows) + 1
+    A = np.zeros((s, s))
+    for i, r in enumerate(rows):
+        A[i + 1, :len(r)] = r
+    return A
+
+
+TABLEAUS.update({
+    # integrators.py:240-251
+    "RK3_SSP5": (_lower(_SSP5_A), np.array([0.19707596384481, 0.11780316509765, 0.11709725193772,
+                                            0.27015874934251, 0.29786487010104]), np.full(5, 0.2)),
+    # integrators.py:253-265
+    "RK3_SSP6": (_lower(_SSP6_A), np.array([0.17016, 0.17016, 0.10198, 0.12563, 0.21604, 0.21604]),
+                 np.full(6, 1 / 6)),
+    # integrators.py:267-278
+    "RK4_SSP5": (_lower(_RK4SSP5_A), np.array([0.14681187618661, 0.24848290924556, 0.10425883036650,
+                                               0.27443890091960, 0.22600748319395]), np.full(5, 0.2)),
+    # integrators.py:280-296
+    "RK4_SSP10": (_lower(_RK4SSP10_A), np.full(10, 0.1),
+                  np.array([0.2, 0, 0, 0.3, 0, 0, 0.2, 0, 0.3, 0])),
+})
 
 
 class OracleSolver:

@@ -1,9 +1,11 @@
 """Generate the golden fixtures by running the reference implementation (CPU path).
 
-Run in a container that has the reference sources (``FVM_REFERENCE_PATH``, default the mounted
-reference checkout)::
+Run where the reference sources are, with ``FVM_REFERENCE_PATH`` naming the checkout (the
+directory that holds ``time_fvm/``)::
 
-    python tests/golden/make_golden.py            # writes tests/golden/fvm_golden_<case>.npz
+    FVM_REFERENCE_PATH=<checkout> python tests/golden/make_golden.py [--case NAME ...]
+    # writes tests/golden/fvm_golden_<case>.npz; NAME in c2d, b3d (default), c2d11k, b3d9k,
+    # c2dvar, ptile
 
 For each case (2D channel-cylinder mesh, 3D box mesh; ``--case c2d11k`` / ``--case b3d9k`` add
 the 2D mesh at the channel-cylinder benchmark's size and a 9 066-tet box, stored light: the
@@ -19,10 +21,34 @@ state, the first residual and the state after ten SSP-RK3 steps, FP32 and FP64) 
   the hand-unrolled ``RK3_SSP4`` class, and ten SSP-RK3 steps;
 * repeats the residual and step evaluations in FP64 in a subprocess under a dtype shim
   (keys suffixed ``_f64``).
+
+Two further fixtures pin what the four cases above leave to the oracle:
+
+* ``--case c2dvar`` (the c2d mesh and state): the first residual with the limiters p = 1, 2, 3, 5
+  (``limiter.py:29-77``; the cases above use the default p = 4), one ``Butcher`` step with each of
+  the tableaus RK3_SSP5, RK3_SSP6, RK4_SSP5 and RK4_SSP10 (``integrators.py:240-296``), and
+  Adams-Bashforth 3 driven by the reference's own residual: two SSP-RK3 start-up steps through
+  ``Butcher._step`` (the three-stage tableau injected) whose first-stage residuals f(U_n) are
+  recorded as they are computed, then three steps U += dt (23 f_n - 16 f_{n-1} + 5 f_{n-2}) / 12
+  with f from ``TSolver._forward_state`` (``t_solvers.py:212-215``).  The reference's own
+  ``Adams3PC`` cannot run (``integrators.py:111``), so the multistep combination is restated here;
+  every residual in it is the reference's.
+* ``--case ptile`` (a periodic Taylor-Green box, the geometry of the 3D benchmark): the reference
+  has no periodic meshes, so a 6^3-point ``meshgen.periodic_box`` is unrolled into 3 x 3 x 3 tiles
+  (explicit vertex copies at lattice shifts, a plain non-periodic tetrahedral mesh of ~40k cells,
+  outer faces characteristic inlets) and run through the reference's ``FVMMesh3D`` +
+  ``FVMEquation.forward`` with the periodic state repeated in every tile.  The central tile's cells
+  come first and keep the periodic numbering; their residual needs cells two neighbours away and one
+  RK4 step eight, all inside the tile ring, so the central tile's residual, limited gradients and
+  RK4 step are the periodic mesh's answer computed by the reference on its own geometry.  Stored:
+  the periodic mesh (vertices, cells, facets, lattice shifts), its state and those central-tile
+  results (the outer tiles differ by ~0.2 rel-L2 in their residual, so the ring is what shields
+  the centre).
 """
 from __future__ import annotations
 
 import argparse
+import itertools
 import os
 import subprocess
 import sys
@@ -173,6 +199,205 @@ def run_reference(case, prim0, dt, fp64):
     return {k: v.detach().cpu().numpy() for k, v in out.items()}
 
 
+VARIANT_LIMITERS = (1, 2, 3, 5)
+VARIANT_TABLEAUS = ("RK3_SSP5", "RK3_SSP6", "RK4_SSP5", "RK4_SSP10")
+AB3_COEF = (23 / 12, -16 / 12, 5 / 12)
+
+
+def run_variants(prim0, dt, fp64):
+    """The ``c2dvar`` results on the c2d mesh: other limiters, other tableaus, AB3."""
+    R = import_reference(fp64=fp64)
+    dtype = torch.float64 if fp64 else torch.float32
+    spec, dim = case_spec("c2d")
+    prim0 = prim0.to(dtype)
+    out = {}
+    for p in VARIANT_LIMITERS:
+        cfg = ref_config(R, dim, dt=dt)
+        cfg.lim_p = p
+        FE = R["fvm_equation"]
+        phy = FE.FluidConstitution2D(cfg, 2)
+        m, r, Q = phy.primatives_to_state(prim0[:, :dim], prim0[:, dim:dim + 1], prim0[:, dim + 1:])
+        eq, _ = build_equation(R, spec, dim, cfg, torch.cat([m, r, Q], -1), dtype)
+        with torch.inference_mode():
+            eq.E_props.cell_grads = None
+            out[f"lim{p}_res1"] = eq.forward(prim0.clone())
+            out[f"lim{p}_grads1"] = eq.E_props.cell_grads.clone()
+    for name in VARIANT_TABLEAUS:
+        cfg = ref_config(R, dim, "Butcher", name, dt)
+        FE = R["fvm_equation"]
+        phy = FE.FluidConstitution2D(cfg, 2)
+        m, r, Q = phy.primatives_to_state(prim0[:, :dim], prim0[:, dim:dim + 1], prim0[:, dim + 1:])
+        U0 = torch.cat([m, r, Q], -1)
+        eq, _ = build_equation(R, spec, dim, cfg, U0, dtype)
+        with torch.inference_mode():
+            eq.E_props.cell_grads = None
+            eq.t_solver.dt = torch.tensor(dt, dtype=dtype)
+            eq.t_solver._solve_step(torch.tensor(0.0))
+        out[f"{name.lower()}_step1"] = eq.cells.state.clone()
+    # Adams-Bashforth 3 on the reference's residual
+    cfg = ref_config(R, dim, "Butcher", "RK4", dt)
+    FE = R["fvm_equation"]
+    phy = FE.FluidConstitution2D(cfg, 2)
+    m, r, Q = phy.primatives_to_state(prim0[:, :dim], prim0[:, dim:dim + 1], prim0[:, dim + 1:])
+    U0 = torch.cat([m, r, Q], -1)
+    eq, _ = build_equation(R, spec, dim, cfg, U0, dtype)
+    ts = eq.t_solver
+    ts.A, ts.b = SSP_RK3[0].to(dtype), SSP_RK3[1].to(dtype).reshape(-1, 1, 1)
+    ts.stages = 3
+    ts.dt = torch.tensor(dt, dtype=dtype)
+    forward_state = ts._forward_state
+    seen = []
+
+    def recording(U):
+        f = forward_state(U)
+        seen.append(f)
+        return f
+
+    hist = []                                 # dt * f(U_n), newest last
+    with torch.inference_mode():
+        eq.E_props.cell_grads = None
+        ts._forward_state = recording
+        for _ in range(2):                    # SSP-RK3 start-up; its first stage is f(U_n)
+            seen.clear()
+            ts._solve_step(torch.tensor(0.0))
+            hist.append(ts.dt * seen[0])
+        ts._forward_state = forward_state
+        for _ in range(3):
+            U = eq.cells.state
+            hist.append(ts.dt * forward_state(U))
+            inc = AB3_COEF[0] * hist[-1] + AB3_COEF[1] * hist[-2] + AB3_COEF[2] * hist[-3]
+            eq.cells.update_cells(U + inc)
+    out["ab3_step5"] = eq.cells.state.clone()
+    return {k: v.detach().cpu().numpy() for k, v in out.items()}
+
+
+PTILE_N, PTILE_SEED, PTILE_NOISE_SEED = 6, 7, 11
+
+
+def tile_periodic(spec, reps: int = 3):
+    """Unroll a periodic ``MeshSpec`` into reps^3 copies of the box (reps odd): vertex copies at the
+    lattice shifts each tile needs, cells of the central tile first (periodic numbering), then the
+    other tiles; facets interior first, then boundary.  Returns (vertices f32, cells, facets,
+    bc mask, number of tiles)."""
+    P = spec.vertices.numpy().astype(np.float64)
+    L = float(spec.period[0])
+    cells = spec.cells.numpy().astype(np.int64)
+    csh = spec.cell_shifts.numpy().astype(np.int64)
+    h = reps // 2
+    tiles = [np.zeros(3, np.int64)] + [np.array(t) for t in itertools.product(range(-h, h + 1), repeat=3) if any(t)]
+    base = 2 * h + 3                         # shifts of a tile vertex lie in [-(h + 1), h + 1]
+    keys = np.concatenate([cells * base ** 3 + ((csh + t) + h + 1) @ np.array([base * base, base, 1])
+                           for t in tiles])
+    uniq, inv = np.unique(keys.reshape(-1), return_inverse=True)
+    tcells = inv.reshape(-1, 4)
+    vid, rem = uniq // base ** 3, uniq % base ** 3
+    shift = np.stack([rem // (base * base), (rem // base) % base, rem % base], 1) - (h + 1)
+    verts = (P[vid] + shift * L).astype(np.float32)
+    pats = [(0, 1, 2), (0, 2, 3), (0, 3, 1), (1, 3, 2)]
+    loc = np.sort(np.stack([tcells[:, list(p)] for p in pats], 1).reshape(-1, 3), axis=1)
+    uq, cnt = np.unique(loc, axis=0, return_counts=True)
+    assert cnt.max() <= 2, "non-manifold facet"
+    facets = np.concatenate([uq[cnt == 2], uq[cnt == 1]])
+    mask = np.concatenate([np.zeros(int((cnt == 2).sum()), bool), np.ones(int((cnt == 1).sum()), bool)])
+    return verts, tcells.astype(np.int32), facets.astype(np.int64), mask, len(tiles)
+
+
+def ptile_inputs():
+    """The periodic box, its perturbed Taylor-Green state and the CFL 0.5 time step."""
+    from fvm_solver_b200 import fvm_mesh as fm, meshgen as mg, tables as tb, workloads as W
+    from oracle.fvm_oracle import cfl_dt, prim_to_state, state_to_prim
+    case = W.taylor_green(n=PTILE_N, seed=PTILE_SEED, device="cpu")
+    spec, cfg = case.spec, case.cfg
+    N = spec.n_cells
+    rng = np.random.default_rng(PTILE_NOISE_SEED)     # perturbations that switch the limiter on
+    prim = state_to_prim(case.state0.numpy().astype(np.float64), 3, cfg.C_v)
+    prim[:, :3] += 0.1 * cfg.v0 * rng.standard_normal((N, 3))
+    prim[:, 3] *= 1 + 0.02 * rng.standard_normal(N)
+    prim[:, 4] *= 1 + 0.01 * rng.standard_normal(N)
+    prim = prim.astype(np.float32)
+    T = tb.FVMTables(fm.mesh_from_spec(spec), cfg, 5, {})
+    U0 = prim_to_state(prim.astype(np.float64), 3, cfg.C_v).astype(np.float32)
+    dt = float(cfl_dt(U0.astype(np.float64), 3, cfg.C_v, cfg.gamma, T.kernel.inv_h.numpy(), 0.5))
+    return spec, cfg, prim, dt
+
+
+def run_ptile(tiled, prim0, dt, fp64):
+    """Residual, limited gradients and one RK4 step of the unrolled periodic box (reference)."""
+    from fvm_solver_b200 import config as cf
+    R = import_reference(fp64=fp64)
+    dtype = torch.float64 if fp64 else torch.float32
+    verts, tcells, facets, mask, n_tiles = tiled
+    tg = cf.TaylorGreenConfig(device="cpu")
+    cfg = ref_config(R, 3, "Butcher", "RK4", dt)
+    for k in ("T_0", "viscosity", "visc_bulk", "thermal_cond", "S_const", "gamma", "C_v", "v_factor",
+              "lim_p", "lim_K"):
+        setattr(cfg, k, getattr(tg, k))
+    cfg.inlet_cfg.v_inf = (0.0, 0.0, 0.0)
+    cfg.exit_cfg.v_inf = (0.0, 0.0, 0.0)
+    st = R["mesh_store"]
+    E = st.FacetBCTypes
+    mesh = R["fvm_mesh"].FVMMesh3D(torch.from_numpy(verts).to(dtype), torch.from_numpy(tcells),
+                                   torch.from_numpy(facets), torch.from_numpy(mask), device="cpu")
+    bc = {i: st.Facet([E.Inlet] * 5, tag="Farfield") for i in range(int(mask.sum()))}
+    FE = R["fvm_equation"]
+    phy = FE.FluidConstitution3D(cfg, 3)
+    prim = torch.from_numpy(np.tile(prim0, (n_tiles, 1))).to(dtype)
+    m, r, Q = phy.primatives_to_state(prim[:, :3], prim[:, 3:4], prim[:, 4:])
+    U0 = torch.cat([m, r, Q], -1)
+    eq = FE.FVMEquation(cfg, phy, mesh, 5, bc, us_init=U0)
+    N = prim0.shape[0]
+    out = {}
+    with torch.inference_mode():
+        eq.E_props.cell_grads = None
+        out["res1"] = eq.forward(prim.clone())[:N]
+        out["grads1"] = eq.E_props.cell_grads[:N].clone()
+        eq.E_props.cell_grads = None
+        eq.cells.state = U0.clone()
+        eq.t_solver.dt = torch.tensor(dt, dtype=dtype)
+        eq.t_solver._solve_step(torch.tensor(0.0))
+        out["rk4_step1"] = eq.cells.state[:N].clone()
+    return {k: v.detach().cpu().numpy() for k, v in out.items()}
+
+
+def make_variants():
+    g = dict(np.load(os.path.join(HERE, "fvm_golden_c2d.npz")))
+    prim0, dt = torch.from_numpy(g["prim0"]), float(g["dt"])
+    res32 = run_variants(prim0, dt, fp64=False)
+    res64 = _fp64_subprocess("c2dvar", dict(prim0=g["prim0"], dt=dt))
+    out = {k: g[k] for k in ("prim0", "dt", "state0", "vertices", "cells", "facets", "bc_facet_mask", "bc_tags",
+                             "dim")}
+    out.update(res32)
+    out.update({k + "_f64": v for k, v in res64.items()})
+    return out
+
+
+def make_ptile():
+    spec, cfg, prim, dt = ptile_inputs()
+    tiled = tile_periodic(spec, 3)
+    res32 = run_ptile(tiled, prim, dt, fp64=False)
+    verts, tcells, facets, mask, n_tiles = tiled
+    res64 = _fp64_subprocess("ptile", dict(prim0=prim, dt=dt, verts=verts, tcells=tcells, facets=facets,
+                                           mask=mask, n_tiles=n_tiles))
+    from oracle.fvm_oracle import prim_to_state
+    out = dict(prim0=prim, dt=np.float64(dt), state0=prim_to_state(prim.astype(np.float64), 3, cfg.C_v).astype(np.float32),
+               vertices=spec.vertices.numpy(), cells=spec.cells.numpy(), facets=spec.facets.numpy(),
+               period=np.asarray(spec.period), cell_shifts=spec.cell_shifts.numpy(),
+               facet_shifts=spec.facet_shifts.numpy(), dim=np.int64(3), n=np.int64(PTILE_N),
+               seed=np.int64(PTILE_SEED), tiled_cells=np.int64(len(tcells)))
+    out.update(res32)
+    out.update({k + "_f64": v for k, v in res64.items()})
+    return out
+
+
+def _fp64_subprocess(case, inputs: dict) -> dict:
+    """Run one case's FP64 reference in a fresh process (the dtype shim must precede the import)."""
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.npz"), os.path.join(td, "out.npz")
+        np.savez(fin, **inputs)
+        subprocess.run([sys.executable, os.path.abspath(__file__), "--fp64-worker", case, fin, fout], check=True)
+        return dict(np.load(fout))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", action="append")
@@ -181,7 +406,13 @@ def main():
     if args.fp64_worker:
         case, fin, fout = args.fp64_worker
         d = np.load(fin)
-        res = run_reference(case, torch.from_numpy(d["prim0"]), float(d["dt"]), fp64=True)
+        if case == "c2dvar":
+            res = run_variants(torch.from_numpy(d["prim0"]), float(d["dt"]), fp64=True)
+        elif case == "ptile":
+            tiled = (d["verts"], d["tcells"], d["facets"], d["mask"], int(d["n_tiles"]))
+            res = run_ptile(tiled, d["prim0"], float(d["dt"]), fp64=True)
+        else:
+            res = run_reference(case, torch.from_numpy(d["prim0"]), float(d["dt"]), fp64=True)
         np.savez(fout, **res)
         return
 
@@ -190,6 +421,12 @@ def main():
     from oracle.fvm_oracle import cfl_dt
     from fvm_solver_b200 import fvm_mesh as fm, tables as tb, config as cf, mesh_store as ms
     for case in args.case or ["c2d", "b3d"]:
+        if case in ("c2dvar", "ptile"):
+            out = make_variants() if case == "c2dvar" else make_ptile()
+            path = os.path.join(HERE, f"fvm_golden_{case}.npz")
+            np.savez_compressed(path, **out)
+            print(f"wrote {path} ({os.path.getsize(path) / 1e3:.0f} kB)")
+            continue
         spec, dim = case_spec(case)
         prim0 = initial_prims(spec, dim)
         cfg = cf.ConfigEllipse()

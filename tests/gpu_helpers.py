@@ -9,9 +9,12 @@ import torch
 from conftest import golden_setup
 
 
-def make_equation(case, solver_name="Butcher", solver_extra="RK4", dt=None, cfl=None, state0=None):
+def make_equation(case, solver_name="Butcher", solver_extra="RK4", dt=None, cfl=None, state0=None,
+                  **cfg_overrides):
+    """(fixture, FVMEquation on cuda, FVMTables, cfg) of a golden case; ``cfg_overrides`` set
+    config fields (e.g. ``lim_p``) for both the tables and the equation."""
     from fvm_solver_b200 import equation as E, mesh_store as ms
-    g, spec, tables, cfg = golden_setup(case)
+    g, spec, tables, cfg = golden_setup(case, **cfg_overrides)
     cfg = copy.deepcopy(cfg)
     cfg.device = "cuda"
     cfg.solver_name, cfg.solver_extra = solver_name, solver_extra
@@ -19,7 +22,8 @@ def make_equation(case, solver_name="Butcher", solver_extra="RK4", dt=None, cfl=
     cfg.cfl = cfl
     dim = int(g["dim"])
     phy = E.FluidConstitution2D(cfg) if dim == 2 else E.FluidConstitution3D(cfg)
-    eq = E.FVMEquation(cfg, phy, spec, dim + 2, ms.default_bc_tags(spec.bc_tags, dim),
+    bc = {} if case == "ptile" else ms.default_bc_tags(spec.bc_tags, dim)
+    eq = E.FVMEquation(cfg, phy, spec, dim + 2, bc,
                        us_init=torch.from_numpy(g["state0"]) if state0 is None else state0)
     return g, eq, tables, cfg
 

@@ -162,6 +162,52 @@ def test_ab3_vs_oracle(case):
     assert rel_l2(to_np(eq.cells.state), s.state) < 1e-5
 
 
+def test_ab3_vs_reference_residual():
+    """AB3 (two SSP-RK3 start-up steps, three AB3 steps) against the same scheme driven by the
+    reference's own residual (fixture c2dvar): FP32 and FP64 bar 1e-5."""
+    g, eq, T, cfg = make_equation("c2dvar", "AB3", "")
+    eq.t_solver.step(5)
+    st = to_np(eq.cells.state)
+    assert rel_l2(st, g["ab3_step5"]) < 1e-5
+    assert rel_l2(st, g["ab3_step5_f64"]) < 1e-5
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 5])
+def test_limiter_variants_vs_reference(p):
+    """Limiters p1, p2, p3, p5 (the other cases use p4): residual and limited gradients vs the
+    reference, 1e-5."""
+    g, eq, T, cfg = make_equation("c2dvar", lim_p=p)
+    r1 = eq.forward(torch.from_numpy(g["prim0"]))
+    assert rel_l2(to_np(r1), g[f"lim{p}_res1"]) < 1e-5
+    assert rel_l2(to_np(eq.cell_grads), g[f"lim{p}_grads1"]) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["RK3_SSP5", "RK3_SSP6", "RK4_SSP5", "RK4_SSP10"])
+def test_tableau_variants_vs_reference(name):
+    """One Butcher step with each remaining tableau vs the reference: FP32 and FP64 bar 1e-5."""
+    g, eq, T, cfg = make_equation("c2dvar", "Butcher", name)
+    eq.t_solver.step(1)
+    st = to_np(eq.cells.state)
+    assert rel_l2(st, g[f"{name.lower()}_step1"]) < 1e-5
+    assert rel_l2(st, g[f"{name.lower()}_step1_f64"]) < 1e-5
+
+
+def test_periodic_box_vs_unrolled_reference():
+    """The benchmark's geometry (periodic Taylor-Green box) against the reference's own geometry:
+    the central tile of the box unrolled 3 x 3 x 3 and run through the reference's FVMMesh3D /
+    FVMEquation.forward (fixture ptile).  Residual, limited gradients and one RK4 step: 1e-5, the
+    per-step parity bar; the RK4 step also against the FP64 reference."""
+    g, eq, T, cfg = make_equation("ptile", "Butcher", "RK4")
+    r1 = eq.forward(torch.from_numpy(g["prim0"]))
+    assert rel_l2(to_np(r1), g["res1"]) < 1e-5
+    assert rel_l2(to_np(eq.cell_grads), g["grads1"]) < 1e-5
+    eq.reset_gradients()
+    eq.t_solver.step(1)
+    st = to_np(eq.cells.state)
+    assert rel_l2(st, g["rk4_step1"]) < 1e-5
+    assert rel_l2(st, g["rk4_step1_f64"]) < 1e-5
+
+
 @pytest.mark.parametrize("case", CASES)
 def test_cfl_and_conservation(case):
     from oracle import fvm_oracle as O
