@@ -1259,14 +1259,14 @@ static Phys make_phys(const fvm_physics_t* ph) {
     return p;
 }
 
-static bool aligned16(const void* p) { return ((uintptr_t)p & 31u) == 0; }   // rows use 256-bit accesses
+static bool aligned32(const void* p) { return ((uintptr_t)p & 31u) == 0; }   // rows use 256-bit accesses
 
 static bool mesh_ok(const fvm_mesh_t* m) {
     if (!m || (m->dim != 2 && m->dim != 3) || m->n_comp != m->dim + 2) return false;
     if (m->n_cells <= 0 || m->n_facets <= 0 || m->n_bc < 0 || m->n_char < 0) return false;
     if (m->kg != m->dim + 2 || m->kf < 1 || m->kf > m->dim + 1) return false;
     if (!m->cell_rec || !m->div_rec || !m->face_rec || !m->inv_h || !m->volumes) return false;
-    if (!aligned16(m->cell_rec) || !aligned16(m->div_rec) || !aligned16(m->face_rec)) return false;
+    if (!aligned32(m->cell_rec) || !aligned32(m->div_rec) || !aligned32(m->face_rec)) return false;
     if (m->n_bc > 0 && (!m->bc_cell || !m->bc_kind || !m->bc_b || !m->bc_l || !m->bc_ga || !m->bc_gb ||
                         !m->bc_char))
         return false;
@@ -1283,7 +1283,7 @@ static bool mesh_ok(const fvm_mesh_t* m) {
 }
 
 static bool work_ok(const fvm_mesh_t* m, const fvm_work_t* w) {
-    return w && w->flux && w->red && aligned16(w->flux) && (m->n_bc == 0 || (w->bc_vals && aligned16(w->bc_vals)));
+    return w && w->flux && w->red && aligned32(w->flux) && (m->n_bc == 0 || (w->bc_vals && aligned32(w->bc_vals)));
 }
 
 static inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
@@ -1518,7 +1518,7 @@ extern "C" int fvm_residual(const fvm_mesh_t* mesh, const fvm_physics_t* phys, c
                             void* stream) {
     if (const int rc = check_common(mesh)) return rc;
     if (!phys || !prims || !grads || !has_grads || !dudt || !work_ok(mesh, work) || !work->prims ||
-        !aligned16(work->prims) || !aligned16(grads))
+        !aligned32(work->prims) || !aligned32(grads))
         return FVM_E_ARG;
     const Phys p = make_phys(phys);
     cudaStream_t s = (cudaStream_t)stream;
@@ -1546,7 +1546,9 @@ static constexpr int kMaxDevices = 64;
 static float* g_noalloc_dev_ptr[kMaxDevices];   // device address of g_noalloc_scratch, per device
 
 // The symbol's device address, looked up once per device with that device current (host code may
-// not use the symbol's name as an address).  Returns nullptr on failure.
+// not use the symbol's name as an address) and kept for the life of the process: a
+// cudaDeviceReset on that device would leave the kept address naming freed memory, which the
+// header rules out for callers.  Returns nullptr on failure.
 static float* noalloc_scratch_address() {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
@@ -1561,8 +1563,8 @@ static float* noalloc_scratch_address() {
 static inline int64_t align64(int64_t n) { return (n + 63) / 64 * 64; }   // 256-byte units of floats
 
 static bool bufs_ok(const fvm_solver_bufs_t* b) {
-    return b && b->state && b->prims && b->grads && b->k && b->dt && b->has_grads && aligned16(b->prims) &&
-           aligned16(b->grads);
+    return b && b->state && b->prims && b->grads && b->k && b->dt && b->has_grads && aligned32(b->prims) &&
+           aligned32(b->grads);
 }
 
 static bool tab_ok(const fvm_tableau_t* t) { return t && t->stages >= 1 && t->stages <= FVM_MAX_STAGES; }
@@ -1779,7 +1781,7 @@ extern "C" int fvm_fused_status(const fvm_work_t* work, int32_t* status) {
 
 extern "C" int fvm_state_to_prims(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const float* state,
                                   float* prims, void* stream) {
-    if (!mesh_ok(mesh) || !phys || !state || !prims || !aligned16(prims)) return FVM_E_ARG;
+    if (!mesh_ok(mesh) || !phys || !state || !prims || !aligned32(prims)) return FVM_E_ARG;
     const Phys p = make_phys(phys);
     cudaStream_t st = (cudaStream_t)stream;
     if (mesh->dim == 2)
@@ -1832,7 +1834,7 @@ extern "C" int fvm_conservation(const fvm_mesh_t* mesh, const float* state, doub
 extern "C" int fvm_residual_noalloc(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const float* prims,
                                     float* grads, int32_t* has_grads, float* dudt, void* stream) {
     if (const int rc = check_common(mesh)) return rc;
-    if (!phys || !prims || !grads || !has_grads || !dudt || !aligned16(grads)) return FVM_E_ARG;
+    if (!phys || !prims || !grads || !has_grads || !dudt || !aligned32(grads)) return FVM_E_ARG;
     if (mesh->char_scale_given) return FVM_E_ARG;   // its scratch holds no per-part slots
     const int64_t R = FVM_ROW(mesh->dim);
     const int64_t n_bc = align64((int64_t)mesh->n_bc * R);

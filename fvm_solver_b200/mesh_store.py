@@ -1,11 +1,22 @@
-"""Boundary-facet specification, mirroring ``time_fvm/mesh_utils/mesh_store.py:5-59``.
+"""Boundary-facet specification: the ``Facet`` / ``FacetBCTypes`` interface of the reference
+(``time_fvm/mesh_utils/mesh_store.py:5-59``), which callers build and pass as ``bc_tags``.
 
-A ``Facet`` lists, per state component, which boundary treatment applies (Dirichlet value,
-Neumann normal gradient, or membership of a characteristic inlet / exit boundary).  The same
-consistency rules as the reference are enforced with the same ``AssertionError`` behaviour.
+The table build (``tables.bc_spec_from_tags``) only reads ``dirichlet()``, ``neumann()``, ``U``,
+``dUdn``, ``farfield()`` and ``inlet()``, so the reference's own ``Facet`` objects can be passed in
+unchanged (duck typing).  This module's ``Facet`` carries the same fields for callers without the
+reference installed.  Its rules, per state component c of a boundary group:
+
+* a Dirichlet component needs a value ``U[c]`` and takes no normal gradient;
+* a Neumann component needs a normal gradient ``dUdn[c]`` and takes no value;
+* characteristic inlet / exit membership (``Inlet`` / ``Farfield``) holds for every component of
+  the group or for none.
+
+A broken rule raises ``AssertionError`` (the reference's behaviour); lists of different lengths
+raise ``ValueError``.  Unset values and gradients are stored as NaN.
 """
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass
 from enum import Flag, auto
 
@@ -18,6 +29,25 @@ class FacetBCTypes(Flag):
     Inlet = auto()
 
 
+def _check_component(c: int, kind: FacetBCTypes, value, grad) -> None:
+    """The value / gradient a component's treatment requires (and forbids)."""
+    if kind & FacetBCTypes.Dirich:
+        if value is None or grad is not None:
+            raise AssertionError(f"component {c}: a Dirichlet boundary takes a value and no gradient "
+                                 f"(got value={value!r}, gradient={grad!r})")
+    if kind & FacetBCTypes.Neuman:
+        if grad is None or value is not None:
+            raise AssertionError(f"component {c}: a Neumann boundary takes a gradient and no value "
+                                 f"(got value={value!r}, gradient={grad!r})")
+
+
+def _all_or_none(kinds, flag: FacetBCTypes, what: str) -> bool:
+    hits = sum(1 for k in kinds if k & flag)
+    if 0 < hits < len(kinds):
+        raise AssertionError(f"{what}: {hits} of {len(kinds)} components are {what}; it must be all or none")
+    return hits == len(kinds)
+
+
 @dataclass
 class Facet:
     edge_type: list
@@ -27,39 +57,27 @@ class Facet:
     tag: str | None = None
 
     def __post_init__(self):
-        if self.U is None:
-            self.U = [None] * len(self.edge_type)
-        if self.dUdn is None:
-            self.dUdn = [None] * len(self.edge_type)
+        n = len(self.edge_type)
+        values = [None] * n if self.U is None else list(self.U)
+        grads = [None] * n if self.dUdn is None else list(self.dUdn)
+        if len(values) != n or len(grads) != n:
+            raise ValueError(f"edge_type has {n} components, U {len(values)}, dUdn {len(grads)}")
+        for c in range(n):
+            _check_component(c, self.edge_type[c], values[c], grads[c])
+        self.U = [math.nan if v is None else v for v in values]
+        self.dUdn = [math.nan if g is None else g for g in grads]
 
-        for e, u, dudn in zip(self.edge_type, self.U, self.dUdn, strict=True):
-            if FacetBCTypes.Dirich in e:
-                assert u is not None, "Dirichlet BC requires a value."
-                assert dudn is None, "Dirichlet BC does not require a gradient."
-            if FacetBCTypes.Neuman in e:
-                assert dudn is not None, "Neumann BC requires a gradient."
-                assert u is None, "Neumann BC does not require a value."
+    def dirichlet(self) -> list:
+        return [bool(k & FacetBCTypes.Dirich) for k in self.edge_type]
 
-        self.U = [float("nan") if u is None else u for u in self.U]
-        self.dUdn = [float("nan") if d is None else d for d in self.dUdn]
-
-    def dirichlet(self):
-        return [FacetBCTypes.Dirich in e for e in self.edge_type]
-
-    def neumann(self):
-        return [FacetBCTypes.Neuman in e for e in self.edge_type]
+    def neumann(self) -> list:
+        return [bool(k & FacetBCTypes.Neuman) for k in self.edge_type]
 
     def farfield(self) -> bool:
-        farfield = [FacetBCTypes.Farfield in e for e in self.edge_type]
-        is_farfield = all(farfield)
-        assert is_farfield or not any(farfield), f"All boundary must be farfield if any are: {farfield}"
-        return is_farfield
+        return _all_or_none(self.edge_type, FacetBCTypes.Farfield, "farfield")
 
     def inlet(self) -> bool:
-        inlet = [FacetBCTypes.Inlet in e for e in self.edge_type]
-        is_inlet = all(inlet)
-        assert is_inlet or not any(inlet), f"All boundary must be inlet if any are: {inlet}"
-        return is_inlet
+        return _all_or_none(self.edge_type, FacetBCTypes.Inlet, "inlet")
 
 
 def wall_facet(dim: int, tag: str = "NavierWall") -> Facet:

@@ -127,7 +127,7 @@ class TSolver:
         self.bufs = _lib.SolverBufs(state=_lib.ptr(cells.state), prims=_lib.ptr(self.prims),
                                     grads=_lib.ptr(eq.grads), k=_lib.ptr(self.k), dt=_lib.ptr(self.dt),
                                     has_grads=_lib.ptr(eq.has_grads), cons=None)
-        self.cfl = cfg.cfl
+        self.cfl = getattr(cfg, "cfl", None)      # a reference ConfigFVM has no cfl field
         if self.cfl:
             self.update_cfl_dt()
 
@@ -378,7 +378,7 @@ class TSolver:
 class Butcher(TSolver):
     def __init__(self, cells, eq, name, cfg, adaptive=False, **kw):
         self.name = name
-        self.tab = make_tableau(name, adaptive=adaptive, cfl=None if adaptive else cfg.cfl, **kw)
+        self.tab = make_tableau(name, adaptive=adaptive, cfl=None if adaptive else getattr(cfg, "cfl", None), **kw)
         self.n_k = self.tab.stages
         self.stages = self.tab.stages
         super().__init__(cells, eq, cfg)

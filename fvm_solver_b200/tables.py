@@ -446,7 +446,8 @@ class FVMTables:
             specs.setdefault(bcfg.mode, []).append((bcfg, mask, self.facet_to_cell_bc[mask], normals))
         groups = {}
         for mode, sp in specs.items():
-            if mode != BCMode.Characteristic:
+            # by name, so that the reference's own BCMode enum (a different class) is accepted too
+            if getattr(mode, "name", None) != BCMode.Characteristic.name:
                 raise NotImplementedError(
                     f"BCMode {mode} is not supported: only Characteristic boundaries are implemented "
                     "(the reference's Farfield mode cannot run: facet_boundary.py:607)")

@@ -207,7 +207,9 @@ int fvm_residual(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float 
  * FVM_E_CAPACITY before anything is launched; a partitioned mesh with char_scale_given = 1 is
  * rejected with FVM_E_ARG (the scratch has no per-part slots).  The function never allocates;
  * the first call on each device looks up the array's device address (with that device
- * current), so make that first call before any stream capture.  Every call overwrites the
+ * current) and keeps it for the life of the process, so make that first call before any stream
+ * capture, and do not call this function on a device after cudaDeviceReset in the same process
+ * (the kept address would name freed memory).  Every call overwrites the
  * scratch it reads, so no clearing is needed; all calls on a device share the array, so calls
  * that overlap on the GPU race and must be serialised by the caller. */
 int fvm_residual_noalloc(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *prims,

@@ -1,6 +1,7 @@
 """Import the reference implementation (Python, CPU path) for fixture generation and checks.
 
-Only the machine that generates the fixtures has the reference sources; the GPU tests, the smoke
+Only the machine that generates the fixtures has the reference sources, named by the environment
+variable ``FVM_REFERENCE_PATH`` (the directory that holds ``time_fvm/``); the GPU tests, the smoke
 test and the benchmark never import this.
 The stubs in ``refstubs/`` stand in for the reference's plotting / coloured-print dependencies,
 which are absent here.  ``fp64=True`` applies a dtype shim (default dtype float64 and
@@ -12,15 +13,18 @@ from __future__ import annotations
 import os
 import sys
 
-REFERENCE_PATH = os.environ.get("FVM_REFERENCE_PATH", "/root/reference")
+REFERENCE_PATH = os.environ.get("FVM_REFERENCE_PATH", "")
 _HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def reference_available() -> bool:
-    return os.path.isdir(os.path.join(REFERENCE_PATH, "time_fvm"))
+    """Whether ``FVM_REFERENCE_PATH`` names a checkout of the reference (its ``time_fvm`` package)."""
+    return bool(REFERENCE_PATH) and os.path.isdir(os.path.join(REFERENCE_PATH, "time_fvm"))
 
 
 def import_reference(fp64: bool = False):
+    if not reference_available():
+        raise RuntimeError("set FVM_REFERENCE_PATH to a checkout of the reference (the directory holding time_fvm/)")
     import torch
     if fp64:
         torch.set_default_dtype(torch.float64)

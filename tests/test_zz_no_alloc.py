@@ -3,10 +3,13 @@
 ``fvm_residual_noalloc`` serves callers that cannot allocate device memory where they call the
 residual (an application whose pool allocator already owns the GPU's memory, or a loop that
 forbids allocation once it runs): it takes its scratch from a 16 MiB static device array instead
-of caller-provided buffers.  The check: two calls in a row -- the first without, the second with
-carried limited gradients -- give the same dU/dt and gradients as the existing entry point,
-within the residual tolerance used by the parity tests (rel-L2 <= 1e-5); and a mesh whose
-scratch does not fit is rejected before anything runs.  This file is collected last.
+of caller-provided buffers.  It launches the same kernels with the same launch shapes as
+``fvm_residual``, so the checks are bitwise: two calls in a row -- the first without, the second
+with carried limited gradients -- give the same dU/dt and gradients as the existing entry point,
+on single meshes and on a batch of two channel cases with characteristic boundaries (whose
+per-case reduction slots also live in the static array); the comparison with the reference's
+vectors keeps the parity tolerance (rel-L2 <= 1e-5); and a mesh whose scratch does not fit is
+rejected before anything runs.  This file is collected last.
 """
 import ctypes as ct
 
@@ -50,8 +53,8 @@ def test_noalloc_matches_residual(case):
         assert _call(lib, lib.fvm_residual, eq, prims, ga, fa, ra, eq.work.struct) == 0
         assert _call(lib, lib.fvm_residual_noalloc, eq, prims, gb, fb, rb) == 0
         torch.cuda.synchronize()
-        assert rel_l2(rb.cpu().numpy(), ra.cpu().numpy()) < 1e-5
-        assert rel_l2(gb.cpu().numpy(), ga.cpu().numpy()) < 1e-5
+        assert torch.equal(rb, ra)
+        assert torch.equal(gb, ga)
         assert int(fb.item()) == 1
     # the Python wrapper goes through the same entry point
     out = torch.empty((N, C), device="cuda")
@@ -59,6 +62,37 @@ def test_noalloc_matches_residual(case):
     eq.forward_noalloc(p1, out)
     ref = torch.from_numpy(g["res1"])
     assert rel_l2(out.cpu().numpy(), ref.numpy()) < 1e-5
+
+
+def test_noalloc_matches_residual_batched():
+    """Two channel cases stepped as one batch: characteristic inlet / exit facets, so the per-case
+    scale of the characteristic boundary goes through the static array's reduction slots."""
+    if not torch.cuda.is_available():
+        pytest.skip("needs CUDA")
+    from fvm_solver_b200 import _lib, batched as B, workloads as W
+    cases = []
+    for i, n in enumerate([2300, 3100]):
+        p = W.ensemble_params(i)
+        p["n_cells"] = n
+        cases.append(W.channel_cylinder(device="cuda", solver_name="AB3", solver_extra="SSP_RK3", **p))
+    batch = B.BatchedFVM([B.build_case_tables(c) for c in cases], cases[0].cfg, device="cuda")
+    assert batch.kt.n_char > 0
+    lib = _lib.load()
+    N, C = batch.n_cells, batch.n_comp
+    p1 = batch.cells.get_values()[0].contiguous()
+    p2 = (p1 * 1.001).contiguous()
+    ga = torch.zeros((N, batch.dev.grow), device="cuda")
+    gb = torch.zeros((N, batch.dev.grow), device="cuda")
+    fa = torch.zeros(1, dtype=torch.int32, device="cuda")
+    fb = torch.zeros(1, dtype=torch.int32, device="cuda")
+    for prims in (p1, p2):
+        ra = torch.empty((N, C), device="cuda")
+        rb = torch.empty((N, C), device="cuda")
+        assert _call(lib, lib.fvm_residual, batch, prims, ga, fa, ra, batch.work.struct) == 0
+        assert _call(lib, lib.fvm_residual_noalloc, batch, prims, gb, fb, rb) == 0
+        torch.cuda.synchronize()
+        assert torch.equal(rb, ra)
+        assert torch.equal(gb, ga)
 
 
 def test_noalloc_rejects_oversized_mesh():
