@@ -64,12 +64,17 @@ def parse():
     ap.add_argument("--parts", type=int, default=4,
                     help="partitioned workload on one GPU: parts the box is split into")
     ap.add_argument("--windows", type=int, default=50, help="corrector rollout windows of k = 8 steps")
+    ap.add_argument("--checkpoint", default=None, help="corrector: evaluate this stored model (no training)")
+    ap.add_argument("--save-checkpoint", default=None, help="corrector: save the trained model here")
     ap.add_argument("--workload", default="taylor_green",
                     choices=["taylor_green", "channel_cylinder", "ensemble", "corrector", "corrector3d",
                              "partitioned"],
                     help="taylor_green: the headline 3D box; channel_cylinder: the 2D cylinder case (11k cells); "
                          "ensemble: batched 2D ensemble vs the same cases run one by one")
     ap.add_argument("--cases", type=int, default=256, help="ensemble size")
+    ap.add_argument("--ensemble-cfl", type=float, default=None, help="ensemble: CFL of the fixed per-case dt")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline line without the channel / ensemble / corrector keys")
     return ap.parse_args()
 
 
@@ -231,7 +236,20 @@ def cpu_replicas(sample_n: int, steps: int | None = None, warmup: int = 1, budge
     return {"value": value, "unit": "cell-steps/s", "cores": workers, "kind": "port",
             "sample": f"{workers} single-threaded numpy oracle replicas ({cpu_model}), periodic TGV box "
                       f"{sample_n}^3 points ({N} tets) each, >= {k_min} RK4 steps each in {el_max:.1f} s",
-            "ms_per_step": 1e3 * el_max / max(k_min, 1)}
+            "ms_per_step": 1e3 * el_max / max(k_min, 1), "anchor": cpu_anchor()}
+
+
+def cpu_anchor():
+    """How fast the port runs next to the reference's own torch CPU path on one host
+    (``oracle/cpu_anchor.json``, measured by ``oracle/time_reference_cpu.py`` where the reference
+    sources are): the port's all-core throughput over the reference's all-thread throughput."""
+    p = os.path.join(ROOT, "oracle", "cpu_anchor.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return {"port_over_reference_all_threads": d["port_replicas_over_reference_all_threads"],
+            "port_over_reference_one_thread": d["port_over_reference_one_thread"],
+            "host": d["host"], "source": "oracle/cpu_anchor.json"}
 
 
 def cpu_baseline(sample_n: int, budget_s: float = 15.0):
@@ -274,7 +292,7 @@ def run_reference(args):
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": cpu["ms_per_step"],
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
            "config": {"workload": "taylor_green_periodic_box_rk4_cfl0.5", "sample_points_per_axis": args.sample_n},
-           "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+           "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample", "anchor")},
            "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
@@ -378,15 +396,8 @@ def partitioned_bench(args):
                       "clocks": clk.summary()}))
 
 
-def secondary(args):
-    """Secondary workloads (single GPU): the 2D channel-cylinder case and the batched ensemble."""
-    from fvm_solver_b200 import _lib, workloads as W
-    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and args.workload != "partitioned":
-        sys.exit(f"--workload {args.workload} runs on one GPU; several ranks run the default workload "
-                 f"(one box per rank) or --workload partitioned (one box split across the ranks)")
-    torch.cuda.set_device(0)
-    stream = torch.cuda.current_stream()
-
+def graph_timer(stream):
+    """Device time (ms) of K steps replayed from one CUDA graph, after an untimed upload replay."""
     def timed(sol, steps):
         replay = sol.graph_steps(steps)
         replay()                             # untimed: the first replay also uploads the graph
@@ -397,96 +408,195 @@ def secondary(args):
         b.record(stream)
         torch.cuda.synchronize()
         return a.elapsed_time(b)
+    return timed
 
-    if args.workload in ("corrector", "corrector3d"):
-        return corrector_bench(args, timed)
-    if args.workload == "partitioned":
-        return partitioned_bench(args)
-    if args.workload == "channel_cylinder":
-        case = W.channel_cylinder(device="cuda")
-        eq = case.equation()
-        sol = eq.t_solver
-        from fvm_solver_b200.autotune import autotune, tune_fused
-        autotune(eq)
-        fused = tune_fused(eq)
-        sol.step(args.warmup)
-        with ClockSampler(0) as clk:
-            ms = timed(sol, args.steps)
-        N = eq.mesh.n_cells
-        cpu = None
-        if not args.no_cpu_baseline:
-            from oracle import fvm_oracle as O
-            T = eq.tables
-            res = O.OracleResidual(T, case.cfg, np.float32)
-            s = O.OracleSolver(res, case.state0.numpy(), 1e-4)
-            inv_h = T.kernel.inv_h.numpy()
-            t0, n = time.perf_counter(), 0
-            while time.perf_counter() - t0 < 15.0:
-                s.dt = res.dt(O.cfl_dt(s.state, 2, case.cfg.C_v, case.cfg.gamma, inv_h, 0.5))
-                s.butcher_step("SSP_RK3")
-                n += 1
-            el = time.perf_counter() - t0
-            cpu = {"value": N * n / el, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+
+def channel_cylinder_result(steps: int, warmup: int, drift_steps: int, cpu: bool, timed) -> dict:
+    """Config 1: the 2D channel-cylinder case (11 323 triangles), SSP-RK3 at CFL 0.5, cell-steps/s
+    from a graph replay of ``steps`` steps; the CPU oracle on the same mesh (1 core, ~15 s); the
+    ``drift_steps``-step trajectory against the FP32 and FP64 oracle."""
+    from fvm_solver_b200 import workloads as W
+    from fvm_solver_b200.autotune import autotune, tune_fused
+    case = W.channel_cylinder(device="cuda")
+    eq = case.equation()
+    sol = eq.t_solver
+    autotune(eq)
+    fused = tune_fused(eq)
+    sol.step(warmup)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms = timed(sol, steps)
+    N = eq.mesh.n_cells
+    cpu_out = None
+    if cpu:
+        from oracle import fvm_oracle as O
+        T = eq.tables
+        res = O.OracleResidual(T, case.cfg, np.float32)
+        s = O.OracleSolver(res, case.state0.numpy(), 1e-4)
+        inv_h = T.kernel.inv_h.numpy()
+        t0, n = time.perf_counter(), 0
+        while time.perf_counter() - t0 < 15.0:
+            s.dt = res.dt(O.cfl_dt(s.state, 2, case.cfg.C_v, case.cfg.gamma, inv_h, 0.5))
+            s.butcher_step("SSP_RK3")
+            n += 1
+        el = time.perf_counter() - t0
+        cpu_out = {"value": N * n / el, "unit": "cell-steps/s", "cores": 1, "kind": "port",
                    "sample": f"numpy oracle, same mesh ({N} cells), {n} SSP-RK3 steps, {el:.1f} s"}
-        drift = None
-        if args.drift_steps:
-            drift = channel_drift(args.drift_steps)
-        out = {"metric": "cell-steps/s", "value": N * args.steps / (ms / 1e3), "unit": "cell-steps/s", "n_gpus": 1,
-               "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-               "dtype": "f32", "data": "synthetic",
-               "config": {"workload": "channel_cylinder_2d_ssprk3_cfl0.5", "cells": N, "facets": eq.dev.n_facets,
-                          "l2": "working set fits in L2 (launch/latency bound case)", "timing": "cuda graph replay",
-                          "step": "fused (one cooperative launch per step)" if fused["fused"] else "separate launches",
-                          "ms_per_step_by_variant": fused["ms_per_step"]},
-               "cpu_baseline": cpu, "drift_vs_oracle": drift, "clocks": clk.summary()}
-        print(json.dumps(out))
-        return
+    drift = channel_drift(drift_steps) if drift_steps else None
+    return {"metric": "cell-steps/s", "value": N * steps / (ms / 1e3), "unit": "cell-steps/s",
+            "steps": steps, "warmup": warmup, "ms_per_step": ms / steps, "dtype": "f32",
+            "config": {"workload": "channel_cylinder_2d_ssprk3_cfl0.5", "cells": N, "facets": eq.dev.n_facets,
+                       "l2": "working set fits in L2 (launch/latency bound case)", "timing": "cuda graph replay",
+                       "step": "fused (one cooperative launch per step)" if fused["fused"] else "separate launches",
+                       "ms_per_step_by_variant": fused["ms_per_step"]},
+            "cpu_baseline": cpu_out, "drift_vs_oracle": drift, "clocks": clk.summary()}
 
-    # ensemble: batched vs one-by-one
-    from fvm_solver_b200 import batched as B
+
+ENSEMBLE_CFL = 0.3
+
+
+def ensemble_result(cases: int, steps: int, warmup: int, timed, cfl: float = ENSEMBLE_CFL) -> dict:
+    """Config 3: 256 seeded channel-cylinder cases (2k-60k cells each) advanced by one launch per
+    kernel (AB3 after two SSP-RK3 start-up steps), against the same cases run one after another,
+    each with its own CUDA graph, autotuned block sizes and its faster step form."""
+    from fvm_solver_b200 import batched as B, workloads as W
+    from fvm_solver_b200.autotune import autotune, tune_fused
     from fvm_solver_b200.equation import FVMEquation, FluidConstitution2D
     t0 = time.time()
-    parts = B.build_ensemble_tables(args.cases, workers=min(16, os.cpu_count() or 1))
+    parts = B.build_ensemble_tables(cases, workers=min(16, os.cpu_count() or 1))
     t_build = time.time() - t0
-    cfg = W.ensemble_case(0, device="cuda", cfl=0.3).cfg
+    cfg = W.ensemble_case(0, device="cuda", cfl=cfl).cfg
     batch = B.BatchedFVM(parts, cfg, device="cuda")
     Nt = batch.n_cells
-    from fvm_solver_b200.autotune import autotune, tune_fused
     tuned = {k: v["threads"] for k, v in autotune(batch).items()}
-    batch.t_solver.step(max(args.warmup, 3))
+    batch.t_solver.step(max(warmup, 3))
     fused_b = tune_fused(batch)
-    with ClockSampler(0) as clk:
-        ms_b = timed(batch.t_solver, args.steps)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms_b = timed(batch.t_solver, steps)
+    finite = bool(torch.isfinite(batch.cells.state).all())
     roof = batched_roofline(batch, steps=10)
     del batch
     torch.cuda.empty_cache()
-    # plain: every case alone, each with its own captured graph of the same number of steps
     ms_p, cells_p, n_fused = 0.0, 0, 0
     for k, p in enumerate(parts):
-        c = W.ensemble_case(k, device="cuda", cfl=0.3).cfg
+        c = W.ensemble_case(k, device="cuda", cfl=cfl).cfg
         eq = FVMEquation.from_kernel_tables(c, FluidConstitution2D(c), p.kt, p.state0)
         autotune(eq)                       # per size bucket (cached), so small cases get their own
-        eq.t_solver.step(max(args.warmup, 3))
+        eq.t_solver.step(max(warmup, 3))
         n_fused += tune_fused(eq)["fused"]  # each case alone also gets its faster step form
-        ms_p += timed(eq.t_solver, args.steps)
+        ms_p += timed(eq.t_solver, steps)
         cells_p += p.kt.n_cells
         del eq
-    vb = Nt * args.steps / (ms_b / 1e3)
-    vp = cells_p * args.steps / (ms_p / 1e3)
+    vb = Nt * steps / (ms_b / 1e3)
+    vp = cells_p * steps / (ms_p / 1e3)
     sizes = [p.kt.n_cells for p in parts]
-    out = {"metric": "cell-steps/s", "value": vb, "unit": "cell-steps/s", "n_gpus": 1, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": ms_b / args.steps, "higher_is_better": True, "dtype": "f32",
-           "data": "synthetic",
-           "config": {"workload": "ensemble_2d_ab3_batched", "cases": args.cases, "cells_total": Nt,
-                      "cells_min": min(sizes), "cells_max": max(sizes), "integrator": "AB3 (SSP-RK3 start), CFL 0.3",
-                      "timing": "cuda graph replay", "table_build_s": t_build, "host_cpus": os.cpu_count(),
-                      "block_sizes": tuned, "fused_step": fused_b},
-           "roofline": roof,
-           "plain": {"value": vp, "unit": "cell-steps/s", "ms_per_step_all_cases": ms_p / args.steps,
-                     "how": "each case alone, own CUDA graph, sequential",
-                     "cases_with_fused_step": n_fused},
-           "batched_over_plain": vb / vp, "clocks": clk.summary()}
-    print(json.dumps(out))
+    return {"metric": "cell-steps/s", "value": vb, "unit": "cell-steps/s", "steps": steps, "warmup": warmup,
+            "ms_per_step": ms_b / steps, "dtype": "f32",
+            "config": {"workload": "ensemble_2d_ab3_batched", "cases": cases, "cells_total": Nt,
+                       "cells_min": min(sizes), "cells_max": max(sizes),
+                       "integrator": f"AB3 (SSP-RK3 start), fixed per-case dt from CFL {cfl} at the start",
+                       "cfl_note": ENSEMBLE_CFL_NOTE if cfl != 0.5 else None,
+                       "timing": "cuda graph replay", "table_build_s": t_build, "host_cpus": os.cpu_count(),
+                       "block_sizes": tuned, "fused_step": fused_b},
+            "state_finite_after_timed_steps": finite,
+            "roofline": roof,
+            "plain": {"value": vp, "unit": "cell-steps/s", "ms_per_step_all_cases": ms_p / steps,
+                      "how": "each case alone, own CUDA graph, sequential",
+                      "cases_with_fused_step": n_fused},
+            "batched_over_plain": vb / vp, "clocks": clk.summary()}
+
+
+ENSEMBLE_CFL_NOTE = ("AB3 with a time step fixed at the start: CFL 0.3 keeps every case inside AB3's "
+                     "stability region for 2000 steps; see DESIGN section 5")
+
+
+def ensemble_sharded(args):
+    """The ensemble under torchrun: cases split across the ranks by cell count
+    (``sharding.partition_cases``), one ``BatchedFVM`` per rank, no collective in the step, the
+    graph-replayed steps timed on each rank's device and reduced with MAX; one all-gather of the
+    per-case results (cells, final dt, sum of the state, finite flag) at the end.  The total work
+    is fixed as ranks are added (strong scaling)."""
+    import torch.distributed as dist
+    from datetime import timedelta
+    from fvm_solver_b200 import batched as B, workloads as W
+    from fvm_solver_b200.autotune import autotune
+    from fvm_solver_b200.sharding import run_sharded
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    rank, world = dist.get_rank(), dist.get_world_size()
+    cfl = args.ensemble_cfl or ENSEMBLE_CFL
+    sizes = [p["n_cells"] for p in (W.ensemble_params(i) for i in range(args.cases))]
+    stream = torch.cuda.current_stream()
+    timed = graph_timer(stream)
+    dev = torch.device("cuda", local)
+    holder = {}
+
+    def make_batch(ids):
+        if not ids:
+            return None
+        workers = max(1, min(16, (os.cpu_count() or 1) // world))
+        parts = B.build_ensemble_tables(args.cases, workers=workers, indices=ids)
+        cfg = W.ensemble_case(ids[0], device=f"cuda:{local}", cfl=cfl).cfg
+        batch = B.BatchedFVM(parts, cfg, device=f"cuda:{local}")
+        holder["tuned"] = {k: v["threads"] for k, v in autotune(batch).items()}
+        batch.t_solver.step(max(args.warmup, 3))
+        return batch
+
+    def advance(batch, steps):
+        with ClockSampler(local) as clk:
+            ms = timed(batch.t_solver, steps)
+        holder["clocks"] = clk.summary()
+        return ms
+
+    def rows(batch):
+        out = []
+        for k in range(batch.n_cases):
+            st = batch.case_state(k)
+            out.append(torch.stack([torch.tensor(float(st.shape[0]), device=dev, dtype=torch.float64),
+                                    batch.t_solver.dt[k].double(), st.double().sum(),
+                                    torch.isfinite(st).all().double()]))
+        return torch.stack(out)
+
+    res = run_sharded(sizes, args.steps, make_batch, advance, rows, row_width=4, device=dev)
+    table = res["rows"].cpu()
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank == 0:
+        ms = res["ms_max"]
+        print(json.dumps({"metric": "cell-steps/s", "value": res["cells_total"] * args.steps / (ms / 1e3),
+                          "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+                          "dtype": "f32", "data": "synthetic",
+                          "config": {"workload": "ensemble_2d_ab3_batched_sharded", "cases": args.cases,
+                                     "cells_total": res["cells_total"], "cells_rank0": res["cells_local"],
+                                     "integrator": f"AB3 (SSP-RK3 start), fixed per-case dt from CFL {cfl}",
+                                     "sharding": "cases by cell count (LPT), one BatchedFVM per rank, "
+                                                 "no collective in the step; one all-gather of results",
+                                     "block_sizes_rank0": holder.get("tuned"), "timing": "cuda graph replay, "
+                                     "max over ranks"},
+                          "cases_finite": int(table[:, 3].sum().item()), "clocks": holder.get("clocks")}))
+
+
+def secondary(args):
+    """Secondary workloads (single GPU) as their own benchmark lines."""
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and args.workload not in ("partitioned", "ensemble"):
+        sys.exit(f"--workload {args.workload} runs on one GPU; several ranks run the default workload "
+                 f"(one box per rank), --workload ensemble (cases split across the ranks) or "
+                 f"--workload partitioned (one box split across the ranks)")
+    if args.workload == "partitioned":
+        return partitioned_bench(args)
+    if args.workload == "ensemble" and int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        return ensemble_sharded(args)
+    torch.cuda.set_device(0)
+    timed = graph_timer(torch.cuda.current_stream())
+    if args.workload in ("corrector", "corrector3d"):
+        return corrector_bench(args, timed)
+    common = {"n_gpus": 1, "higher_is_better": True, "data": "synthetic"}
+    if args.workload == "channel_cylinder":
+        out = channel_cylinder_result(args.steps, args.warmup, args.drift_steps, not args.no_cpu_baseline, timed)
+    else:
+        out = ensemble_result(args.cases, args.steps, args.warmup, timed, cfl=args.ensemble_cfl or ENSEMBLE_CFL)
+    print(json.dumps({**out, **common}))
 
 
 def batched_roofline(batch, steps: int = 10) -> dict:
@@ -522,76 +632,91 @@ def batched_roofline(batch, steps: int = 10) -> dict:
             "frac": kern[dom]["achieved_gbs"] / peak, "peak_source": peak_kind, "kernels": kern}
 
 
-def corrector_bench(args, timed):
-    """Learned k-step corrector (k = 8) + FVM fallback vs plain FVM on held-out 2D cases.
+CORRECTOR_CKPT = os.path.join(ROOT, "fvm_solver_b200", "checkpoints", "corrector_2d_k8.pt")
 
-    Training: 32 seeded channel-cylinder cases stepped together (SSP-RK3, fixed per-case dt from
-    CFL 0.5 at the start), spin-up then recorded; random 8-step windows.  Evaluation: held-out
-    cases (other seeds), same spin-up, then R windows advanced (a) by plain FVM (a CUDA graph of 8
-    steps replayed per window) and (b) by the corrector with per-case checks and FVM fallback (the
-    proposal + checks graph, one host read of the verdicts, the 8-step graph when a case failed);
-    both timed on the device with CUDA events.
-    """
-    import copy
-    from fvm_solver_b200 import batched as B, workloads as W
-    from fvm_solver_b200.corrector import CheckedRollout, CorrectorModel, record_trajectory, train
-    workers = min(16, os.cpu_count() or 1)
-    three_d = args.workload == "corrector3d"
-    if args.train_cases is None:
-        args.train_cases = 4 if three_d else 32
-    if args.iters is None:
-        args.iters = 2000 if three_d else 6000
-    family = "sphere" if three_d else "channel"
+
+def _corrector_family(three_d: bool):
+    from fvm_solver_b200 import workloads as W
     params = (lambda i, seed: W.sphere_params(i, seed)) if three_d else W.ensemble_params
     seeds = (5678, 9100) if three_d else (1234, 9000)
+    return params, seeds
 
-    def make(n, seed):
-        parts = B.build_ensemble_tables(n, base_seed=seed, workers=workers, family=family)
-        case0 = W.sphere_case(0, device="cuda", base_seed=seed, cells=(20_000, 20_000)) if three_d else \
-            W.ensemble_case(0, device="cuda", base_seed=seed)
-        cfg = copy.deepcopy(case0.cfg)
-        cfg.solver_name, cfg.solver_extra, cfg.cfl = "Butcher", "SSP_RK3", None
-        prm = torch.tensor([[params(i, seed)["mach"], np.log10(params(i, seed)["reynolds"])]
-                            for i in range(n)], dtype=torch.float32)
-        return parts, cfg, prm
 
+def _corrector_cases(n, seed, three_d):
+    """Tables, solver config (SSP-RK3, dt fixed per case from CFL 0.5 at the start) and per-case
+    (Mach, log10 Re) of ``n`` seeded cases of the channel (2D) or sphere (3D) family."""
+    import copy
+    from fvm_solver_b200 import batched as B, workloads as W
+    params, _ = _corrector_family(three_d)
+    parts = B.build_ensemble_tables(n, base_seed=seed, workers=min(16, os.cpu_count() or 1),
+                                    family="sphere" if three_d else "channel")
+    case0 = W.sphere_case(0, device="cuda", base_seed=seed, cells=(20_000, 20_000)) if three_d else \
+        W.ensemble_case(0, device="cuda", base_seed=seed)
+    cfg = copy.deepcopy(case0.cfg)
+    cfg.solver_name, cfg.solver_extra, cfg.cfl = "Butcher", "SSP_RK3", None
+    prm = torch.tensor([[params(i, seed)["mach"], np.log10(params(i, seed)["reynolds"])] for i in range(n)],
+                       dtype=torch.float32)
+    return parts, cfg, prm
+
+
+def corrector_train(args, three_d: bool):
+    """Train the corrector on trajectories of ``args.train_cases`` seeded cases; returns the model
+    and a summary (loss history, seconds)."""
+    from fvm_solver_b200 import batched as B
+    from fvm_solver_b200.corrector import CorrectorModel, record_trajectory, train
+    _, seeds = _corrector_family(three_d)
     t0 = time.time()
-    parts, cfg, prm = make(args.train_cases, seeds[0])
+    parts, cfg, prm = _corrector_cases(args.train_cases, seeds[0], three_d)
     batch = B.BatchedFVM(parts, cfg, device="cuda")
     batch.t_solver.update_cfl_dt(0.5)
     traj = record_trajectory(batch, steps=200 if three_d else 400, spinup=200)
     model = CorrectorModel(batch, prm, k=8, seed=0, lr=1e-3)
-    batch_cells = batch.n_cells
     torch.cuda.synchronize()
     t1 = time.time()
     hist = train(model, traj, iters=args.iters, log_every=max(1, args.iters // 10))
     torch.cuda.synchronize()
-    t_train = time.time() - t1
+    info = {"train_cases": args.train_cases, "train_cells": int(batch.n_cells), "iters": args.iters,
+            "loss_first": hist[0][1], "loss_last": hist[-1][1], "seconds": time.time() - t1,
+            "setup_seconds": t1 - t0}
     del traj
     torch.cuda.empty_cache()
+    return model, info
 
-    eparts, ecfg, eprm = make(args.eval_cases, seeds[1])
+
+def corrector_evaluate(model_src, args, three_d: bool, ratios=(3.0, 1.2), spinup: int = 200) -> dict:
+    """Held-out cases advanced ``args.windows`` windows of k = 8 steps (a) by plain FVM (a CUDA graph
+    of 8 steps per window) and (b) by the corrector with per-case checks and FVM fallback (the
+    proposal + checks graph, one host read of the verdicts, the 8-step graph for failed cases), both
+    from the same spun-up start and timed with CUDA events; the corrected states are compared with
+    the plain ones at the end.  ``model_src``: a trained model, or a checkpoint path."""
+    from fvm_solver_b200 import batched as B
+    from fvm_solver_b200.corrector import CheckedRollout, CorrectorModel
+    _, seeds = _corrector_family(three_d)
+    eparts, ecfg, eprm = _corrector_cases(args.eval_cases, seeds[1], three_d)
+    stream = torch.cuda.current_stream()
     plain = B.BatchedFVM(eparts, ecfg, device="cuda")
     plain.t_solver.update_cfl_dt(0.5)
-    plain.t_solver.step(200)
+    plain.t_solver.step(spinup)
     plain_window = plain.t_solver.graph_steps(8)
-    stream = torch.cuda.current_stream()
     e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     torch.cuda.synchronize()
-    e[0].record(stream)
-    for _ in range(args.windows):
-        plain_window()
-    e[1].record(stream)
-    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        e[0].record(stream)
+        for _ in range(args.windows):
+            plain_window()
+        e[1].record(stream)
+        torch.cuda.synchronize()
     ms_plain = e[0].elapsed_time(e[1])
 
     def rollout(ratio):
-        """Corrector + fallback from the same spun-up start as the plain run, with residual-norm
-        ratio `ratio` in the acceptance check."""
         corr = B.BatchedFVM(eparts, ecfg, device="cuda")
         corr.t_solver.update_cfl_dt(0.5)
-        corr.t_solver.step(200)
-        ro = CheckedRollout(CorrectorModel(corr, eprm, like=model), residual_ratio=ratio)
+        corr.t_solver.step(spinup)
+        if isinstance(model_src, str):
+            model = CorrectorModel.load(model_src, corr, eprm)
+        else:
+            model = CorrectorModel(corr, eprm, like=model_src)
+        ro = CheckedRollout(model, residual_ratio=ratio)
         # capture every CUDA graph before timing (capturing executes nothing; the state stays put)
         ro._run_propose()
         corr.t_solver._sync_prims()
@@ -620,21 +745,53 @@ def corrector_bench(args, timed):
                                     "cases_compared": len(err)},
                 "nonfinite_cases": {"plain": bad_plain, "corrected": bad_corr}}
 
-    spec = rollout(3.0)
-    strict = rollout(1.2)
-    out = {"metric": "sim-time/s corrector+fallback over plain FVM", "value": spec["speedup"], "unit": "x",
-           "higher_is_better": True, "n_gpus": 1, "dtype": "bf16 GEMM / f32 state", "data": "synthetic",
-           "config": {"workload": "corrector_3d_sphere_k8" if three_d else "corrector_2d_k8",
-                      "train_cases": args.train_cases, "eval_cases": args.eval_cases,
-                      "train_cells": int(batch_cells), "eval_cells": int(plain.n_cells),
-                      "iters": args.iters, "windows": args.windows, "fvm": "SSP-RK3, fixed per-case dt (CFL 0.5)",
-                      "net": "4 message-passing layers, width 64, SiLU, tcgen05 BF16 GEMMs",
-                      "checks": "drift <= 1e-4, residual norm <= 3x, admissible state"},
-           "ms_plain": ms_plain, **{k: v for k, v in spec.items() if k != "speedup"},
-           "stricter_residual_check": strict,
-           "train": {"loss_first": hist[0][1], "loss_last": hist[-1][1], "seconds": t_train,
-                     "setup_seconds": t1 - t0}}
+    runs = [rollout(r) for r in ratios]
+    main, others = runs[0], runs[1:]
+    return {"metric": "sim-time/s corrector+fallback over plain FVM", "value": main["speedup"], "unit": "x",
+            "higher_is_better": True, "dtype": "bf16 GEMM / f32 state",
+            "config": {"workload": "corrector_3d_sphere_k8" if three_d else "corrector_2d_k8",
+                       "eval_cases": args.eval_cases, "eval_cells": int(plain.n_cells), "windows": args.windows,
+                       "steps_per_rollout": 8 * args.windows, "spinup_steps": spinup,
+                       "fvm": "SSP-RK3, fixed per-case dt (CFL 0.5)",
+                       "net": "4 message-passing layers, width 64, SiLU, tcgen05 BF16 GEMMs",
+                       "checks": f"drift <= 1e-4, residual norm <= {ratios[0]}x, admissible state"},
+            "ms_plain": ms_plain, **{k: v for k, v in main.items() if k != "speedup"},
+            "other_residual_checks": others, "clocks": clk.summary()}
+
+
+def corrector_bench(args, timed):
+    """Learned k-step corrector (k = 8) + FVM fallback vs plain FVM on held-out cases: trains (or,
+    with ``--checkpoint``, loads) the model, optionally saves it (``--save-checkpoint``), evaluates."""
+    three_d = args.workload == "corrector3d"
+    if args.train_cases is None:
+        args.train_cases = 4 if three_d else 32
+    if args.iters is None:
+        args.iters = 2000 if three_d else 6000
+    info = None
+    if args.checkpoint:
+        model_src = args.checkpoint
+    else:
+        model_src, info = corrector_train(args, three_d)
+        if args.save_checkpoint:
+            os.makedirs(os.path.dirname(os.path.abspath(args.save_checkpoint)), exist_ok=True)
+            model_src.save(args.save_checkpoint, meta=info)
+    out = corrector_evaluate(model_src, args, three_d)
+    out.update({"n_gpus": 1, "data": "synthetic", "train": info,
+                "model": args.checkpoint or "trained in this run"})
     print(json.dumps(out))
+
+
+def corrector_checkpoint_result(args, timed) -> dict:
+    """The headline line's corrector key: the stored 2D model (trained offline by
+    ``--workload corrector --save-checkpoint``) evaluated on the held-out cases; training is not
+    part of this run."""
+    if not os.path.exists(CORRECTOR_CKPT):
+        return {"unavailable": "no stored corrector checkpoint"}
+    d = torch.load(CORRECTOR_CKPT, map_location="cpu", weights_only=True)
+    ev = argparse.Namespace(eval_cases=args.eval_cases, windows=args.windows)
+    out = corrector_evaluate(CORRECTOR_CKPT, ev, three_d=False)
+    out["model"] = {"checkpoint": os.path.relpath(CORRECTOR_CKPT, ROOT), "trained": d.get("meta", {})}
+    return out
 
 
 def main():
@@ -646,7 +803,7 @@ def main():
 
     import torch.distributed as dist
     from fvm_solver_b200 import _lib, workloads as W
-    from fvm_solver_b200.roofline import kernel_bytes, div_stage_bytes, tableau_terms
+    from fvm_solver_b200.roofline import kernel_bytes, div_stage_bytes, step_compulsory_bytes, tableau_terms
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -725,23 +882,32 @@ def main():
     tot = sum(v["ms_total"] for v in kern.values())
     for v in kern.values():
         v["share"] = v["ms_total"] / tot
-    kb = kernel_bytes(3, N, F, Fb, eq.dev.kf)
-    per_launch = {"cell": kb["cell"], "face": kb["face"], "bc": kb["bc"]}
-    dsb = div_stage_bytes(3, N, F, Fb, tableau_terms(sol.tab), eq.dev.kf)
-    per_launch["div_stage"] = float(np.mean(dsb))
+    def launch_bytes(widths):
+        kb = kernel_bytes(3, N, F, Fb, eq.dev.kf, widths=widths)
+        out = {"cell": kb["cell"], "face": kb["face"], "bc": kb["bc"]}
+        out["div_stage"] = float(np.mean(div_stage_bytes(3, N, F, Fb, tableau_terms(sol.tab), eq.dev.kf, widths)))
+        return out
+    per_launch = launch_bytes("element")             # 4 B per used element (the roofline's count)
+    per_launch_stored = launch_bytes("stored")       # 4 B per stored float, row padding included
     dom = max((k for k in kern if k in per_launch), key=lambda k: kern[k]["ms_total"])
     peak, peak_kind = measured_peaks()
     achieved = per_launch[dom] / (kern[dom]["ms_mean"] / 1e3) / 1e9
-    traffic = None
+    achieved_stored = per_launch_stored[dom] / (kern[dom]["ms_mean"] / 1e3) / 1e9
+    step_bytes = step_compulsory_bytes(3, N, F, sol.tab.stages)
+    step_gbs = step_bytes / (ms_max / args.steps / 1e3) / 1e9
+    traffic = traffic_src = None
     tf = os.path.join(ROOT, "profiles", "dram_bytes_per_cell.json")
     if os.path.exists(tf):
         d = json.load(open(tf))
         if dom in d.get("kernels", {}):
             traffic = d["kernels"][dom] * N
+            traffic_src = d.get("source")
     for k, v in kern.items():
         if k in per_launch:
             v["algorithmic_bytes_per_launch"] = per_launch[k]
             v["achieved_gbs"] = per_launch[k] / (v["ms_mean"] / 1e3) / 1e9
+            v["frac"] = v["achieved_gbs"] / peak
+            v["stored_bytes_per_launch"] = per_launch_stored[k]
 
     # end-to-end through the public API with host buffers
     ke = args.e2e_steps or max(args.steps, 50)
@@ -827,6 +993,15 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         parity = parity_check(args.sample_n)
     launches_per_step = n_launch / args.steps
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        # The north star's other targets, each with its own CUDA-event timing and clock record:
+        # config 1 (2D channel, with its trajectory against the oracle), config 3 (batched
+        # ensemble vs the cases one by one) and configs 4 (corrector from a stored checkpoint).
+        timed = graph_timer(stream)
+        extras["channel_cylinder"] = channel_cylinder_result(50, 5, args.drift_steps, not args.no_cpu_baseline, timed)
+        extras["ensemble"] = ensemble_result(args.cases, 20, 5, timed, cfl=args.ensemble_cfl or ENSEMBLE_CFL)
+        extras["corrector"] = corrector_checkpoint_result(args, timed)
     if rank == 0:
         out = {
             "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
@@ -840,7 +1015,17 @@ def main():
                        "block_sizes": tuned, "l2_prefetch": prefetch},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": per_launch[dom]},
+                         "traffic_source": traffic_src,
+                         "algorithmic_bytes_per_launch": per_launch[dom],
+                         "bytes": "4 B per used element (row padding not counted)",
+                         "frac_stored": achieved_stored / peak,
+                         "stored_bytes_per_launch": per_launch_stored[dom],
+                         "step_compulsory_bytes": step_bytes,
+                         "step_compulsory_gbs": step_gbs,
+                         "step_compulsory_frac": step_gbs / peak,
+                         "step_compulsory_def": "one-pass stage traffic x stages: 4 B x (per cell 2C + dim KG + KG "
+                                                "+ K + K dim + 2 + 4K; per facet 2 dim + 3); 328 B per cell-stage "
+                                                "in 3D"},
             "kernels": kern,
             "cpu_baseline": cpu,
             "parity": parity,
@@ -858,6 +1043,7 @@ def main():
                     "chained_mode": "state round-trips through the host every step (no overlap possible)"},
             "gpu_launches": int(round(launches_per_step * args.steps)),
             "clocks": clocks,
+            **extras,
         }
         print(json.dumps(out))
     del replay

@@ -89,19 +89,18 @@ _SIGS = [
     ("fvm_set_prefetch", ct.c_int, [ct.c_int32, ct.c_int32]),
     ("fvm_gemm_bf16", ct.c_int, [_P, ct.c_int64, _P, ct.c_int64, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32,
                                  _P, _P, ct.c_int64, _P, _P, ct.c_int64, _P, ct.c_int32, _P, _P]),
-    ("fvm_mp_gather", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, ct.c_int32, _P, _P]),
+    ("fvm_mp_gather_f32", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, _P, _P]),
+    ("fvm_mp_layer", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, _P, _P, _P, _P, _P, ct.c_int32, _P, _P, _P]),
     ("fvm_mp_scatter_back", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, ct.c_int32, _P, _P, _P]),
     ("fvm_silu_back", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, _P, _P, ct.c_int64, _P, _P]),
     ("fvm_transpose_bf16", ct.c_int, [_P, ct.c_int32, ct.c_int32, ct.c_int64, _P, ct.c_int64, _P]),
-    ("fvm_decoder", ct.c_int, [_P, _P, _P, ct.c_int32, ct.c_int32, ct.c_int32, _P, _P]),
-    ("fvm_decoder_back", ct.c_int, [_P, _P, _P, ct.c_int32, ct.c_int32, ct.c_int32, _P, _P, _P, _P]),
+    ("fvm_decoder_f32", ct.c_int, [_P, _P, _P, ct.c_int32, ct.c_int32, _P, _P]),
+    ("fvm_decoder_back_f32", ct.c_int, [_P, _P, _P, ct.c_int32, ct.c_int32, _P, _P, _P, _P]),
     ("fvm_mse", ct.c_int, [_P, _P, ct.c_int64, _P, _P, _P]),
     ("fvm_adam", ct.c_int, [_P, _P, _P, _P, ct.c_int64, ct.c_float, ct.c_float, ct.c_float, ct.c_float,
                             ct.c_int32, _P, _P, ct.c_int32, ct.c_int32, _P]),
     ("fvm_corrector_features", ct.c_int, [_P, ct.c_int32, ct.c_int32, _P, _P, _P, ct.c_int32, _P, ct.c_int32, _P]),
     ("fvm_apply_increment", ct.c_int, [_P, _P, _P, ct.c_int32, ct.c_int32, _P, _P]),
-    ("fvm_mp_gemm", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, _P, _P, _P, ct.c_int64, _P, _P, ct.c_int64,
-                               ct.c_int32, _P, _P]),
     ("fvm_corrector_inputs", ct.c_int, [_P, _P, _P, _P, ct.c_int32, ct.c_int32, _P, _P, _P, ct.c_int32, _P, _P,
                                         ct.c_int32, _P]),
     ("fvm_corrector_combine", ct.c_int, [_P, _P, _P, _P, _P, _P, ct.c_int32, ct.c_int32, _P, _P]),

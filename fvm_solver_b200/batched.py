@@ -60,11 +60,14 @@ def _worker_init():
 
 
 def build_ensemble_tables(n_cases: int, base_seed: int = 1234, workers: int = 0, family: str = "channel",
-                          cells=(300_000, 800_000)) -> list:
+                          cells=(300_000, 800_000), indices=None) -> list:
     """Per-case tables of a seeded ensemble -- ``family`` "channel" (2D channel-cylinder cases) or
     "sphere" (3D flow over a sphere, ``cells`` the tet-count range); ``workers > 0`` builds them in
-    spawned processes."""
-    jobs = [(i, base_seed, family, tuple(cells)) for i in range(n_cases)]
+    spawned processes.  ``indices`` builds only those cases of the ensemble (one rank's share)."""
+    ids = range(n_cases) if indices is None else list(indices)
+    jobs = [(i, base_seed, family, tuple(cells)) for i in ids]
+    if not jobs:
+        return []
     if workers > 0:
         ctx = mp.get_context("spawn")
         with cfut.ProcessPoolExecutor(max_workers=workers, mp_context=ctx, initializer=_worker_init) as ex:

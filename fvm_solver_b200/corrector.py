@@ -14,8 +14,8 @@ the k-step change, and the conservation check cannot be failed by the network.
 
 Network (width W = 64, L = 4 message-passing layers, SiLU):
     X  = [normalised U, normalised base, geometry, case parameters]   (bf16 [N][64])
-    h0 = SiLU(X Win^T + b_in)
-    h_{l+1} = h_l + SiLU([h_l, mean_{j in nbr} h_l,j] W_l^T + b_l)  (l = 0..3)
+    h0 = SiLU(X Win^T + b_in)                                        (h: fp32 residual stream)
+    h_{l+1} = h_l + SiLU([bf16(h_l), bf16(mean_{j in nbr} h_l,j)] W_l^T + b_l)  (l = 0..3)
     out = h_L Wout^T + b_out                                        (normalised U_{t+k} - U_t - base)
 All matrix products run on ``fvm_gemm_bf16`` (tcgen05, BF16 operands, FP32 accumulation in tensor
 memory, bias / SiLU / residual fused into the epilogue); the backward pass (SiLU derivative,
@@ -114,7 +114,6 @@ class CorrectorNet:
              "XT": torch.zeros((XW, Np), dtype=torch.bfloat16, device=d),
              "Z": [torch.zeros((N, W), device=d) for _ in range(L + 1)],
              "hf": [torch.zeros((N, W), device=d) for _ in range(L + 1)],
-             "hb": [torch.zeros((Np, W), dtype=torch.bfloat16, device=d) for _ in range(L + 1)],
              "A": [torch.zeros((Np, 2 * W), dtype=torch.bfloat16, device=d) for _ in range(L)],
              "AT": torch.zeros((2 * W, Np), dtype=torch.bfloat16, device=d),
              "dZ": torch.zeros((Np, W), dtype=torch.bfloat16, device=d),
@@ -142,29 +141,38 @@ class CorrectorNet:
         return b["X"]
 
     def forward(self, nbr: torch.Tensor, store_pre: bool = True) -> torch.Tensor:
-        """Network output for the features already in the X buffer (``features``).  Inference
-        (``store_pre=False``) skips the pre-activation stores the backward pass needs."""
+        """Network output for the features already in the X buffer (``features``).
+
+        Training (``store_pre=True``): the input GEMM, then per layer the gather of
+        [bf16(h_i), bf16(mean_j h_j)] from the fp32 residual stream (kept for the backward pass)
+        and a GEMM whose epilogue adds bias, SiLU and the residual, storing the pre-activations;
+        the decoder reads the last fp32 activations.  Inference (``store_pre=False``): the input
+        GEMM, then one persistent fused kernel per layer (``fvm_mp_layer``: the gather built in
+        shared memory, tcgen05 MMA, epilogue), the last one with the decoder in its epilogue.  Both
+        forms do the same arithmetic in the same order and give bitwise the same output."""
         b = self._bufs
         N, L = b["N"], self.L
         p, s = self.params, _lib.stream_ptr()
         Z = b["Z"] if store_pre else [None] * (L + 1)
-        self._gemm(b["X"], XW, self.bf["W_in"], XW, N, W, XW, Df=b["hf"][0], Db=b["hb"][0], ldd=W, bias=p["b_in"],
-                   pre=Z[0], act=1)
+        self._gemm(b["X"], XW, self.bf["W_in"], XW, N, W, XW, Df=b["hf"][0], ldd=W, bias=p["b_in"], pre=Z[0], act=1)
         for l in range(L):
             if not store_pre:
-                # inference: the neighbour mean is built inside the layer's GEMM (bitwise the same)
-                _lib.check(self.lib.fvm_mp_gemm(b["hb"][l].data_ptr(), nbr.data_ptr(), N, nbr.shape[1],
-                                                self.bf[f"W{l}"].data_ptr(), p[f"b{l}"].data_ptr(),
-                                                b["hf"][l].data_ptr(), W, b["hf"][l + 1].data_ptr(),
-                                                b["hb"][l + 1].data_ptr(), W, 1, self.err.data_ptr(), s),
-                           "fvm_mp_gemm")
+                last = l == L - 1
+                _lib.check(self.lib.fvm_mp_layer(b["hf"][l].data_ptr(), nbr.data_ptr(), N, nbr.shape[1],
+                                                 self.bf[f"W{l}"].data_ptr(), p[f"b{l}"].data_ptr(),
+                                                 None if last else b["hf"][l + 1].data_ptr(),
+                                                 p["W_out"].data_ptr() if last else None,
+                                                 p["b_out"].data_ptr() if last else None, self.O,
+                                                 b["out"].data_ptr() if last else None, self.err.data_ptr(), s),
+                           "fvm_mp_layer")
                 continue
-            _lib.check(self.lib.fvm_mp_gather(b["hb"][l].data_ptr(), nbr.data_ptr(), N, W, nbr.shape[1],
-                                              b["A"][l].data_ptr(), s), "fvm_mp_gather")
-            self._gemm(b["A"][l], 2 * W, self.bf[f"W{l}"], 2 * W, N, W, 2 * W, Df=b["hf"][l + 1], Db=b["hb"][l + 1],
-                       ldd=W, bias=p[f"b{l}"], resid=b["hf"][l], ldr=W, pre=Z[l + 1], act=1)
-        _lib.check(self.lib.fvm_decoder(b["hb"][L].data_ptr(), p["W_out"].data_ptr(), p["b_out"].data_ptr(), N, W,
-                                        self.O, b["out"].data_ptr(), s), "fvm_decoder")
+            _lib.check(self.lib.fvm_mp_gather_f32(b["hf"][l].data_ptr(), nbr.data_ptr(), N, nbr.shape[1],
+                                                  b["A"][l].data_ptr(), s), "fvm_mp_gather_f32")
+            self._gemm(b["A"][l], 2 * W, self.bf[f"W{l}"], 2 * W, N, W, 2 * W, Df=b["hf"][l + 1], ldd=W,
+                       bias=p[f"b{l}"], resid=b["hf"][l], ldr=W, pre=Z[l + 1], act=1)
+        if store_pre:
+            _lib.check(self.lib.fvm_decoder_f32(b["hf"][L].data_ptr(), p["W_out"].data_ptr(), p["b_out"].data_ptr(),
+                                                N, self.O, b["out"].data_ptr(), s), "fvm_decoder_f32")
         return b["out"]
 
     # -- backward + optimiser --------------------------------------------------------------------
@@ -179,9 +187,9 @@ class CorrectorNet:
         b["loss"].zero_()
         _lib.check(self.lib.fvm_mse(b["out"].data_ptr(), target.data_ptr(), N * self.O, b["loss"].data_ptr(),
                                     b["dout"].data_ptr(), s), "fvm_mse")
-        _lib.check(self.lib.fvm_decoder_back(b["hb"][L].data_ptr(), p["W_out"].data_ptr(), b["dout"].data_ptr(), N,
-                                             W, self.O, b["dh"].data_ptr(), g["W_out"].data_ptr(),
-                                             g["b_out"].data_ptr(), s), "fvm_decoder_back")
+        _lib.check(self.lib.fvm_decoder_back_f32(b["hf"][L].data_ptr(), p["W_out"].data_ptr(), b["dout"].data_ptr(),
+                                                 N, self.O, b["dh"].data_ptr(), g["W_out"].data_ptr(),
+                                                 g["b_out"].data_ptr(), s), "fvm_decoder_back_f32")
         dh, dh2 = b["dh"], b["dh2"]
         splits = max(1, min(512, (Np // 64) // 8))
         for l in reversed(range(L)):
@@ -215,6 +223,20 @@ class CorrectorNet:
             _lib.check(self.lib.fvm_adam(prm.data_ptr(), self.grads[k].data_ptr(), self.m[k].data_ptr(),
                                          self.v[k].data_ptr(), prm.numel(), self.lr, beta1, beta2, eps,
                                          self.step_count, _lib.ptr(pb), _lib.ptr(pbT), rows, cols, s), "fvm_adam")
+
+    def state_dict(self) -> dict:
+        """FP32 master weights and the layer count (the Adam moments are not kept)."""
+        return {"layers": self.L, "n_out": self.O, "params": {k: v.detach().cpu().clone() for k, v in self.params.items()}}
+
+    def load_state_dict(self, d: dict):
+        if d["layers"] != self.L or d["n_out"] != self.O:
+            raise ValueError("checkpoint network shape differs")
+        for k, v in d["params"].items():
+            self.params[k].copy_(v.to(self.dev))
+        for k in self.bf:
+            self.bf[k].copy_(_bf(self.params[k]))
+        for k in self.bfT:
+            self.bfT[k].copy_(_bf(self.params[k].t()))
 
     def check_errors(self):
         if int(self.err.item()) != 0:
@@ -280,6 +302,22 @@ class CorrectorModel:
         self.scale = torch.ones(C, device=dev)
         if like is not None:
             self.fmean, self.finv, self.scale = like.fmean, like.finv, like.scale
+
+    def save(self, path: str, meta: dict | None = None):
+        """Network weights, the input / output normalisation and k (mesh-independent: a model
+        loaded onto another batch of meshes with ``load`` proposes the same way)."""
+        torch.save({"net": self.net.state_dict(), "k": self.k, "fmean": self.fmean.cpu(), "finv": self.finv.cpu(),
+                    "scale": self.scale.cpu(), "meta": meta or {}}, path)
+
+    @classmethod
+    def load(cls, path: str, batch, case_params: torch.Tensor) -> "CorrectorModel":
+        d = torch.load(path, map_location="cpu", weights_only=True)
+        m = cls(batch, case_params, k=int(d["k"]))
+        m.net.load_state_dict(d["net"])
+        dev = batch.device
+        m.fmean, m.finv, m.scale = d["fmean"].to(dev), d["finv"].to(dev), d["scale"].to(dev)
+        m.meta = d.get("meta", {})
+        return m
 
     def kdt(self) -> torch.Tensor:
         """k * dt of each cell's case, [N][1] (read from the solver's device time steps)."""

@@ -319,147 +319,6 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
                      "r"((uint32_t)(N < 32 ? 32 : N)));
 }
 
-// One message-passing layer with the neighbour mean built in shared memory (inference):
-//   D = epilogue([h_i, mean_{j in nbr(i)} h_j] . W^T),  h: bf16 [M][64], W: bf16 [64][128].
-// Thread r of the CTA stages row m0 + r of the A tile directly in the MMA's core-matrix layout:
-// K slice 0 = h_i, slice 1 = the neighbour mean, computed with the arithmetic of k_mp_gather
-// (fp32 sum over the valid neighbours in table order, times 1 / count, rounded to bf16), so the
-// result is bitwise that of fvm_mp_gather followed by fvm_gemm_bf16 -- without writing and reading
-// back the [M][128] gathered matrix.  Weights arrive by cp.async; MMA, bounded completion wait and
-// epilogue are those of k_gemm.
-constexpr int kMpW = 64;
-__global__ void __launch_bounds__(kGemmThreads) k_mp_gemm(GemmArgs g, const __nv_bfloat16* __restrict__ h,
-                                                          const int32_t* __restrict__ nbr, int KN) {
-    constexpr int N = kMpW;
-    extern __shared__ __align__(1024) uint8_t smem[];
-    constexpr int kStageBytes = TM * TK * 2 + N * TK * 2;
-    __shared__ __align__(8) uint64_t mbar;
-    __shared__ uint32_t s_taddr;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * TM;
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_taddr)),
-                     "r"((uint32_t)N));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
-        asm volatile("fence.mbarrier_init.release.cluster;");
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    const uint32_t taddr = s_taddr;
-    const uint32_t idesc = make_idesc(N);
-    const int rows_a = min(TM, g.M - m0);
-    if (threadIdx.x == 0 && g.resid && g.vec && rows_a > 0) {
-        const uint32_t bytes = (uint32_t)((int64_t)rows_a * g.ldr * 4) & ~15u;
-        if (bytes) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g.resid + (int64_t)m0 * g.ldr),
-                                "r"(bytes) : "memory");
-    }
-    // weights: both K slices
-    for (int c = 0; c < 2; ++c)
-        stage_tile_async(smem + c * kStageBytes + TM * TK * 2, g.B, g.ldb, 0, N, N, c * TK, 2 * kMpW);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    // A rows: slice 0 = own row, slice 1 = neighbour mean.  First each tile row's neighbour list
-    // and 1 / count go to shared memory; then the 128 x 8 (row, 8-channel unit) items are staged with
-    // the conflict-free lane mapping of stage_tile_async (a warp: 8 rows x 4 units), several items per
-    // thread in flight.
-    __shared__ int s_nb[TM * 8];
-    __shared__ float s_inv[TM];
-    {
-        const int r = threadIdx.x;
-        const bool valid = r < rows_a;
-        int cnt = 0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const int j = (valid && k < KN) ? __ldg(nbr + ((int64_t)m0 + r) * KN + k) : -1;
-            s_nb[r * 8 + k] = j;
-            cnt += j >= 0;
-        }
-        s_inv[r] = cnt > 0 ? 1.f / (float)cnt : 0.f;
-    }
-    __syncthreads();
-    {
-        const int slice_bytes = (TM / 8) * 256;
-#pragma unroll 2
-        for (int t = threadIdx.x; t < TM * 8; t += kGemmThreads) {
-            const int r = (t & 7) + 8 * (t >> 6), u = (t >> 3) & 7;
-            const bool valid = r < rows_a;
-            const int64_t row = (int64_t)m0 + r;
-            const int off = (u >> 1) * slice_bytes + (r >> 3) * 256 + (u & 1) * 128 + (r & 7) * 16;
-            const uint4 self = valid ? *reinterpret_cast<const uint4*>(h + row * kMpW + 8 * u) : make_uint4(0, 0, 0, 0);
-            float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int j = s_nb[r * 8 + k];
-                if (j < 0) continue;
-                const uint4 v = *reinterpret_cast<const uint4*>(h + (int64_t)j * kMpW + 8 * u);
-                const __nv_bfloat16* bv = reinterpret_cast<const __nv_bfloat16*>(&v);
-#pragma unroll
-                for (int q = 0; q < 8; ++q) acc[q] += __bfloat162float(bv[q]);
-            }
-            const float inv = s_inv[r];
-            __align__(16) __nv_bfloat16 mv[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) mv[q] = valid ? __float2bfloat16(acc[q] * inv) : __float2bfloat16(0.f);
-            *reinterpret_cast<uint4*>(smem + off) = self;
-            *reinterpret_cast<uint4*>(smem + kStageBytes + off) = *reinterpret_cast<const uint4*>(mv);
-        }
-    }
-    asm volatile("cp.async.wait_all;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        for (int c = 0; c < 2; ++c) {
-            const uint32_t sa = smem_u32(smem + c * kStageBytes), sb = sa + TM * TK * 2;
-#pragma unroll
-            for (int s = 0; s < TK / 16; ++s) {
-                const uint64_t ad = make_desc(sa + s * (TM / 8) * 256, 128, 256);
-                const uint64_t bd = make_desc(sb + s * (N / 8) * 256, 128, 256);
-                const uint32_t acc = (c > 0 || s > 0) ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "setp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(taddr),
-                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-            }
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         smem_u32(&mbar))
-                     : "memory");
-    }
-    bool done = mbar_wait(&mbar, 0u);
-    if (!done) done = mbar_wait(&mbar, 0u) && false;      // second bounded chance, then report
-    const bool ok = __syncthreads_and(done) != 0;
-    if (!ok && threadIdx.x == 0 && g.err) atomicExch(g.err, 1);
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    const int row = m0 + warp * 32 + lane;
-    if (ok) {
-#pragma unroll 1
-        for (int c0 = 0; c0 < N; c0 += 32) {
-            uint32_t r[32];
-            const uint32_t a = taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
-                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
-                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-                : "r"(a));
-            asm volatile("tcgen05.wait::ld.sync.aligned;");
-            if (row < g.M) epilogue_vec(g, row, c0, r);
-        }
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"((uint32_t)N));
-}
-
 template <int N>
 static int launch_gemm(const GemmArgs& g, cudaStream_t s) {
     // one staging buffer per K slice a CTA handles, at most two (fewer bytes: more CTAs per SM)
@@ -510,33 +369,6 @@ extern "C" int fvm_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t 
 namespace fvm {
 namespace corr {
 
-// out[i] = [h_i, mean_{j in nbr(i)} h_j]  (bf16 [N][2W]); one thread per (cell, 8-channel group).
-__global__ void k_mp_gather(const __nv_bfloat16* __restrict__ h, const int32_t* __restrict__ nbr, int N, int W, int KN,
-                            __nv_bfloat16* __restrict__ out) {
-    const int groups = W / 8;
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= (int64_t)N * groups) return;
-    const int i = (int)(t / groups), g = (int)(t % groups);
-    const uint4 self = *reinterpret_cast<const uint4*>(h + (int64_t)i * W + 8 * g);
-    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    int cnt = 0;
-    for (int k = 0; k < KN; ++k) {
-        const int j = __ldg(nbr + (int64_t)i * KN + k);
-        if (j < 0) continue;
-        const uint4 v = *reinterpret_cast<const uint4*>(h + (int64_t)j * W + 8 * g);
-        const __nv_bfloat16* b = reinterpret_cast<const __nv_bfloat16*>(&v);
-#pragma unroll
-        for (int q = 0; q < 8; ++q) acc[q] += __bfloat162float(b[q]);
-        ++cnt;
-    }
-    const float inv = cnt > 0 ? 1.f / (float)cnt : 0.f;
-    __align__(16) __nv_bfloat16 m[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) m[q] = __float2bfloat16(acc[q] * inv);
-    *reinterpret_cast<uint4*>(out + (int64_t)i * 2 * W + 8 * g) = self;
-    *reinterpret_cast<uint4*>(out + (int64_t)i * 2 * W + W + 8 * g) = *reinterpret_cast<const uint4*>(m);
-}
-
 // dh_out[i] = dh_in[i] + dA[i][:W] + sum_{j in nbr(i)} dA[j][W:] / deg(j)   (adjacency symmetric).
 __global__ void k_mp_scatter_back(const float* __restrict__ dA, const int32_t* __restrict__ nbr, int N, int W, int KN,
                                   const float* __restrict__ dh_in, float* __restrict__ dh_out) {
@@ -586,46 +418,6 @@ __global__ void k_transpose_bf16(const __nv_bfloat16* __restrict__ src, int R, i
     }
 }
 
-// out[i][o] = sum_c h[i][c] Wo[o][c] + bo[o]  (decoder, CUDA cores; O <= 8 outputs).
-__global__ void k_decoder(const __nv_bfloat16* __restrict__ h, const float* __restrict__ Wo, const float* __restrict__ bo,
-                          int N, int W, int O, float* __restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    float acc[8];
-    for (int o = 0; o < O; ++o) acc[o] = bo[o];
-    for (int c = 0; c < W; c += 8) {
-        const uint4 v = *reinterpret_cast<const uint4*>(h + (int64_t)i * W + c);
-        const __nv_bfloat16* b = reinterpret_cast<const __nv_bfloat16*>(&v);
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const float x = __bfloat162float(b[q]);
-            for (int o = 0; o < O; ++o) acc[o] = fmaf(x, Wo[o * W + c + q], acc[o]);
-        }
-    }
-    for (int o = 0; o < O; ++o) out[(int64_t)i * O + o] = acc[o];
-}
-
-// Decoder backward: dh[i][c] = sum_o dOut[i][o] Wo[o][c]; dWo[o][c] += sum_i dOut[i][o] h[i][c];
-// dbo[o] += sum_i dOut[i][o].  One thread per (cell, channel); weight gradients through atomics.
-__global__ void k_decoder_back(const __nv_bfloat16* __restrict__ h, const float* __restrict__ Wo,
-                               const float* __restrict__ dOut, int N, int W, int O, float* __restrict__ dh,
-                               float* __restrict__ dWo, float* __restrict__ dbo) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= (int64_t)N * W) return;
-    const int i = (int)(t / W), c = (int)(t % W);
-    const float x = __bfloat162float(h[t]);
-    float v = 0.f;
-    for (int o = 0; o < O; ++o) {
-        const float d = dOut[(int64_t)i * O + o];
-        v = fmaf(d, Wo[o * W + c], v);
-        atomicAdd(dWo + o * W + c, d * x);
-        if (c == 0) atomicAdd(dbo + o, d);
-    }
-    dh[t] = v;
-}
-
-// Masked mean-squared error: loss += sum (pred - tgt)^2 / n over rows with mask != 0 (mask may be
-// null); dpred = 2 (pred - tgt) / n.
 __global__ void k_mse(const float* __restrict__ pred, const float* __restrict__ tgt, int64_t n_elem, float inv_n,
                       double* __restrict__ loss, float* __restrict__ dpred) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -746,16 +538,6 @@ static inline unsigned nblk(int64_t n, int bs) { return (unsigned)((n + bs - 1) 
 }  // namespace corr
 }  // namespace fvm
 
-extern "C" int fvm_mp_gather(const void* h, const int32_t* nbr, int32_t N, int32_t W, int32_t KN, void* out,
-                             void* stream) {
-    if (!h || !nbr || !out || N <= 0 || W % 8 || KN <= 0) return FVM_E_ARG;
-    cudaStream_t s = (cudaStream_t)stream;
-    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_mp_gather<<<corr::nblk((int64_t)N * (W / 8), 256), 256, 0, s>>>(
-                                     static_cast<const __nv_bfloat16*>(h), nbr, N, W, KN,
-                                     static_cast<__nv_bfloat16*>(out)));
-    return launch_status();
-}
-
 extern "C" int fvm_mp_scatter_back(const float* dA, const int32_t* nbr, int32_t N, int32_t W, int32_t KN,
                                    const float* dh_in, float* dh_out, void* stream) {
     if (!dA || !nbr || !dh_out || N <= 0 || W <= 0 || KN <= 0) return FVM_E_ARG;
@@ -783,24 +565,6 @@ extern "C" int fvm_transpose_bf16(const void* src, int32_t R, int32_t Cc, int64_
     FVM_LAUNCH(KID_CORRECTOR, s, corr::k_transpose_bf16<<<grid, dim3(32, 8), 0, s>>>(
                                      static_cast<const __nv_bfloat16*>(src), R, Cc, lds,
                                      static_cast<__nv_bfloat16*>(dst), ldd));
-    return launch_status();
-}
-
-extern "C" int fvm_decoder(const void* h, const float* Wo, const float* bo, int32_t N, int32_t W, int32_t O,
-                           float* out, void* stream) {
-    if (!h || !Wo || !bo || !out || N <= 0 || W % 8 || O < 1 || O > 8) return FVM_E_ARG;
-    cudaStream_t s = (cudaStream_t)stream;
-    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_decoder<<<corr::nblk(N, 256), 256, 0, s>>>(
-                                     static_cast<const __nv_bfloat16*>(h), Wo, bo, N, W, O, out));
-    return launch_status();
-}
-
-extern "C" int fvm_decoder_back(const void* h, const float* Wo, const float* dOut, int32_t N, int32_t W, int32_t O,
-                                float* dh, float* dWo, float* dbo, void* stream) {
-    if (!h || !Wo || !dOut || !dh || !dWo || !dbo || N <= 0 || W <= 0 || O < 1 || O > 8) return FVM_E_ARG;
-    cudaStream_t s = (cudaStream_t)stream;
-    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_decoder_back<<<corr::nblk((int64_t)N * W, 256), 256, 0, s>>>(
-                                     static_cast<const __nv_bfloat16*>(h), Wo, dOut, N, W, O, dh, dWo, dbo));
     return launch_status();
 }
 
@@ -874,26 +638,442 @@ extern "C" int fvm_corrector_combine(const float* state, const float* base, cons
     return launch_status();
 }
 
-extern "C" int fvm_mp_gemm(const void* h, const int32_t* nbr, int32_t M, int32_t KN, const void* Wt,
-                           const float* bias, const float* resid, int64_t ldr, float* Df, void* Db, int64_t ldd,
-                           int32_t act, int32_t* err, void* stream) {
-    if (!h || !nbr || !Wt || M <= 0 || KN <= 0 || KN > 8 || (!Df && !Db) || !err) return FVM_E_ARG;
-    if ((uintptr_t)h % 16 || (uintptr_t)Wt % 16) return FVM_E_ARG;
+
+// ------------------------------------------------------------------------------------------
+// Persistent message-passing layer on an fp32 residual stream (fvm_mp_layer).
+//
+//   h'_i = h_i + SiLU([bf16(h_i), bf16(mean_{j in nbr(i)} h_j)] . W^T + b)       (W: bf16 [64][128])
+//   and, for the last layer, out_i = W_out h'_i + b_out instead of storing h'.
+//
+// One CTA per SM slot runs a grid-stride loop over 128-row tiles with three roles:
+//   * warps 0-3 (loaders): stage tile k's A operand (128 x 128 bf16, canonical no-swizzle K-major
+//     core-matrix layout, two K slices: own row, neighbour mean) into shared-memory stage k % 2;
+//     the neighbour mean is an fp32 sum over the valid neighbours in table order times 1 / count;
+//   * thread 0 (a loader) issues the tile's eight tcgen05.mma (M 128, N 64, K 16) into tensor-memory
+//     accumulator k % 2 and commits to two mbarriers: "stage free" and "accumulator full";
+//   * warps 4-7 (epilogue): read accumulator k % 2 (warp 4 + w owns TMEM lanes 32w..32w+31 = tile
+//     rows), free it for tile k + 2 (an mbarrier), add bias, SiLU, the fp32 residual and store h'
+//     (or the decoder's outputs) with 256-bit accesses.
+// So the gathers of tile k + 1, the MMAs of tile k and the epilogue of tile k - 1 overlap.  The
+// weights stay in shared memory for the whole launch.  Every mbarrier wait is bounded; a wait that
+// gives up sets *err and ends the role's loop, and the final MMA wait is bounded too, so the kernel
+// always returns and frees its tensor memory.
+// ------------------------------------------------------------------------------------------
+namespace fvm {
+namespace corr {
+
+constexpr int kLayerThreads = 256;
+constexpr int kLayerW = 64;                              // channels
+constexpr int kLayerStageBytes = 2 * TM * TK * 2;        // two K slices of 128 x 64 bf16
+constexpr int kLayerWBytes = kLayerW * 2 * kLayerW * 2;  // W: 64 x 128 bf16
+constexpr int kLayerSmem = kLayerWBytes + 2 * kLayerStageBytes + 1024;
+
+struct LayerArgs {
+    const float* h;              // [M][64] fp32 residual stream (input)
+    const int32_t* nbr;          // [M][KN]
+    int M, KN;
+    const __nv_bfloat16* Wt;     // [64][128]
+    const float* bias;           // [64]
+    float* h_out;                // [M][64] or null (decoder only)
+    const float* Wo;             // [O][64] decoder weights or null
+    const float* bo;             // [O]
+    int O;
+    float* out;                  // [M][O] decoder outputs or null
+    int* err;
+};
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void loader_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+// Named barrier of the 128 loader threads that also returns whether any of them passed v != 0,
+// so every loader takes the same branch afterwards.
+__device__ __forceinline__ int loader_sync_or(int v) {
+    int r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.b32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, 1, 128, p;\n\t"
+        "selp.b32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"(v)
+        : "memory");
+    return r;
+}
+
+// 32 accumulator columns [c0, c0 + 32) of this warp's TMEM lanes.
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(addr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Stage rows [m0, m0 + 128) of tile into the two K slices at sA (own row, neighbour mean), bf16.
+// Loader thread lt (0..127) handles the 8-channel units u = (lt >> 3) & 7 of rows
+// (lt & 7) + 8 * (lt >> 6) + 16 q, q = 0..7: a warp covers 8 rows x 4 units per q, so its 16-byte
+// shared-memory stores hit all 32 banks once per 8 lanes and its global reads are 128-byte row
+// segments.
+__device__ __forceinline__ void stage_layer_tile(uint8_t* sA, const LayerArgs& g, int m0, const int* s_nb,
+                                                 const float* s_inv, int lt) {
+    const int u = (lt >> 3) & 7;
+    const int slice_bytes = (TM / 8) * 256;
+#pragma unroll 2
+    for (int q = 0; q < 8; ++q) {
+        const int r = (lt & 7) + 8 * (lt >> 6) + 16 * q;
+        const int64_t row = (int64_t)m0 + r;
+        const bool valid = row < g.M;
+        float own[8], acc[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) own[e] = acc[e] = 0.f;
+        if (valid) {
+            ld8(g.h + row * kLayerW + 8 * u, own);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                if (k >= g.KN) break;
+                const int j = s_nb[r * 8 + k];
+                if (j < 0) continue;
+                float v[8];
+                ld8(g.h + (int64_t)j * kLayerW + 8 * u, v);
+#pragma unroll
+                for (int e = 0; e < 8; ++e) acc[e] += v[e];
+            }
+        }
+        const float inv = s_inv[r];
+        __align__(16) __nv_bfloat16 a[8], b[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            a[e] = __float2bfloat16(own[e]);
+            b[e] = __float2bfloat16(acc[e] * inv);
+        }
+        const int off = (u >> 1) * slice_bytes + (r >> 3) * 256 + (u & 1) * 128 + (r & 7) * 16;
+        *reinterpret_cast<uint4*>(sA + off) = *reinterpret_cast<const uint4*>(a);
+        *reinterpret_cast<uint4*>(sA + TM * TK * 2 + off) = *reinterpret_cast<const uint4*>(b);
+    }
+}
+
+__global__ void __launch_bounds__(kLayerThreads, 1) k_mp_layer(LayerArgs g) {
+    extern __shared__ __align__(1024) uint8_t dsmem[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)dsmem + 1023) & ~(uintptr_t)1023);
+    uint8_t* sW = smem;                                   // B operand, both K slices
+    uint8_t* sStage = smem + kLayerWBytes;                // two stages of A
+    __shared__ __align__(8) uint64_t bar_free[2], bar_full[2], bar_empty[2];
+    __shared__ uint32_t s_taddr;
+    __shared__ int s_nb[TM * 8];
+    __shared__ float s_inv[TM];
+    __shared__ float s_bias[kLayerW];
+    __shared__ float s_wo[8 * kLayerW];
+    __shared__ int s_fail;
+    __shared__ int s_last;                                // last local tile whose MMAs were issued
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntiles = (g.M + TM - 1) / TM;
+    const int nlocal = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_taddr)),
+                     "r"(128u));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&bar_free[b], 1);
+            mbar_init(&bar_full[b], 1);
+            mbar_init(&bar_empty[b], 4);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;");
+        s_fail = 0;
+        s_last = -1;
+    }
+    // weights into the B-operand layout (both K slices), bias and decoder weights
+    for (int t = threadIdx.x; t < 2 * kLayerW * 8; t += blockDim.x) {
+        const int c = t / (kLayerW * 8), rem = t % (kLayerW * 8);
+        const int r = rem >> 3, u = rem & 7;
+        const uint4 v = *reinterpret_cast<const uint4*>(g.Wt + (int64_t)r * 2 * kLayerW + c * TK + 8 * u);
+        const int off = c * (kLayerW * TK * 2) + (u >> 1) * ((kLayerW / 8) * 256) + (r >> 3) * 256 + (u & 1) * 128 +
+                        (r & 7) * 16;
+        *reinterpret_cast<uint4*>(sW + off) = v;
+    }
+    for (int t = threadIdx.x; t < kLayerW; t += blockDim.x) s_bias[t] = g.bias[t];
+    if (g.out)
+        for (int t = threadIdx.x; t < g.O * kLayerW; t += blockDim.x) s_wo[t] = g.Wo[t];
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t taddr = s_taddr;
+    const uint32_t idesc = make_idesc(kLayerW);
+
+    if (warp < 4) {
+        // ---- loaders (and, thread 0, the MMA issuer) ----
+        // Every decision to stop is taken together (loader_sync_or), so no loader is left waiting
+        // at a named barrier: a loader's own bounded wait that gave up, or thread 0's, counts.
+        const int lt = threadIdx.x;
+        int fail = 0;
+        for (int k = 0; k < nlocal; ++k) {
+            const int tile = (int)blockIdx.x + k * (int)gridDim.x;
+            const int m0 = tile * TM, s = k & 1;
+            uint8_t* sA = sStage + s * kLayerStageBytes;
+            if (k >= 2 && !fail)   // the MMAs of tile k - 2 read this stage
+                fail = !mbar_wait(&bar_free[s], (uint32_t)(((k >> 1) - 1) & 1));
+            // this tile's neighbour lists (every loader finished reading the last ones before the
+            // previous loader_sync)
+            {
+                const int64_t row = (int64_t)m0 + lt;
+                int cnt = 0;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int j = (row < g.M && q < g.KN) ? __ldg(g.nbr + row * g.KN + q) : -1;
+                    s_nb[lt * 8 + q] = j;
+                    cnt += j >= 0;
+                }
+                s_inv[lt] = cnt > 0 ? 1.f / (float)cnt : 0.f;
+            }
+            fail = loader_sync_or(fail);
+            if (fail) break;
+            stage_layer_tile(sA, g, m0, s_nb, s_inv, lt);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            loader_sync();
+            if (lt == 0) {
+                const int a = k & 1;
+                if (k >= 2) fail = !mbar_wait(&bar_empty[a], (uint32_t)(((k >> 1) - 1) & 1));
+                if (!fail) {
+                    asm volatile("tcgen05.fence::after_thread_sync;");
+                    const uint32_t d = taddr + (uint32_t)(a * kLayerW);
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        const uint32_t sa = smem_u32(sA + c * TM * TK * 2);
+                        const uint32_t sb = smem_u32(sW + c * kLayerW * TK * 2);
+#pragma unroll
+                        for (int q = 0; q < TK / 16; ++q) {
+                            const uint64_t ad = make_desc(sa + q * (TM / 8) * 256, 128, 256);
+                            const uint64_t bd = make_desc(sb + q * (kLayerW / 8) * 256, 128, 256);
+                            const uint32_t acc = (c > 0 || q > 0) ? 1u : 0u;
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\t"
+                                "setp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                                    d),
+                                "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+                        }
+                    }
+                    tc_commit(&bar_free[s]);
+                    tc_commit(&bar_full[a]);
+                    s_last = k;
+                }
+            }
+        }
+        if (fail) atomicExch(&s_fail, 1);
+    } else {
+        // ---- epilogue ----
+        const int we = warp - 4;                          // TMEM lane quarter = warp % 4
+        for (int k = 0; k < nlocal; ++k) {
+            const int tile = (int)blockIdx.x + k * (int)gridDim.x;
+            const int a = k & 1;
+            bool ok = mbar_wait(&bar_full[a], (uint32_t)((k >> 1) & 1));
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) atomicExch(&s_fail, 1);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const int64_t row = (int64_t)tile * TM + 32 * we + lane;
+            const uint32_t base = taddr + ((uint32_t)(32 * we) << 16) + (uint32_t)(a * kLayerW);
+            uint32_t r0[32], r1[32];
+            tmem_ld32(base, r0);
+            tmem_ld32(base + 32, r1);
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bar_empty[a]);   // accumulator a may take tile k + 2
+            if (row < g.M) {
+                float dec[8];
+#pragma unroll
+                for (int o = 0; o < 8; ++o) dec[o] = (g.out && o < g.O) ? __ldg(g.bo + o) : 0.f;
+#pragma unroll
+                for (int half = 0; half < 2; ++half) {
+                    const uint32_t* r = half ? r1 : r0;
+                    const int c0 = 32 * half;
+                    float v[32], x[32];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) ld8(g.h + row * kLayerW + c0 + 8 * q, x + 8 * q);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) v[j] = silu(__uint_as_float(r[j]) + s_bias[c0 + j]) + x[j];
+                    if (g.h_out)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) st8(g.h_out + row * kLayerW + c0 + 8 * q, v + 8 * q);
+                    if (g.out) {
+#pragma unroll
+                        for (int o = 0; o < 8; ++o) {
+                            if (o < g.O) {
+#pragma unroll
+                                for (int j = 0; j < 32; ++j)
+                                    dec[o] = fmaf(v[j], s_wo[o * kLayerW + c0 + j], dec[o]);
+                            }
+                        }
+                    }
+                }
+                if (g.out)
+#pragma unroll
+                    for (int o = 0; o < 8; ++o)
+                        if (o < g.O) g.out[row * g.O + o] = dec[o];
+            }
+        }
+    }
+    // All MMAs of this CTA have completed once the last accumulator was read.  If a role gave up,
+    // wait (bounded) for the commit of the last tile whose MMAs were issued (one thread issued them
+    // in order, so they complete in order) before the tensor memory is released.
+    __syncthreads();
+    if (s_fail && threadIdx.x == 0) {
+        const int k = s_last;
+        if (k >= 0) mbar_wait(&bar_full[k & 1], (uint32_t)((k >> 1) & 1));
+        if (g.err) atomicExch(g.err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(128u));
+}
+
+// Training-path gather with the fused layer's arithmetic: out[i] = [bf16(h_i), bf16(mean_j h_j)]
+// from the fp32 residual stream (mean = fp32 sum over the valid neighbours in table order times
+// 1 / count); bf16 [N][128].  One thread per (cell, 8-channel unit).
+__global__ void k_mp_gather_f32(const float* __restrict__ h, const int32_t* __restrict__ nbr, int N, int KN,
+                                __nv_bfloat16* __restrict__ out) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)N * 8) return;
+    const int i = (int)(t >> 3), u = (int)(t & 7);
+    float own[8], acc[8];
+    ld8(h + (int64_t)i * kLayerW + 8 * u, own);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) acc[e] = 0.f;
+    int cnt = 0;
+    for (int k = 0; k < KN; ++k) {
+        const int j = __ldg(nbr + (int64_t)i * KN + k);
+        cnt += j >= 0;
+    }
+    const float inv = cnt > 0 ? 1.f / (float)cnt : 0.f;
+    for (int k = 0; k < KN && k < 8; ++k) {
+        const int j = __ldg(nbr + (int64_t)i * KN + k);
+        if (j < 0) continue;
+        float v[8];
+        ld8(h + (int64_t)j * kLayerW + 8 * u, v);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) acc[e] += v[e];
+    }
+    __align__(16) __nv_bfloat16 a[8], b[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        a[e] = __float2bfloat16(own[e]);
+        b[e] = __float2bfloat16(acc[e] * inv);
+    }
+    *reinterpret_cast<uint4*>(out + (int64_t)i * 2 * kLayerW + 8 * u) = *reinterpret_cast<const uint4*>(a);
+    *reinterpret_cast<uint4*>(out + (int64_t)i * 2 * kLayerW + kLayerW + 8 * u) = *reinterpret_cast<const uint4*>(b);
+}
+
+// Decoder on the fp32 stream with the fused layer's order: out[i][o] = b[o] + sum_c h[i][c] Wo[o][c]
+// (fp32 fma over c ascending).
+__global__ void k_decoder_f32(const float* __restrict__ h, const float* __restrict__ Wo, const float* __restrict__ bo,
+                              int N, int O, float* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float acc[8];
+#pragma unroll
+    for (int o = 0; o < 8; ++o) acc[o] = o < O ? bo[o] : 0.f;
+    for (int c0 = 0; c0 < kLayerW; c0 += 8) {
+        float x[8];
+        ld8(h + (int64_t)i * kLayerW + c0, x);
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+#pragma unroll
+            for (int o = 0; o < 8; ++o)
+                if (o < O) acc[o] = fmaf(x[e], Wo[o * kLayerW + c0 + e], acc[o]);
+    }
+    for (int o = 0; o < O; ++o) out[(int64_t)i * O + o] = acc[o];
+}
+
+// Decoder backward on the fp32 stream: dh[i][c] = sum_o dOut[i][o] Wo[o][c];
+// dWo[o][c] += sum_i dOut[i][o] h[i][c]; dbo[o] += sum_i dOut[i][o].
+__global__ void k_decoder_back_f32(const float* __restrict__ h, const float* __restrict__ Wo,
+                                   const float* __restrict__ dOut, int N, int O, float* __restrict__ dh,
+                                   float* __restrict__ dWo, float* __restrict__ dbo) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)N * kLayerW) return;
+    const int i = (int)(t / kLayerW), c = (int)(t % kLayerW);
+    const float x = h[t];
+    float v = 0.f;
+    for (int o = 0; o < O; ++o) {
+        const float d = dOut[(int64_t)i * O + o];
+        v = fmaf(d, Wo[o * kLayerW + c], v);
+        atomicAdd(dWo + o * kLayerW + c, d * x);
+        if (c == 0) atomicAdd(dbo + o, d);
+    }
+    dh[t] = v;
+}
+
+}  // namespace corr
+}  // namespace fvm
+
+extern "C" int fvm_mp_layer(const float* h, const int32_t* nbr, int32_t M, int32_t KN, const void* Wt,
+                            const float* bias, float* h_out, const float* Wo, const float* bo, int32_t O, float* out,
+                            int32_t* err, void* stream) {
+    if (!h || !nbr || !Wt || !bias || M <= 0 || KN <= 0 || KN > 8 || !err) return FVM_E_ARG;
+    if (!h_out && !out) return FVM_E_ARG;
+    if (out && (!Wo || !bo || O < 1 || O > 8)) return FVM_E_ARG;
     auto a32 = [](const void* p) { return ((uintptr_t)p & 31u) == 0; };
-    const bool vec = a32(bias) && a32(resid) && a32(Df) && a32(Db) && (!resid || ldr % 8 == 0) &&
-                     (!Df || ldd % 8 == 0) && (!Db || ldd % 16 == 0);
-    if (!vec) return FVM_E_ARG;                              // the fused layer has only the 256-bit epilogue
-    corr::GemmArgs g{nullptr, 0, static_cast<const __nv_bfloat16*>(Wt), 2 * corr::kMpW, M, corr::kMpW,
-                     2 * corr::kMpW, 1, bias, resid, ldr, Df, static_cast<__nv_bfloat16*>(Db), ldd, nullptr, act,
-                     err, 1};
-    const size_t smem = 2 * ((size_t)corr::TM * corr::TK * 2 + (size_t)corr::kMpW * corr::TK * 2);
+    if (!a32(h) || !a32(h_out) || (uintptr_t)Wt % 16) return FVM_E_ARG;
+    if (h_out == h) return FVM_E_ARG;                    // the neighbours of later tiles read h
+    static int sms = 0;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(corr::k_mp_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaFuncSetAttribute(corr::k_mp_layer, cudaFuncAttributeMaxDynamicSharedMemorySize, corr::kLayerSmem) !=
+                cudaSuccess) {
+            launch_status();
+            return FVM_E_CUDA;
+        }
         attr = true;
     }
+    const int ntiles = (M + corr::TM - 1) / corr::TM;
+    const unsigned grid = (unsigned)std::min(ntiles, sms);
+    corr::LayerArgs g{h, nbr, M, KN, static_cast<const __nv_bfloat16*>(Wt), bias, h_out, Wo, bo, O, out, err};
     cudaStream_t s = (cudaStream_t)stream;
-    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_mp_gemm<<<(unsigned)((M + corr::TM - 1) / corr::TM), corr::kGemmThreads,
-                                                   smem, s>>>(g, static_cast<const __nv_bfloat16*>(h), nbr, KN));
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_mp_layer<<<grid, corr::kLayerThreads, corr::kLayerSmem, s>>>(g));
+    return launch_status();
+}
+
+extern "C" int fvm_mp_gather_f32(const float* h, const int32_t* nbr, int32_t N, int32_t KN, void* out, void* stream) {
+    if (!h || !nbr || !out || N <= 0 || KN <= 0 || KN > 8 || ((uintptr_t)h & 31u) || ((uintptr_t)out & 15u))
+        return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_mp_gather_f32<<<corr::nblk((int64_t)N * 8, 256), 256, 0, s>>>(
+                                     h, nbr, N, KN, static_cast<__nv_bfloat16*>(out)));
+    return launch_status();
+}
+
+extern "C" int fvm_decoder_f32(const float* h, const float* Wo, const float* bo, int32_t N, int32_t O, float* out,
+                               void* stream) {
+    if (!h || !Wo || !bo || !out || N <= 0 || O < 1 || O > 8 || ((uintptr_t)h & 31u)) return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_decoder_f32<<<corr::nblk(N, 256), 256, 0, s>>>(h, Wo, bo, N, O, out));
+    return launch_status();
+}
+
+extern "C" int fvm_decoder_back_f32(const float* h, const float* Wo, const float* dOut, int32_t N, int32_t O,
+                                    float* dh, float* dWo, float* dbo, void* stream) {
+    if (!h || !Wo || !dOut || !dh || !dWo || !dbo || N <= 0 || O < 1 || O > 8) return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_decoder_back_f32<<<corr::nblk((int64_t)N * corr::kLayerW, 256), 256, 0, s>>>(
+                                     h, Wo, dOut, N, O, dh, dWo, dbo));
     return launch_status();
 }

@@ -44,6 +44,7 @@ constexpr int kMaxBlock = 512;   // largest block size the autotuner may pick
 struct Phys {
     float T_0, mu, mu_b, S, C_v, gamma, kappa, v_factor;
     float R, gR, inv_Cv, T0pS, T0sq;  // derived, rounded to float as the reference's scalars are
+    float inv_T0, inv_T0sq;           // 1 / T_0 and 1 / T_0^2, for the facet kernel's transport terms
     int lim_p;
 };
 
@@ -209,6 +210,18 @@ __device__ __forceinline__ void next_cols(const fvm_mesh_t& m, int i, int NA, in
 }
 
 
+// n / d with the fast-division intrinsic (__fdividef, within 2 ulp where 2^-126 <= |d| <= 2^126).
+// Denominators outside [2^-100, 2^100] have both operands scaled by an exact power of two first,
+// so the intrinsic always sees a denominator inside its range.  The limiter and facet kernels use
+// it in place of IEEE division: their quotients then differ from correctly rounded ones by at most
+// 2 ulp (relative 2.4e-7), far inside the 1e-5 parity bar, and a limiter evaluation costs about a
+// third of its former instructions.
+__device__ __forceinline__ float fast_div(float n, float d) {
+    const float ad = fabsf(d);
+    const float s = ad < 0x1p-100f ? 0x1p64f : (ad > 0x1p100f ? 0x1p-64f : 1.f);
+    return __fdividef(n * s, d * s);
+}
+
 // ------------------------------------------------------------------------------------------
 // Slope limiters (limiter.py:29-77).  delta: allowed range, dU: unlimited increment.
 // ------------------------------------------------------------------------------------------
@@ -218,20 +231,20 @@ __device__ __forceinline__ float limiter_phi(int p, float delta, float dU, float
         const float a2 = a * a;
         const float a_eps = a2 * a2 + eps;
         const float S = b2 * fmaf(b2, b2 - a, a2);
-        const float phi = fmaf(a, S, a_eps) / fmaf(b, delta * delta * delta + S, a_eps);
+        const float phi = fast_div(fmaf(a, S, a_eps), fmaf(b, delta * delta * delta + S, a_eps));
         return a < b2 ? phi : 1.f;
     }
     if (p == 1) {
         const float s = 2.f * ((dU > 0.f ? 1.f : 0.f) - 0.5f) * (fabsf(dU) + 1e-8f);
-        return fminf(fmaxf(delta / s, 0.f), 1.f);
+        return fminf(fmaxf(fast_div(delta, s), 0.f), 1.f);
     }
     if (p == 2) {
-        return (delta * delta + eps + 2.f * delta * dU) / (delta * delta + 2.f * dU * dU + delta * dU + eps);
+        return fast_div(delta * delta + eps + 2.f * delta * dU, delta * delta + 2.f * dU * dU + delta * dU + eps);
     }
     const float a = fabsf(delta), b = fabsf(dU);
     if (p == 3) {
         const float a_eps = a * a * a + eps, S = 4.f * b * b;
-        const float phi = (a_eps + a * S) / (a_eps + b * (delta * delta + S));
+        const float phi = fast_div(a_eps + a * S, a_eps + b * (delta * delta + S));
         return a < 2.f * b ? phi : 1.f;
     }
     // p == 5
@@ -239,7 +252,7 @@ __device__ __forceinline__ float limiter_phi(int p, float delta, float dU, float
     const float a_eps = a2 * a2 * a + eps;
     const float S = 8.f * b * b * (a2 - 2.f * b * (a - b));
     const float d2 = delta * delta;
-    const float phi = (a_eps + a * S) / (a_eps + b * (d2 * d2 + S));
+    const float phi = fast_div(a_eps + a * S, a_eps + b * (d2 * d2 + S));
     return a < 2.f * b ? phi : 1.f;
 }
 
@@ -514,11 +527,12 @@ __device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, co
     ld_vec<Ly::FR>(m.face_rec + (int64_t)f * Ly::FR, rec);
     nxt = next_codes<DIM>(m, f + stride, nF, skip_frozen);
     const float size = rec[Ly::SIZE];
+    const float inv_size = 1.f / size;
     float n[DIM], nh[DIM];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
         n[d] = rec[Ly::NRM + d];
-        nh[d] = n[d] / size;
+        nh[d] = n[d] * inv_size;
     }
     float UL[RS], UR[RS];
 #pragma unroll
@@ -624,8 +638,10 @@ __device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, co
 #pragma unroll
         for (int c = 0; c < DIM; ++c) D[a][c] = 0.5f * (gF[a][c] + gF[c][a]);
     const float I1 = D[0][0] + D[1][1];
-    const float mu = mu0 * powf(Tm / p.T_0, 1.5f) * p.T0pS / (Tm + p.S);
-    const float mub = mub0 * (Tm * Tm) / p.T0sq;
+    // Sutherland: mu0 (Tm / T_0)^1.5 (T_0 + S) / (Tm + S), the power as q sqrt(q)
+    const float q = Tm * p.inv_T0;
+    const float mu = fast_div(mu0 * (q * sqrtf(q)) * p.T0pS, Tm + p.S);
+    const float mub = mub0 * (Tm * Tm) * p.inv_T0sq;
     const float a0 = -mub * I1, a1 = -2.f * mu;
     float tau[DIM][DIM];
 #pragma unroll
@@ -667,7 +683,7 @@ __device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, co
     // Kurganov-Tadmor diffusion (fvm_equation.py:337-368)
     const float vmax = fmaxf(sqrtf(vm2[0]), sqrtf(vm2[1]));
     const float cmax = fmaxf(cs[0], cs[1]);
-    const float M = fabsf(vmax / (cmax + 1e-8f));
+    const float M = fabsf(fast_div(vmax, cmax + 1e-8f));
     const float vf = fminf(fmaxf(M, p.v_factor), 1.f);
     const float a_vel = vf * cmax + vmax, a_oth = cmax + vmax;
 #pragma unroll
@@ -1256,6 +1272,8 @@ static Phys make_phys(const fvm_physics_t* ph) {
     p.inv_Cv = (float)(1.0 / (double)ph->C_v);
     p.T0pS = (float)((double)ph->T_0 + (double)ph->S_const);
     p.T0sq = (float)((double)ph->T_0 * (double)ph->T_0);
+    p.inv_T0 = (float)(1.0 / (double)ph->T_0);
+    p.inv_T0sq = (float)(1.0 / ((double)ph->T_0 * (double)ph->T_0));
     return p;
 }
 

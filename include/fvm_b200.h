@@ -298,18 +298,21 @@ int fvm_gemm_bf16(const void *A, int64_t lda, const void *B, int64_t ldb, int32_
                   int32_t k_splits, const float *bias, const float *resid, int64_t ldr, float *Df, void *Db,
                   int64_t ldd, float *preact, int32_t act, int32_t *err, void *stream);
 
-/* Corrector kernels (no reference counterpart).  Activations are bf16 [N][W] (W % 8 == 0, rows
- * 16-byte aligned); nbr is an int32 [N][KN] neighbour table (-1 = none, adjacency symmetric). */
-/* A message-passing layer in one kernel (W = 64): D = epilogue([h_i, mean_{j in nbr(i)} h_j] . Wt^T)
- * with Wt bf16 [64][128] (K-major), epilogue as fvm_gemm_bf16 (bias, SiLU if act = 1, residual add,
- * fp32 Df and/or bf16 Db [M][ldd]); the gathered [M][128] matrix is built in shared memory and never
- * stored.  Bitwise equal to fvm_mp_gather + fvm_gemm_bf16.  KN <= 8; bias/resid/Df/Db 32-byte
- * aligned with ldr, ldd multiples of 8 (16 for Db). */
-int fvm_mp_gemm(const void *h, const int32_t *nbr, int32_t M, int32_t KN, const void *Wt, const float *bias,
-                const float *resid, int64_t ldr, float *Df, void *Db, int64_t ldd, int32_t act, int32_t *err,
-                void *stream);
-/* out[i] = [h_i, mean_{j in nbr(i)} h_j]  (bf16 [N][2W]). */
-int fvm_mp_gather(const void *h, const int32_t *nbr, int32_t N, int32_t W, int32_t KN, void *out, void *stream);
+/* Corrector kernels (no reference counterpart).  The network's activations are an fp32 residual
+ * stream h [N][64] (rows 32-byte aligned); GEMM operands are bf16; nbr is an int32 [N][KN] neighbour
+ * table (-1 = none, adjacency symmetric, KN <= 8). */
+/* One message-passing layer in one persistent kernel (inference):
+ *   h_out_i = h_i + SiLU([bf16(h_i), bf16(mean_{j in nbr(i)} h_j)] . Wt^T + bias)
+ * with Wt bf16 [64][128] (K-major); the mean is an fp32 sum over the valid neighbours in table
+ * order times 1 / count.  With out != NULL (the last layer) the decoder is applied in the
+ * epilogue instead: out_i[o] = bo[o] + sum_c h_out_i[c] Wo[o][c] (fp32 fma over c ascending, O <= 8
+ * outputs, Wo fp32 [O][64]) and h_out may be NULL.  Bitwise equal to fvm_mp_gather_f32 +
+ * fvm_gemm_bf16 (bias, SiLU, residual h) + fvm_decoder_f32.  h_out must not alias h.  A bounded
+ * mbarrier wait that gives up sets *err (results invalid). */
+int fvm_mp_layer(const float *h, const int32_t *nbr, int32_t M, int32_t KN, const void *Wt, const float *bias,
+                 float *h_out, const float *Wo, const float *bo, int32_t O, float *out, int32_t *err, void *stream);
+/* out[i] = [bf16(h_i), bf16(mean_{j in nbr(i)} h_j)]  (bf16 [N][128]) from the fp32 stream. */
+int fvm_mp_gather_f32(const float *h, const int32_t *nbr, int32_t N, int32_t KN, void *out, void *stream);
 /* dh_out[i] = dh_in[i] + dA[i][:W] + sum_{j in nbr(i)} dA[j][W:] / deg(j)  (fp32; dh_in may be NULL). */
 int fvm_mp_scatter_back(const float *dA, const int32_t *nbr, int32_t N, int32_t W, int32_t KN, const float *dh_in,
                         float *dh_out, void *stream);
@@ -318,12 +321,11 @@ int fvm_silu_back(const float *dh, const float *Z, int32_t N, int32_t W, void *d
                   void *stream);
 /* dst[c][r] = src[r][c] for a bf16 [R][Cc] matrix (leading dimensions lds, ldd). */
 int fvm_transpose_bf16(const void *src, int32_t R, int32_t Cc, int64_t lds, void *dst, int64_t ldd, void *stream);
-/* out[i][o] = h[i] . Wo[o] + bo[o] for O <= 8 outputs (h bf16, Wo fp32 [O][W]). */
-int fvm_decoder(const void *h, const float *Wo, const float *bo, int32_t N, int32_t W, int32_t O, float *out,
-                void *stream);
-/* Decoder backward: dh = dOut Wo; dWo += dOut^T h; dbo += column sums of dOut. */
-int fvm_decoder_back(const void *h, const float *Wo, const float *dOut, int32_t N, int32_t W, int32_t O, float *dh,
-                     float *dWo, float *dbo, void *stream);
+/* out[i][o] = bo[o] + sum_c h[i][c] Wo[o][c] (fp32 fma over c ascending; h fp32 [N][64], O <= 8). */
+int fvm_decoder_f32(const float *h, const float *Wo, const float *bo, int32_t N, int32_t O, float *out, void *stream);
+/* Decoder backward: dh = dOut Wo; dWo += dOut^T h; dbo += column sums of dOut (h fp32 [N][64]). */
+int fvm_decoder_back_f32(const float *h, const float *Wo, const float *dOut, int32_t N, int32_t O, float *dh,
+                         float *dWo, float *dbo, void *stream);
 /* loss[0] += mean((pred - tgt)^2) over n_elem values (FP64); dpred = 2 (pred - tgt) / n_elem. */
 int fvm_mse(const float *pred, const float *tgt, int64_t n_elem, double *loss, float *dpred, void *stream);
 /* Adam on fp32 master weights p with gradient g (zeroed afterwards), moments m, v; step >= 1.

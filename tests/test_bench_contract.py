@@ -37,7 +37,10 @@ def test_reference_arm_other_ranks_do_nothing():
 
 
 def test_single_gpu_workloads_refuse_several_ranks():
+    """The channel and corrector workloads run on one GPU; under several ranks they exit with an
+    error instead of all running on GPU 0 (the ensemble and the default box shard instead)."""
     env = dict(os.environ, RANK="0", WORLD_SIZE="2")
-    r = subprocess.run([sys.executable, "bench.py", "--workload", "ensemble"], cwd=ROOT, env=env,
-                       capture_output=True, text=True, timeout=300)
-    assert r.returncode != 0 and "runs on one GPU" in r.stderr
+    for w in ("channel_cylinder", "corrector"):
+        r = subprocess.run([sys.executable, "bench.py", "--workload", w], cwd=ROOT, env=env,
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode != 0 and "runs on one GPU" in r.stderr

@@ -1,7 +1,7 @@
 """Corrector network: hand-written forward/backward vs torch autograd, training, checked rollout.
 
 The torch reference rounds to bf16 exactly where the CUDA path does (GEMM operands: features,
-activations, weights) and accumulates in fp32, so forward outputs agree to ~1e-3 relative and
+the fp32 activations and their neighbour mean, weights) and accumulates in fp32, so forward outputs agree to ~1e-3 relative and
 weight gradients to ~1e-2 relative (bf16 rounding of the backward operands dZ and A).
 Needs a B200.
 """
@@ -45,13 +45,13 @@ def _torch_reference(net, X, nbr, target, N):
     nb = nbr.long()
     valid = (nb >= 0)
     for l in range(net.L):
-        hb = bf(h)
-        gathered = torch.where(valid.unsqueeze(-1), hb[nb.clamp(min=0)], torch.zeros(()).cuda())
+        # the neighbour mean of the fp32 stream, then both halves of the GEMM operand in bf16
+        gathered = torch.where(valid.unsqueeze(-1), h[nb.clamp(min=0)], torch.zeros(()).cuda())
         mean = gathered.sum(1) / valid.sum(1, keepdim=True).clamp(min=1)
-        A = torch.cat([hb, bf(mean)], 1)
+        A = torch.cat([bf(h), bf(mean)], 1)
         z = A @ bf(P[f"W{l}"]).t() + P[f"b{l}"]
         h = h + torch.nn.functional.silu(z)
-    out = bf(h) @ P["W_out"].t() + P["b_out"]
+    out = h @ P["W_out"].t() + P["b_out"]
     loss = ((out - target) ** 2).mean()
     loss.backward()
     return out.detach(), loss.detach(), {k: v.grad for k, v in P.items()}
@@ -70,7 +70,8 @@ def test_forward_backward_vs_autograd(small_batch):
     ref_out, ref_loss, ref_g = _torch_reference(model.net, X, model.nbr, target, N)
     out = model.net.forward(model.nbr).clone()
     assert rel_l2(out.cpu().numpy(), ref_out.cpu().numpy()) < 2e-3
-    # inference builds the neighbour mean inside the GEMM: bitwise the same output
+    # inference runs one persistent fused kernel per layer (neighbour mean in shared memory, the
+    # decoder in the last layer's epilogue): bitwise the same output
     assert torch.equal(model.net.forward(model.nbr, store_pre=False), out)
     grads_before = {k: v.clone() for k, v in model.net.grads.items()}
     assert all(float(v.abs().max()) == 0.0 for v in grads_before.values())
@@ -157,3 +158,51 @@ def test_corrector_3d_sphere_batch():
     for _ in range(2):
         assert ro.window().shape == (2,)
     assert torch.isfinite(batch.cells.state).all()
+
+
+@pytest.mark.parametrize("N,KN", [(1000, 4), (77, 3), (300_001, 4)])
+def test_fused_layer_matches_separate_kernels(N, KN):
+    """fvm_mp_layer (persistent: loader warps, tcgen05 MMA, epilogue warps, two stages) against
+    fvm_mp_gather_f32 + fvm_gemm_bf16 + fvm_decoder_f32: bitwise, on a ragged last tile, a single
+    partial tile and enough tiles that every CTA cycles its stages and accumulators many times."""
+    if not torch.cuda.is_available():
+        pytest.skip("needs CUDA")
+    from fvm_solver_b200 import _lib
+    lib = _lib.load()
+    g = torch.Generator(device="cuda").manual_seed(N + KN)
+    h = torch.randn(N, 64, device="cuda", generator=g)
+    nbr = torch.randint(-1, N, (N, KN), device="cuda", generator=g, dtype=torch.int32)
+    Wt = (0.1 * torch.randn(64, 128, device="cuda", generator=g)).to(torch.bfloat16).contiguous()
+    bias = torch.randn(64, device="cuda", generator=g)
+    Wo = torch.randn(5, 64, device="cuda", generator=g)
+    bo = torch.randn(5, device="cuda", generator=g)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    s = _lib.stream_ptr()
+    # separate kernels
+    A = torch.empty(N, 128, dtype=torch.bfloat16, device="cuda")
+    _lib.check(lib.fvm_mp_gather_f32(h.data_ptr(), nbr.data_ptr(), N, KN, A.data_ptr(), s), "gather")
+    want = torch.empty(N, 64, device="cuda")
+    _lib.check(lib.fvm_gemm_bf16(A.data_ptr(), 128, Wt.data_ptr(), 128, N, 64, 128, 1, bias.data_ptr(), h.data_ptr(),
+                                 64, want.data_ptr(), None, 64, None, 1, err.data_ptr(), s), "gemm")
+    want_out = torch.empty(N, 5, device="cuda")
+    _lib.check(lib.fvm_decoder_f32(want.data_ptr(), Wo.data_ptr(), bo.data_ptr(), N, 5, want_out.data_ptr(), s), "dec")
+    # fused layer: h_out, then the decoder form
+    got = torch.full((N, 64), float("nan"), device="cuda")
+    _lib.check(lib.fvm_mp_layer(h.data_ptr(), nbr.data_ptr(), N, KN, Wt.data_ptr(), bias.data_ptr(), got.data_ptr(),
+                                None, None, 5, None, err.data_ptr(), s), "layer")
+    got_out = torch.full((N, 5), float("nan"), device="cuda")
+    _lib.check(lib.fvm_mp_layer(h.data_ptr(), nbr.data_ptr(), N, KN, Wt.data_ptr(), bias.data_ptr(), None,
+                                Wo.data_ptr(), bo.data_ptr(), 5, got_out.data_ptr(), err.data_ptr(), s), "layer+dec")
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert torch.equal(got, want)
+    assert torch.equal(got_out, want_out)
+    # and against torch (bf16 operands, fp32 accumulation)
+    hv = h.double()
+    valid = nbr >= 0
+    nb = nbr.long().clamp(min=0)
+    mean = (torch.where(valid.unsqueeze(-1), h[nb], torch.zeros((), device="cuda")).sum(1)
+            * (1.0 / valid.sum(1, keepdim=True).clamp(min=1).float()))
+    Aref = torch.cat([h.to(torch.bfloat16), mean.to(torch.bfloat16)], 1).double()
+    ref = hv + torch.nn.functional.silu(Aref @ Wt.double().t() + bias.double())
+    assert rel_l2(got.cpu().numpy(), ref.cpu().numpy()) < 1e-5

@@ -65,3 +65,66 @@ def test_gather_two_ranks_gloo():
     for rank, out, t in res:
         assert out == [[0.0, 200.0], [1.0, 80.0], [2.0, 140.0], [3.0, 20.0], [4.0, 110.0]]
         assert t == 2.5
+
+
+class _FakeBatch:
+    """Stand-in for a batch of cases: per-case vectors advanced by a fixed affine map."""
+
+    def __init__(self, ids, sizes):
+        self.ids = list(ids)
+        self.x = [torch.arange(sizes[i], dtype=torch.float64) * (i + 1) for i in ids]
+
+    def step(self, n):
+        for _ in range(n):
+            self.x = [0.5 * v + 1.0 for v in self.x]
+
+
+def _rows(b):
+    return torch.stack([torch.stack([v.sum(), torch.tensor(float(v.numel()), dtype=torch.float64)]) for v in b.x])
+
+
+def _sharded_worker(rank, world, port, sizes, q):
+    import torch.distributed as dist
+    from fvm_solver_b200.sharding import run_sharded
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        def advance(b, steps):
+            b.step(steps)
+            return 10.0 * (rank + 1)          # a device time per rank; the max must win
+        out = run_sharded(sizes, 3, lambda ids: _FakeBatch(ids, sizes), advance, _rows, row_width=2)
+        q.put((rank, out["ids"], out["rows"].tolist(), out["ms_max"], out["cells_total"]))
+    finally:
+        dist.destroy_process_group()
+
+
+def _run_world(world, sizes):
+    ctx = tmp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_sharded_worker, args=(r, world, port, sizes, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    return res
+
+
+def test_run_sharded_gloo_matches_serial():
+    """The sharded orchestration on 2 gloo ranks (and on 3 ranks with 2 cases: one rank idle) gives
+    every rank the same per-case rows as one rank stepping all cases, and the max time."""
+    from fvm_solver_b200.sharding import run_sharded
+    for world, sizes in ((2, [7, 3, 12, 5, 9]), (3, [4, 6])):
+        serial = run_sharded(sizes, 3, lambda ids: _FakeBatch(ids, sizes),
+                             lambda b, n: (b.step(n), 1.0)[1], _rows, row_width=2)
+        res = _run_world(world, sizes)
+        owned = sorted(i for _, ids, _, _, _ in res for i in ids)
+        assert owned == list(range(len(sizes)))
+        for rank, ids, rows, ms_max, cells in res:
+            assert rows == serial["rows"].tolist()
+            assert cells == sum(sizes)
+            assert ms_max == 10.0 * max(r + 1 for r, i, _, _, _ in res if i)
