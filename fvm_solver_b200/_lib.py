@@ -76,6 +76,8 @@ _SIGS = [
     ("fvm_cfl_dt", ct.c_int, [ct.POINTER(Mesh), ct.POINTER(Physics), _P, ct.c_float, _P, ct.POINTER(Work), _P]),
     ("fvm_conservation", ct.c_int, [ct.POINTER(Mesh), _P, _P, ct.POINTER(Work), _P]),
     ("fvm_residual_noalloc", ct.c_int, [ct.POINTER(Mesh), ct.POINTER(Physics), _P, _P, _P, _P, _P]),
+    ("fvm_residual_state", ct.c_int, [ct.POINTER(Mesh), ct.POINTER(Physics), _P, _P, _P, _P, ct.POINTER(Work), _P]),
+    ("fvm_facet_values", ct.c_int, [ct.POINTER(Mesh), _P, _P, ct.POINTER(Work), _P, _P]),
     ("fvm_profile_start", ct.c_int, [ct.c_int32]),
     ("fvm_step_fused", ct.c_int, [_P, _P, _P, _P, _P, _P]),
     ("fvm_multistep_fused", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, _P, _P, _P, _P, _P]),

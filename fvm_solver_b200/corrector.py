@@ -257,11 +257,11 @@ class ResidualEval:
         self.flag = torch.zeros(1, dtype=torch.int32, device=batch.device)
 
     def __call__(self, state: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
-        prims = self.b.cells.phys_setup.state_to_primative(state)[0].contiguous()
         self.flag.zero_()
-        _lib.check(self.lib.fvm_residual(ct.byref(self.b.dev.struct), ct.byref(self.b.phys), prims.data_ptr(),
-                                         self.grads.data_ptr(), self.flag.data_ptr(), out.data_ptr(),
-                                         ct.byref(self.b.work.struct), _lib.stream_ptr()), "fvm_residual")
+        _lib.check(self.lib.fvm_residual_state(ct.byref(self.b.dev.struct), ct.byref(self.b.phys),
+                                               state.contiguous().data_ptr(), self.grads.data_ptr(),
+                                               self.flag.data_ptr(), out.data_ptr(), ct.byref(self.b.work.struct),
+                                               _lib.stream_ptr()), "fvm_residual_state")
         return out
 
 
@@ -373,19 +373,23 @@ def record_trajectory(batch, steps: int, spinup: int) -> torch.Tensor:
     return traj
 
 
-def train(model: CorrectorModel, traj: torch.Tensor, iters: int, seed: int = 0, log_every: int = 0) -> list:
-    """Adam on random windows (U_t -> U_{t+k}) of a recorded trajectory; returns the loss history."""
+def train(model: CorrectorModel, traj: torch.Tensor, iters: int, seed: int = 0, log_every: int = 0,
+          normalise: bool = True) -> list:
+    """Adam on random windows (U_t -> U_{t+k}) of a recorded trajectory; returns the loss history.
+    ``normalise``: first set the input / output normalisation from this trajectory (off when the
+    model continues training on a new batch of meshes)."""
     k = model.k
     T = traj.shape[0] - k
     r0 = torch.empty_like(traj[0])
-    feats, tg = [], []
-    for t in range(0, T, max(1, T // 40)):
-        model.res(traj[t], r0)
-        base = model.kdt() * r0
-        feats.append(torch.cat([traj[t], base], 1))
-        tg.append(traj[t + k] - traj[t] - base)
-    model.set_normalisation(torch.stack(feats), torch.stack(tg))
-    del feats, tg
+    if normalise:
+        feats, tg = [], []
+        for t in range(0, T, max(1, T // 40)):
+            model.res(traj[t], r0)
+            base = model.kdt() * r0
+            feats.append(torch.cat([traj[t], base], 1))
+            tg.append(traj[t + k] - traj[t] - base)
+        model.set_normalisation(torch.stack(feats), torch.stack(tg))
+        del feats, tg
     g = torch.Generator().manual_seed(seed)
     target = torch.empty_like(traj[0])
     losses = []
@@ -401,6 +405,37 @@ def train(model: CorrectorModel, traj: torch.Tensor, iters: int, seed: int = 0, 
             losses.append((it, float(loss.item())))
     model.net.check_errors()
     return losses
+
+
+def train_streaming(make_batch, n_batches: int, iters: int, k: int = 8, record: int = 100, spinup: int = 200,
+                    seed: int = 0, lr: float = 1e-3, prefetch=None, log=None) -> tuple:
+    """Train one network on a stream of mesh batches (many more cases than fit on the device).
+
+    ``make_batch(b)`` -> (BatchedFVM with its time steps set, case parameters [cases][2]) builds
+    batch b; ``prefetch(b)`` (optional) starts building batch b ahead of time.  Each batch is
+    spun up ``spinup`` steps and ``record`` + k steps are recorded; ``iters / n_batches`` Adam
+    iterations then draw random windows from it.  The normalisation comes from the first batch,
+    and the network and the Adam moments carry over.  Returns (model, loss history, cases seen)."""
+    model, hist, cases = None, [], 0
+    per = max(1, iters // n_batches)
+    done = 0
+    for b in range(n_batches):
+        if prefetch is not None and b + 1 < n_batches:
+            prefetch(b + 1)
+        batch, prm = make_batch(b)
+        traj = record_trajectory(batch, steps=record + k, spinup=spinup)
+        m = CorrectorModel(batch, prm, k=k, seed=seed, lr=lr) if model is None else \
+            CorrectorModel(batch, prm, like=model)
+        n_it = per if b < n_batches - 1 else max(per, iters - done)
+        h = train(m, traj, iters=n_it, seed=seed + b, log_every=max(1, n_it // 2), normalise=model is None)
+        hist.extend((done + it, loss) for it, loss in h)
+        done += n_it
+        cases += batch.n_cases
+        model = m
+        if log is not None:
+            log(b, done, cases, h[-1][1])
+        del traj
+    return model, hist, cases
 
 
 class CheckedRollout:

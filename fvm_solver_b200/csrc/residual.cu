@@ -702,6 +702,46 @@ __global__ void __launch_bounds__(kMaxBlock) k_face(fvm_mesh_t m, Phys p, const 
     face_body<DIM, false>(m, p, prims, bcv, grads, flux, waves);
 }
 
+// Both sides' limited facet values [F][2][C] (the reference's U_face_all, facet_process.py:349-354),
+// rebuilt exactly as face_body rebuilds them: a cell side is U + sum_d grad_lim[d] r[d], a boundary
+// side is the boundary value.  On demand only (the residual never stores them).
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_facet_values(fvm_mesh_t m, const float* __restrict__ prims,
+                                                          const float* __restrict__ bcv,
+                                                          const float* __restrict__ grads, float* __restrict__ out) {
+    using Ly = L<DIM>;
+    constexpr int C = Ly::C, RS = Ly::RS, GS = Ly::GS;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.n_facets) return;
+    float rec[Ly::FR];
+    ld_vec<Ly::FR>(m.face_rec + (int64_t)f * Ly::FR, rec);
+    const int code[2] = {as_int(rec[Ly::FA]), as_int(rec[Ly::FB])};
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        float v[C];
+        if (code[s] >= 0) {
+            float P[RS], G[GS];
+            ld_vec<RS>(prims + (int64_t)code[s] * RS, P);
+            ld_vec<GS>(grads + (int64_t)code[s] * GS, G);
+            const int roff = s == 0 ? Ly::RA : Ly::RB;
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                float acc = G[Ly::gi(0, c)] * rec[roff];
+#pragma unroll
+                for (int d = 1; d < DIM; ++d) acc = fmaf(G[Ly::gi(d, c)], rec[roff + d], acc);
+                v[c] = P[c] + acc;
+            }
+        } else {
+            float B[RS];
+            ld_vec<RS>(bcv + (int64_t)(-1 - code[s]) * RS, B);
+#pragma unroll
+            for (int c = 0; c < C; ++c) v[c] = B[c];
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) out[((int64_t)f * 2 + s) * C + c] = v[c];
+    }
+}
+
 // ------------------------------------------------------------------------------------------
 // k_div_stage: divergence + stage combination.
 // ------------------------------------------------------------------------------------------
@@ -1417,6 +1457,19 @@ static int residual_impl(const fvm_mesh_t* m, const Phys& p, const float* prims_
     return launch_div<DIM>(m, p, w->flux, a, nullptr, nullptr, nullptr, nullptr, nullptr, dudt, s);
 }
 
+// dU/dt of a conserved state: one kernel writes the padded primitives into work->prims (the
+// stage kernels' conversion), then the residual kernels as in residual_impl.
+template <int DIM>
+static int residual_state_impl(const fvm_mesh_t* m, const Phys& p, const float* state, float* grads,
+                               int32_t* has_grads, float* dudt, const fvm_work_t* w, cudaStream_t s) {
+    FVM_LAUNCH(KID_STATE_TO_PRIMS, s, k_state_to_prims<DIM><<<blocks_for(m->n_cells), kBlock, 0, s>>>(
+                                          m->n_cells, p.inv_Cv, state, w->prims));
+    int rc = launch_fluxes<DIM>(m, p, w->prims, grads, has_grads, w, s);
+    if (rc) return rc;
+    StageArgs a{};
+    return launch_div<DIM>(m, p, w->flux, a, nullptr, nullptr, nullptr, nullptr, nullptr, dudt, s);
+}
+
 static StageArgs stage_args(const fvm_tableau_t* tab, int s) {
     StageArgs a{};
     const int S = tab->stages;
@@ -1542,6 +1595,35 @@ extern "C" int fvm_residual(const fvm_mesh_t* mesh, const fvm_physics_t* phys, c
     cudaStream_t s = (cudaStream_t)stream;
     return mesh->dim == 2 ? residual_impl<2>(mesh, p, prims, grads, has_grads, dudt, work, s)
                           : residual_impl<3>(mesh, p, prims, grads, has_grads, dudt, work, s);
+}
+
+extern "C" int fvm_residual_state(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const float* state,
+                                  float* grads, int32_t* has_grads, float* dudt, const fvm_work_t* work,
+                                  void* stream) {
+    if (const int rc = check_common(mesh)) return rc;
+    if (!phys || !state || !grads || !has_grads || !dudt || !work_ok(mesh, work) || !work->prims ||
+        !aligned32(work->prims) || !aligned32(grads))
+        return FVM_E_ARG;
+    const Phys p = make_phys(phys);
+    cudaStream_t s = (cudaStream_t)stream;
+    return mesh->dim == 2 ? residual_state_impl<2>(mesh, p, state, grads, has_grads, dudt, work, s)
+                          : residual_state_impl<3>(mesh, p, state, grads, has_grads, dudt, work, s);
+}
+
+extern "C" int fvm_facet_values(const fvm_mesh_t* mesh, const float* prims_padded, const float* grads,
+                                const fvm_work_t* work, float* out, void* stream) {
+    if (const int rc = check_common(mesh)) return rc;
+    if (!prims_padded || !grads || !out || !work || (mesh->n_bc > 0 && !work->bc_vals) || !aligned32(prims_padded) ||
+        !aligned32(grads))
+        return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (mesh->dim == 2)
+        FVM_LAUNCH(KID_FACE, s, k_facet_values<2><<<blocks_for(mesh->n_facets), kBlock, 0, s>>>(
+                                    *mesh, prims_padded, work->bc_vals, grads, out));
+    else
+        FVM_LAUNCH(KID_FACE, s, k_facet_values<3><<<blocks_for(mesh->n_facets), kBlock, 0, s>>>(
+                                    *mesh, prims_padded, work->bc_vals, grads, out));
+    return launch_status();
 }
 
 // ------------------------------------------------------------------------------------------

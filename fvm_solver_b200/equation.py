@@ -292,6 +292,36 @@ class FVMEquation:
         self._has_grads_host = True
         return out
 
+    def facet_state(self, primatives: torch.Tensor):
+        """The facet attributes the reference's ``FacetCalc.compute_facet`` leaves on ``E_props``
+        (``facet_process.py:349-359``) and its consumers read (``Saver.save``,
+        ``saving.py:54-57``): ``Vs_facet`` [F, 2, dim], ``rho_facet`` / ``T_facet`` [F, 2, 1],
+        ``mom_facet``, ``Q_facet`` and ``phi`` [F, 2] for the primitives ``primatives`` [N, C].
+
+        On demand: one residual evaluation on scratch gradients (first-call semantics, the carried
+        gradients are left alone) and one kernel that rebuilds both sides of every facet as the
+        facet kernel does.  The hot path stores none of this."""
+        from types import SimpleNamespace
+        prims = primatives.to(device=self.device, dtype=torch.float32).contiguous()
+        dim, C = self.mesh.dim, self.n_comp
+        grads = torch.zeros_like(self.grads)
+        flag = torch.zeros(1, dtype=torch.int32, device=self.device)
+        dudt = torch.empty_like(prims)
+        _lib.check(self.lib.fvm_residual(ct.byref(self.dev.struct), ct.byref(self.phys), _lib.ptr(prims),
+                                         _lib.ptr(grads), _lib.ptr(flag), _lib.ptr(dudt), ct.byref(self.work.struct),
+                                         _lib.stream_ptr()), "fvm_residual")
+        U = torch.empty((self.dev.n_facets, 2, C), device=self.device)
+        _lib.check(self.lib.fvm_facet_values(ct.byref(self.dev.struct), _lib.ptr(self.work.prims), _lib.ptr(grads),
+                                             ct.byref(self.work.struct), _lib.ptr(U), _lib.stream_ptr()),
+                   "fvm_facet_values")
+        Vs, rho, T = U[:, :, :dim].contiguous(), U[:, :, dim:dim + 1].contiguous(), U[:, :, dim + 1:].contiguous()
+        mom, _, Q = self.phy_setup.primatives_to_state(Vs, rho, T)
+        phi = None
+        if self.tables is not None:
+            phi = (Vs * self.tables.normals.to(self.device).unsqueeze(1)).sum(dim=-1)
+        return SimpleNamespace(Vs_facet=Vs, rho_facet=rho, T_facet=T, mom_facet=mom, Q_facet=Q, phi=phi,
+                               cell_grads=grads_to_reference(grads, dim), dudt=dudt)
+
     def conservation(self, state: torch.Tensor | None = None) -> torch.Tensor:
         """FP64 totals sum_i vol_i U_i [C] of ``state`` (default: the current cell state)."""
         s = (self.cells.state if state is None else state).contiguous()

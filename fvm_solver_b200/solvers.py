@@ -356,23 +356,67 @@ class TSolver:
     def _load_extra_state(self, d: dict):
         pass
 
+    def _dt_changes_on_device(self) -> bool:
+        tab = getattr(self, "tab", None)
+        return bool(self.cfl) or bool(tab is not None and tab.adaptive)
+
     def solve(self):
-        """Run ``n_iter`` steps (or until ``end_t`` with host-side time accounting)."""
+        """The reference's main loop (``TSolver._solve``, ``t_solvers.py:77-154``) on the device solver.
+
+        Runs until ``n_iter`` steps or ``t >= end_t``.  ``t`` advances by the time step each step
+        used (read from the device before the step when the step size changes on the device:
+        adaptive or CFL solvers; fixed time steps need no read).  Every ``print_i`` steps: a
+        progress line and a NaN check of the state.  Every ``plot_t`` of simulated time: the
+        reference's NaN check of the primitives (``ValueError``; no plotting here).  With
+        ``save_t`` and ``save_dir``: snapshots in the reference's ``Saver`` format, the initial
+        state at t = 0 and then every ``save_t`` (``trajectory_io.TrajectorySaver``); with
+        ``exact_interval`` the step that would cross a save time is shortened to land on it and
+        the step size is restored afterwards.  Returns the final time."""
+        cfg = self.cfg
         if self.n_steps is None and self.end_t is None:
             raise ValueError("Either n_iter or end_t must be set in ConfigFVM")
-        i = 0
+        saver = None
+        save_t, plot_t = getattr(cfg, "save_t", None), getattr(cfg, "plot_t", None)
+        if save_t and getattr(cfg, "save_dir", None) and self.n_cases == 1:
+            from .trajectory_io import TrajectorySaver
+            saver = TrajectorySaver(self.eq, cfg.save_dir)
+            saver.save(0.0)
+        exact = bool(getattr(cfg, "exact_interval", False)) and saver is not None
+        read_dt = self._dt_changes_on_device()
+        dt_fixed = float(self.dt[0].item())
+        t, i = self.t, 0
+        save_count, next_save = 1, save_t
+        next_plot = 0.0
         while True:
             if self.n_steps is not None and i >= self.n_steps:
                 break
-            if self.end_t is not None and self.t >= self.end_t:
+            if self.end_t is not None and t >= self.end_t:
                 break
-            dt = float(self.dt.item()) if self.end_t is not None else 0.0
-            self._solve_step()
-            self.t += dt
+            dt = float(self.dt[0].item()) if read_dt else dt_fixed
+            if exact and t + dt > next_save:
+                saved = self.dt.clone()
+                self.dt.fill_(next_save - t)
+                t = next_save
+                self._solve_step()
+                self.dt.copy_(saved)
+            else:
+                t += dt
+                self._solve_step()
             if self.print_i and i % self.print_i == 0:
                 if not torch.isfinite(self.cells.state).all():
                     raise ValueError("Nan detected in primatives")
+                print(f"progress: i = {i}, t = {t:.4g}, dt = {dt:.3g}", flush=True)
+            if plot_t and t >= next_plot:
+                next_plot = t + plot_t
+                if torch.isnan(self.cells.get_values()[0]).any():
+                    raise ValueError("Nan detected in primatives")
+            if saver is not None and t >= next_save:
+                save_count += 1
+                next_save = save_count * save_t
+                saver.save(t)
             i += 1
+        self.t = t
+        return t
 
 
 class Butcher(TSolver):

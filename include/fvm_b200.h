@@ -194,6 +194,20 @@ int fvm_residual(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float 
                  float *grads, int32_t *has_grads, float *dudt, const fvm_work_t *work,
                  void *stream);
 
+/* dU/dt of a conserved state [N][C] (no reference counterpart: the reference converts with
+ * FluidConstitution.state_to_primative, fvm_equation.py:35-44, before FVMEquation.forward): one
+ * kernel converts to padded primitives in work->prims (the stage kernels' arithmetic), then the
+ * residual as fvm_residual. */
+int fvm_residual_state(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *state, float *grads,
+                       int32_t *has_grads, float *dudt, const fvm_work_t *work, void *stream);
+
+/* Both sides' limited facet values out[F][2][C] -- the reference's U_face_all, split by
+ * FacetCalc.compute_facet into Vs_facet / rho_facet / T_facet (facet_process.py:349-359) -- for
+ * the padded primitives, limited gradients and boundary values (work->bc_vals) of the last
+ * residual evaluation on them; exactly the values the facet kernel uses.  On demand only. */
+int fvm_facet_values(const fvm_mesh_t *mesh, const float *prims_padded, const float *grads, const fvm_work_t *work,
+                     float *out, void *stream);
+
 /* Allocation-free fvm_residual.  No counterpart in the reference: it exists for callers that
  * cannot allocate device memory where they call the residual -- an application whose own pool
  * allocator has already reserved the GPU's memory, or a time-critical loop that forbids

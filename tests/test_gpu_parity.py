@@ -335,3 +335,39 @@ def test_saver_boundary_values_vs_oracle(tmp_path):
     path = saver.save(0.5)
     t, cell, bc = tio.load_step(path)
     assert bc.shape == (T.n_bc, 4) and os.path.exists(str(tmp_path / "mesh_props.npz"))
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_residual_from_state_vs_reference(case):
+    """fvm_residual_state (conserved state in, one conversion kernel, then the residual) against the
+    reference's residual of the same state's primitives: 1e-5 (the conversion rounds like the
+    stage kernels' rather than like the reference's torch ops)."""
+    import ctypes as ct
+    from fvm_solver_b200 import _lib
+    g, eq, T, cfg = make_equation(case)
+    st = torch.from_numpy(g["state0"]).cuda().contiguous()
+    out = torch.empty_like(st)
+    flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+    grads = torch.zeros_like(eq.grads)
+    _lib.check(eq.lib.fvm_residual_state(ct.byref(eq.dev.struct), ct.byref(eq.phys), st.data_ptr(), grads.data_ptr(),
+                                         flag.data_ptr(), out.data_ptr(), ct.byref(eq.work.struct),
+                                         _lib.stream_ptr()), "fvm_residual_state")
+    assert rel_l2(to_np(out), g["res1"]) < 1e-5
+    assert int(flag.item()) == 1
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_facet_state_vs_oracle(case):
+    """FVMEquation.facet_state: both sides of every facet (Vs/rho/T_facet, the reference's
+    U_face_all, facet_process.py:349-359) and phi against the oracle's facet values, 1e-5."""
+    from oracle import fvm_oracle as O
+    g, eq, T, cfg = make_equation(case)
+    fs = eq.facet_state(torch.from_numpy(g["prim0"]))
+    _, _, faces = O.OracleResidual(T, cfg, np.float32).forward(g["prim0"], return_faces=True)
+    dim = int(g["dim"])
+    got = torch.cat([fs.Vs_facet, fs.rho_facet, fs.T_facet], -1)
+    assert rel_l2(to_np(got), faces) < 1e-5
+    phi = (faces[:, :, :dim] * T.normals.numpy()[:, None, :]).sum(-1)
+    assert rel_l2(to_np(fs.phi), phi) < 1e-5
+    assert rel_l2(to_np(fs.cell_grads), g["grads1"]) < 1e-5
+    assert eq.cell_grads is None              # the equation's carried gradients are untouched
