@@ -65,6 +65,9 @@ def parse():
                     help="partitioned workload on one GPU: parts the box is split into")
     ap.add_argument("--windows", type=int, default=50, help="corrector rollout windows of k = 8 steps")
     ap.add_argument("--checkpoint", default=None, help="corrector: evaluate this stored model (no training)")
+    ap.add_argument("--cases-per-batch", type=int, default=0,
+                    help="corrector: stream the training cases in batches of this many meshes (0: one batch)")
+    ap.add_argument("--record-steps", type=int, default=100, help="corrector streaming: steps recorded per batch")
     ap.add_argument("--save-checkpoint", default=None, help="corrector: save the trained model here")
     ap.add_argument("--workload", default="taylor_green",
                     choices=["taylor_green", "channel_cylinder", "ensemble", "corrector", "corrector3d",
@@ -659,9 +662,64 @@ def _corrector_cases(n, seed, three_d):
     return parts, cfg, prm
 
 
+def corrector_train_streaming(args, three_d: bool):
+    """Config 4 scale: ``args.train_cases`` seeded cases in batches of ``args.cases_per_batch``
+    meshes (a batch's tables are built by a pool of host processes while the GPU trains on the
+    previous batch), ``args.iters`` Adam iterations in all (``corrector.train_streaming``)."""
+    import concurrent.futures as cfut
+    import copy
+    import multiprocessing as mp
+    from fvm_solver_b200 import batched as B, workloads as W
+    from fvm_solver_b200.corrector import train_streaming
+    params, seeds = _corrector_family(three_d)
+    family = "sphere" if three_d else "channel"
+    per = args.cases_per_batch
+    n_batches = max(1, args.train_cases // per)
+    case0 = W.sphere_case(0, device="cuda", base_seed=seeds[0], cells=(20_000, 20_000)) if three_d else \
+        W.ensemble_case(0, device="cuda", base_seed=seeds[0])
+    cfg = copy.deepcopy(case0.cfg)
+    cfg.solver_name, cfg.solver_extra, cfg.cfl = "Butcher", "SSP_RK3", None
+    pool = cfut.ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1), mp_context=mp.get_context("spawn"),
+                                    initializer=B._worker_init)
+    pending = {}
+
+    def prefetch(b):
+        if b not in pending:
+            jobs = [(i, seeds[0], family, (300_000, 800_000)) for i in range(b * per, (b + 1) * per)]
+            pending[b] = [pool.submit(B._ensemble_worker, j) for j in jobs]
+
+    def make_batch(b):
+        prefetch(b)
+        parts = [f.result() for f in pending.pop(b)]
+        batch = B.BatchedFVM(parts, cfg, device="cuda")
+        batch.t_solver.update_cfl_dt(0.5)
+        prm = torch.tensor([[params(i, seeds[0])["mach"], np.log10(params(i, seeds[0])["reynolds"])]
+                            for i in range(b * per, (b + 1) * per)], dtype=torch.float32)
+        return batch, prm
+
+    def log(b, done, cases, loss):
+        if b % max(1, n_batches // 20) == 0 or b == n_batches - 1:
+            print(f"batch {b + 1}/{n_batches}: {done} iterations, {cases} cases, loss {loss:.4g}", file=sys.stderr,
+                  flush=True)
+
+    t0 = time.time()
+    try:
+        model, hist, cases = train_streaming(make_batch, n_batches, args.iters, k=8, record=args.record_steps,
+                                             spinup=200, prefetch=prefetch, log=log)
+    finally:
+        pool.shutdown(cancel_futures=True)
+    torch.cuda.synchronize()
+    info = {"train_cases": cases, "cases_per_batch": per, "batches": n_batches, "iters": args.iters,
+            "recorded_steps_per_case": args.record_steps + 8, "loss_first": hist[0][1], "loss_last": hist[-1][1],
+            "loss_history": hist[:: max(1, len(hist) // 20)], "seconds": time.time() - t0}
+    return model, info
+
+
 def corrector_train(args, three_d: bool):
     """Train the corrector on trajectories of ``args.train_cases`` seeded cases; returns the model
     and a summary (loss history, seconds)."""
+    if args.cases_per_batch:
+        return corrector_train_streaming(args, three_d)
     from fvm_solver_b200 import batched as B
     from fvm_solver_b200.corrector import CorrectorModel, record_trajectory, train
     _, seeds = _corrector_family(three_d)

@@ -5,6 +5,9 @@ presets at ``time_fvm/config_fvm.py:71-178``.  Every field of the reference keep
 meaning so an existing config object can be handed to this package unchanged.  Added fields:
 
 * ``backend`` -- ``"b200"`` (the only backend; kept so callers can select it explicitly).
+* ``grad_stencil`` -- least-squares gradient stencil slots per cell, the cell included (at most
+  16): None keeps the reference's face-neighbour stencil (dim + 2 slots); a larger value adds the
+  nearest second-ring cells (``fvm_mesh.FVMMesh.widen_gradient_stencil``).
 * ``cfl`` -- when set, the time step is ``cfl * min_i h_i / (|u_i| + c_i)`` recomputed on the
   device every step (FP64 min-reduction); ``h_i = vol_i / max face area``.  The reference has no
   CFL control (fixed ``dt`` or error-adaptive ``dt``); this is a new, documented extension.
@@ -91,6 +94,7 @@ class ConfigFVM(ABC):
     # Additions of this package
     backend: str = "b200"
     cfl: float | None = None
+    grad_stencil: int | None = None
 
     @property
     def R(self) -> float:

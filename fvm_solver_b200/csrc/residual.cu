@@ -486,6 +486,105 @@ __device__ __forceinline__ void cell_body(const fvm_mesh_t& m, const Phys& p, co
     }
 }
 
+// Generic stencil width (kg > dim + 2, up to FVM_MAX_KG): record width FVM_CELL_REC_KG(DIM, kg),
+// offsets from the runtime kg.  The gradient sums the valid slots in column order (the ELL row's
+// order, as cell_body does); the limiter's bounds take the face neighbours only (their slots are in
+// the record's meta, 4 bits each), which for the dim + 2 stencil are all valid slots but the cell
+// itself.  Stencil columns stream through in groups of four, so registers do not grow with kg.
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_cell_wide(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+                                                       const float* __restrict__ bcv, float* __restrict__ grads,
+                                                       int32_t* __restrict__ has_grads) {
+    using Ly = L<DIM>;
+    constexpr int C = Ly::C, K = Ly::K, RS = Ly::RS;
+    const int kg = m.kg;
+    const int CRW = FVM_CELL_REC_KG(DIM, kg);
+    const int GC = DIM * kg, DISP = GC + kg, EPS = DISP + K * DIM, META = EPS + 1;
+    const int N = m.n_cells;
+    const int NA = m.n_owned > 0 ? m.n_owned : N;
+    const int stride = gridDim.x * blockDim.x;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *has_grads = 1;
+    for (; i < NA; i += stride) {
+        if (m.case_active && !case_on(m, m.cell_case, i)) continue;
+        const float* rec = m.cell_rec + (int64_t)i * CRW;
+        const int meta = as_int(__ldg(rec + META));
+        const int nvalid = (meta >> 24) & 31;
+        unsigned face = 0;
+#pragma unroll
+        for (int j = 0; j < K; ++j) face |= 1u << ((meta >> (4 * j)) & 15);
+        float U[RS];
+        ld_vec<RS>(prims + (int64_t)i * RS, U);
+        float g[DIM][C];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+#pragma unroll
+            for (int c = 0; c < C; ++c) g[d][c] = 0.f;
+        float up[C], lo[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) up[c] = lo[c] = U[c];
+        for (int k0 = 0; k0 < nvalid; k0 += 4) {
+            float X[4][RS];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (k0 + q < nvalid) {
+                    const int col = as_int(__ldg(rec + GC + k0 + q));
+                    if (col < N) ld_vec<RS>(prims + (int64_t)col * RS, X[q]);
+                    else ld_vec_cg<RS>(bcv + (int64_t)(col - N) * RS, X[q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int k = k0 + q;
+                if (k >= nvalid) break;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    const float w = __ldg(rec + d * kg + k);
+#pragma unroll
+                    for (int c = 0; c < C; ++c) g[d][c] = fmaf(w, X[q][c], g[d][c]);
+                }
+                if ((face >> k) & 1u) {
+#pragma unroll
+                    for (int c = 0; c < C; ++c) {
+                        up[c] = fmaxf(up[c], X[q][c]);
+                        lo[c] = fminf(lo[c], X[q][c]);
+                    }
+                }
+            }
+        }
+        const float eps = __ldg(rec + EPS);
+        float phim[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            up[c] -= U[c];
+            lo[c] -= U[c];
+            phim[c] = INFINITY;
+        }
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            float r[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) r[d] = __ldg(rec + DISP + j * DIM + d);
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                float du = g[0][c] * r[0];
+#pragma unroll
+                for (int d = 1; d < DIM; ++d) du = fmaf(g[d][c], r[d], du);
+                const float num = du > 0.f ? up[c] : lo[c];
+                phim[c] = fminf(phim[c], limiter_phi(p.lim_p, num, du, eps));
+            }
+        }
+        float go[Ly::GS];
+#pragma unroll
+        for (int q = 0; q < Ly::GS; ++q) go[q] = 0.f;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+#pragma unroll
+            for (int c = 0; c < C; ++c) go[Ly::gi(d, c)] = g[d][c] * phim[c];
+        st_vec<Ly::GS>(grads + (int64_t)i * Ly::GS, go);
+    }
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(kMaxBlock) k_cell(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
                                                   const float* __restrict__ bcv, float* __restrict__ grads,
@@ -1322,7 +1421,7 @@ static bool aligned32(const void* p) { return ((uintptr_t)p & 31u) == 0; }   // 
 static bool mesh_ok(const fvm_mesh_t* m) {
     if (!m || (m->dim != 2 && m->dim != 3) || m->n_comp != m->dim + 2) return false;
     if (m->n_cells <= 0 || m->n_facets <= 0 || m->n_bc < 0 || m->n_char < 0) return false;
-    if (m->kg != m->dim + 2 || m->kf < 1 || m->kf > m->dim + 1) return false;
+    if (m->kg < m->dim + 2 || m->kg > FVM_MAX_KG || m->kf < 1 || m->kf > m->dim + 1) return false;
     if (!m->cell_rec || !m->div_rec || !m->face_rec || !m->inv_h || !m->volumes) return false;
     if (!aligned32(m->cell_rec) || !aligned32(m->div_rec) || !aligned32(m->face_rec)) return false;
     if (m->n_bc > 0 && (!m->bc_cell || !m->bc_kind || !m->bc_b || !m->bc_l || !m->bc_ga || !m->bc_gb ||
@@ -1398,6 +1497,11 @@ static int launch_begin(const fvm_mesh_t* m, const Phys& p, const float* prims, 
             FVM_LAUNCH(KID_BC, s, k_char_scale<DIM><<<m->n_cases, kBlock, 0, s>>>(*m, p, prims, w->red));
         FVM_LAUNCH(KID_BC, s, k_bc<DIM><<<blocks_for(m->n_bc), kBlock, 0, s>>>(*m, p, prims, grads, has_grads,
                                                                                w->bc_vals, w->red));
+    }
+    if (m->kg != DIM + 2) {
+        const unsigned gw = persistent_grid(owned_cells(m), kBlock, wave_blocks(k_cell_wide<DIM>, kBlock));
+        FVM_LAUNCH(KID_CELL, s, k_cell_wide<DIM><<<gw, kBlock, 0, s>>>(*m, p, prims, w->bc_vals, grads, has_grads));
+        return launch_status();
     }
     const unsigned gc = persistent_grid(owned_cells(m), g_block_cell, wave_blocks(k_cell<DIM>, g_block_cell));
     FVM_LAUNCH(KID_CELL, s, k_cell<DIM><<<gc, g_block_cell, 0, s>>>(*m, p, prims, w->bc_vals, grads, has_grads,
@@ -1580,7 +1684,7 @@ static int multistep_impl(const fvm_mesh_t* m, const Phys& p, int store, int n_t
 using namespace fvm;
 
 static int check_common(const fvm_mesh_t* mesh) {
-    if (mesh && mesh->dim >= 2 && mesh->dim <= 3 && mesh->kg != mesh->dim + 2) return FVM_E_UNSUPPORTED;
+    if (mesh && mesh->dim >= 2 && mesh->dim <= 3 && mesh->kg > FVM_MAX_KG) return FVM_E_UNSUPPORTED;
     return mesh_ok(mesh) ? FVM_OK : FVM_E_ARG;
 }
 
@@ -1806,6 +1910,7 @@ extern "C" int fvm_step_fused(const fvm_mesh_t* mesh, const fvm_physics_t* phys,
     if (!phys || !tab_ok(tab) || !bufs_ok(bufs) || !work_ok(mesh, work)) return FVM_E_ARG;
     if (mesh->n_cases > 0 && tab->adaptive) return FVM_E_UNSUPPORTED;
     if (mesh->n_owned > 0 || mesh->char_scale_given) return FVM_E_UNSUPPORTED;   // partitions use the split stages
+    if (mesh->kg != mesh->dim + 2) return FVM_E_UNSUPPORTED;                      // widened stencils: separate launches
     FusedArgs f{};
     f.stages = tab->stages;
     for (int s = 0; s < tab->stages; ++s) {
@@ -1825,7 +1930,7 @@ extern "C" int fvm_multistep_fused(const fvm_mesh_t* mesh, const fvm_physics_t* 
     if (!phys || !bufs_ok(bufs) || !work_ok(mesh, work) || n_terms < 0 || n_terms > FVM_MAX_STAGES ||
         (n_terms > 0 && (!idx || !coef)) || store < 0)
         return FVM_E_ARG;
-    if (mesh->n_owned > 0 || mesh->char_scale_given) return FVM_E_UNSUPPORTED;
+    if (mesh->n_owned > 0 || mesh->char_scale_given || mesh->kg != mesh->dim + 2) return FVM_E_UNSUPPORTED;
     FusedArgs f{};
     f.stages = 1;
     StageArgs& a = f.st[0];

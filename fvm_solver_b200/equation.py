@@ -208,6 +208,8 @@ class FVMEquation:
             raise RuntimeError("fvm_solver_b200 runs on CUDA devices only (no CPU fallback)")
         self.lib = _lib.load()
         self.mesh = _host_mesh(mesh)
+        if getattr(cfg, "grad_stencil", None):
+            self.mesh.widen_gradient_stencil(int(cfg.grad_stencil))
         self.n_comp = n_comp
         assert n_comp == self.mesh.dim + 2, "n_comp must be dim + 2"
         self.tables = FVMTables(self.mesh, cfg, n_comp, bc_tag)

@@ -170,6 +170,7 @@ class FVMMesh:
             neigh_cents = torch.where(combined_bc.unsqueeze(-1), neigh_cents + sh,
                                       neigh_cents - nb_shift + sh)
 
+        self._neigh_pos, self._neigh_is_bc = neigh_cents, combined_bc   # kept for widen_gradient_stencil
         center_expanded = self.centroids.unsqueeze(1)
         d = neigh_cents - center_expanded
         w = 1 / torch.norm(d.double(), dim=2) ** 0.25
@@ -216,15 +217,70 @@ class FVMMesh:
         other = np.where(sa == pos, sb, sa)
         return other % K
 
+    # -- wider gradient stencils (an extension; the reference uses the face neighbours) ---------
+    def widen_gradient_stencil(self, width: int):
+        """Least-squares gradients over up to ``width`` slots per cell (the cell itself included,
+        at most 16) instead of the reference's dim + 2: the face neighbours (cells and boundary
+        facets) plus the nearest cells of the second ring -- the face neighbours of the face
+        neighbours, each counted once -- in the same weighted least squares
+        (w = |d|^-1/4, boundary facets x 7.5, ``fvm_mesh.py:263-344``).  Periodic meshes compose
+        the frame shifts of the two facets crossed.  The limiter keeps using the face neighbours
+        only (``neigh_combine``), as in the reference."""
+        N, K = self.cell_to_facet.shape
+        dim = self.dim
+        if width <= K + 1:
+            return
+        if width > 16:
+            raise ValueError("gradient stencils are at most 16 slots wide")
+        E = min(width - 1 - K, K * K)                   # second-ring slots (at most K^2 candidates)
+        nb = self.cell_grad_stuff[3].numpy().astype(np.int64)          # [N, K] cells or N + bc index
+        isbc = self._neigh_is_bc.numpy()
+        P1 = self._neigh_pos.numpy().astype(np.float64)                 # [N, K, dim] in the cell's frame
+        c = self.centroids.numpy().astype(np.float64)
+        nbc = np.where(isbc, 0, nb)
+        off = np.where(isbc[..., None], 0.0, P1 - c[nbc])              # neighbour frame -> cell frame
+        cand = nb[nbc].reshape(N, K * K)                                # [N, K*K]
+        cbc = (isbc[nbc] | isbc[:, :, None]).reshape(N, K * K)
+        cpos = (P1[nbc] + off[:, :, None, :]).reshape(N, K * K, dim)
+        own = np.arange(N)[:, None]
+        bad = cbc | (cand == own) | (cand[:, :, None] == np.where(isbc, -1, nb)[:, None, :]).any(axis=2)
+        key = np.where(bad, np.iinfo(np.int64).max, cand)
+        order = np.argsort(key, axis=1, kind="stable")
+        ks = np.take_along_axis(key, order, 1)
+        dup = np.zeros_like(bad)
+        dup_sorted = np.concatenate([np.zeros((N, 1), bool), ks[:, 1:] == ks[:, :-1]], 1)
+        np.put_along_axis(dup, order, dup_sorted, 1)
+        bad |= dup
+        dist = np.linalg.norm(cpos - c[:, None, :], axis=2)
+        pick = np.argsort(np.where(bad, np.inf, dist), axis=1, kind="stable")[:, :E]
+        ok = ~np.take_along_axis(bad, pick, 1)
+        ext = np.where(ok, np.take_along_axis(cand, pick, 1), -1)
+        epos = np.take_along_axis(cpos, pick[:, :, None], 1)
+        cols = np.concatenate([nb, ext], 1)                             # [N, K + E], -1 = empty slot
+        pos = np.concatenate([P1, epos], 1)
+        d = torch.from_numpy(pos - c[:, None, :])
+        valid = torch.from_numpy(cols >= 0)
+        w = 1 / torch.norm(d, dim=2) ** 0.25
+        w[torch.from_numpy(np.concatenate([isbc, np.zeros((N, E), bool)], 1))] *= 7.5
+        w = torch.where(valid, w, torch.zeros((), dtype=w.dtype))
+        w2 = w ** 2
+        dT = d.transpose(1, 2)
+        A = torch.bmm(dT, d * w2.unsqueeze(-1))
+        self.lsq_weights = torch.bmm(torch.inverse(A), dT * w2.unsqueeze(1)).float()   # [N, dim, K + E]
+        self._stencil = torch.from_numpy(cols)
+
     # -- reference-format sparse gradient matrices -------------------------------------------
     def gradient_coo(self, d: int) -> torch.Tensor:
         """Sparse COO gradient matrix for spatial direction ``d`` (``fvm_mesh.py:5-42``).
 
         Row i holds the LSQ weights of cell i's neighbours and the diagonal
-        ``-(((0 + g_0) + g_1) + ...)`` accumulated in FP32 in local-facet order.
+        ``-(((0 + g_0) + g_1) + ...)`` accumulated in FP32 in local-facet order (a widened
+        stencil: its face neighbours, then its second-ring cells, empty slots left out).
         """
         G = self.lsq_weights[:, d, :]
-        neigh = self.cell_grad_stuff[3]
+        neigh = getattr(self, "_stencil", None)
+        if neigh is None:
+            neigh = self.cell_grad_stuff[3].long()
         N, K = G.shape
         diag = 0.0 + G[:, 0]
         for k in range(1, K):
@@ -232,7 +288,8 @@ class FVMMesh:
         rows = torch.arange(N).unsqueeze(1).expand(N, K + 1).reshape(-1)
         cols = torch.cat([neigh.long(), torch.arange(N).unsqueeze(1)], dim=1).reshape(-1)
         vals = torch.cat([G, (-diag).unsqueeze(1)], dim=1).reshape(-1)
-        return torch.sparse_coo_tensor(torch.stack([rows, cols]), vals,
+        keep = cols >= 0
+        return torch.sparse_coo_tensor(torch.stack([rows[keep], cols[keep]]), vals[keep],
                                        (N, N + self.n_bc_facet))
 
 
@@ -275,10 +332,15 @@ class FVMMesh3D(FVMMesh):
         return torch.abs(det) / 6.0
 
 
-def mesh_from_spec(spec, device="cpu") -> FVMMesh:
-    """Build the host mesh for a ``meshgen.MeshSpec``."""
+def mesh_from_spec(spec, device="cpu", grad_stencil: int | None = None) -> FVMMesh:
+    """Build the host mesh for a ``meshgen.MeshSpec``; ``grad_stencil`` widens the gradient
+    stencil to that many slots (``FVMMesh.widen_gradient_stencil``)."""
     cls = FVMMesh2D if spec.dim == 2 else FVMMesh3D
     if spec.period is not None:
-        return cls(spec.vertices, spec.cells, spec.facets, spec.bc_facet_mask, device=device,
-                   period=spec.period, cell_shifts=spec.cell_shifts, facet_shifts=spec.facet_shifts)
-    return cls(spec.vertices, spec.cells, spec.facets, spec.bc_facet_mask, device=device)
+        m = cls(spec.vertices, spec.cells, spec.facets, spec.bc_facet_mask, device=device,
+                period=spec.period, cell_shifts=spec.cell_shifts, facet_shifts=spec.facet_shifts)
+    else:
+        m = cls(spec.vertices, spec.cells, spec.facets, spec.bc_facet_mask, device=device)
+    if grad_stencil:
+        m.widen_gradient_stencil(int(grad_stencil))
+    return m

@@ -224,7 +224,7 @@ class KernelTables:
         side-1 centroid->facet displacements [dim] each, padding.
         """
         dim, N, F, K, kg, kf = self.dim, self.n_cells, self.n_facets, self.dim + 1, self.kg, self.kf
-        CR, FR, DR = record_sizes(dim)
+        CR, FR, DR = record_sizes(dim, kg)
         bits = lambda t: t.to(torch.int32).view(torch.float32)
         cell = torch.zeros((N, CR), dtype=torch.float32)
         o = 0
@@ -262,9 +262,13 @@ class KernelTables:
         return dict(cell_rec=cell, div_rec=div, face_rec=face)
 
 
-def record_sizes(dim: int):
-    """(cell record, facet record, divergence record) widths in floats (FVM_CELL_REC etc.)."""
-    return (24, 16, 8) if dim == 2 else (40, 16, 8)
+def record_sizes(dim: int, kg: int | None = None):
+    """(cell record, facet record, divergence record) widths in floats (FVM_CELL_REC_KG etc.): the
+    cell record holds kg gradient slots (default dim + 2, the reference's stencil) and is padded to
+    a multiple of 8 floats."""
+    kg = dim + 2 if kg is None else kg
+    cr = (dim * kg + kg + (dim + 1) * dim + 2 + 7) // 8 * 8
+    return (cr, 16, 8)
 
 
 def row_sizes(dim: int):

@@ -55,7 +55,8 @@ class Case:
     def tables(self):
         from .fvm_mesh import mesh_from_spec
         from .tables import FVMTables
-        return FVMTables(mesh_from_spec(self.spec), self.cfg, self.dim + 2, self.bc_tags)
+        return FVMTables(mesh_from_spec(self.spec, grad_stencil=getattr(self.cfg, "grad_stencil", None)),
+                         self.cfg, self.dim + 2, self.bc_tags)
 
 
 def taylor_green(n: int = 66, seed: int = 0, device: str = "cuda", **cfg_kw) -> Case:

@@ -51,11 +51,15 @@ extern "C" {
 #define FVM_ROW(dim) ((dim) == 2 ? 4 : 8)
 #define FVM_GROW(dim) ((dim) == 2 ? 8 : 16)
 #define FVM_CELL_REC(dim) ((dim) == 2 ? 24 : 40)
+/* Cell record width of a mesh with kg gradient slots (kg = dim + 2: FVM_CELL_REC). */
+#define FVM_CELL_REC_KG(dim, kg) ((((dim) * (kg) + (kg) + ((dim) + 1) * (dim) + 2) + 7) / 8 * 8)
 #define FVM_FACE_REC(dim) ((dim) == 2 ? 16 : 16)
 #define FVM_DIV_REC 8
 
 /* Mesh tables (built by fvm_solver_b200/tables.py).  N cells, F facets, Fb boundary facets,
- * Fc characteristic facets, K = dim + 1 facets per cell, KG = kg gradient slots (= dim + 2).
+ * Fc characteristic facets, K = dim + 1 facets per cell, KG = kg gradient slots: dim + 2 (the
+ * reference's face-neighbour stencil) up to FVM_MAX_KG (a widened stencil); the cell record is then
+ * FVM_CELL_REC_KG(dim, kg) floats wide.
  * Integer fields inside float records are stored bit-cast (int32 bits in a float slot). */
 typedef struct fvm_mesh {
     int32_t dim, n_comp, n_cells, n_facets, n_bc, n_char, kg, kf;
@@ -189,7 +193,7 @@ int fvm_ell_spmm(const float *vals, const int32_t *cols, int64_t M, int32_t K,
 /* dU/dt [N][C] (conserved variables) of the primitives prims [N][C].  grads [N][FVM_GROW] is
  * read as the previous limited gradient when the device flag *has_grads != 0 (the reference's
  * FacetCalc.cell_grads is not None) and overwritten with this evaluation's limited gradient;
- * the call sets *has_grads = 1.  Returns FVM_E_UNSUPPORTED if mesh->kg != dim + 2. */
+ * the call sets *has_grads = 1.  Meshes with kg > dim + 2 take the generic-width cell kernel. */
 int fvm_residual(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const float *prims,
                  float *grads, int32_t *has_grads, float *dudt, const fvm_work_t *work,
                  void *stream);

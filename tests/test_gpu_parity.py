@@ -371,3 +371,24 @@ def test_facet_state_vs_oracle(case):
     assert rel_l2(to_np(fs.phi), phi) < 1e-5
     assert rel_l2(to_np(fs.cell_grads), g["grads1"]) < 1e-5
     assert eq.cell_grads is None              # the equation's carried gradients are untouched
+
+
+@pytest.mark.parametrize("case", ["c2d", "b3d", "ptile"])
+@pytest.mark.parametrize("width", [9, 16])
+def test_widened_stencil_vs_oracle(case, width):
+    """Widened gradient stencils (up to 16 slots; no reference counterpart, the reference's width is
+    dim + 2): the generic-width cell kernel against the oracle on the same tables -- residual and
+    limited gradients 1e-5, one RK4 step 1e-5."""
+    from oracle import fvm_oracle as O
+    g, eq, T, cfg = make_equation(case, "Butcher", "RK4", grad_stencil=width)
+    assert eq.dev.kg > int(g["dim"]) + 2
+    orc = O.OracleResidual(eq.tables, cfg, np.float32)
+    want, wg = orc.forward(g["prim0"])
+    got = eq.forward(torch.from_numpy(g["prim0"]))
+    assert rel_l2(to_np(got), want) < 1e-5
+    assert rel_l2(to_np(eq.cell_grads), wg) < 1e-5
+    eq.reset_gradients()
+    eq.t_solver.step(1)
+    s = O.OracleSolver(orc, g["state0"], float(g["dt"]))
+    s.butcher_step("RK4")
+    assert rel_l2(to_np(eq.cells.state), s.state) < 1e-5

@@ -105,3 +105,31 @@ def test_device_mesh_struct_on_host():
         assert getattr(m, f), f
     assert m.n_cases == 0 and not m.case_active and m.n_owned == 0 and m.char_scale_given == 0
     assert m.n_cells == tables.kernel.n_cells and m.kg == tables.kernel.kg
+
+
+def test_widened_gradient_stencil_exact_for_linear_fields():
+    """Widened least-squares stencils (config 2's 'gradient stencil width up to 16'; the reference's
+    is dim + 2): every width reproduces the gradient of a linear field exactly (to FP32 rounding,
+    1e-4 absolute on unit-size coefficients) and a constant field's gradient is zero on a periodic
+    box; rows hold at most the requested slots, the face neighbours and the cell itself always."""
+    import numpy as np
+    import torch
+    from fvm_solver_b200 import fvm_mesh as fm, meshgen as mg
+    for spec in (mg.box3d(6, seed=4), mg.channel_cylinder(h=0.05, seed=3), mg.periodic_box(7, seed=5)):
+        dim = spec.dim
+        for width in (None, 9, 16):
+            m = fm.mesh_from_spec(spec, grad_stencil=width)
+            N = m.n_cells
+            G = [m.gradient_coo(d).coalesce() for d in range(dim)]
+            nnz = torch.bincount(G[0].indices()[0], minlength=N)
+            assert int(nnz.min()) >= dim + 2 and int(nnz.max()) <= (width or dim + 2)
+            a = np.array([0.7, -1.3, 0.4][:dim])
+            if spec.period is None:
+                f = np.concatenate([m.centroids.double().numpy() @ a,
+                                    m.midpoints[m.bc_facet_mask].double().numpy() @ a])
+                want = a
+            else:
+                f, want = np.ones(N), np.zeros(dim)
+            for d in range(dim):
+                y = torch.sparse.mm(G[d].double(), torch.from_numpy(f)[:, None]).numpy()[:, 0]
+                assert np.abs(y - want[d]).max() < 1e-4
