@@ -17,6 +17,7 @@ FVM_OK, FVM_E_ARG, FVM_E_CUDA, FVM_E_UNSUPPORTED, FVM_E_CAPACITY = 0, -1, -2, -3
 FVM_NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024
 FVM_MAX_STAGES = 12
 FVM_RED_DOUBLES = 64
+FVM_PHASE_BC, FVM_PHASE_CELLS, FVM_PHASE_FACES, FVM_PHASE_DIV = 1, 2, 4, 8
 
 _P = ct.c_void_p
 
@@ -28,7 +29,8 @@ class Mesh(ct.Structure):
                           "bc_char", "ch_cell", "ch_normal", "ch_rho", "ch_vn", "ch_p", "ch_vt")] + [
         ("n_cases", ct.c_int32)] + [
         (n, _P) for n in ("cell_case", "face_case", "bc_case", "ch_off", "case_mu", "case_mu_b", "case_kappa")] + [
-        ("n_owned", ct.c_int32), ("char_scale_given", ct.c_int32), ("case_active", _P)]
+        ("n_owned", ct.c_int32), ("char_scale_given", ct.c_int32), ("case_active", _P),
+        ("cell_lo", ct.c_int32), ("facet_lo", ct.c_int32)]
 
 MESH_PTR_FIELDS = [f for f, t in Mesh._fields_ if t is _P]
 
@@ -86,6 +88,7 @@ _SIGS = [
     ("fvm_stage_begin", ct.c_int, [_P, _P, _P, _P, _P]),
     ("fvm_stage_end", ct.c_int, [_P, _P, _P, ct.c_int32, _P, _P, ct.c_int32, _P]),
     ("fvm_stage_finalize", ct.c_int, [_P, _P, _P, _P, _P]),
+    ("fvm_stage_phase", ct.c_int, [_P, _P, _P, ct.c_int32, _P, _P, ct.c_int32, ct.c_int32, _P]),
     ("fvm_char_partial", ct.c_int, [_P, _P, _P, _P, _P]),
     ("fvm_set_block_size", ct.c_int, [ct.c_int32, ct.c_int32]),
     ("fvm_set_prefetch", ct.c_int, [ct.c_int32, ct.c_int32]),

@@ -68,8 +68,9 @@ struct L {
     static constexpr int C = DIM + 2, K = DIM + 1, KG = DIM + 2;
     static constexpr int RS = FVM_ROW(DIM), GS = FVM_GROW(DIM);
     static constexpr int CR = FVM_CELL_REC(DIM), FR = FVM_FACE_REC(DIM), DR = FVM_DIV_REC;
-    // cell record offsets
-    static constexpr int GV = 0, GC = DIM * KG, DISP = GC + KG, EPS = DISP + K * DIM, META = EPS + 1;
+    // compact cell record offsets: weights [DIM][KG], neighbour columns [KG - 1], displacements, eps
+    static constexpr int GV = 0, GC = DIM * KG, DISP = GC + KG - 1, EPS = DISP + K * DIM;
+    static constexpr int SELF_SHIFT = 28;                 // own slot: bits 28..30 of the first column
     // face record offsets
     static constexpr int FA = 0, FB = 1, INVD = 2, SIZE = 3, NRM = 4, XO = 4 + DIM, RA = 4 + 2 * DIM,
                          RB = 4 + 3 * DIM;
@@ -77,7 +78,7 @@ struct L {
     static __host__ __device__ __forceinline__ constexpr int gi(int d, int comp) {
         return comp == DIM ? DIM * (DIM + 1) + d : d * (DIM + 1) + (comp < DIM ? comp : DIM);
     }
-    static_assert(META + 1 <= CR && RB + DIM <= FR && 2 * K <= DR, "record layout");
+    static_assert(EPS + 1 <= CR && RB + DIM <= FR && 2 * K <= DR, "record layout");
 };
 
 // N consecutive floats -> registers.  Rows whose width is a multiple of 8 floats start on 32-byte
@@ -200,13 +201,26 @@ __device__ __forceinline__ int2 next_codes(const fvm_mesh_t& m, int f, int nF, b
     const bool on = f < nF && (!skip_frozen || case_on(m, m.face_case, f));
     return on ? ld_codes(m.face_rec + (int64_t)f * L<DIM>::FR) : make_int2(0, 0);
 }
+// The KG stencil columns of cell i in slot order, from its compact record: the KG - 1 stored
+// neighbour columns with the cell's own index inserted at its slot (selects only, no indexing of
+// register arrays by a runtime value).  Items not loaded get the column 0 everywhere.
 template <int DIM>
 __device__ __forceinline__ void next_cols(const fvm_mesh_t& m, int i, int NA, int* cols, bool skip_frozen) {
     using Ly = L<DIM>;
     const bool on = i < NA && (!skip_frozen || case_on(m, m.cell_case, i));
+    int nb[Ly::KG - 1];
 #pragma unroll
-    for (int k = 0; k < Ly::KG; ++k)
-        cols[k] = on ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)i * Ly::CR + Ly::GC + k) : 0;
+    for (int k = 0; k < Ly::KG - 1; ++k)
+        nb[k] = on ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)i * Ly::CR + Ly::GC + k) : 0;
+    const int own = (nb[0] >> Ly::SELF_SHIFT) & 7;
+    nb[0] &= (1 << Ly::SELF_SHIFT) - 1;
+    const int self = on ? i : 0;
+#pragma unroll
+    for (int k = 0; k < Ly::KG; ++k) {
+        const int below = k < Ly::KG - 1 ? nb[k] : 0;
+        const int above = k > 0 ? nb[k - 1] : 0;
+        cols[k] = k < own ? below : (k == own ? self : above);
+    }
 }
 
 
@@ -407,15 +421,16 @@ __device__ __forceinline__ void cell_body(const fvm_mesh_t& m, const Phys& p, co
     using Ly = L<DIM>;
     constexpr int C = Ly::C, K = Ly::K, KG = Ly::KG, RS = Ly::RS;
     const int N = m.n_cells;                              // columns < N are cells (halo included)
-    const int NA = m.n_owned > 0 ? m.n_owned : N;         // cells this launch updates
+    const int NA = m.n_owned > 0 ? m.n_owned : N;         // cells this launch updates: [lo, NA)
+    const int lo = m.cell_lo;
     const int stride = gridDim.x * blockDim.x;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) *has_grads = 1;
-    const bool skip_frozen = frozen_skip(m, NA, stride);
+    int i = lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *has_grads = 1;
+    const bool skip_frozen = frozen_skip(m, NA - lo, stride);
     int cols[KG];
     next_cols<DIM>(m, i, NA, cols, skip_frozen);
     for (int64_t tile = blockIdx.x; i < NA; i += stride, tile += gridDim.x) {
-        if (waves > 0) prefetch_tile(m.cell_rec, NA, Ly::CR, tile + (int64_t)waves * gridDim.x);
+        if (waves > 0) prefetch_tile(m.cell_rec + (int64_t)lo * Ly::CR, NA - lo, Ly::CR, tile + (int64_t)waves * gridDim.x);
         if (m.case_active && !case_on(m, m.cell_case, i)) {
             next_cols<DIM>(m, i + stride, NA, cols, skip_frozen);
             continue;
@@ -431,7 +446,6 @@ __device__ __forceinline__ void cell_body(const fvm_mesh_t& m, const Phys& p, co
         float rec[Ly::CR];
         ld_vec<Ly::CR>(m.cell_rec + (int64_t)i * Ly::CR, rec);
         next_cols<DIM>(m, i + stride, NA, cols, skip_frozen);
-        const int nvalid = (as_int(rec[Ly::META]) >> 24) & 31;
         float g[DIM][C];
 #pragma unroll
         for (int d = 0; d < DIM; ++d)
@@ -448,12 +462,11 @@ __device__ __forceinline__ void cell_body(const fvm_mesh_t& m, const Phys& p, co
 #pragma unroll
                 for (int c = 0; c < C; ++c) g[d][c] = fmaf(w, X[k][c], g[d][c]);
             }
-            if (k < nvalid) {
+            // every slot of the reference's stencil is valid: the face neighbours and the cell
 #pragma unroll
-                for (int c = 0; c < C; ++c) {
-                    up[c] = fmaxf(up[c], X[k][c]);
-                    lo[c] = fminf(lo[c], X[k][c]);
-                }
+            for (int c = 0; c < C; ++c) {
+                up[c] = fmaxf(up[c], X[k][c]);
+                lo[c] = fminf(lo[c], X[k][c]);
             }
         }
         const float eps = rec[Ly::EPS];
@@ -503,8 +516,8 @@ __global__ void __launch_bounds__(kBlock) k_cell_wide(fvm_mesh_t m, Phys p, cons
     const int N = m.n_cells;
     const int NA = m.n_owned > 0 ? m.n_owned : N;
     const int stride = gridDim.x * blockDim.x;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) *has_grads = 1;
+    int i = m.cell_lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *has_grads = 1;
     for (; i < NA; i += stride) {
         if (m.case_active && !case_on(m, m.cell_case, i)) continue;
         const float* rec = m.cell_rec + (int64_t)i * CRW;
@@ -601,13 +614,14 @@ __device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, co
                                           float* __restrict__ flux, int waves) {
     using Ly = L<DIM>;
     constexpr int C = Ly::C, NG = DIM + 1, RS = Ly::RS, GS = Ly::GS;
-    const int nF = m.n_facets;
+    const int nF = m.n_facets;                            // facets this launch evaluates: [lo, nF)
+    const int lo = m.facet_lo;
     const int stride = gridDim.x * blockDim.x;
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool skip_frozen = frozen_skip(m, nF, stride);
+    int f = lo + blockIdx.x * blockDim.x + threadIdx.x;
+    const bool skip_frozen = frozen_skip(m, nF - lo, stride);
     int2 nxt = next_codes<DIM>(m, f, nF, skip_frozen);
     for (int64_t tile = blockIdx.x; f < nF; f += stride, tile += gridDim.x) {
-    if (waves > 0) prefetch_tile(m.face_rec, nF, Ly::FR, tile + (int64_t)waves * gridDim.x);
+    if (waves > 0) prefetch_tile(m.face_rec + (int64_t)lo * Ly::FR, nF - lo, Ly::FR, tile + (int64_t)waves * gridDim.x);
     const int ca = nxt.x, cb = nxt.y;
     if (m.case_active && !case_on(m, m.face_case, f)) {
         nxt = next_codes<DIM>(m, f + stride, nF, skip_frozen);
@@ -1418,6 +1432,8 @@ static Phys make_phys(const fvm_physics_t* ph) {
 
 static bool aligned32(const void* p) { return ((uintptr_t)p & 31u) == 0; }   // rows use 256-bit accesses
 
+static inline int owned_cells(const fvm_mesh_t* m) { return m->n_owned > 0 ? m->n_owned : m->n_cells; }
+
 static bool mesh_ok(const fvm_mesh_t* m) {
     if (!m || (m->dim != 2 && m->dim != 3) || m->n_comp != m->dim + 2) return false;
     if (m->n_cells <= 0 || m->n_facets <= 0 || m->n_bc < 0 || m->n_char < 0) return false;
@@ -1432,6 +1448,8 @@ static bool mesh_ok(const fvm_mesh_t* m) {
     if (m->n_cases < 0) return false;
     if (m->n_owned < 0 || m->n_owned > m->n_cells || m->char_scale_given < 0 || m->char_scale_given > 1) return false;
     if (m->n_cases > 0 && (m->n_owned > 0 || m->char_scale_given)) return false;
+    if (m->cell_lo < 0 || m->cell_lo > owned_cells(m) || m->facet_lo < 0 || m->facet_lo > m->n_facets) return false;
+    if (m->n_cases > 0 && (m->cell_lo || m->facet_lo)) return false;
     if (m->n_cases == 0 && m->case_active) return false;
     if (m->n_cases > 0 && (!m->cell_case || !m->face_case || !m->ch_off || !m->case_mu || !m->case_mu_b ||
                            !m->case_kappa || (m->n_bc > 0 && !m->bc_case)))
@@ -1444,7 +1462,6 @@ static bool work_ok(const fvm_mesh_t* m, const fvm_work_t* w) {
 }
 
 static inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
-static inline int owned_cells(const fvm_mesh_t* m) { return m->n_owned > 0 ? m->n_owned : m->n_cells; }
 
 // Threads per block of the cell, facet and divergence kernels (set by the autotuner through
 // fvm_set_block_size).  The boundary kernels keep kBlock: their per-block reduction order must not
@@ -1498,12 +1515,14 @@ static int launch_begin(const fvm_mesh_t* m, const Phys& p, const float* prims, 
         FVM_LAUNCH(KID_BC, s, k_bc<DIM><<<blocks_for(m->n_bc), kBlock, 0, s>>>(*m, p, prims, grads, has_grads,
                                                                                w->bc_vals, w->red));
     }
+    if (owned_cells(m) - m->cell_lo <= 0) return launch_status();   // empty range: nothing to launch
     if (m->kg != DIM + 2) {
-        const unsigned gw = persistent_grid(owned_cells(m), kBlock, wave_blocks(k_cell_wide<DIM>, kBlock));
+        const unsigned gw = persistent_grid(owned_cells(m) - m->cell_lo, kBlock, wave_blocks(k_cell_wide<DIM>, kBlock));
         FVM_LAUNCH(KID_CELL, s, k_cell_wide<DIM><<<gw, kBlock, 0, s>>>(*m, p, prims, w->bc_vals, grads, has_grads));
         return launch_status();
     }
-    const unsigned gc = persistent_grid(owned_cells(m), g_block_cell, wave_blocks(k_cell<DIM>, g_block_cell));
+    const unsigned gc =
+        persistent_grid(owned_cells(m) - m->cell_lo, g_block_cell, wave_blocks(k_cell<DIM>, g_block_cell));
     FVM_LAUNCH(KID_CELL, s, k_cell<DIM><<<gc, g_block_cell, 0, s>>>(*m, p, prims, w->bc_vals, grads, has_grads,
                                                                     waves_of(g_pf_cell)));
     return launch_status();
@@ -1512,7 +1531,9 @@ static int launch_begin(const fvm_mesh_t* m, const Phys& p, const float* prims, 
 template <int DIM>
 static int launch_face(const fvm_mesh_t* m, const Phys& p, const float* prims, const float* grads,
                        const fvm_work_t* w, cudaStream_t s) {
-    const unsigned gf = persistent_grid(m->n_facets, g_block_face, wave_blocks(k_face<DIM>, g_block_face));
+    if (m->n_facets - m->facet_lo <= 0) return launch_status();
+    const unsigned gf =
+        persistent_grid(m->n_facets - m->facet_lo, g_block_face, wave_blocks(k_face<DIM>, g_block_face));
     FVM_LAUNCH(KID_FACE, s, k_face<DIM><<<gf, g_block_face, 0, s>>>(*m, p, prims, w->bc_vals, grads, w->flux,
                                                                     waves_of(g_pf_face)));
     return launch_status();
@@ -1629,6 +1650,35 @@ static int stage_finish(const fvm_mesh_t* m, const Phys& p, const fvm_tableau_t*
     rc = launch_div<DIM>(m, p, w->flux, a, b->state, b->prims, b->k, b->dt, w->red, nullptr, st);
     if (rc) return rc;
     if (finalize && a.final_ && (a.adaptive || a.cfl || a.cons)) rc = finalize_impl(m, tab, b, w, a.cons, st);
+    return rc;
+}
+
+// The phases of stage s that `phases` selects, in their order (FVM_PHASE_* bits).
+template <int DIM>
+static int stage_phase_impl(const fvm_mesh_t* m, const Phys& p, const fvm_tableau_t* tab, int s,
+                            const fvm_solver_bufs_t* b, const fvm_work_t* w, int phases, int finalize,
+                            cudaStream_t st) {
+    int rc = FVM_OK;
+    if (phases & (FVM_PHASE_BC | FVM_PHASE_CELLS)) {
+        fvm_mesh_t mm = *m;
+        if (!(phases & FVM_PHASE_BC)) mm.n_bc = 0;                                   // cells only
+        if (!(phases & FVM_PHASE_CELLS)) mm.cell_lo = owned_cells(m);               // boundary values only
+        rc = launch_begin<DIM>(&mm, p, b->prims, b->grads, b->has_grads, w, st);
+        if (rc) return rc;
+    }
+    if (phases & FVM_PHASE_FACES) {
+        rc = launch_face<DIM>(m, p, b->prims, b->grads, w, st);
+        if (rc) return rc;
+    }
+    if (phases & FVM_PHASE_DIV) {
+        fvm_mesh_t mm = *m;
+        mm.cell_lo = 0;
+        StageArgs a = stage_args(tab, s);
+        a.cons = a.final_ && b->cons != nullptr;
+        rc = launch_div<DIM>(&mm, p, w->flux, a, b->state, b->prims, b->k, b->dt, w->red, nullptr, st);
+        if (rc) return rc;
+        if (finalize && a.final_ && (a.adaptive || a.cfl || a.cons)) rc = finalize_impl(&mm, tab, b, w, a.cons, st);
+    }
     return rc;
 }
 
@@ -1835,6 +1885,20 @@ extern "C" int fvm_stage_end(const fvm_mesh_t* mesh, const fvm_physics_t* phys, 
                           : stage_finish<3>(mesh, p, tab, s, bufs, work, finalize != 0, st);
 }
 
+extern "C" int fvm_stage_phase(const fvm_mesh_t* mesh, const fvm_physics_t* phys, const fvm_tableau_t* tab,
+                               int32_t s, const fvm_solver_bufs_t* bufs, const fvm_work_t* work, int32_t phases,
+                               int32_t finalize, void* stream) {
+    if (const int rc = check_common(mesh)) return rc;
+    if (!phys || !tab_ok(tab) || s < 0 || s >= tab->stages || !bufs_ok(bufs) || !work_ok(mesh, work) ||
+        phases <= 0 || phases > 15)
+        return FVM_E_ARG;
+    if (mesh->n_cases > 0 && tab->adaptive) return FVM_E_UNSUPPORTED;
+    const Phys p = make_phys(phys);
+    cudaStream_t st = (cudaStream_t)stream;
+    return mesh->dim == 2 ? stage_phase_impl<2>(mesh, p, tab, s, bufs, work, phases, finalize != 0, st)
+                          : stage_phase_impl<3>(mesh, p, tab, s, bufs, work, phases, finalize != 0, st);
+}
+
 extern "C" int fvm_stage_finalize(const fvm_mesh_t* mesh, const fvm_tableau_t* tab, const fvm_solver_bufs_t* bufs,
                                   const fvm_work_t* work, void* stream) {
     if (!mesh_ok(mesh) || !tab_ok(tab) || !bufs_ok(bufs) || !work || !work->red) return FVM_E_ARG;
@@ -1911,6 +1975,7 @@ extern "C" int fvm_step_fused(const fvm_mesh_t* mesh, const fvm_physics_t* phys,
     if (mesh->n_cases > 0 && tab->adaptive) return FVM_E_UNSUPPORTED;
     if (mesh->n_owned > 0 || mesh->char_scale_given) return FVM_E_UNSUPPORTED;   // partitions use the split stages
     if (mesh->kg != mesh->dim + 2) return FVM_E_UNSUPPORTED;                      // widened stencils: separate launches
+    if (mesh->cell_lo || mesh->facet_lo) return FVM_E_UNSUPPORTED;
     FusedArgs f{};
     f.stages = tab->stages;
     for (int s = 0; s < tab->stages; ++s) {
@@ -1930,7 +1995,9 @@ extern "C" int fvm_multistep_fused(const fvm_mesh_t* mesh, const fvm_physics_t* 
     if (!phys || !bufs_ok(bufs) || !work_ok(mesh, work) || n_terms < 0 || n_terms > FVM_MAX_STAGES ||
         (n_terms > 0 && (!idx || !coef)) || store < 0)
         return FVM_E_ARG;
-    if (mesh->n_owned > 0 || mesh->char_scale_given || mesh->kg != mesh->dim + 2) return FVM_E_UNSUPPORTED;
+    if (mesh->n_owned > 0 || mesh->char_scale_given || mesh->kg != mesh->dim + 2 || mesh->cell_lo ||
+        mesh->facet_lo)
+        return FVM_E_UNSUPPORTED;
     FusedArgs f{};
     f.stages = 1;
     StageArgs& a = f.st[0];

@@ -11,14 +11,16 @@ One explicit stage on every part is then (the reference's per-step work, ``FVMEq
 and the stage combination, ``time_fvm/time_solvers/integrators.py:369-393``, split around two
 exchanges):
 
-  1. halo exchange of the stage input's primitives (rows of ``FVM_ROW`` floats);
-  2. characteristic BC only: each part's sum of the interior sound speed and its count, summed over
+  1. characteristic BC only: each part's sum of the interior sound speed and its count, summed over
      the parts (the reference takes one global mean, ``facet_boundary.py:427``);
-  3. ``fvm_stage_begin``: boundary values and limited gradients of the own cells;
-  4. halo exchange of the limited gradients (rows of ``FVM_GROW`` floats) -- facets on the part
-     boundary rebuild both sides' facet values from them;
-  5. ``fvm_stage_end``: facet fluxes, divergence, stage combination of the own cells;
-  6. last stage: the FP64 CFL maximum and conservation sums combined over the parts, then
+  2. halo exchange of the stage input's primitives (rows of ``FVM_ROW`` floats), overlapped with
+     the boundary values and the limited gradients of the part's inner cells (stencils inside the
+     part), then the limited gradients of the cells next to the halo;
+  3. halo exchange of the limited gradients (rows of ``FVM_GROW`` floats) -- facets on the part
+     boundary rebuild both sides' facet values from them -- overlapped with the fluxes of the
+     inner facets, then the fluxes of the facets on the part boundary;
+  4. divergence, stage combination of the own cells (``fvm_stage_phase`` runs each piece);
+  5. last stage: the FP64 CFL maximum and conservation sums combined over the parts, then
      ``fvm_stage_finalize`` (every part computes the same dt).
 
 Each part evaluates the facets on its boundary itself (both parts do the same arithmetic on the
@@ -68,6 +70,8 @@ class MeshPart:
     tables: KernelTables           # the part's tables, renumbered
     face_rec: torch.Tensor | None = None       # [F_local][FVM_FACE_REC] facet records (see below)
     global_n_char: int = 0                     # characteristic facets of the whole mesh (same on every part)
+    n_inner_cells: int = 0                     # own cells [0, n_inner_cells) have no halo cell in their stencil
+    n_inner_facets: int = 0                    # facets [0, n_inner_facets) have no halo cell on either side
     recv: dict = field(default_factory=dict)   # q -> (start, stop): halo rows owned by part q
     send: dict = field(default_factory=dict)   # q -> local ids of own cells part q keeps in its halo
 
@@ -112,6 +116,18 @@ def split_tables(kt: KernelTables, parts: int, owner: torch.Tensor | None = None
         mine[own] = True
         fmask = mine[fcell[:, 0]] | mine[fcell[:, 1]]
         facets = torch.nonzero(fmask).flatten()
+        # inner facets (both sides this part's cells or a boundary) first, then the facets on the
+        # part boundary; inner cells (stencil within the part) first, then the cells next to the
+        # halo -- so the inner work can run while the halo exchange is in flight
+        cross = ~(mine[fcell[facets, 0]] & mine[fcell[facets, 1]])
+        facets = torch.cat([facets[~cross], facets[cross]])
+        n_inner_f = int((~cross).sum())
+        sc = g_cols[:, own]
+        used = (kt.g_vals[:, :, own] != 0).any(dim=0)
+        foreign = used & (sc < N) & ~mine[sc.clamp(max=N - 1)]
+        adj = foreign.any(dim=0)
+        own = torch.cat([own[~adj], own[adj]])
+        n_inner_c = int((~adj).sum())
         # halo: facet neighbours and gradient-stencil cells of own cells that are not own
         near = torch.cat([fcell[facets].flatten(), g_cols[:, own].flatten()])
         near = near[near < N]
@@ -177,7 +193,8 @@ def split_tables(kt: KernelTables, parts: int, owner: torch.Tensor | None = None
             raise RuntimeError("partition: a facet side points outside the part")
         fr[:, :2] = loc.to(torch.int32).view(torch.float32)
         part = MeshPart(rank=p, parts=parts, n_owned=n_own, cells=cells, facets=facets, bcs=bcs, tables=t,
-                        face_rec=fr, global_n_char=int(kt.n_char))
+                        face_rec=fr, global_n_char=int(kt.n_char), n_inner_cells=n_inner_c,
+                        n_inner_facets=n_inner_f)
         ho = owner[halo]
         for q in range(parts):
             sel = torch.nonzero(ho == q).flatten()
@@ -213,6 +230,14 @@ class LocalComm:
             for q, (a, b) in part.recv.items():
                 torch.index_select(bufs[q], 0, self.send[q][p], out=bufs[p][a:b])
 
+    def start(self, bufs: list[torch.Tensor]):
+        """Begin an exchange whose completion ``finish`` waits for (here: device copies, done at once
+        on the current stream)."""
+        self.exchange(bufs)
+
+    def finish(self, handle):
+        pass
+
     def allreduce(self, tensors: list[torch.Tensor], op: str):
         """Combine the parts' tensors elementwise (``sum`` / ``max`` / ``min``) into every one."""
         acc = tensors[0].clone()
@@ -239,6 +264,12 @@ class DistComm:
         self.send = {q: idx.to(device) for q, idx in part.send.items()}
 
     def exchange(self, bufs: list[torch.Tensor]):
+        self.finish(self.start(bufs))
+
+    def start(self, bufs: list[torch.Tensor]):
+        """Pack the rows each neighbour needs (on the current stream) and post the sends and
+        receives; returns a handle for ``finish``.  With NCCL the transfers run on the
+        communicator's stream, so kernels launched meanwhile overlap them."""
         dist = self.dist
         buf = bufs[0]
         ops, keep = [], []
@@ -248,9 +279,14 @@ class DistComm:
             ops.append(dist.P2POp(dist.isend, packed, q, group=self.group))
         for q, (a, b) in sorted(self.part.recv.items()):
             ops.append(dist.P2POp(dist.irecv, buf[a:b], q, group=self.group))
-        if ops:
-            for req in dist.batch_isend_irecv(ops):
-                req.wait()
+        return (dist.batch_isend_irecv(ops) if ops else [], keep)
+
+    def finish(self, handle):
+        """Make the current stream wait for the transfers (the packed send buffers stay alive
+        until then)."""
+        reqs, _keep = handle
+        for req in reqs:
+            req.wait()
 
     def allreduce(self, tensors: list[torch.Tensor], op: str):
         dist = self.dist
@@ -272,6 +308,18 @@ class _PartState:
         # the characteristic-BC scale is the mean over all parts, formed by PartitionedSolver
         self.dev.struct.char_scale_given = 1
         self.work = self.dev.work()
+        # copies of the mesh struct for the overlapped stage: inner cells, the other own cells,
+        # inner facets, the other facets (fvm_mesh_t cell_lo / n_owned, facet_lo / n_facets)
+        mk = lambda: _lib.Mesh.from_buffer_copy(self.dev.struct)
+        self.m_inner_cells, self.m_outer_cells = mk(), mk()
+        self.m_inner_faces, self.m_outer_faces = mk(), mk()
+        if part.n_inner_cells > 0:
+            self.m_inner_cells.n_owned = part.n_inner_cells
+        else:                                     # no inner cell: the first launch computes boundary values only
+            self.m_inner_cells.cell_lo = part.n_owned
+        self.m_outer_cells.cell_lo = part.n_inner_cells
+        self.m_inner_faces.n_facets = part.n_inner_facets
+        self.m_outer_faces.facet_lo = part.n_inner_facets
         N, C = part.n_local, part.tables.n_comp
         R, G = row_sizes(part.tables.dim)
         self.state = torch.zeros((N, C), device=device)
@@ -368,24 +416,38 @@ class PartitionedSolver:
         """Rows received per exchange, summed over this process's parts."""
         return sum(ps.part.n_local - ps.part.n_owned for ps in self.parts)
 
+    def _phase(self, ps, mesh, s, phases):
+        _lib.check(self.lib.fvm_stage_phase(ct.byref(mesh), ct.byref(self.phys), ct.byref(self.tab), s,
+                                            ct.byref(ps.bufs), ct.byref(ps.work.struct), phases, 0,
+                                            _lib.stream_ptr()), "fvm_stage_phase")
+
     def step(self, n: int = 1):
+        """``n`` steps.  Each stage overlaps its two halo exchanges with the work that does not
+        need the halo: boundary values and the inner cells' gradients run while the primitives are
+        exchanged, the inner facets' fluxes while the limited gradients are; the cells and facets
+        next to the halo follow each exchange.  (The characteristic-BC mean, a reduction over own
+        cells, comes first, so no collective waits behind an exchange.)"""
         S = self.tab.stages
         final_red = self.tab.cfl > 0
         s_ptr = _lib.stream_ptr()
+        BC, CELLS, FACES, DIV = _lib.FVM_PHASE_BC, _lib.FVM_PHASE_CELLS, _lib.FVM_PHASE_FACES, _lib.FVM_PHASE_DIV
         for _ in range(n):
             for s in range(S):
-                self.comm.exchange([ps.prims for ps in self.parts])
                 if self.has_char:
                     self._char_scale()
+                h = self.comm.start([ps.prims for ps in self.parts])
                 for ps in self.parts:
-                    _lib.check(self.lib.fvm_stage_begin(ct.byref(ps.dev.struct), ct.byref(self.phys),
-                                                        ct.byref(ps.bufs), ct.byref(ps.work.struct), s_ptr),
-                               "fvm_stage_begin")
-                self.comm.exchange([ps.grads for ps in self.parts])
+                    self._phase(ps, ps.m_inner_cells, s, BC | CELLS)
+                self.comm.finish(h)
                 for ps in self.parts:
-                    _lib.check(self.lib.fvm_stage_end(ct.byref(ps.dev.struct), ct.byref(self.phys),
-                                                      ct.byref(self.tab), s, ct.byref(ps.bufs),
-                                                      ct.byref(ps.work.struct), 0, s_ptr), "fvm_stage_end")
+                    self._phase(ps, ps.m_outer_cells, s, CELLS)
+                h = self.comm.start([ps.grads for ps in self.parts])
+                for ps in self.parts:
+                    self._phase(ps, ps.m_inner_faces, s, FACES)
+                self.comm.finish(h)
+                for ps in self.parts:
+                    self._phase(ps, ps.m_outer_faces, s, FACES)
+                    self._phase(ps, ps.dev.struct, s, DIV)
             if final_red:
                 self.comm.allreduce([ps.work.red[16:17] for ps in self.parts], "max")
                 for ps in self.parts:

@@ -10,8 +10,8 @@ Used elements per row (stored width in brackets, 2D / 3D):
 
 * primitives, fluxes, boundary values  C              [4 / 8]
 * limited gradients                    d C            [8 / 16]
-* cell record   LSQ weights d KG, their columns KG, displacements K d, limiter eps, meta
-                                       20 / 34        [24 / 40]
+* cell record   LSQ weights d KG, the KG - 1 neighbour columns, displacements K d, limiter eps
+                                       18 / 32        [20 / 32]
 * facet record  two side codes, 1/d, |S|, normal d, non-orthogonal vector d, two displacements
                 d each                 12 / 16        [16 / 16]
 * divergence record  +-1/vol K, facet ids K      6 / 8   [8 / 8]
@@ -40,7 +40,7 @@ from .tables import record_sizes, row_sizes
 def used_record_sizes(dim: int) -> tuple:
     """(cell, facet, divergence) record elements that carry data."""
     K, KG = dim + 1, dim + 2
-    cell = dim * KG + KG + K * dim + 2
+    cell = dim * KG + (KG - 1) + K * dim + 1        # compact record: weights, neighbour columns, disp, eps
     face = 4 + 4 * dim
     div = 2 * K
     return cell, face, div

@@ -215,8 +215,10 @@ class KernelTables:
     def records(self) -> dict:
         """The device record layout of ``include/fvm_b200.h`` (cell, divergence and facet records).
 
-        Cell record [N][CR]: G weights [dim][KG], G columns [KG] (int32 bits), centroid->facet
-        displacements [K][dim], limiter epsilon, meta (int32 bits), zero padding.
+        Cell record [N][CR]: G weights [dim][KG], then for the reference's stencil (compact, CR =
+        20 / 32) the KG - 1 neighbour columns in slot order (int32 bits, the own slot in bits
+        28..30 of the first), centroid->facet displacements [K][dim], limiter epsilon; for a
+        widened stencil G columns [KG], displacements, epsilon, meta (int32 bits), zero padding.
         Divergence record [N][8]: weights [kf], facet indices [kf] (int32 bits), padding.
         Facet record [F][FR]: side-0 cell, side-1 cell (int32 bits; a boundary side holds
         -1 - boundary index), +-1/d (negative: side 1's cell has the lower index), |S|, normal [dim],
@@ -230,12 +232,35 @@ class KernelTables:
         o = 0
         cell[:, o:o + dim * kg] = self.g_vals.permute(2, 0, 1).reshape(N, dim * kg)
         o += dim * kg
-        cell[:, o:o + kg] = bits(self.g_cols.t().contiguous())
-        o += kg
-        cell[:, o:o + K * dim] = self.disp.permute(2, 0, 1).reshape(N, K * dim)
-        o += K * dim
-        cell[:, o] = self.eps
-        cell[:, o + 1] = bits(self.nb_slot)
+        if kg == dim + 1 + 1:
+            # compact record (the reference's stencil: every slot valid, the cell itself in one of
+            # them): the kg - 1 neighbour columns in slot order, the own slot in the top bits of the
+            # first; no meta word
+            cols = self.g_cols.t().long()                                   # [N, kg]
+            own = torch.arange(N).unsqueeze(1)
+            is_self = cols == own
+            one = is_self.sum(1) == 1
+            # rows without their own column are never updated (a partition's halo copies, whose
+            # stencil is left empty): they keep their first kg - 1 columns and the last slot
+            empty = (self.g_vals == 0).all(dim=0).all(dim=0)
+            assert bool((one | empty).all()), "gradient row without exactly one own column"
+            assert N + self.n_bc < (1 << SELF_SLOT_SHIFT), "mesh too large for the compact cell record"
+            is_self = torch.where(one.unsqueeze(1), is_self, torch.arange(kg).unsqueeze(0) == kg - 1)
+            slot = is_self.int().argmax(1)
+            nbr = cols[~is_self].view(N, kg - 1)
+            nbr[:, 0] |= slot.long() << SELF_SLOT_SHIFT
+            cell[:, o:o + kg - 1] = bits(nbr.to(torch.int32))
+            o += kg - 1
+            cell[:, o:o + K * dim] = self.disp.permute(2, 0, 1).reshape(N, K * dim)
+            o += K * dim
+            cell[:, o] = self.eps
+        else:
+            cell[:, o:o + kg] = bits(self.g_cols.t().contiguous())
+            o += kg
+            cell[:, o:o + K * dim] = self.disp.permute(2, 0, 1).reshape(N, K * dim)
+            o += K * dim
+            cell[:, o] = self.eps
+            cell[:, o + 1] = bits(self.nb_slot)
         div = torch.zeros((N, DR), dtype=torch.float32)
         div[:, :kf] = self.f_vals.t()
         div[:, K:K + kf] = bits(self.f_cols.t().contiguous())
@@ -263,12 +288,15 @@ class KernelTables:
 
 
 def record_sizes(dim: int, kg: int | None = None):
-    """(cell record, facet record, divergence record) widths in floats (FVM_CELL_REC_KG etc.): the
-    cell record holds kg gradient slots (default dim + 2, the reference's stencil) and is padded to
-    a multiple of 8 floats."""
-    kg = dim + 2 if kg is None else kg
-    cr = (dim * kg + kg + (dim + 1) * dim + 2 + 7) // 8 * 8
-    return (cr, 16, 8)
+    """(cell record, facet record, divergence record) widths in floats.  The reference's stencil
+    (kg = dim + 2) has the compact cell record FVM_CELL_REC(dim) (20 / 32); a widened stencil the
+    generic one FVM_CELL_REC_KG(dim, kg) (kg slots and a meta word, padded to 8 floats)."""
+    if kg is None or kg == dim + 2:
+        return ((20 if dim == 2 else 32), 16, 8)
+    return ((dim * kg + kg + (dim + 1) * dim + 2 + 7) // 8 * 8, 16, 8)
+
+
+SELF_SLOT_SHIFT = 28     # compact cell record: bits 28..30 of the first column word = the cell's own slot
 
 
 def row_sizes(dim: int):

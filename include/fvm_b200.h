@@ -50,7 +50,7 @@ extern "C" {
  *   state and stage increments keep the plain [N][C] layout. */
 #define FVM_ROW(dim) ((dim) == 2 ? 4 : 8)
 #define FVM_GROW(dim) ((dim) == 2 ? 8 : 16)
-#define FVM_CELL_REC(dim) ((dim) == 2 ? 24 : 40)
+#define FVM_CELL_REC(dim) ((dim) == 2 ? 20 : 32)
 /* Cell record width of a mesh with kg gradient slots (kg = dim + 2: FVM_CELL_REC). */
 #define FVM_CELL_REC_KG(dim, kg) ((((dim) * (kg) + (kg) + ((dim) + 1) * (dim) + 2) + 7) / 8 * 8)
 #define FVM_FACE_REC(dim) ((dim) == 2 ? 16 : 16)
@@ -63,9 +63,12 @@ extern "C" {
  * Integer fields inside float records are stored bit-cast (int32 bits in a float slot). */
 typedef struct fvm_mesh {
     int32_t dim, n_comp, n_cells, n_facets, n_bc, n_char, kg, kf;
-    /* [N][FVM_CELL_REC]: LSQ gradient weights [dim][KG], their columns [KG] (into
-     * [cells ; boundary facets]), centroid->facet displacements [K][dim], limiter epsilon, meta
-     * (bits 24..28: number of valid gradient slots), padding */
+    /* Cell records.  kg = dim + 2 (the reference's stencil): [N][FVM_CELL_REC] = LSQ gradient
+     * weights [dim][KG] in slot order, the KG - 1 neighbour columns in slot order (into
+     * [cells ; boundary facets]; bits 28..30 of the first hold the slot of the cell itself, whose
+     * column is its own index), centroid->facet displacements [K][dim], limiter epsilon.
+     * kg > dim + 2: [N][FVM_CELL_REC_KG] = weights [dim][KG], columns [KG], displacements, epsilon,
+     * meta (bits 4j..4j+3: slot of face neighbour j; bits 24..28: valid slots), padding. */
     const float *cell_rec;
     /* [N][FVM_DIV_REC]: divergence weights +-1/vol [K], facet indices [K] */
     const float *div_rec;
@@ -113,6 +116,12 @@ typedef struct fvm_mesh {
      * facets are skipped by every kernel and its dt / conservation slots are left alone (a
      * corrector's fallback advances only the cases whose proposal failed).  NULL = all active. */
     const uint8_t *case_active;
+    /* Sub-ranges (single meshes only; 0 = from the start): the cell kernel updates cells
+     * [cell_lo, n_owned or n_cells), the facet kernel evaluates facets [facet_lo, n_facets) --
+     * with n_owned / n_facets lowered in a copy of the struct a caller runs any contiguous range,
+     * e.g. a part's inner cells and facets while its halo exchange is in flight. */
+    int32_t cell_lo;
+    int32_t facet_lo;
 } fvm_mesh_t;
 
 /* Gas and scheme constants (ConfigFVM fields, time_fvm/config_fvm.py:52-63). */
@@ -266,6 +275,20 @@ int fvm_stage_end(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const fvm_t
                   const fvm_solver_bufs_t *bufs, const fvm_work_t *work, int32_t finalize, void *stream);
 int fvm_stage_finalize(const fvm_mesh_t *mesh, const fvm_tableau_t *tab, const fvm_solver_bufs_t *bufs,
                        const fvm_work_t *work, void *stream);
+/* Any phases of stage s (no reference counterpart), bits of `phases`: FVM_PHASE_BC (boundary
+ * values), FVM_PHASE_CELLS (limited gradients of cells [cell_lo, n_owned)), FVM_PHASE_FACES (fluxes
+ * of facets [facet_lo, n_facets)), FVM_PHASE_DIV (divergence, stage combination and the next
+ * stage's primitives of the owned cells; the last stage's reductions as fvm_stage_end with
+ * `finalize`).  fvm_stage_begin = BC | CELLS, fvm_stage_end = FACES | DIV; a partitioned stage that
+ * overlaps its exchanges runs BC | CELLS on the inner cells, CELLS on the rest, FACES on the inner
+ * facets, FACES on the rest, then DIV. */
+#define FVM_PHASE_BC 1
+#define FVM_PHASE_CELLS 2
+#define FVM_PHASE_FACES 4
+#define FVM_PHASE_DIV 8
+int fvm_stage_phase(const fvm_mesh_t *mesh, const fvm_physics_t *phys, const fvm_tableau_t *tab, int32_t s,
+                    const fvm_solver_bufs_t *bufs, const fvm_work_t *work, int32_t phases, int32_t finalize,
+                    void *stream);
 /* Partitioned meshes: this part's sum of the interior sound speed over its characteristic
  * facets and their count into work->red[FVM_RED_DOUBLES + 6] and [+ 7] (padded primitives
  * `prims`).  The caller sums both over the parts and stores 10 / (float)(sum / count) at [+ 6]

@@ -86,6 +86,30 @@ def _worker(rank, world, port, case, P_out):
         dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("case,P", [("c2d", 2), ("c2d", 3), ("b3d", 2), ("b3d", 4)])
+def test_inner_ranges_need_no_halo(case, P):
+    """The overlapped stage runs the inner cells' gradients and the inner facets' fluxes while the
+    halo is still being exchanged: their stencils and sides must read no halo row."""
+    kt, parts = _parts(case, P)
+    for p in parts:
+        t, n_loc, n_own = p.tables, p.n_local, p.n_owned
+        ni, nf = p.n_inner_cells, p.n_inner_facets
+        assert 0 <= ni <= n_own and 0 <= nf <= t.n_facets
+        cols = t.g_cols[:, :ni].long()
+        w = (t.g_vals[:, :, :ni] != 0).any(0)
+        halo_col = (cols >= n_own) & (cols < n_loc)
+        assert not bool((halo_col & w).any())
+        sides = t.fcell[:nf].long()
+        assert not bool(((sides >= n_own) & (sides < n_loc)).any())
+        # and the split loses nothing: the other facets each touch a halo cell
+        rest = t.fcell[nf:].long()
+        assert bool(((rest >= n_own) & (rest < n_loc)).any(1).all())
+        # own cells after the inner ones each have a halo cell in their stencil
+        cols_o = t.g_cols[:, ni:n_own].long()
+        w_o = (t.g_vals[:, :, ni:n_own] != 0).any(0)
+        assert bool((((cols_o >= n_own) & (cols_o < n_loc)) & w_o).any(0).all())
+
+
 @pytest.mark.parametrize("case", ["c2d", "b3d"])
 def test_dist_halo_exchange_gloo(case):
     import socket
