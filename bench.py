@@ -886,9 +886,10 @@ def main():
     tuned_full = autotune(eq)
     tuned = {k: v["threads"] for k, v in tuned_full.items()}
     prefetch = {k: v["prefetch"] for k, v in tuned_full.items()}
+    variants = {k: v["variant"] for k, v in tuned_full.items()}
     if os.environ.get("FVM_BENCH_VERBOSE"):
         for k, v in tuned_full.items():
-            print(k, {f"{bs}/{pf}": round(ms * 1e3, 1) for (bs, pf), ms in v["ms"].items()}, file=sys.stderr)
+            print(k, {c: round(ms * 1e3, 1) for c, ms in v["ms"].items()}, file=sys.stderr)
 
     # warm-up
     sol.step(args.warmup)
@@ -1070,7 +1071,7 @@ def main():
                        "cells_per_gpu": N, "facets_per_gpu": F, "state": "fp32 [N,5]",
                        "l2": "inputs larger than L2 (>1 GB touched per stage), no flush",
                        "parallelism": f"{world} independent boxes (one per rank)", "timing": "cuda graph replay",
-                       "block_sizes": tuned, "l2_prefetch": prefetch},
+                       "block_sizes": tuned, "l2_prefetch": prefetch, "kernel_variants": variants},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                          "traffic_source": traffic_src,

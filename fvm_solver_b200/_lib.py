@@ -92,6 +92,7 @@ _SIGS = [
     ("fvm_char_partial", ct.c_int, [_P, _P, _P, _P, _P]),
     ("fvm_set_block_size", ct.c_int, [ct.c_int32, ct.c_int32]),
     ("fvm_set_prefetch", ct.c_int, [ct.c_int32, ct.c_int32]),
+    ("fvm_set_variant", ct.c_int, [ct.c_int32, ct.c_int32]),
     ("fvm_gemm_bf16", ct.c_int, [_P, ct.c_int64, _P, ct.c_int64, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32,
                                  _P, _P, ct.c_int64, _P, _P, ct.c_int64, _P, ct.c_int32, _P, _P]),
     ("fvm_mp_gather_f32", ct.c_int, [_P, _P, ct.c_int32, ct.c_int32, _P, _P]),

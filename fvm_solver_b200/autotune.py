@@ -6,7 +6,8 @@ fastest depends on the mesh (cell count, boundary fraction, batched or not) beca
 many warps each SM keeps in flight against the gather latency and whether the records still come
 from DRAM when a block reads them.  ``autotune`` times each candidate (block size, prefetch) on the
 caller's own mesh -- residual evaluations bracketed by the library's per-launch CUDA events --
-keeps the fastest per kernel, and installs it with ``fvm_set_block_size`` / ``fvm_set_prefetch``.
+keeps the fastest per kernel, and installs it with ``fvm_set_block_size`` / ``fvm_set_prefetch``
+(for the facet kernel also the record-staging variant, ``fvm_set_variant``).
 Results do not change with either (every thread's arithmetic is the same), only the time does.
 Choices are cached per (dim, cell-count bucket, batch size).
 """
@@ -41,9 +42,23 @@ def set_prefetch(kernel: str, blocks_ahead: int):
     _lib.check(_lib.load().fvm_set_prefetch(kid, int(blocks_ahead)), "fvm_set_prefetch")
 
 
+def set_variant(kernel: str, variant: int):
+    kid = {v: k for k, v in KERNELS.items()}[kernel]
+    _lib.check(_lib.load().fvm_set_variant(kid, int(variant)), "fvm_set_variant")
+
+
+STAGED = "staged"           # facet kernel: records staged in shared memory by the bulk-copy unit
+
+
 def _install(kernel: str, cfg: tuple):
     set_block_size(kernel, cfg[0])
+    if cfg[1] == STAGED:
+        set_prefetch(kernel, 0)
+        set_variant(kernel, 1)
+        return
     set_prefetch(kernel, cfg[1])
+    if kernel == "face":
+        set_variant(kernel, 0)
 
 
 def _time_residual(eq, prims, out, reps: int) -> dict:
@@ -64,7 +79,8 @@ def _time_residual(eq, prims, out, reps: int) -> dict:
     return {KERNELS[k]: float(ms[ids == k].mean()) for k in KERNELS if np.any(ids == k)}
 
 
-def autotune(eq, reps: int = 5, candidates=CANDIDATES, prefetch=PREFETCH, use_cache: bool = True) -> dict:
+def autotune(eq, reps: int = 5, candidates=CANDIDATES, prefetch=PREFETCH, use_cache: bool = True,
+             staged: bool = True) -> dict:
     """Pick and install the fastest (block size, prefetch) per kernel for ``eq`` (FVMEquation or
     BatchedFVM).
 
@@ -74,23 +90,27 @@ def autotune(eq, reps: int = 5, candidates=CANDIDATES, prefetch=PREFETCH, use_ca
     key = _key(eq)
     if use_cache and key in _cache:
         for k, v in _cache[key].items():
-            _install(k, (v["threads"], v["prefetch"]))
+            _install(k, v["cfg"])
         return _cache[key]
     prims = eq.cells.get_values()[0].contiguous()
     out = torch.empty_like(prims)
     g_save, f_save = eq.grads.clone(), eq.has_grads.clone()
     timings = {k: {} for k in KERNELS.values()}
     for bs in candidates:
-        for pf in prefetch:
+        for pf in tuple(prefetch) + ((STAGED,) if staged else ()):
             for k in KERNELS.values():
-                _install(k, (bs, pf))
+                _install(k, (bs, pf if (pf != STAGED or k == "face") else 0))
             _time_residual(eq, prims, out, 1)               # warm-up at this configuration
             for k, ms in _time_residual(eq, prims, out, reps).items():
+                if pf == STAGED and k != "face":
+                    continue
                 timings[k][(bs, pf)] = ms
     best = {}
     for k, t in timings.items():
         cfg = min(t, key=t.get)
-        best[k] = {"threads": cfg[0], "prefetch": cfg[1], "ms": t}
+        best[k] = {"threads": cfg[0], "prefetch": 0 if cfg[1] == STAGED else cfg[1],
+                   "variant": "staged" if cfg[1] == STAGED else "registers", "cfg": cfg,
+                   "ms": {f"{a}/{b}": v for (a, b), v in t.items()}}
         _install(k, cfg)
     eq.grads.copy_(g_save)
     eq.has_grads.copy_(f_save)
@@ -100,7 +120,8 @@ def autotune(eq, reps: int = 5, candidates=CANDIDATES, prefetch=PREFETCH, use_ca
 
 
 def reset():
-    """Back to the defaults (256 threads, no prefetch) for every tunable kernel."""
+    """Back to the defaults (256 threads, no prefetch, per-thread record loads) for every tunable
+    kernel."""
     for k in KERNELS.values():
         _install(k, (256, 0))
 

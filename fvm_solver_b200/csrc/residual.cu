@@ -608,37 +608,17 @@ __global__ void __launch_bounds__(kMaxBlock) k_cell(fvm_mesh_t m, Phys p, const 
 // ------------------------------------------------------------------------------------------
 // k_face: facet fluxes.
 // ------------------------------------------------------------------------------------------
-template <int DIM, bool COH>
-__device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, const float* __restrict__ prims,
-                                          const float* __restrict__ bcv, const float* __restrict__ grads,
-                                          float* __restrict__ flux, int waves) {
+// One facet's flux from its record, side codes ca / cb and both sides' primitives P0, P1 and
+// limited gradients G0, G1 (cell sides; a boundary side's value is read here): the arithmetic of
+// every facet kernel, so all of them give the same bits.
+template <int DIM>
+__device__ __forceinline__ void face_eval(const fvm_mesh_t& m, const Phys& p, const float* __restrict__ bcv,
+                                          float* __restrict__ flux, int f, int ca, int cb,
+                                          const float (&rec)[L<DIM>::FR], const float (&P0)[L<DIM>::RS],
+                                          const float (&P1)[L<DIM>::RS], const float (&G0)[L<DIM>::GS],
+                                          const float (&G1)[L<DIM>::GS]) {
     using Ly = L<DIM>;
-    constexpr int C = Ly::C, NG = DIM + 1, RS = Ly::RS, GS = Ly::GS;
-    const int nF = m.n_facets;                            // facets this launch evaluates: [lo, nF)
-    const int lo = m.facet_lo;
-    const int stride = gridDim.x * blockDim.x;
-    int f = lo + blockIdx.x * blockDim.x + threadIdx.x;
-    const bool skip_frozen = frozen_skip(m, nF - lo, stride);
-    int2 nxt = next_codes<DIM>(m, f, nF, skip_frozen);
-    for (int64_t tile = blockIdx.x; f < nF; f += stride, tile += gridDim.x) {
-    if (waves > 0) prefetch_tile(m.face_rec + (int64_t)lo * Ly::FR, nF - lo, Ly::FR, tile + (int64_t)waves * gridDim.x);
-    const int ca = nxt.x, cb = nxt.y;
-    if (m.case_active && !case_on(m, m.face_case, f)) {
-        nxt = next_codes<DIM>(m, f + stride, nF, skip_frozen);
-        continue;
-    }
-    // Both sides: primitives and limited gradient of the cell(s); a boundary side (code < 0) takes
-    // the boundary value, and its gradient is the interior cell's (facet_process.py:364-368).
-    const int cell0 = ca >= 0 ? ca : cb;
-    const int cell1 = cb >= 0 ? cb : ca;
-    float P0[RS], P1[RS], G0[GS], G1[GS];
-    ld_mut<COH, RS>(prims + (int64_t)cell0 * RS, P0);
-    ld_mut<COH, RS>(prims + (int64_t)cell1 * RS, P1);
-    ld_vec_cg<GS>(grads + (int64_t)cell0 * GS, G0);
-    ld_vec_cg<GS>(grads + (int64_t)cell1 * GS, G1);
-    float rec[Ly::FR];
-    ld_vec<Ly::FR>(m.face_rec + (int64_t)f * Ly::FR, rec);
-    nxt = next_codes<DIM>(m, f + stride, nF, skip_frozen);
+    constexpr int C = Ly::C, NG = DIM + 1, RS = Ly::RS;
     const float size = rec[Ly::SIZE];
     const float inv_size = 1.f / size;
     float n[DIM], nh[DIM];
@@ -804,6 +784,145 @@ __device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, co
     F[DIM] += 0.5f * (a_oth * (rho[0] - rho[1])) * size;
     F[DIM + 1] += 0.5f * (a_oth * (Q[0] - Q[1])) * size;
     st_vec<RS>(flux + (int64_t)f * RS, F);
+}
+
+template <int DIM, bool COH>
+__device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, const float* __restrict__ prims,
+                                          const float* __restrict__ bcv, const float* __restrict__ grads,
+                                          float* __restrict__ flux, int waves) {
+    using Ly = L<DIM>;
+    constexpr int C = Ly::C, NG = DIM + 1, RS = Ly::RS, GS = Ly::GS;
+    const int nF = m.n_facets;                            // facets this launch evaluates: [lo, nF)
+    const int lo = m.facet_lo;
+    const int stride = gridDim.x * blockDim.x;
+    int f = lo + blockIdx.x * blockDim.x + threadIdx.x;
+    const bool skip_frozen = frozen_skip(m, nF - lo, stride);
+    int2 nxt = next_codes<DIM>(m, f, nF, skip_frozen);
+    for (int64_t tile = blockIdx.x; f < nF; f += stride, tile += gridDim.x) {
+    if (waves > 0) prefetch_tile(m.face_rec + (int64_t)lo * Ly::FR, nF - lo, Ly::FR, tile + (int64_t)waves * gridDim.x);
+    const int ca = nxt.x, cb = nxt.y;
+    if (m.case_active && !case_on(m, m.face_case, f)) {
+        nxt = next_codes<DIM>(m, f + stride, nF, skip_frozen);
+        continue;
+    }
+    // Both sides: primitives and limited gradient of the cell(s); a boundary side (code < 0) takes
+    // the boundary value, and its gradient is the interior cell's (facet_process.py:364-368).
+    const int cell0 = ca >= 0 ? ca : cb;
+    const int cell1 = cb >= 0 ? cb : ca;
+    float P0[RS], P1[RS], G0[GS], G1[GS];
+    ld_mut<COH, RS>(prims + (int64_t)cell0 * RS, P0);
+    ld_mut<COH, RS>(prims + (int64_t)cell1 * RS, P1);
+    ld_vec_cg<GS>(grads + (int64_t)cell0 * GS, G0);
+    ld_vec_cg<GS>(grads + (int64_t)cell1 * GS, G1);
+    float rec[Ly::FR];
+    ld_vec<Ly::FR>(m.face_rec + (int64_t)f * Ly::FR, rec);
+    nxt = next_codes<DIM>(m, f + stride, nF, skip_frozen);
+    face_eval<DIM>(m, p, bcv, flux, f, ca, cb, rec, P0, P1, G0, G1);
+    }
+}
+
+// Facet records staged by the bulk-copy unit.  Each block walks tiles of blockDim.x facets; thread
+// 0 has the next tile's records (one contiguous range) copied into the other half of a two-stage
+// shared-memory ring with cp.async.bulk, completion counted on that stage's mbarrier, while the
+// block works on the current tile -- so the records (half the facet kernel's DRAM bytes) leave the
+// per-thread load path and its registers, and each thread issues its side gathers as soon as the
+// tile's barrier completes.  Waits are bounded: a thread whose wait gives up reads its record from
+// global memory instead (same values), and after any such wait the block stops staging and reads
+// every later record from global memory; before the block exits it waits (bounded) for copies still
+// in flight.  Bitwise the same results as k_face (face_eval).
+constexpr long long kStageWaitLimit = 1LL << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done = 0;
+    for (long long it = 0; it < kStageWaitLimit && !done; ++it) {
+        asm volatile(
+            "{\n\t.reg .pred q;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, q;\n\t}\n"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+    }
+    return done != 0;
+}
+__device__ __forceinline__ void stage_copy(float* dst, const float* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kMaxBlock) k_face_staged(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+                                                         const float* __restrict__ bcv,
+                                                         const float* __restrict__ grads, float* __restrict__ flux) {
+    using Ly = L<DIM>;
+    constexpr int RS = Ly::RS, GS = Ly::GS, FR = Ly::FR;
+    extern __shared__ __align__(128) float s_rec[];       // [2][blockDim.x][FR]
+    __shared__ __align__(8) uint64_t bar[2];
+    const int B = blockDim.x;
+    const int lo = m.facet_lo, nF = m.n_facets;
+    const int64_t n = (int64_t)nF - lo;
+    const int64_t ntiles = (n + B - 1) / B;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    auto issue = [&](int64_t tile, int st) {
+        const int64_t first = (int64_t)lo + tile * B;
+        const int64_t rows = min((int64_t)B, (int64_t)nF - first);
+        stage_copy(s_rec + (int64_t)st * B * FR, m.face_rec + first * FR, (uint32_t)(rows * FR * 4), &bar[st]);
+    };
+    bool staged = true;
+    int issued_last = -1;                                  // local index of the last tile copied (thread 0)
+    if (threadIdx.x == 0 && blockIdx.x < ntiles) {
+        issue(blockIdx.x, 0);
+        issued_last = 0;
+    }
+    int j = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++j) {
+        const int st = j & 1;
+        if (threadIdx.x == 0 && staged && tile + gridDim.x < ntiles) {
+            issue(tile + gridDim.x, st ^ 1);               // that stage was last read before the previous sync
+            issued_last = j + 1;
+        }
+        const bool ok = staged && stage_wait(&bar[st], (uint32_t)((j >> 1) & 1));
+        const int64_t f = (int64_t)lo + tile * B + threadIdx.x;
+        if (f < nF && !(m.case_active && !case_on(m, m.face_case, (int)f))) {
+            float rec[FR];
+            if (ok) {
+                const float* r = s_rec + ((int64_t)st * B + threadIdx.x) * FR;
+#pragma unroll
+                for (int q = 0; q < FR; q += 4) {
+                    const float4 t = *reinterpret_cast<const float4*>(r + q);
+                    rec[q] = t.x; rec[q + 1] = t.y; rec[q + 2] = t.z; rec[q + 3] = t.w;
+                }
+            } else {
+                ld_vec<FR>(m.face_rec + f * FR, rec);
+            }
+            const int ca = as_int(rec[Ly::FA]), cb = as_int(rec[Ly::FB]);
+            const int cell0 = ca >= 0 ? ca : cb;
+            const int cell1 = cb >= 0 ? cb : ca;
+            float P0[RS], P1[RS], G0[GS], G1[GS];
+            ld_vec<RS>(prims + (int64_t)cell0 * RS, P0);
+            ld_vec<RS>(prims + (int64_t)cell1 * RS, P1);
+            ld_vec_cg<GS>(grads + (int64_t)cell0 * GS, G0);
+            ld_vec_cg<GS>(grads + (int64_t)cell1 * GS, G1);
+            face_eval<DIM>(m, p, bcv, flux, (int)f, ca, cb, rec, P0, P1, G0, G1);
+        }
+        staged = staged && !__syncthreads_or(!ok);
+    }
+    // copies that may still be in flight after a wait gave up: wait for them (bounded) before the
+    // block's shared memory is released
+    if (threadIdx.x == 0 && !staged) {
+        for (int k = max(0, issued_last - 1); k <= issued_last; ++k) stage_wait(&bar[k & 1], (uint32_t)((k >> 1) & 1));
     }
 }
 
@@ -1470,6 +1589,9 @@ static int g_block_cell = kBlock, g_block_face = kBlock, g_block_div = kBlock;
 // Record prefetch distance in waves of resident blocks per kernel: -1 = default (off: with the
 // persistent kernels' index look-ahead it measured slower on the 2M-tet box), 0 = off.
 static int g_pf_cell = -1, g_pf_face = -1, g_pf_div = -1;
+// Facet kernel variant (fvm_set_variant): 0 = records loaded by each thread (k_face), 1 = records
+// staged through shared memory by the bulk-copy unit (k_face_staged).  Same results.
+static int g_face_variant = 0;
 static inline int waves_of(int setting) { return setting < 0 ? 0 : setting; }
 
 // Resident blocks of `kernel` at `threads` per block over the whole GPU (one wave), cached.
@@ -1528,10 +1650,47 @@ static int launch_begin(const fvm_mesh_t* m, const Phys& p, const float* prims, 
     return launch_status();
 }
 
+// Resident blocks of the staged facet kernel at `threads` per block (its dynamic shared memory
+// counted), cached per block size and device.
+template <int DIM>
+static int staged_wave(int threads) {
+    static int cache[2][kMaxBlock / 32 + 1][64];
+    static bool attr[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev >= 64) return 0;
+    int& c = cache[DIM - 2][threads / 32][dev];
+    if (c > 0) return c;
+    const int smem = 2 * threads * L<DIM>::FR * 4;
+    if (!attr[dev]) {
+        if (cudaFuncSetAttribute(k_face_staged<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 2 * kMaxBlock * L<DIM>::FR * 4) != cudaSuccess)
+            return 0;
+        attr[dev] = true;
+    }
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_face_staged<DIM>, threads, smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 0;
+    c = per_sm * sms;
+    return c;
+}
+
 template <int DIM>
 static int launch_face(const fvm_mesh_t* m, const Phys& p, const float* prims, const float* grads,
                        const fvm_work_t* w, cudaStream_t s) {
     if (m->n_facets - m->facet_lo <= 0) return launch_status();
+    if (g_face_variant == 1) {
+        const int wave = staged_wave<DIM>(g_block_face);
+        if (wave <= 0) {
+            launch_status();
+            return FVM_E_CUDA;
+        }
+        const unsigned gf = persistent_grid(m->n_facets - m->facet_lo, g_block_face, wave);
+        const size_t smem = (size_t)2 * g_block_face * L<DIM>::FR * 4;
+        FVM_LAUNCH(KID_FACE, s, k_face_staged<DIM><<<gf, g_block_face, smem, s>>>(*m, p, prims, w->bc_vals, grads,
+                                                                                  w->flux));
+        return launch_status();
+    }
     const unsigned gf =
         persistent_grid(m->n_facets - m->facet_lo, g_block_face, wave_blocks(k_face<DIM>, g_block_face));
     FVM_LAUNCH(KID_FACE, s, k_face<DIM><<<gf, g_block_face, 0, s>>>(*m, p, prims, w->bc_vals, grads, w->flux,
@@ -2138,6 +2297,12 @@ extern "C" int fvm_set_prefetch(int32_t kernel_id, int32_t waves_ahead) {
         case KID_DIV_STAGE: g_pf_div = waves_ahead; return FVM_OK;
         default: return FVM_E_ARG;
     }
+}
+
+extern "C" int fvm_set_variant(int32_t kernel_id, int32_t variant) {
+    if (kernel_id != KID_FACE || variant < 0 || variant > 1) return FVM_E_ARG;
+    g_face_variant = variant;
+    return FVM_OK;
 }
 
 extern "C" int fvm_set_block_size(int32_t kernel_id, int32_t threads) {

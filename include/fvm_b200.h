@@ -175,6 +175,10 @@ const char *fvm_version(void);
  * the events.  Kernel ids: 0 ell_spmv, 1 ell_spmm, 2 bc, 3 cell, 4 face, 5 div_stage,
  * 6 finalize, 7 state_to_prims, 8 reduce_state, 9 batched, 10 corrector, 11 fused step. */
 int fvm_profile_start(int32_t capacity);
+/* Kernel variant (no reference counterpart; results unchanged): for the facet kernel
+ * (kernel_id 4), 0 = each thread loads its facet record, 1 = the records of a block's next tile
+ * are staged in shared memory by the bulk-copy unit (cp.async.bulk + mbarrier, two stages). */
+int fvm_set_variant(int32_t kernel_id, int32_t variant);
 /* Launch configuration (no reference counterpart): threads per block of the cell (id 3), facet
  * (id 4) and divergence/stage (id 5) kernels for all later launches of this process; a multiple
  * of 32 in [64, 512].  Results do not depend on it (each thread's arithmetic is unchanged); the

@@ -284,10 +284,11 @@ def test_block_size_invariance_and_autotune():
     outs = []
     try:
         for bs in (64, 128, 256, 512):
-            for pf in (0, 1, 3):
+            for pf in (0, 1, 3, "staged"):
                 for k in ("cell", "face", "div_stage"):
                     autotune.set_block_size(k, bs)
-                    autotune.set_prefetch(k, pf)
+                    autotune.set_prefetch(k, 0 if pf == "staged" else pf)
+                autotune.set_variant("face", 1 if pf == "staged" else 0)
                 eq.reset_gradients()
                 outs.append(eq.forward(p))
         assert all(torch.equal(outs[0], o) for o in outs)
@@ -295,6 +296,7 @@ def test_block_size_invariance_and_autotune():
         assert set(best) == {"cell", "face", "div_stage"}
         assert all(v["threads"] in autotune.CANDIDATES for v in best.values())
         assert all(v["prefetch"] in autotune.PREFETCH for v in best.values())
+        assert best["face"]["variant"] in ("registers", "staged")
         eq.reset_gradients()
         assert torch.equal(eq.forward(p), outs[0])
     finally:
