@@ -839,6 +839,57 @@ def corrector_bench(args, timed):
     print(json.dumps(out))
 
 
+def ell_result(tables, reps: int = 20) -> dict:
+    """The ELL operator seam (``SPMB200``, the drop-in for the reference's Triton ELL path) on the
+    benchmark box's own operators, timed as the reference's micro-benchmark does
+    (``benchmark/bench_utils.py:27-55``: random dense operand, warm-up, a loop of products) but with
+    CUDA events: G_mats (LSQ gradients, [dim N] x [N + F_b], K = dim + 2) times the C-component
+    state, flux_mat (divergence, [N] x [F], K = dim + 1) times C-component facet fluxes, and G_mats
+    times one column (the reference script's case).  Algorithmic bytes per product: the ELL values
+    and int32 columns (8 B per slot), the operand and the output once each (4 B per element).
+    torch's CSR SpMM on the same matrices is timed beside it."""
+    from fvm_solver_b200.sparse import SPMB200
+    peak, peak_kind = measured_peaks()
+    stream = torch.cuda.current_stream()
+    C = tables.n_comp
+    out = {}
+    for name, A, B in (("G_mats_spmm", tables.ops.G_mats, C), ("flux_mat_spmm", tables.ops.flux_mat, C),
+                       ("G_mats_spmv", tables.ops.G_mats, 1)):
+        op = SPMB200(A, "cuda")
+        X = torch.randn((A.shape[1], B), device="cuda", generator=torch.Generator(device="cuda").manual_seed(0))
+        f = (lambda: op.spMM(X)) if B > 1 else (lambda: op.spMV(X[:, 0]))
+        for _ in range(5):
+            f()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            f()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        byts = op.M * op.K * 8 + A.shape[1] * B * 4 + op.M * B * 4
+        Ad = A.to_sparse_csr().cuda()
+        g = lambda: torch.sparse.mm(Ad, X)
+        for _ in range(3):
+            g()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            g()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_t = e0.elapsed_time(e1) / reps
+        out[name] = {"rows": op.M, "K": op.K, "B": B, "ms": ms, "algorithmic_bytes": byts,
+                     "achieved_gbs": byts / (ms / 1e3) / 1e9, "frac": byts / (ms / 1e3) / 1e9 / peak,
+                     "torch_csr_ms": ms_t}
+        del op, Ad
+    torch.cuda.empty_cache()
+    return {"peak_gbs": peak, "peak_source": peak_kind, "ops": out,
+            "method": "CUDA events over 20 products after 5 warm-up ones (output allocated per call, "
+                      "as SPM.spMM does)"}
+
+
 def corrector_checkpoint_result(args, timed) -> dict:
     """The headline line's corrector key: the stored 2D model (trained offline by
     ``--workload corrector --save-checkpoint``) evaluated on the held-out cases; training is not
@@ -1061,6 +1112,7 @@ def main():
         extras["channel_cylinder"] = channel_cylinder_result(50, 5, args.drift_steps, not args.no_cpu_baseline, timed)
         extras["ensemble"] = ensemble_result(args.cases, 20, 5, timed, cfl=args.ensemble_cfl or ENSEMBLE_CFL)
         extras["corrector"] = corrector_checkpoint_result(args, timed)
+        extras["ell"] = ell_result(eq.tables)
     if rank == 0:
         out = {
             "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,

@@ -8,11 +8,17 @@
 //  * SpMM with few columns (B = 4 or 5 conserved variables) gives each thread a whole row and up to
 //    8 columns, so no lanes are masked (the reference's BLOCK_B >= 16 masks >= 69 % of them);
 //  * SpMV of a multi-column x is one launch, not one launch per column (ell_kernel.py:157-165);
-//  * the bias is added in-kernel after the K-slot accumulation (same order as the reference).
+//  * the bias is added in-kernel after the K-slot accumulation (same order as the reference);
+//  * the slot loop is unrolled to a compile-time bound (K <= FVM_MAX_ELL_K = 16), so a row's
+//    gathers are issued together instead of one dependent load chain per slot.
 #include "fvm_common.cuh"
 
 namespace fvm {
 
+// Every kernel is templated on an upper bound KT of the slot count (4, 8 or 16) and unrolls the
+// slot loop, so the values, columns and gathers of all slots of a row are in flight together (one
+// dependent round trip per row instead of K); slots are summed in order k = 0, 1, ... as before.
+template <int KT>
 __global__ void __launch_bounds__(kBlock) k_ell_spmv(const float* __restrict__ vals,
                                                       const int32_t* __restrict__ cols, int64_t M,
                                                       int K, const float* __restrict__ x,
@@ -20,18 +26,26 @@ __global__ void __launch_bounds__(kBlock) k_ell_spmv(const float* __restrict__ v
                                                       float* __restrict__ y, int64_t incy) {
     const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (r >= M) return;
-    float acc = 0.f;
-    for (int k = 0; k < K; ++k) {
-        const float v = __ldg(vals + k * M + r);
-        const int32_t c = __ldg(cols + k * M + r);
-        acc = fmaf(v, __ldg(x + c * incx), acc);
+    float v[KT], xv[KT];
+#pragma unroll
+    for (int k = 0; k < KT; ++k) {
+        v[k] = 0.f;
+        xv[k] = 0.f;
+        if (k < K) {
+            v[k] = __ldg(vals + k * M + r);
+            xv[k] = __ldg(x + (int64_t)__ldg(cols + k * M + r) * incx);
+        }
     }
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < KT; ++k)
+        if (k < K) acc = fmaf(v[k], xv[k], acc);
     if (bias) acc += __ldg(bias + r);
     y[r * incy] = acc;
 }
 
 // One thread per (row, group of CB columns).
-template <int CB>
+template <int KT, int CB>
 __global__ void __launch_bounds__(kBlock) k_ell_spmm(const float* __restrict__ vals,
                                                       const int32_t* __restrict__ cols, int64_t M,
                                                       int K, const float* __restrict__ X,
@@ -42,15 +56,25 @@ __global__ void __launch_bounds__(kBlock) k_ell_spmm(const float* __restrict__ v
     if (r >= M) return;
     const int c0 = blockIdx.y * CB;
     const int nb = min(CB, B - c0);
+    float v[KT];
+    int64_t xo[KT];
+#pragma unroll
+    for (int k = 0; k < KT; ++k) {
+        v[k] = k < K ? __ldg(vals + k * M + r) : 0.f;
+        xo[k] = k < K ? (int64_t)__ldg(cols + k * M + r) * ldx + c0 : 0;
+    }
     float acc[CB];
 #pragma unroll
     for (int j = 0; j < CB; ++j) acc[j] = 0.f;
-    for (int k = 0; k < K; ++k) {
-        const float v = __ldg(vals + k * M + r);
-        const float* xr = X + (int64_t)__ldg(cols + k * M + r) * ldx + c0;
+#pragma unroll
+    for (int k = 0; k < KT; ++k) {
+        if (k >= K) break;
+        float xr[CB];
+#pragma unroll
+        for (int j = 0; j < CB; ++j) xr[j] = j < nb ? __ldg(X + xo[k] + j) : 0.f;
 #pragma unroll
         for (int j = 0; j < CB; ++j)
-            if (j < nb) acc[j] = fmaf(v, __ldg(xr + j), acc[j]);
+            if (j < nb) acc[j] = fmaf(v[k], xr[j], acc[j]);
     }
     float b = bias ? __ldg(bias + r) : 0.f;
     float* yr = Y + r * ldy + c0;
@@ -60,6 +84,7 @@ __global__ void __launch_bounds__(kBlock) k_ell_spmm(const float* __restrict__ v
 }
 
 // Specialisation for 4 contiguous, 16-byte aligned columns: one float4 gather per slot.
+template <int KT>
 __global__ void __launch_bounds__(kBlock) k_ell_spmm4(const float* __restrict__ vals,
                                                        const int32_t* __restrict__ cols, int64_t M,
                                                        int K, const float* __restrict__ X,
@@ -67,14 +92,23 @@ __global__ void __launch_bounds__(kBlock) k_ell_spmm4(const float* __restrict__ 
                                                        float* __restrict__ Y) {
     const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (r >= M) return;
-    float a[4] = {0.f, 0.f, 0.f, 0.f};
-    for (int k = 0; k < K; ++k) {
-        const float v = __ldg(vals + k * M + r);
-        float x[4];
-        load_row<4>(X + 4 * (int64_t)__ldg(cols + k * M + r), x);
+    float v[KT], x[KT][4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) a[j] = fmaf(v, x[j], a[j]);
+    for (int k = 0; k < KT; ++k) {
+        v[k] = 0.f;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) x[k][j] = 0.f;
+        if (k < K) {
+            v[k] = __ldg(vals + k * M + r);
+            load_row<4>(X + 4 * (int64_t)__ldg(cols + k * M + r), x[k]);
+        }
     }
+    float a[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int k = 0; k < KT; ++k)
+        if (k < K)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) a[j] = fmaf(v[k], x[k][j], a[j]);
     if (bias) {
         const float b = __ldg(bias + r);
 #pragma unroll
@@ -173,10 +207,15 @@ extern "C" int fvm_ell_spmv(const float* vals, const int32_t* cols, int64_t M, i
                             void* stream) {
     if (M < 0 || K < 0 || (M > 0 && (!vals && K > 0)) || (M > 0 && (!x || !y))) return FVM_E_ARG;
     if (M == 0) return FVM_OK;
+    if (K > FVM_MAX_ELL_K) return FVM_E_UNSUPPORTED;
     const int64_t grid = (M + fvm::kBlock - 1) / fvm::kBlock;
-    FVM_LAUNCH(fvm::KID_ELL_SPMV, (cudaStream_t)stream,
-               fvm::k_ell_spmv<<<(unsigned)grid, fvm::kBlock, 0, (cudaStream_t)stream>>>(vals, cols, M, K, x,
-                                                                                        incx, bias, y, incy));
+    cudaStream_t s = (cudaStream_t)stream;
+#define FVM_SPMV(KT) FVM_LAUNCH(fvm::KID_ELL_SPMV, s, fvm::k_ell_spmv<KT><<<(unsigned)grid, fvm::kBlock, 0, s>>>( \
+                                    vals, cols, M, K, x, incx, bias, y, incy))
+    if (K <= 4) FVM_SPMV(4);
+    else if (K <= 8) FVM_SPMV(8);
+    else FVM_SPMV(16);
+#undef FVM_SPMV
     return launch_status();
 }
 
@@ -188,15 +227,23 @@ extern "C" int fvm_ell_spmm(const float* vals, const int32_t* cols, int64_t M, i
     if (M == 0 || B == 0) return FVM_OK;
     const int64_t gx = (M + fvm::kBlock - 1) / fvm::kBlock;
     cudaStream_t s = (cudaStream_t)stream;
+    if (K > FVM_MAX_ELL_K) return FVM_E_UNSUPPORTED;
     const bool aligned = ((uintptr_t)X % 16 == 0) && ((uintptr_t)Y % 16 == 0);
     if (B == 4 && ldx == 4 && ldy == 4 && aligned) {
-        FVM_LAUNCH(fvm::KID_ELL_SPMM, s,
-                   fvm::k_ell_spmm4<<<(unsigned)gx, fvm::kBlock, 0, s>>>(vals, cols, M, K, X, bias, Y));
+#define FVM_SPMM4(KT) FVM_LAUNCH(fvm::KID_ELL_SPMM, s, fvm::k_ell_spmm4<KT><<<(unsigned)gx, fvm::kBlock, 0, s>>>( \
+                                     vals, cols, M, K, X, bias, Y))
+        if (K <= 4) FVM_SPMM4(4);
+        else if (K <= 8) FVM_SPMM4(8);
+        else FVM_SPMM4(16);
+#undef FVM_SPMM4
     } else {
         const unsigned gy = (unsigned)((B + 7) / 8);
-        FVM_LAUNCH(fvm::KID_ELL_SPMM, s,
-                   fvm::k_ell_spmm<8><<<dim3((unsigned)gx, gy), fvm::kBlock, 0, s>>>(vals, cols, M, K, X, ldx,
-                                                                                     B, bias, Y, ldy));
+#define FVM_SPMM(KT) FVM_LAUNCH(fvm::KID_ELL_SPMM, s, fvm::k_ell_spmm<KT, 8><<<dim3((unsigned)gx, gy), fvm::kBlock, 0, s>>>( \
+                                    vals, cols, M, K, X, ldx, B, bias, Y, ldy))
+        if (K <= 4) FVM_SPMM(4);
+        else if (K <= 8) FVM_SPMM(8);
+        else FVM_SPMM(16);
+#undef FVM_SPMM
     }
     return launch_status();
 }

@@ -9,7 +9,8 @@ Semantics kept from the reference:
 * ``spMV(x, b)``: x 1-D [N] -> y [M]; x 2-D [N, B] -> y [M, B]; strided 1-D views are read in
   place (``ell_kernel.py:148-171``); ``b`` is added after the product.
 * ``spMM(X, b)``: X [N, B] -> Y [M, B] (+ b[:, None]); B == 1 goes through the SpMV kernel.
-* Outputs are newly allocated; errors are Python exceptions (``ValueError`` for ELL overflow).
+* Outputs are newly allocated; errors are Python exceptions (``ValueError`` for ELL overflow, and
+  for rows wider than 16 slots -- every operator of the residual has at most dim + 2).
 * ``to_sparse(A, device)`` picks the implementation by device type.  Only CUDA devices are
   supported: there is no CPU fallback, so a non-CUDA device raises ``RuntimeError``.
 """
@@ -50,6 +51,8 @@ class SPMB200(SPM):
         if cols.numel() and int(cols.max()) >= 2 ** 31:
             raise ValueError("column index does not fit int32")
         self.M, self.K = vals.shape
+        if self.K > 16:
+            raise ValueError(f"ELL rows of {self.K} slots: at most 16 are supported (FVM_MAX_ELL_K)")
         self.N = A.shape[1]
         dev = torch.device(device)
         self.vals = vals.t().contiguous().to(torch.float32).to(dev)       # [K][M]

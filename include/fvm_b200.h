@@ -38,6 +38,7 @@ extern "C" {
 
 #define FVM_MAX_STAGES 12
 #define FVM_MAX_KG 16
+#define FVM_MAX_ELL_K 16    /* widest ELL row fvm_ell_spmv / fvm_ell_spmm take (FVM_E_UNSUPPORTED above) */
 #define FVM_RED_DOUBLES 64
 #define FVM_NOALLOC_SCRATCH_BYTES (16 * 1024 * 1024)
 
