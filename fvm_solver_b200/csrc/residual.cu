@@ -598,8 +598,14 @@ __global__ void __launch_bounds__(kBlock) k_cell_wide(fvm_mesh_t m, Phys p, cons
     }
 }
 
+#ifndef FVM_CELL_MAXNREG
+#define FVM_CELL_MAXNREG 96
+#endif
+// Register budget of the cell kernel: left to ptxas it settles on 64 with a spill in the loop;
+// the budget trades resident warps against registers for the one-ahead loads and the unrolled
+// stencil (chosen by timing on the 1.97 M-tet box).
 template <int DIM>
-__global__ void __launch_bounds__(kMaxBlock) k_cell(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+__global__ void __maxnreg__(FVM_CELL_MAXNREG) k_cell(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
                                                   const float* __restrict__ bcv, float* __restrict__ grads,
                                                   int32_t* __restrict__ has_grads, int waves) {
     cell_body<DIM, false>(m, p, prims, bcv, grads, has_grads, waves);
@@ -791,7 +797,7 @@ __device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, co
                                           const float* __restrict__ bcv, const float* __restrict__ grads,
                                           float* __restrict__ flux, int waves) {
     using Ly = L<DIM>;
-    constexpr int C = Ly::C, NG = DIM + 1, RS = Ly::RS, GS = Ly::GS;
+    constexpr int RS = Ly::RS, GS = Ly::GS;
     const int nF = m.n_facets;                            // facets this launch evaluates: [lo, nF)
     const int lo = m.facet_lo;
     const int stride = gridDim.x * blockDim.x;
