@@ -787,6 +787,14 @@ def corrector_evaluate(model_src, args, three_d: bool, ratios=(3.0, 1.2), spinup
         f[1].record(stream)
         torch.cuda.synchronize()
         ms_corr = f[0].elapsed_time(f[1])
+        # the proposal + checks graph alone (it reads the state and writes only its own buffers)
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(10):
+            ro._run_propose()
+        g1.record(stream)
+        torch.cuda.synchronize()
+        ms_propose = g0.elapsed_time(g1) / 10
         err, bad_plain, bad_corr = [], 0, 0
         for c in range(args.eval_cases):
             a = corr.case_state(c).double()
@@ -797,6 +805,8 @@ def corrector_evaluate(model_src, args, three_d: bool, ratios=(3.0, 1.2), spinup
             if fa and fr:
                 err.append(float(((a - r).norm() / r.norm()).item()))
         return {"residual_ratio": ratio, "speedup": ms_plain / ms_corr, "ms_corrected": ms_corr,
+                "ms_per_window": {"corrected": ms_corr / args.windows, "plain": ms_plain / args.windows,
+                                  "proposal_and_checks": ms_propose},
                 "accept_rate": ro.accepted / max(ro.windows, 1),
                 "windows_without_fallback": ro.full_windows / max(args.windows, 1),
                 "rel_l2_vs_plain": {"max": max(err) if err else None, "mean": float(np.mean(err)) if err else None,

@@ -453,8 +453,10 @@ class CheckedRollout:
         self.prop = torch.empty((N, C), device=d)
         self.r0 = torch.empty((N, C), device=d)
         self.r1 = torch.empty((N, C), device=d)
-        self.sq = torch.empty((N, C), device=d)
-        self.ok = torch.zeros(b.n_cases, dtype=torch.bool, device=d)
+        self.vol32 = model.vol.float().contiguous()
+        self.check_sums = torch.zeros((b.n_cases, 3 * C + 3), dtype=torch.float64, device=d)
+        self.ok_u8 = torch.zeros(b.n_cases, dtype=torch.uint8, device=d)
+        self.ok = self.ok_u8.view(torch.bool)
         self.use_graphs = use_graphs
         self._g_propose = None
         self._fallback = None
@@ -463,37 +465,25 @@ class CheckedRollout:
         self.windows = 0
         self.full_windows = 0
 
-    def _sums(self, x) -> torch.Tensor:
-        out = torch.empty((self.b.n_cases, x.shape[1]), dtype=torch.float64, device=x.device)
-        _lib.check(self.lib.fvm_conservation(ct.byref(self.b.dev.struct), x.contiguous().data_ptr(), out.data_ptr(),
-                                             ct.byref(self.b.work.struct), _lib.stream_ptr()), "fvm_conservation")
-        return out
-
     def _propose(self):
-        """Proposal and both checks; leaves the per-case verdicts in ``self.ok`` (device)."""
+        """Proposal and its checks; leaves the per-case verdicts in ``self.ok`` (device).
+
+        ``fvm_corrector_checks`` reduces, per case and in FP64, the volume-weighted sums of the state,
+        the proposal and r0 (conservation: the proposal's mass and energy must equal the state's plus
+        k dt times r0's, to ``drift_tol`` relative), the squared residual norms of state and proposal
+        (|r1|^2 <= ratio^2 |r0|^2) and the number of inadmissible proposal cells (density or internal
+        energy <= 0, or not finite), then writes the verdicts: two launches after the proposal."""
         b, k = self.b, self.m.k
         U = b.cells.state
-        dim = b.mesh.dim
         self.m.res(U, self.r0)
         self.m.predict(U, self.prop, self.r0)
         self.m.res(self.prop, self.r1)
-        M0, Mp, R0 = self._sums(U), self._sums(self.prop), self._sums(self.r0)
-        dt = b.t_solver.dt.double()
-        cons = slice(dim, dim + 2)                           # mass and energy
-        expected = M0[:, cons] + k * dt[:, None] * R0[:, cons]
-        drift = ((Mp[:, cons] - expected).abs() / M0[:, cons].abs()).max(dim=1).values
-        torch.mul(self.r0, self.r0, out=self.sq)
-        n0 = self._sums(self.sq).sum(dim=1)
-        torch.mul(self.r1, self.r1, out=self.sq)
-        n1 = self._sums(self.sq).sum(dim=1)
-        # admissibility: density and internal energy positive in every cell of the case
-        P = self.prop
-        rho = P[:, dim]
-        e_int = P[:, dim + 1] - 0.5 * P[:, :dim].square().sum(dim=1) / rho
-        self.sq.zero_()
-        self.sq[:, 0] = ((rho <= 0) | (e_int <= 0) | ~torch.isfinite(e_int)).float()
-        bad = self._sums(self.sq)[:, 0]
-        self.ok.copy_((drift <= self.drift_tol) & (n1 <= self.ratio ** 2 * n0) & torch.isfinite(drift) & (bad == 0))
+        N, C = U.shape
+        _lib.check(self.lib.fvm_corrector_checks(
+            U.data_ptr(), self.prop.data_ptr(), self.r0.data_ptr(), self.r1.data_ptr(), self.vol32.data_ptr(),
+            self.m.cell_case32.data_ptr(), N, C, b.n_cases, b.t_solver.dt.data_ptr(), k, float(self.drift_tol),
+            float(self.ratio), self.check_sums.data_ptr(), self.ok_u8.data_ptr(), None, _lib.stream_ptr()),
+            "fvm_corrector_checks")
 
     def _run_propose(self):
         if not self.use_graphs:

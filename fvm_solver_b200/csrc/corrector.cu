@@ -20,6 +20,8 @@
 #include <cuda_bf16.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "fvm_common.cuh"
 
 namespace fvm {
@@ -1075,5 +1077,151 @@ extern "C" int fvm_decoder_back_f32(const float* h, const float* Wo, const float
     cudaStream_t s = (cudaStream_t)stream;
     FVM_LAUNCH(KID_CORRECTOR, s, corr::k_decoder_back_f32<<<corr::nblk((int64_t)N * corr::kLayerW, 256), 256, 0, s>>>(
                                      h, Wo, dOut, N, O, dh, dWo, dbo));
+    return launch_status();
+}
+
+// ------------------------------------------------------------------------------------------
+// Acceptance checks of a corrector proposal, per case, in two launches (fvm_corrector_checks).
+//   sums[c] (FP64, 3C + 3 slots): sum vol U, sum vol P, sum vol r0 (C each), sum vol |r0|^2,
+//   sum vol |r1|^2, number of inadmissible cells of P (rho <= 0, internal energy <= 0 or not finite).
+//   ok[c] = drift <= tol && |r1|^2 <= ratio^2 |r0|^2 && drift finite && no inadmissible cell, with
+//   drift = max over mass and energy of |sum vol P - (sum vol U + k dt_c sum vol r0)| / |sum vol U|.
+// The reduction walks one contiguous chunk of cells per warp and flushes per case change (cells of
+// a case are contiguous), as the conservation sums do; the verdict kernel clears the sums after
+// reading them, so the pair can be replayed from a CUDA graph.
+// ------------------------------------------------------------------------------------------
+namespace fvm {
+namespace corr {
+
+template <int C>
+__global__ void k_checks_reduce(const float* __restrict__ U, const float* __restrict__ P,
+                                const float* __restrict__ r0, const float* __restrict__ r1,
+                                const float* __restrict__ vol, const int32_t* __restrict__ cell_case, int N,
+                                double* __restrict__ sums) {
+    constexpr int DIM = C - 2, NS = 3 * C + 3;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t chunk = (((int64_t)N + warps - 1) / warps + 31) & ~(int64_t)31;
+    const int64_t beg = w * chunk, end = beg + chunk < N ? beg + chunk : (int64_t)N;
+    int cur = -1;
+    double acc[NS];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) acc[q] = 0.0;
+    auto flush = [&]() {
+        if (cur < 0) return;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            double v = acc[q];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(full, v, o);
+            if (lane == 0) atomicAdd(sums + (int64_t)cur * NS + q, v);
+            acc[q] = 0.0;
+        }
+    };
+    for (int64_t i0 = beg; i0 < end; i0 += 32) {
+        const int64_t i = i0 + lane;
+        const bool live = i < end;
+        const int cse = live ? __ldg(cell_case + i) : -1;
+        double v[NS];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) v[q] = 0.0;
+        if (live) {
+            const double vo = (double)__ldg(vol + i);
+            float u[C], pp[C], a[C], b[C];
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                u[c] = __ldg(U + i * C + c);
+                pp[c] = __ldg(P + i * C + c);
+                a[c] = __ldg(r0 + i * C + c);
+                b[c] = __ldg(r1 + i * C + c);
+            }
+            double n0 = 0.0, n1 = 0.0;
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                v[c] = vo * (double)u[c];
+                v[C + c] = vo * (double)pp[c];
+                v[2 * C + c] = vo * (double)a[c];
+                n0 += vo * (double)(a[c] * a[c]);
+                n1 += vo * (double)(b[c] * b[c]);
+            }
+            v[3 * C] = n0;
+            v[3 * C + 1] = n1;
+            const float rho = pp[DIM];
+            float k2 = 0.f;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) k2 += pp[d] * pp[d];
+            const float e_int = pp[DIM + 1] - 0.5f * k2 / rho;
+            v[3 * C + 2] = (rho <= 0.f || e_int <= 0.f || !isfinite(e_int)) ? 1.0 : 0.0;
+        }
+        unsigned pending = __ballot_sync(full, live);
+        while (pending) {
+            const int lc = __shfl_sync(full, cse, __ffs(pending) - 1);
+            if (lc != cur) {
+                flush();
+                cur = lc;
+            }
+            const bool mine = live && cse == lc;
+            if (mine)
+#pragma unroll
+                for (int q = 0; q < NS; ++q) acc[q] += v[q];
+            pending &= ~__ballot_sync(full, mine);
+        }
+    }
+    flush();
+}
+
+__global__ void k_checks_verdict(double* __restrict__ sums, int n_cases, int C, const float* __restrict__ dt, int k,
+                                 double tol, double ratio2, uint8_t* __restrict__ ok, double* __restrict__ keep) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_cases) return;
+    const int NS = 3 * C + 3, DIM = C - 2;
+    double* s = sums + (int64_t)c * NS;
+    const double kdt = (double)k * (double)dt[c];
+    double drift = 0.0;
+    for (int q = DIM; q < DIM + 2; ++q) {
+        const double m0 = s[q], mp = s[C + q], r = s[2 * C + q];
+        const double d = fabs(mp - (m0 + kdt * r)) / fabs(m0);
+        drift = (d > drift || isnan(d)) ? d : drift;
+    }
+    ok[c] = (drift <= tol && s[3 * C + 1] <= ratio2 * s[3 * C] && isfinite(drift) && s[3 * C + 2] == 0.0) ? 1 : 0;
+    for (int q = 0; q < NS; ++q) {
+        if (keep) keep[(int64_t)c * NS + q] = s[q];
+        s[q] = 0.0;
+    }
+}
+
+}  // namespace corr
+}  // namespace fvm
+
+extern "C" int fvm_corrector_checks(const float* U, const float* P, const float* r0, const float* r1,
+                                    const float* volumes, const int32_t* cell_case, int32_t N, int32_t C,
+                                    int32_t n_cases, const float* dt, int32_t k, double drift_tol, double ratio,
+                                    double* sums, uint8_t* ok, double* keep, void* stream) {
+    if (!U || !P || !r0 || !r1 || !volumes || !cell_case || !dt || !sums || !ok || N <= 0 || n_cases <= 0 ||
+        (C != 4 && C != 5) || k < 1)
+        return FVM_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                      cudaSuccess) {
+            launch_status();
+            return FVM_E_CUDA;
+        }
+    }
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(4LL * sms, ((int64_t)N + 255) / 256));
+    if (C == 4)
+        FVM_LAUNCH(KID_CORRECTOR, s, corr::k_checks_reduce<4><<<grid, 256, 0, s>>>(U, P, r0, r1, volumes, cell_case, N,
+                                                                                    sums));
+    else
+        FVM_LAUNCH(KID_CORRECTOR, s, corr::k_checks_reduce<5><<<grid, 256, 0, s>>>(U, P, r0, r1, volumes, cell_case, N,
+                                                                                    sums));
+    int rc = launch_status();
+    if (rc) return rc;
+    FVM_LAUNCH(KID_CORRECTOR, s, corr::k_checks_verdict<<<(n_cases + 127) / 128, 128, 0, s>>>(
+                                     sums, n_cases, C, dt, k, drift_tol, ratio * ratio, ok, keep));
     return launch_status();
 }

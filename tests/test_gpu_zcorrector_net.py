@@ -206,3 +206,71 @@ def test_fused_layer_matches_separate_kernels(N, KN):
     Aref = torch.cat([h.to(torch.bfloat16), mean.to(torch.bfloat16)], 1).double()
     ref = hv + torch.nn.functional.silu(Aref @ Wt.double().t() + bias.double())
     assert rel_l2(got.cpu().numpy(), ref.cpu().numpy()) < 1e-5
+
+
+def _checks_torch(U, P, r0, r1, vol, cc, n, dt, k, tol, ratio, dim):
+    """The acceptance checks written as torch reductions (FP64 sums of FP32 products)."""
+    def sums(x):
+        return torch.zeros((n, x.shape[1]), dtype=torch.float64, device=x.device).index_add_(
+            0, cc, x.double() * vol.double()[:, None])
+    M0, Mp, R0 = sums(U), sums(P), sums(r0)
+    cons = slice(dim, dim + 2)
+    drift = ((Mp[:, cons] - (M0[:, cons] + k * dt.double()[:, None] * R0[:, cons])).abs()
+             / M0[:, cons].abs()).max(dim=1).values
+    n0, n1 = sums(r0 * r0).sum(dim=1), sums(r1 * r1).sum(dim=1)
+    rho = P[:, dim]
+    e_int = P[:, dim + 1] - 0.5 * P[:, :dim].square().sum(dim=1) / rho
+    bad = torch.zeros(n, dtype=torch.float64, device=U.device).index_add_(
+        0, cc, ((rho <= 0) | (e_int <= 0) | ~torch.isfinite(e_int)).double())
+    return (drift <= tol) & (n1 <= ratio ** 2 * n0) & torch.isfinite(drift) & (bad == 0), M0, Mp, R0, n0, n1, bad
+
+
+@pytest.mark.parametrize("C", [4, 5])
+def test_checks_kernel_matches_torch(C):
+    """fvm_corrector_checks against the torch reductions, with failures of each kind planted in
+    their own cases, and twice in a row (the kernel leaves its sums buffer zeroed)."""
+    if not torch.cuda.is_available():
+        pytest.skip("needs CUDA")
+    from fvm_solver_b200 import _lib
+    lib = _lib.load()
+    g = torch.Generator().manual_seed(C)
+    dim, n, k, tol, ratio = C - 2, 41, 8, 1e-4, 3.0
+    sizes = torch.randint(1, 9000, (n,), generator=g)
+    cc = torch.repeat_interleave(torch.arange(n), sizes).cuda()
+    N = int(sizes.sum())
+    vol = (0.5 + torch.rand(N, generator=g)).cuda()
+    U = torch.rand((N, C), generator=g).cuda()
+    U[:, dim] += 1.0                                     # density
+    U[:, dim + 1] += 3.0                                 # energy above the kinetic part
+    r0 = (torch.rand((N, C), generator=g) - 0.5).cuda()
+    dt = (1e-4 * (1 + torch.rand(n, generator=g))).cuda()
+    P = U + k * dt[cc, None] * r0
+    r1 = 0.5 * r0
+    first = torch.cumsum(sizes, 0) - sizes
+    P[int(first[1]), dim] = -1.0                          # case 1: negative density in one cell
+    P[cc == 2, dim + 1] *= 1.01                          # case 2: energy drift
+    r1[cc == 3] = 4.0 * r0[cc == 3]                       # case 3: residual grew beyond the ratio
+    P[int(first[4]) + int(sizes[4]) - 1, 0] = float("nan")  # case 4: non-finite proposal
+    P[cc == 5, dim] *= 1.00001                           # case 5: mass drift 1e-5, inside the tolerance
+    want, *want_sums = _checks_torch(U, P, r0, r1, vol, cc, n, dt, k, tol, ratio, dim)
+    assert want[[0, 5]].all() and not want[[1, 2, 3, 4]].any()
+    sums = torch.zeros((n, 3 * C + 3), dtype=torch.float64, device="cuda")
+    keep = torch.empty_like(sums)
+    cc32 = cc.int()
+    for _ in range(2):
+        ok = torch.zeros(n, dtype=torch.uint8, device="cuda")
+        _lib.check(lib.fvm_corrector_checks(U.data_ptr(), P.data_ptr(), r0.data_ptr(), r1.data_ptr(), vol.data_ptr(),
+                                            cc32.data_ptr(), N, C, n, dt.data_ptr(), k, tol, ratio, sums.data_ptr(),
+                                            ok.data_ptr(), keep.data_ptr(), _lib.stream_ptr()), "fvm_corrector_checks")
+        torch.cuda.synchronize()
+        assert torch.equal(ok.bool(), want)
+        assert float(sums.abs().max()) == 0.0
+        M0, Mp, R0, n0, n1, bad = want_sums
+        scale = sizes.double().cuda()                    # bound on each sum's absolute terms (order 1 each)
+        for got, ref in ((keep[:, :C], M0), (keep[:, 2 * C:3 * C], R0), (keep[:, 3 * C], n0),
+                         (keep[:, 3 * C + 1], n1)):
+            sc = scale if got.dim() == 1 else scale[:, None]
+            assert float(((got - ref).abs() / sc).max()) < 1e-13
+        finite = torch.isfinite(Mp).all(dim=1)
+        assert float(((keep[finite, C:2 * C] - Mp[finite]).abs() / scale[finite, None]).max()) < 1e-13
+        assert torch.equal(keep[:, 3 * C + 2], bad)
