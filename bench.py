@@ -948,6 +948,10 @@ def main():
     tuned = {k: v["threads"] for k, v in tuned_full.items()}
     prefetch = {k: v["prefetch"] for k, v in tuned_full.items()}
     variants = {k: v["variant"] for k, v in tuned_full.items()}
+    dv = tuned_full.get("div_stage", {})
+    if "residual_ms" in dv:
+        variants["residual"] = {"owner_computes" if dv["residual_variant"] else "separate": True,
+                                "ms": {k: round(v, 5) for k, v in dv["residual_ms"].items()}}
     if os.environ.get("FVM_BENCH_VERBOSE"):
         for k, v in tuned_full.items():
             print(k, {c: round(ms * 1e3, 1) for c, ms in v["ms"].items()}, file=sys.stderr)

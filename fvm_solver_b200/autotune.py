@@ -80,17 +80,21 @@ def _time_residual(eq, prims, out, reps: int) -> dict:
 
 
 def autotune(eq, reps: int = 5, candidates=CANDIDATES, prefetch=PREFETCH, use_cache: bool = True,
-             staged: bool = True) -> dict:
+             staged: bool = True, owner: bool = True) -> dict:
     """Pick and install the fastest (block size, prefetch) per kernel for ``eq`` (FVMEquation or
     BatchedFVM).
 
     The carried limited gradients are saved and restored, so the tuning runs leave the solver's
     state untouched.  Returns ``{kernel: {"threads": bs, "prefetch": pf, "ms": {(bs, pf): mean ms}}}``.
+    With ``owner``, residual evaluations then time the owner-computes divergence (each cell
+    evaluates its own facets' fluxes, no flux array) against facet kernel + divergence kernel and
+    keep the faster (``best["div_stage"]["residual_variant"]``: 1 owner computes, 0 separate).
     """
     key = _key(eq)
     if use_cache and key in _cache:
         for k, v in _cache[key].items():
             _install(k, v["cfg"])
+        set_variant("div_stage", _cache[key]["div_stage"].get("residual_variant", 0))
         return _cache[key]
     prims = eq.cells.get_values()[0].contiguous()
     out = torch.empty_like(prims)
@@ -112,6 +116,17 @@ def autotune(eq, reps: int = 5, candidates=CANDIDATES, prefetch=PREFETCH, use_ca
                    "variant": "staged" if cfg[1] == STAGED else "registers", "cfg": cfg,
                    "ms": {f"{a}/{b}": v for (a, b), v in t.items()}}
         _install(k, cfg)
+    set_variant("div_stage", 0)
+    if owner:
+        sep = _time_residual(eq, prims, out, reps)
+        t_sep = sep.get("face", 0.0) + sep.get("div_stage", 0.0)
+        set_variant("div_stage", 1)
+        _time_residual(eq, prims, out, 1)
+        t_own = _time_residual(eq, prims, out, reps).get("div_stage", float("inf"))
+        variant = 1 if t_own < t_sep else 0
+        set_variant("div_stage", variant)
+        best["div_stage"]["residual_variant"] = variant
+        best["div_stage"]["residual_ms"] = {"separate": t_sep, "owner_computes": t_own}
     eq.grads.copy_(g_save)
     eq.has_grads.copy_(f_save)
     torch.cuda.synchronize()
@@ -120,10 +135,11 @@ def autotune(eq, reps: int = 5, candidates=CANDIDATES, prefetch=PREFETCH, use_ca
 
 
 def reset():
-    """Back to the defaults (256 threads, no prefetch, per-thread record loads) for every tunable
-    kernel."""
+    """Back to the defaults (256 threads, no prefetch, per-thread record loads, separate facet and
+    divergence kernels) for every tunable kernel."""
     for k in KERNELS.values():
         _install(k, (256, 0))
+    set_variant("div_stage", 0)
 
 
 def tune_fused(eq, steps: int = 10, reps: int = 3) -> dict:

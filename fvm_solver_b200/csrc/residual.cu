@@ -614,15 +614,16 @@ __global__ void __maxnreg__(FVM_CELL_MAXNREG) k_cell(fvm_mesh_t m, Phys p, const
 // ------------------------------------------------------------------------------------------
 // k_face: facet fluxes.
 // ------------------------------------------------------------------------------------------
-// One facet's flux from its record, side codes ca / cb and both sides' primitives P0, P1 and
-// limited gradients G0, G1 (cell sides; a boundary side's value is read here): the arithmetic of
-// every facet kernel, so all of them give the same bits.
+// One facet's flux F (the C components, padded with zeros to a row) from its record, side codes
+// ca / cb and both sides' primitives P0, P1 and limited gradients G0, G1 (cell sides; a boundary
+// side's value is read here): the arithmetic of every facet kernel, so all of them give the same
+// bits.
 template <int DIM>
 __device__ __forceinline__ void face_eval(const fvm_mesh_t& m, const Phys& p, const float* __restrict__ bcv,
-                                          float* __restrict__ flux, int f, int ca, int cb,
-                                          const float (&rec)[L<DIM>::FR], const float (&P0)[L<DIM>::RS],
-                                          const float (&P1)[L<DIM>::RS], const float (&G0)[L<DIM>::GS],
-                                          const float (&G1)[L<DIM>::GS]) {
+                                          int f, int ca, int cb, const float (&rec)[L<DIM>::FR],
+                                          const float (&P0)[L<DIM>::RS], const float (&P1)[L<DIM>::RS],
+                                          const float (&G0)[L<DIM>::GS], const float (&G1)[L<DIM>::GS],
+                                          float (&F)[L<DIM>::RS]) {
     using Ly = L<DIM>;
     constexpr int C = Ly::C, NG = DIM + 1, RS = Ly::RS;
     const float size = rec[Ly::SIZE];
@@ -748,7 +749,6 @@ __device__ __forceinline__ void face_eval(const fvm_mesh_t& m, const Phys& p, co
 #pragma unroll
         for (int c = 0; c < DIM; ++c) tau[a][c] = (a == c ? a0 : 0.f) + a1 * D[a][c];
 
-    float F[RS];
 #pragma unroll
     for (int c = 0; c < RS; ++c) F[c] = 0.f;
     // Advection (fvm_equation.py:210-231)
@@ -789,7 +789,6 @@ __device__ __forceinline__ void face_eval(const fvm_mesh_t& m, const Phys& p, co
     for (int d = 0; d < DIM; ++d) F[d] += 0.5f * (a_vel * (mom[0][d] - mom[1][d])) * size;
     F[DIM] += 0.5f * (a_oth * (rho[0] - rho[1])) * size;
     F[DIM + 1] += 0.5f * (a_oth * (Q[0] - Q[1])) * size;
-    st_vec<RS>(flux + (int64_t)f * RS, F);
 }
 
 template <int DIM, bool COH>
@@ -823,7 +822,9 @@ __device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, co
     float rec[Ly::FR];
     ld_vec<Ly::FR>(m.face_rec + (int64_t)f * Ly::FR, rec);
     nxt = next_codes<DIM>(m, f + stride, nF, skip_frozen);
-    face_eval<DIM>(m, p, bcv, flux, f, ca, cb, rec, P0, P1, G0, G1);
+    float F[RS];
+    face_eval<DIM>(m, p, bcv, f, ca, cb, rec, P0, P1, G0, G1, F);
+    st_vec<RS>(flux + (int64_t)f * RS, F);
     }
 }
 
@@ -921,7 +922,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_face_staged(fvm_mesh_t m, Phys p,
             ld_vec<RS>(prims + (int64_t)cell1 * RS, P1);
             ld_vec_cg<GS>(grads + (int64_t)cell0 * GS, G0);
             ld_vec_cg<GS>(grads + (int64_t)cell1 * GS, G1);
-            face_eval<DIM>(m, p, bcv, flux, (int)f, ca, cb, rec, P0, P1, G0, G1);
+            float F[RS];
+            face_eval<DIM>(m, p, bcv, (int)f, ca, cb, rec, P0, P1, G0, G1, F);
+            st_vec<RS>(flux + f * RS, F);
         }
         staged = staged && !__syncthreads_or(!ok);
     }
@@ -938,6 +941,67 @@ __global__ void __launch_bounds__(kMaxBlock) k_face(fvm_mesh_t m, Phys p, const 
                                                   const float* __restrict__ grads, float* __restrict__ flux,
                                                   int waves) {
     face_body<DIM, false>(m, p, prims, bcv, grads, flux, waves);
+}
+
+// ------------------------------------------------------------------------------------------
+// k_face_div: owner-computes residual (divergence-kernel variant 1, residual evaluations only).
+// ------------------------------------------------------------------------------------------
+// dU/dt of each cell from its own facets' fluxes, with no flux array: lanes 4q .. 4q + 3 of a warp
+// own cell q's facet slots 0 .. K - 1 (the fourth lane idles in 2D); each evaluates its facet with
+// face_eval, and the group's first lane sums the slots in order k = 0, 1, ... with the fused
+// multiply-adds of k_div_stage, so dU/dt is bitwise that of k_face followed by k_div_stage.  Every
+// interior facet is evaluated twice (once from each side) in exchange for the flux array's write,
+// its gathered re-read and one launch.  Whole meshes only (no cell or facet sub-range).
+template <int DIM>
+__global__ void __launch_bounds__(kMaxBlock) k_face_div(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+                                                      const float* __restrict__ bcv,
+                                                      const float* __restrict__ grads, float* __restrict__ dudt) {
+    using Ly = L<DIM>;
+    constexpr int C = Ly::C, RS = Ly::RS, GS = Ly::GS, FR = Ly::FR, K = Ly::K;
+    static_assert(K <= 4, "four lanes per cell");
+    const unsigned full = 0xffffffffu;
+    const int NA = m.n_owned > 0 ? m.n_owned : m.n_cells;
+    const int lane = threadIdx.x & 31, k = lane & 3, base = lane & ~3;
+    const int64_t step = ((int64_t)gridDim.x * blockDim.x) >> 2;
+    // warp-uniform loop: the warp's first cell decides, so every lane reaches the shuffles
+    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 2; i - (lane >> 2) < NA; i += step) {
+        const bool cell_on = i < NA && (m.case_active == nullptr || case_on(m, m.cell_case, (int)i));
+        const bool live = cell_on && k < K && k < m.kf;
+        float F[RS], w = 0.f;
+#pragma unroll
+        for (int c = 0; c < RS; ++c) F[c] = 0.f;
+        if (live) {
+            const float* drec = m.div_rec + i * Ly::DR;
+            w = __ldg(drec + k);
+            const int f = as_int(__ldg(drec + K + k));
+            float rec[FR];
+            ld_vec<FR>(m.face_rec + (int64_t)f * FR, rec);
+            const int ca = as_int(rec[Ly::FA]), cb = as_int(rec[Ly::FB]);
+            const int cell0 = ca >= 0 ? ca : cb;
+            const int cell1 = cb >= 0 ? cb : ca;
+            float P0[RS], P1[RS], G0[GS], G1[GS];
+            ld_vec<RS>(prims + (int64_t)cell0 * RS, P0);
+            ld_vec<RS>(prims + (int64_t)cell1 * RS, P1);
+            ld_vec_cg<GS>(grads + (int64_t)cell0 * GS, G0);
+            ld_vec_cg<GS>(grads + (int64_t)cell1 * GS, G1);
+            face_eval<DIM>(m, p, bcv, f, ca, cb, rec, P0, P1, G0, G1, F);
+        }
+        float r[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) r[c] = 0.f;
+#pragma unroll
+        for (int s = 0; s < K; ++s) {
+            const float ws = __shfl_sync(full, w, base + s);
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const float fs = __shfl_sync(full, F[c], base + s);
+                if (s < m.kf) r[c] = fmaf(ws, fs, r[c]);
+            }
+        }
+        if (cell_on && k == 0)
+#pragma unroll
+            for (int c = 0; c < C; ++c) dudt[i * C + c] = r[c];
+    }
 }
 
 // Both sides' limited facet values [F][2][C] (the reference's U_face_all, facet_process.py:349-354),
@@ -1598,6 +1662,9 @@ static int g_pf_cell = -1, g_pf_face = -1, g_pf_div = -1;
 // Facet kernel variant (fvm_set_variant): 0 = records loaded by each thread (k_face), 1 = records
 // staged through shared memory by the bulk-copy unit (k_face_staged).  Same results.
 static int g_face_variant = 0;
+// Residual evaluations (fvm_residual, fvm_residual_state): 0 = facet kernel then divergence
+// kernel, 1 = owner-computes k_face_div (whole meshes; same bits).  Stages always use 0.
+static int g_div_variant = 0;
 static inline int waves_of(int setting) { return setting < 0 ? 0 : setting; }
 
 // Resident blocks of `kernel` at `threads` per block over the whole GPU (one wave), cached.
@@ -1736,15 +1803,32 @@ static int launch_div(const fvm_mesh_t* m, const Phys& p, const float* flux, con
     return launch_status();
 }
 
+// dU/dt from the padded primitives in work->prims: bc -> cell -> face -> divergence, or with the
+// owner-computes variant bc -> cell -> k_face_div (whole meshes; same bits).
+template <int DIM>
+static int launch_residual(const fvm_mesh_t* m, const Phys& p, float* grads, int32_t* has_grads, float* dudt,
+                           const fvm_work_t* w, cudaStream_t s) {
+    if (g_div_variant == 1 && m->cell_lo == 0 && m->facet_lo == 0 && owned_cells(m) > 0) {
+        const int rc = launch_begin<DIM>(m, p, w->prims, grads, has_grads, w, s);
+        if (rc) return rc;
+        const unsigned g = persistent_grid(4 * (int64_t)owned_cells(m), g_block_face,
+                                           wave_blocks(k_face_div<DIM>, g_block_face));
+        FVM_LAUNCH(KID_DIV_STAGE, s, k_face_div<DIM><<<g, g_block_face, 0, s>>>(*m, p, w->prims, w->bc_vals, grads,
+                                                                                dudt));
+        return launch_status();
+    }
+    const int rc = launch_fluxes<DIM>(m, p, w->prims, grads, has_grads, w, s);
+    if (rc) return rc;
+    StageArgs a{};
+    return launch_div<DIM>(m, p, w->flux, a, nullptr, nullptr, nullptr, nullptr, nullptr, dudt, s);
+}
+
 template <int DIM>
 static int residual_impl(const fvm_mesh_t* m, const Phys& p, const float* prims_user, float* grads,
                          int32_t* has_grads, float* dudt, const fvm_work_t* w, cudaStream_t s) {
     FVM_LAUNCH(KID_STATE_TO_PRIMS, s, k_pad_prims<DIM><<<blocks_for(m->n_cells), kBlock, 0, s>>>(
                                           m->n_cells, prims_user, w->prims));
-    int rc = launch_fluxes<DIM>(m, p, w->prims, grads, has_grads, w, s);
-    if (rc) return rc;
-    StageArgs a{};
-    return launch_div<DIM>(m, p, w->flux, a, nullptr, nullptr, nullptr, nullptr, nullptr, dudt, s);
+    return launch_residual<DIM>(m, p, grads, has_grads, dudt, w, s);
 }
 
 // dU/dt of a conserved state: one kernel writes the padded primitives into work->prims (the
@@ -1754,10 +1838,7 @@ static int residual_state_impl(const fvm_mesh_t* m, const Phys& p, const float* 
                                int32_t* has_grads, float* dudt, const fvm_work_t* w, cudaStream_t s) {
     FVM_LAUNCH(KID_STATE_TO_PRIMS, s, k_state_to_prims<DIM><<<blocks_for(m->n_cells), kBlock, 0, s>>>(
                                           m->n_cells, p.inv_Cv, state, w->prims));
-    int rc = launch_fluxes<DIM>(m, p, w->prims, grads, has_grads, w, s);
-    if (rc) return rc;
-    StageArgs a{};
-    return launch_div<DIM>(m, p, w->flux, a, nullptr, nullptr, nullptr, nullptr, nullptr, dudt, s);
+    return launch_residual<DIM>(m, p, grads, has_grads, dudt, w, s);
 }
 
 static StageArgs stage_args(const fvm_tableau_t* tab, int s) {
@@ -2306,8 +2387,8 @@ extern "C" int fvm_set_prefetch(int32_t kernel_id, int32_t waves_ahead) {
 }
 
 extern "C" int fvm_set_variant(int32_t kernel_id, int32_t variant) {
-    if (kernel_id != KID_FACE || variant < 0 || variant > 1) return FVM_E_ARG;
-    g_face_variant = variant;
+    if ((kernel_id != KID_FACE && kernel_id != KID_DIV_STAGE) || variant < 0 || variant > 1) return FVM_E_ARG;
+    (kernel_id == KID_FACE ? g_face_variant : g_div_variant) = variant;
     return FVM_OK;
 }
 

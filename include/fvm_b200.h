@@ -178,7 +178,11 @@ const char *fvm_version(void);
 int fvm_profile_start(int32_t capacity);
 /* Kernel variant (no reference counterpart; results unchanged): for the facet kernel
  * (kernel_id 4), 0 = each thread loads its facet record, 1 = the records of a block's next tile
- * are staged in shared memory by the bulk-copy unit (cp.async.bulk + mbarrier, two stages). */
+ * are staged in shared memory by the bulk-copy unit (cp.async.bulk + mbarrier, two stages); for
+ * the divergence kernel (kernel_id 5), 1 = residual evaluations (fvm_residual, fvm_residual_state
+ * on a whole mesh) compute each cell's facet fluxes in the divergence kernel itself (owner computes:
+ * no flux array, every interior facet evaluated from both sides), 0 = facet kernel then divergence
+ * kernel; stages always use 0. */
 int fvm_set_variant(int32_t kernel_id, int32_t variant);
 /* Launch configuration (no reference counterpart): threads per block of the cell (id 3), facet
  * (id 4) and divergence/stage (id 5) kernels for all later launches of this process; a multiple

@@ -394,3 +394,38 @@ def test_widened_stencil_vs_oracle(case, width):
     s = O.OracleSolver(orc, g["state0"], float(g["dt"]))
     s.butcher_step("RK4")
     assert rel_l2(to_np(eq.cells.state), s.state) < 1e-5
+
+
+@pytest.mark.parametrize("case", ["c2d", "b3d", "ptile"])
+def test_owner_computes_residual_bitwise(case):
+    """The owner-computes divergence (each cell evaluates its own facets, no flux array) gives the
+    bits of facet kernel + divergence kernel, from primitives and from a conserved state."""
+    import ctypes as ct
+    from fvm_solver_b200 import _lib, autotune
+    g, eq, T, cfg = make_equation(case)
+    p = torch.from_numpy(g["prim0"]).cuda()
+    U = torch.from_numpy(g["state0"]).cuda().contiguous()
+    outs = {}
+    try:
+        for v in (0, 1):
+            autotune.set_variant("div_stage", v)
+            for bs in (64, 256):
+                autotune.set_block_size("face", bs)
+                eq.reset_gradients()
+                r = eq.forward(p).clone()
+                rs = torch.empty_like(U)
+                flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+                grads = torch.zeros_like(eq.grads)
+                _lib.check(eq.lib.fvm_residual_state(ct.byref(eq.dev.struct), ct.byref(eq.phys), U.data_ptr(),
+                                                     grads.data_ptr(), flag.data_ptr(), rs.data_ptr(),
+                                                     ct.byref(eq.work.struct), _lib.stream_ptr()),
+                           "fvm_residual_state")
+                outs[(v, bs)] = (r, rs)
+    finally:
+        autotune.reset()
+    ref = outs[(0, 256)]
+    for k, (r, rs) in outs.items():
+        assert torch.equal(r, ref[0]), k
+        assert torch.equal(rs, ref[1]), k
+    with pytest.raises(RuntimeError):
+        autotune.set_variant("div_stage", 2)
