@@ -442,19 +442,20 @@ class CheckedRollout:
     """Corrector + fallback rollout on a batch, with per-case acceptance checks (see module doc)."""
 
     def __init__(self, model: CorrectorModel, drift_tol: float = 1e-4, residual_ratio: float = 3.0,
-                 use_graphs: bool = True):
+                 use_graphs: bool = True, consistency: float | None = None):
         self.m = model
         b = model.batch
         self.b = b
         self.lib = _lib.load()
         self.drift_tol, self.ratio = drift_tol, residual_ratio
+        self.consistency = consistency or 0.0
         N, C = b.cells.state.shape
         d = b.device
         self.prop = torch.empty((N, C), device=d)
         self.r0 = torch.empty((N, C), device=d)
         self.r1 = torch.empty((N, C), device=d)
         self.vol32 = model.vol.float().contiguous()
-        self.check_sums = torch.zeros((b.n_cases, 3 * C + 3), dtype=torch.float64, device=d)
+        self.check_sums = torch.zeros((b.n_cases, 3 * C + 4), dtype=torch.float64, device=d)
         self.ok_u8 = torch.zeros(b.n_cases, dtype=torch.uint8, device=d)
         self.ok = self.ok_u8.view(torch.bool)
         self.use_graphs = use_graphs
@@ -471,8 +472,10 @@ class CheckedRollout:
         ``fvm_corrector_checks`` reduces, per case and in FP64, the volume-weighted sums of the state,
         the proposal and r0 (conservation: the proposal's mass and energy must equal the state's plus
         k dt times r0's, to ``drift_tol`` relative), the squared residual norms of state and proposal
-        (|r1|^2 <= ratio^2 |r0|^2) and the number of inadmissible proposal cells (density or internal
-        energy <= 0, or not finite), then writes the verdicts: two launches after the proposal."""
+        (|r1|^2 <= ratio^2 |r0|^2), the number of inadmissible proposal cells (density or internal
+        energy <= 0, or not finite) and, with ``consistency``, the proposal's distance to the
+        trapezoidal rule over the window (|U' - U - k dt (r0 + r1) / 2| <= consistency k dt |r0|),
+        then writes the verdicts: two launches after the proposal."""
         b, k = self.b, self.m.k
         U = b.cells.state
         self.m.res(U, self.r0)
@@ -482,7 +485,8 @@ class CheckedRollout:
         _lib.check(self.lib.fvm_corrector_checks(
             U.data_ptr(), self.prop.data_ptr(), self.r0.data_ptr(), self.r1.data_ptr(), self.vol32.data_ptr(),
             self.m.cell_case32.data_ptr(), N, C, b.n_cases, b.t_solver.dt.data_ptr(), k, float(self.drift_tol),
-            float(self.ratio), self.check_sums.data_ptr(), self.ok_u8.data_ptr(), None, _lib.stream_ptr()),
+            float(self.ratio), float(self.consistency), self.check_sums.data_ptr(), self.ok_u8.data_ptr(), None,
+            _lib.stream_ptr()),
             "fvm_corrector_checks")
 
     def _run_propose(self):

@@ -1082,10 +1082,12 @@ extern "C" int fvm_decoder_back_f32(const float* h, const float* Wo, const float
 
 // ------------------------------------------------------------------------------------------
 // Acceptance checks of a corrector proposal, per case, in two launches (fvm_corrector_checks).
-//   sums[c] (FP64, 3C + 3 slots): sum vol U, sum vol P, sum vol r0 (C each), sum vol |r0|^2,
-//   sum vol |r1|^2, number of inadmissible cells of P (rho <= 0, internal energy <= 0 or not finite).
-//   ok[c] = drift <= tol && |r1|^2 <= ratio^2 |r0|^2 && drift finite && no inadmissible cell, with
-//   drift = max over mass and energy of |sum vol P - (sum vol U + k dt_c sum vol r0)| / |sum vol U|.
+//   sums[c] (FP64, 3C + 4 slots): sum vol U, sum vol P, sum vol r0 (C each), sum vol |r0|^2,
+//   sum vol |r1|^2, number of inadmissible cells of P (rho <= 0, internal energy <= 0 or not finite),
+//   sum vol |P - U - k dt_c (r0 + r1) / 2|^2 (the proposal against the trapezoidal rule over the
+//   window).  ok[c] = drift <= tol && |r1|^2 <= ratio^2 |r0|^2 && drift finite && no inadmissible
+//   cell [&& trapezoid distance <= consistency * k dt_c |r0| when consistency > 0], with drift =
+//   max over mass and energy of |sum vol P - (sum vol U + k dt_c sum vol r0)| / |sum vol U|.
 // The reduction walks one contiguous chunk of cells per warp and flushes per case change (cells of
 // a case are contiguous), as the conservation sums do; the verdict kernel clears the sums after
 // reading them, so the pair can be replayed from a CUDA graph.
@@ -1097,8 +1099,8 @@ template <int C>
 __global__ void k_checks_reduce(const float* __restrict__ U, const float* __restrict__ P,
                                 const float* __restrict__ r0, const float* __restrict__ r1,
                                 const float* __restrict__ vol, const int32_t* __restrict__ cell_case, int N,
-                                double* __restrict__ sums) {
-    constexpr int DIM = C - 2, NS = 3 * C + 3;
+                                const float* __restrict__ dt, int k, double* __restrict__ sums) {
+    constexpr int DIM = C - 2, NS = 3 * C + 4;
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -1137,7 +1139,8 @@ __global__ void k_checks_reduce(const float* __restrict__ U, const float* __rest
                 a[c] = __ldg(r0 + i * C + c);
                 b[c] = __ldg(r1 + i * C + c);
             }
-            double n0 = 0.0, n1 = 0.0;
+            const double half_kdt = 0.5 * (double)k * (double)__ldg(dt + cse);
+            double n0 = 0.0, n1 = 0.0, e2 = 0.0;
 #pragma unroll
             for (int c = 0; c < C; ++c) {
                 v[c] = vo * (double)u[c];
@@ -1145,7 +1148,10 @@ __global__ void k_checks_reduce(const float* __restrict__ U, const float* __rest
                 v[2 * C + c] = vo * (double)a[c];
                 n0 += vo * (double)(a[c] * a[c]);
                 n1 += vo * (double)(b[c] * b[c]);
+                const double e = ((double)pp[c] - (double)u[c]) - half_kdt * ((double)a[c] + (double)b[c]);
+                e2 += vo * (e * e);
             }
+            v[3 * C + 3] = e2;
             v[3 * C] = n0;
             v[3 * C + 1] = n1;
             const float rho = pp[DIM];
@@ -1173,10 +1179,11 @@ __global__ void k_checks_reduce(const float* __restrict__ U, const float* __rest
 }
 
 __global__ void k_checks_verdict(double* __restrict__ sums, int n_cases, int C, const float* __restrict__ dt, int k,
-                                 double tol, double ratio2, uint8_t* __restrict__ ok, double* __restrict__ keep) {
+                                 double tol, double ratio2, double consistency, uint8_t* __restrict__ ok,
+                                 double* __restrict__ keep) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n_cases) return;
-    const int NS = 3 * C + 3, DIM = C - 2;
+    const int NS = 3 * C + 4, DIM = C - 2;
     double* s = sums + (int64_t)c * NS;
     const double kdt = (double)k * (double)dt[c];
     double drift = 0.0;
@@ -1185,7 +1192,9 @@ __global__ void k_checks_verdict(double* __restrict__ sums, int n_cases, int C, 
         const double d = fabs(mp - (m0 + kdt * r)) / fabs(m0);
         drift = (d > drift || isnan(d)) ? d : drift;
     }
-    ok[c] = (drift <= tol && s[3 * C + 1] <= ratio2 * s[3 * C] && isfinite(drift) && s[3 * C + 2] == 0.0) ? 1 : 0;
+    const bool near_trapezoid = consistency <= 0.0 || s[3 * C + 3] <= consistency * consistency * kdt * kdt * s[3 * C];
+    ok[c] = (drift <= tol && s[3 * C + 1] <= ratio2 * s[3 * C] && isfinite(drift) && s[3 * C + 2] == 0.0 &&
+             near_trapezoid) ? 1 : 0;
     for (int q = 0; q < NS; ++q) {
         if (keep) keep[(int64_t)c * NS + q] = s[q];
         s[q] = 0.0;
@@ -1198,7 +1207,7 @@ __global__ void k_checks_verdict(double* __restrict__ sums, int n_cases, int C, 
 extern "C" int fvm_corrector_checks(const float* U, const float* P, const float* r0, const float* r1,
                                     const float* volumes, const int32_t* cell_case, int32_t N, int32_t C,
                                     int32_t n_cases, const float* dt, int32_t k, double drift_tol, double ratio,
-                                    double* sums, uint8_t* ok, double* keep, void* stream) {
+                                    double consistency, double* sums, uint8_t* ok, double* keep, void* stream) {
     if (!U || !P || !r0 || !r1 || !volumes || !cell_case || !dt || !sums || !ok || N <= 0 || n_cases <= 0 ||
         (C != 4 && C != 5) || k < 1)
         return FVM_E_ARG;
@@ -1215,13 +1224,13 @@ extern "C" int fvm_corrector_checks(const float* U, const float* P, const float*
     const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(4LL * sms, ((int64_t)N + 255) / 256));
     if (C == 4)
         FVM_LAUNCH(KID_CORRECTOR, s, corr::k_checks_reduce<4><<<grid, 256, 0, s>>>(U, P, r0, r1, volumes, cell_case, N,
-                                                                                    sums));
+                                                                                    dt, k, sums));
     else
         FVM_LAUNCH(KID_CORRECTOR, s, corr::k_checks_reduce<5><<<grid, 256, 0, s>>>(U, P, r0, r1, volumes, cell_case, N,
-                                                                                    sums));
+                                                                                    dt, k, sums));
     int rc = launch_status();
     if (rc) return rc;
     FVM_LAUNCH(KID_CORRECTOR, s, corr::k_checks_verdict<<<(n_cases + 127) / 128, 128, 0, s>>>(
-                                     sums, n_cases, C, dt, k, drift_tol, ratio * ratio, ok, keep));
+                                     sums, n_cases, C, dt, k, drift_tol, ratio * ratio, consistency, ok, keep));
     return launch_status();
 }

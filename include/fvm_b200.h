@@ -400,16 +400,19 @@ int fvm_corrector_combine(const float *state, const float *base, const float *ou
                           const float *shift, const int32_t *cell_case, int32_t N, int32_t C, float *prop,
                           void *stream);
 
-/* The corrector's acceptance checks for a batch (C = 4 or 5, cells of a case contiguous):
- * per case the FP64 sums over its cells of vol U, vol P, vol r0 (C each), vol |r0|^2, vol |r1|^2
- * and the count of inadmissible cells of P (density or internal energy <= 0, or not finite), then
- * ok[c] = 1 iff drift <= drift_tol, |r1|^2 <= ratio^2 |r0|^2, drift finite and no inadmissible
- * cell, where drift = max over mass and energy of |sum vol P - (sum vol U + k dt_c sum vol r0)|
- * / |sum vol U|.  sums: [n_cases][3C + 3] doubles, zero on the first call (each call leaves it
- * zero); keep (or NULL) receives the sums. */
+/* The corrector's acceptance checks for a batch (C = 4 or 5, cells of a case contiguous; r0 =
+ * dU/dt at U, r1 at the proposal P): per case the FP64 sums over its cells of vol U, vol P, vol r0
+ * (C each), vol |r0|^2, vol |r1|^2, the count of inadmissible cells of P (density or internal
+ * energy <= 0, or not finite) and vol |P - U - k dt_c (r0 + r1) / 2|^2; then ok[c] = 1 iff
+ * drift <= drift_tol, |r1|^2 <= ratio^2 |r0|^2, drift finite, no inadmissible cell and, when
+ * consistency > 0, the distance to the trapezoidal rule is at most consistency * k dt_c |r0|
+ * (volume-weighted norms), where drift = max over mass and energy of
+ * |sum vol P - (sum vol U + k dt_c sum vol r0)| / |sum vol U|.  sums: [n_cases][3C + 4] doubles,
+ * zero on the first call (each call leaves it zero); keep (or NULL) receives the sums. */
 int fvm_corrector_checks(const float *U, const float *P, const float *r0, const float *r1, const float *volumes,
                          const int32_t *cell_case, int32_t N, int32_t C, int32_t n_cases, const float *dt, int32_t k,
-                         double drift_tol, double ratio, double *sums, uint8_t *ok, double *keep, void *stream);
+                         double drift_tol, double ratio, double consistency, double *sums, uint8_t *ok, double *keep,
+                         void *stream);
 
 #ifdef __cplusplus
 }

@@ -208,7 +208,7 @@ def test_fused_layer_matches_separate_kernels(N, KN):
     assert rel_l2(got.cpu().numpy(), ref.cpu().numpy()) < 1e-5
 
 
-def _checks_torch(U, P, r0, r1, vol, cc, n, dt, k, tol, ratio, dim):
+def _checks_torch(U, P, r0, r1, vol, cc, n, dt, k, tol, ratio, dim, consistency=0.0):
     """The acceptance checks written as torch reductions (FP64 sums of FP32 products)."""
     def sums(x):
         return torch.zeros((n, x.shape[1]), dtype=torch.float64, device=x.device).index_add_(
@@ -222,13 +222,20 @@ def _checks_torch(U, P, r0, r1, vol, cc, n, dt, k, tol, ratio, dim):
     e_int = P[:, dim + 1] - 0.5 * P[:, :dim].square().sum(dim=1) / rho
     bad = torch.zeros(n, dtype=torch.float64, device=U.device).index_add_(
         0, cc, ((rho <= 0) | (e_int <= 0) | ~torch.isfinite(e_int)).double())
-    return (drift <= tol) & (n1 <= ratio ** 2 * n0) & torch.isfinite(drift) & (bad == 0), M0, Mp, R0, n0, n1, bad
+    kdt = k * dt.double()
+    e = (P.double() - U.double()) - 0.5 * kdt[cc, None] * (r0.double() + r1.double())
+    e2 = torch.zeros(n, dtype=torch.float64, device=U.device).index_add_(0, cc, (e * e).sum(dim=1) * vol.double())
+    ok = (drift <= tol) & (n1 <= ratio ** 2 * n0) & torch.isfinite(drift) & (bad == 0)
+    if consistency > 0:
+        ok &= e2 <= consistency ** 2 * kdt ** 2 * n0
+    return ok, M0, Mp, R0, n0, n1, bad, e2
 
 
 @pytest.mark.parametrize("C", [4, 5])
 def test_checks_kernel_matches_torch(C):
     """fvm_corrector_checks against the torch reductions, with failures of each kind planted in
-    their own cases, and twice in a row (the kernel leaves its sums buffer zeroed)."""
+    their own cases, with and without the trapezoid gate, each twice in a row (the kernel leaves its
+    sums buffer zeroed)."""
     if not torch.cuda.is_available():
         pytest.skip("needs CUDA")
     from fvm_solver_b200 import _lib
@@ -244,33 +251,41 @@ def test_checks_kernel_matches_torch(C):
     U[:, dim + 1] += 3.0                                 # energy above the kinetic part
     r0 = (torch.rand((N, C), generator=g) - 0.5).cuda()
     dt = (1e-4 * (1 + torch.rand(n, generator=g))).cuda()
-    P = U + k * dt[cc, None] * r0
-    r1 = 0.5 * r0
+    kdt = k * dt[cc, None]
+    P = U + kdt * r0
+    r1 = 0.5 * r0                                        # trapezoid distance 0.25 k dt |r0|
     first = torch.cumsum(sizes, 0) - sizes
     P[int(first[1]), dim] = -1.0                          # case 1: negative density in one cell
     P[cc == 2, dim + 1] *= 1.01                          # case 2: energy drift
     r1[cc == 3] = 4.0 * r0[cc == 3]                       # case 3: residual grew beyond the ratio
     P[int(first[4]) + int(sizes[4]) - 1, 0] = float("nan")  # case 4: non-finite proposal
     P[cc == 5, dim] *= 1.00001                           # case 5: mass drift 1e-5, inside the tolerance
-    want, *want_sums = _checks_torch(U, P, r0, r1, vol, cc, n, dt, k, tol, ratio, dim)
-    assert want[[0, 5]].all() and not want[[1, 2, 3, 4]].any()
-    sums = torch.zeros((n, 3 * C + 3), dtype=torch.float64, device="cuda")
+    m6 = cc == 6                                         # case 6: trapezoid distance 0.75 k dt |r0|
+    P[m6] += 0.5 * kdt[m6] * r0[m6]
+    sums = torch.zeros((n, 3 * C + 4), dtype=torch.float64, device="cuda")
     keep = torch.empty_like(sums)
     cc32 = cc.int()
-    for _ in range(2):
-        ok = torch.zeros(n, dtype=torch.uint8, device="cuda")
-        _lib.check(lib.fvm_corrector_checks(U.data_ptr(), P.data_ptr(), r0.data_ptr(), r1.data_ptr(), vol.data_ptr(),
-                                            cc32.data_ptr(), N, C, n, dt.data_ptr(), k, tol, ratio, sums.data_ptr(),
-                                            ok.data_ptr(), keep.data_ptr(), _lib.stream_ptr()), "fvm_corrector_checks")
-        torch.cuda.synchronize()
-        assert torch.equal(ok.bool(), want)
-        assert float(sums.abs().max()) == 0.0
-        M0, Mp, R0, n0, n1, bad = want_sums
-        scale = sizes.double().cuda()                    # bound on each sum's absolute terms (order 1 each)
-        for got, ref in ((keep[:, :C], M0), (keep[:, 2 * C:3 * C], R0), (keep[:, 3 * C], n0),
-                         (keep[:, 3 * C + 1], n1)):
-            sc = scale if got.dim() == 1 else scale[:, None]
-            assert float(((got - ref).abs() / sc).max()) < 1e-13
-        finite = torch.isfinite(Mp).all(dim=1)
-        assert float(((keep[finite, C:2 * C] - Mp[finite]).abs() / scale[finite, None]).max()) < 1e-13
-        assert torch.equal(keep[:, 3 * C + 2], bad)
+    scale = sizes.double().cuda()                        # bound on each sum's absolute terms (order 1 each)
+    for consistency in (0.0, 0.3):
+        want, M0, Mp, R0, n0, n1, bad, e2 = _checks_torch(U, P, r0, r1, vol, cc, n, dt, k, tol, ratio, dim,
+                                                          consistency)
+        assert want[[0, 5]].all() and not want[[1, 2, 3, 4]].any()
+        assert bool(want[6]) == (consistency == 0.0)
+        for _ in range(2):
+            ok = torch.zeros(n, dtype=torch.uint8, device="cuda")
+            _lib.check(lib.fvm_corrector_checks(U.data_ptr(), P.data_ptr(), r0.data_ptr(), r1.data_ptr(),
+                                                vol.data_ptr(), cc32.data_ptr(), N, C, n, dt.data_ptr(), k, tol, ratio,
+                                                consistency, sums.data_ptr(), ok.data_ptr(), keep.data_ptr(),
+                                                _lib.stream_ptr()), "fvm_corrector_checks")
+            torch.cuda.synchronize()
+            assert torch.equal(ok.bool(), want)
+            assert float(sums.abs().max()) == 0.0
+            for got, ref in ((keep[:, :C], M0), (keep[:, 2 * C:3 * C], R0), (keep[:, 3 * C], n0),
+                             (keep[:, 3 * C + 1], n1)):
+                sc = scale if got.dim() == 1 else scale[:, None]
+                assert float(((got - ref).abs() / sc).max()) < 1e-13
+            finite = torch.isfinite(Mp).all(dim=1)
+            assert float(((keep[finite, C:2 * C] - Mp[finite]).abs() / scale[finite, None]).max()) < 1e-13
+            assert torch.equal(keep[:, 3 * C + 2], bad)
+            fin = torch.isfinite(e2)
+            assert float(((keep[fin, 3 * C + 3] - e2[fin]).abs() / (e2[fin] + 1e-30)).max()) < 1e-9
