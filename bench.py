@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--cases-per-batch", type=int, default=0,
                     help="corrector: stream the training cases in batches of this many meshes (0: one batch)")
     ap.add_argument("--record-steps", type=int, default=100, help="corrector streaming: steps recorded per batch")
+    ap.add_argument("--gates", default=None,
+                    help="corrector acceptance gates, 'ratio[:consistency],...' (first one is the headline)")
     ap.add_argument("--save-checkpoint", default=None, help="corrector: save the trained model here")
     ap.add_argument("--workload", default="taylor_green",
                     choices=["taylor_green", "channel_cylinder", "ensemble", "corrector", "corrector3d",
@@ -741,12 +743,28 @@ def corrector_train(args, three_d: bool):
     return model, info
 
 
-def corrector_evaluate(model_src, args, three_d: bool, ratios=(3.0, 1.2), spinup: int = 200) -> dict:
+CORRECTOR_GATES = ((3.0, 0.0), (1.2, 0.0), (3.0, 0.5), (3.0, 0.3), (1.5, 0.3))
+
+
+def parse_gates(text: str | None) -> tuple:
+    """"3.0,1.2:0.3" -> ((3.0, 0.0), (1.2, 0.3)): residual ratio[:trapezoid consistency] per gate."""
+    if not text:
+        return CORRECTOR_GATES
+    out = []
+    for item in text.split(","):
+        r, _, c = item.partition(":")
+        out.append((float(r), float(c) if c else 0.0))
+    return tuple(out)
+
+
+def corrector_evaluate(model_src, args, three_d: bool, gates=None, spinup: int = 200) -> dict:
     """Held-out cases advanced ``args.windows`` windows of k = 8 steps (a) by plain FVM (a CUDA graph
     of 8 steps per window) and (b) by the corrector with per-case checks and FVM fallback (the
     proposal + checks graph, one host read of the verdicts, the 8-step graph for failed cases), both
     from the same spun-up start and timed with CUDA events; the corrected states are compared with
-    the plain ones at the end.  ``model_src``: a trained model, or a checkpoint path."""
+    the plain ones at the end.  ``model_src``: a trained model, or a checkpoint path.  ``gates``:
+    (residual ratio, trapezoid consistency or 0) per rollout; the first is the line's headline."""
+    gates = parse_gates(getattr(args, "gates", None)) if gates is None else gates
     from fvm_solver_b200 import batched as B
     from fvm_solver_b200.corrector import CheckedRollout, CorrectorModel
     _, seeds = _corrector_family(three_d)
@@ -766,7 +784,7 @@ def corrector_evaluate(model_src, args, three_d: bool, ratios=(3.0, 1.2), spinup
         torch.cuda.synchronize()
     ms_plain = e[0].elapsed_time(e[1])
 
-    def rollout(ratio):
+    def rollout(ratio, consistency):
         corr = B.BatchedFVM(eparts, ecfg, device="cuda")
         corr.t_solver.update_cfl_dt(0.5)
         corr.t_solver.step(spinup)
@@ -774,7 +792,7 @@ def corrector_evaluate(model_src, args, three_d: bool, ratios=(3.0, 1.2), spinup
             model = CorrectorModel.load(model_src, corr, eprm)
         else:
             model = CorrectorModel(corr, eprm, like=model_src)
-        ro = CheckedRollout(model, residual_ratio=ratio)
+        ro = CheckedRollout(model, residual_ratio=ratio, consistency=consistency)
         # capture every CUDA graph before timing (capturing executes nothing; the state stays put)
         ro._run_propose()
         corr.t_solver._sync_prims()
@@ -804,7 +822,8 @@ def corrector_evaluate(model_src, args, three_d: bool, ratios=(3.0, 1.2), spinup
             bad_corr += not fa
             if fa and fr:
                 err.append(float(((a - r).norm() / r.norm()).item()))
-        return {"residual_ratio": ratio, "speedup": ms_plain / ms_corr, "ms_corrected": ms_corr,
+        return {"residual_ratio": ratio, "trapezoid_consistency": consistency or None,
+                "speedup": ms_plain / ms_corr, "ms_corrected": ms_corr,
                 "ms_per_window": {"corrected": ms_corr / args.windows, "plain": ms_plain / args.windows,
                                   "proposal_and_checks": ms_propose},
                 "accept_rate": ro.accepted / max(ro.windows, 1),
@@ -813,7 +832,7 @@ def corrector_evaluate(model_src, args, three_d: bool, ratios=(3.0, 1.2), spinup
                                     "cases_compared": len(err)},
                 "nonfinite_cases": {"plain": bad_plain, "corrected": bad_corr}}
 
-    runs = [rollout(r) for r in ratios]
+    runs = [rollout(r, c) for r, c in gates]
     main, others = runs[0], runs[1:]
     return {"metric": "sim-time/s corrector+fallback over plain FVM", "value": main["speedup"], "unit": "x",
             "higher_is_better": True, "dtype": "bf16 GEMM / f32 state",
@@ -822,9 +841,10 @@ def corrector_evaluate(model_src, args, three_d: bool, ratios=(3.0, 1.2), spinup
                        "steps_per_rollout": 8 * args.windows, "spinup_steps": spinup,
                        "fvm": "SSP-RK3, fixed per-case dt (CFL 0.5)",
                        "net": "4 message-passing layers, width 64, SiLU, tcgen05 BF16 GEMMs",
-                       "checks": f"drift <= 1e-4, residual norm <= {ratios[0]}x, admissible state"},
+                       "checks": f"drift <= 1e-4, residual norm <= {gates[0][0]}x, admissible state"
+                                 + (f", trapezoid distance <= {gates[0][1]} k dt |r0|" if gates[0][1] else "")},
             "ms_plain": ms_plain, **{k: v for k, v in main.items() if k != "speedup"},
-            "other_residual_checks": others, "clocks": clk.summary()}
+            "other_checks": others, "clocks": clk.summary()}
 
 
 def corrector_bench(args, timed):
