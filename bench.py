@@ -664,6 +664,16 @@ def _corrector_cases(n, seed, three_d):
     return parts, cfg, prm
 
 
+def host_memory() -> str:
+    """Available host memory and this process's resident size, for the training log."""
+    try:
+        import psutil
+        return (f"host available {psutil.virtual_memory().available / 2**30:.1f} GiB, "
+                f"rss {psutil.Process().memory_info().rss / 2**30:.1f} GiB")
+    except Exception:                                    # psutil missing: no figures
+        return "host memory n/a"
+
+
 def corrector_train_streaming(args, three_d: bool):
     """Config 4 scale: ``args.train_cases`` seeded cases in batches of ``args.cases_per_batch``
     meshes (a batch's tables are built by a pool of host processes while the GPU trains on the
@@ -671,6 +681,7 @@ def corrector_train_streaming(args, three_d: bool):
     import concurrent.futures as cfut
     import copy
     import multiprocessing as mp
+    from concurrent.futures.process import BrokenProcessPool
     from fvm_solver_b200 import batched as B, workloads as W
     from fvm_solver_b200.corrector import train_streaming
     params, seeds = _corrector_family(three_d)
@@ -681,18 +692,46 @@ def corrector_train_streaming(args, three_d: bool):
         W.ensemble_case(0, device="cuda", base_seed=seeds[0])
     cfg = copy.deepcopy(case0.cfg)
     cfg.solver_name, cfg.solver_extra, cfg.cfl = "Butcher", "SSP_RK3", None
-    pool = cfut.ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1), mp_context=mp.get_context("spawn"),
-                                    initializer=B._worker_init)
+    workers = max(1, min(12, (os.cpu_count() or 2) - 2))
+    state = {"pool": None, "restarts": 0}
     pending = {}
+
+    def new_pool():
+        state["pool"] = cfut.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn"),
+                                                 initializer=B._worker_init)
+
+    def jobs_of(b):
+        return [(i, seeds[0], family, (300_000, 800_000)) for i in range(b * per, (b + 1) * per)]
+
+    def restart(err):
+        # a worker that died (out of host memory, signal) breaks the whole pool: replace it and
+        # resubmit every batch still pending; give up after three replacements
+        state["restarts"] += 1
+        print(f"table pool restarted ({type(err).__name__}: {err}); {host_memory()}", file=sys.stderr, flush=True)
+        if state["restarts"] > 3:
+            raise err
+        state["pool"].shutdown(wait=False, cancel_futures=True)
+        new_pool()
+        for b in list(pending):
+            pending[b] = [state["pool"].submit(B._ensemble_worker, j) for j in jobs_of(b)]
 
     def prefetch(b):
         if b not in pending:
-            jobs = [(i, seeds[0], family, (300_000, 800_000)) for i in range(b * per, (b + 1) * per)]
-            pending[b] = [pool.submit(B._ensemble_worker, j) for j in jobs]
+            try:
+                pending[b] = [state["pool"].submit(B._ensemble_worker, j) for j in jobs_of(b)]
+            except BrokenProcessPool as e:
+                pending[b] = []
+                restart(e)
 
     def make_batch(b):
         prefetch(b)
-        parts = [f.result() for f in pending.pop(b)]
+        while True:
+            try:
+                parts = [f.result() for f in pending[b]]
+                break
+            except BrokenProcessPool as e:
+                restart(e)
+        pending.pop(b)
         batch = B.BatchedFVM(parts, cfg, device="cuda")
         batch.t_solver.update_cfl_dt(0.5)
         prm = torch.tensor([[params(i, seeds[0])["mach"], np.log10(params(i, seeds[0])["reynolds"])]
@@ -701,17 +740,22 @@ def corrector_train_streaming(args, three_d: bool):
 
     def log(b, done, cases, loss):
         if b % max(1, n_batches // 20) == 0 or b == n_batches - 1:
-            print(f"batch {b + 1}/{n_batches}: {done} iterations, {cases} cases, loss {loss:.4g}", file=sys.stderr,
-                  flush=True)
+            print(f"batch {b + 1}/{n_batches}: {done} iterations, {cases} cases, loss {loss:.4g}, "
+                  f"{time.time() - t0:.0f} s; {host_memory()}", file=sys.stderr, flush=True)
+        if save_every and (b + 1) % save_every == 0 and args.save_checkpoint:
+            state["model"].save(args.save_checkpoint + ".partial", meta={"batches_done": b + 1, "iters_done": done})
 
+    save_every = max(1, n_batches // 10)
     t0 = time.time()
+    new_pool()
     try:
         model, hist, cases = train_streaming(make_batch, n_batches, args.iters, k=8, record=args.record_steps,
-                                             spinup=200, prefetch=prefetch, log=log)
+                                             spinup=200, prefetch=prefetch, log=log, keep=state)
     finally:
-        pool.shutdown(cancel_futures=True)
+        state["pool"].shutdown(cancel_futures=True)
     torch.cuda.synchronize()
     info = {"train_cases": cases, "cases_per_batch": per, "batches": n_batches, "iters": args.iters,
+            "table_workers": workers, "pool_restarts": state["restarts"],
             "recorded_steps_per_case": args.record_steps + 8, "loss_first": hist[0][1], "loss_last": hist[-1][1],
             "loss_history": hist[:: max(1, len(hist) // 20)], "seconds": time.time() - t0}
     return model, info

@@ -408,14 +408,16 @@ def train(model: CorrectorModel, traj: torch.Tensor, iters: int, seed: int = 0, 
 
 
 def train_streaming(make_batch, n_batches: int, iters: int, k: int = 8, record: int = 100, spinup: int = 200,
-                    seed: int = 0, lr: float = 1e-3, prefetch=None, log=None) -> tuple:
+                    seed: int = 0, lr: float = 1e-3, prefetch=None, log=None, keep: dict | None = None) -> tuple:
     """Train one network on a stream of mesh batches (many more cases than fit on the device).
 
     ``make_batch(b)`` -> (BatchedFVM with its time steps set, case parameters [cases][2]) builds
     batch b; ``prefetch(b)`` (optional) starts building batch b ahead of time.  Each batch is
     spun up ``spinup`` steps and ``record`` + k steps are recorded; ``iters / n_batches`` Adam
     iterations then draw random windows from it.  The normalisation comes from the first batch,
-    and the network and the Adam moments carry over.  Returns (model, loss history, cases seen)."""
+    and the network and the Adam moments carry over.  ``keep`` (a dict), when given, holds the
+    current model under "model" after each batch (for periodic saving by ``log``).  Returns
+    (model, loss history, cases seen)."""
     model, hist, cases = None, [], 0
     per = max(1, iters // n_batches)
     done = 0
@@ -432,9 +434,11 @@ def train_streaming(make_batch, n_batches: int, iters: int, k: int = 8, record: 
         done += n_it
         cases += batch.n_cases
         model = m
+        if keep is not None:
+            keep["model"] = model
+        del traj
         if log is not None:
             log(b, done, cases, h[-1][1])
-        del traj
     return model, hist, cases
 
 
