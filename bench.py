@@ -78,6 +78,8 @@ def parse():
                          "ensemble: batched 2D ensemble vs the same cases run one by one")
     ap.add_argument("--cases", type=int, default=256, help="ensemble size")
     ap.add_argument("--ensemble-cfl", type=float, default=None, help="ensemble: CFL of the fixed per-case dt")
+    ap.add_argument("--launch", default=None,
+                    help="fixed block sizes instead of the autotuner, e.g. cell=128,face=128,div_stage=64")
     ap.add_argument("--no-extras", action="store_true",
                     help="headline line without the channel / ensemble / corrector keys")
     return ap.parse_args()
@@ -584,10 +586,15 @@ def ensemble_sharded(args):
 
 def secondary(args):
     """Secondary workloads (single GPU) as their own benchmark lines."""
-    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and args.workload not in ("partitioned", "ensemble"):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    dp_training = args.workload in ("corrector", "corrector3d") and args.cases_per_batch and not args.checkpoint
+    if world > 1 and args.workload not in ("partitioned", "ensemble") and not dp_training:
         sys.exit(f"--workload {args.workload} runs on one GPU; several ranks run the default workload "
-                 f"(one box per rank), --workload ensemble (cases split across the ranks) or "
-                 f"--workload partitioned (one box split across the ranks)")
+                 f"(one box per rank), --workload ensemble (cases split across the ranks), "
+                 f"--workload partitioned (one box split across the ranks) or corrector training with "
+                 f"--cases-per-batch (data-parallel)")
+    if world > 1 and dp_training:
+        return corrector_bench_dp(args)
     if args.workload == "partitioned":
         return partitioned_bench(args)
     if args.workload == "ensemble" and int(os.environ.get("WORLD_SIZE", "1")) > 1:
@@ -674,10 +681,13 @@ def host_memory() -> str:
         return "host memory n/a"
 
 
-def corrector_train_streaming(args, three_d: bool):
+def corrector_train_streaming(args, three_d: bool, group=None):
     """Config 4 scale: ``args.train_cases`` seeded cases in batches of ``args.cases_per_batch``
     meshes (a batch's tables are built by a pool of host processes while the GPU trains on the
-    previous batch), ``args.iters`` Adam iterations in all (``corrector.train_streaming``)."""
+    previous batch), ``args.iters`` Adam iterations in all (``corrector.train_streaming``).  With a
+    process group of W ranks, training is data-parallel: rank r streams the global batches
+    r, r + W, r + 2W, ... (the cases are split, not repeated) and every iteration averages the
+    gradients of all ranks, so each iteration sees W batches of cases."""
     import concurrent.futures as cfut
     import copy
     import multiprocessing as mp
@@ -687,7 +697,10 @@ def corrector_train_streaming(args, three_d: bool):
     params, seeds = _corrector_family(three_d)
     family = "sphere" if three_d else "channel"
     per = args.cases_per_batch
-    n_batches = max(1, args.train_cases // per)
+    import torch.distributed as dist
+    world = dist.get_world_size(group) if group is not None or dist.is_initialized() else 1
+    rank = dist.get_rank(group) if world > 1 else 0
+    n_batches = max(1, args.train_cases // per // world)
     case0 = W.sphere_case(0, device="cuda", base_seed=seeds[0], cells=(20_000, 20_000)) if three_d else \
         W.ensemble_case(0, device="cuda", base_seed=seeds[0])
     cfg = copy.deepcopy(case0.cfg)
@@ -700,8 +713,12 @@ def corrector_train_streaming(args, three_d: bool):
         state["pool"] = cfut.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn"),
                                                  initializer=B._worker_init)
 
+    def cases_of(b):                                     # local batch b -> global batch b W + r
+        gb = b * world + rank
+        return range(gb * per, (gb + 1) * per)
+
     def jobs_of(b):
-        return [(i, seeds[0], family, (300_000, 800_000)) for i in range(b * per, (b + 1) * per)]
+        return [(i, seeds[0], family, (300_000, 800_000)) for i in cases_of(b)]
 
     def restart(err):
         # a worker that died (out of host memory, signal) breaks the whole pool: replace it and
@@ -735,14 +752,14 @@ def corrector_train_streaming(args, three_d: bool):
         batch = B.BatchedFVM(parts, cfg, device="cuda")
         batch.t_solver.update_cfl_dt(0.5)
         prm = torch.tensor([[params(i, seeds[0])["mach"], np.log10(params(i, seeds[0])["reynolds"])]
-                            for i in range(b * per, (b + 1) * per)], dtype=torch.float32)
+                            for i in cases_of(b)], dtype=torch.float32)
         return batch, prm
 
     def log(b, done, cases, loss):
-        if b % max(1, n_batches // 20) == 0 or b == n_batches - 1:
+        if rank == 0 and (b % max(1, n_batches // 20) == 0 or b == n_batches - 1):
             print(f"batch {b + 1}/{n_batches}: {done} iterations, {cases} cases, loss {loss:.4g}, "
                   f"{time.time() - t0:.0f} s; {host_memory()}", file=sys.stderr, flush=True)
-        if save_every and (b + 1) % save_every == 0 and args.save_checkpoint:
+        if save_every and (b + 1) % save_every == 0 and args.save_checkpoint and rank == 0:
             state["model"].save(args.save_checkpoint + ".partial", meta={"batches_done": b + 1, "iters_done": done})
 
     save_every = max(1, n_batches // 10)
@@ -750,12 +767,12 @@ def corrector_train_streaming(args, three_d: bool):
     new_pool()
     try:
         model, hist, cases = train_streaming(make_batch, n_batches, args.iters, k=8, record=args.record_steps,
-                                             spinup=200, prefetch=prefetch, log=log, keep=state)
+                                             spinup=200, prefetch=prefetch, log=log, keep=state, group=group)
     finally:
         state["pool"].shutdown(cancel_futures=True)
     torch.cuda.synchronize()
-    info = {"train_cases": cases, "cases_per_batch": per, "batches": n_batches, "iters": args.iters,
-            "table_workers": workers, "pool_restarts": state["restarts"],
+    info = {"train_cases": cases * world, "cases_per_batch": per, "batches": n_batches * world, "iters": args.iters,
+            "table_workers": workers, "pool_restarts": state["restarts"], "data_parallel_ranks": world,
             "recorded_steps_per_case": args.record_steps + 8, "loss_first": hist[0][1], "loss_last": hist[-1][1],
             "loss_history": hist[:: max(1, len(hist) // 20)], "seconds": time.time() - t0}
     return model, info
@@ -913,6 +930,33 @@ def corrector_bench(args, timed):
     print(json.dumps(out))
 
 
+def corrector_bench_dp(args):
+    """Data-parallel corrector training under torchrun (one rank per GPU, NCCL): every rank streams
+    its share of the training cases and the gradients are averaged each iteration; rank 0 then
+    saves the model (``--save-checkpoint``) and evaluates it alone, as ``corrector_bench`` does."""
+    import torch.distributed as dist
+    from datetime import timedelta
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    three_d = args.workload == "corrector3d"
+    if args.iters is None:
+        args.iters = 2000 if three_d else 6000
+    model, info = corrector_train_streaming(args, three_d, group=dist.group.WORLD)
+    dist.barrier()
+    rank = dist.get_rank()
+    dist.destroy_process_group()
+    if rank != 0:
+        return
+    if args.save_checkpoint:
+        os.makedirs(os.path.dirname(os.path.abspath(args.save_checkpoint)), exist_ok=True)
+        model.save(args.save_checkpoint, meta=info)
+    out = corrector_evaluate(model, args, three_d)
+    out.update({"n_gpus": info["data_parallel_ranks"], "data": "synthetic", "train": info,
+                "model": "trained in this run (data-parallel)"})
+    print(json.dumps(out))
+
+
 def ell_result(tables, reps: int = 20) -> dict:
     """The ELL operator seam (``SPMB200``, the drop-in for the reference's Triton ELL path) on the
     benchmark box's own operators, timed as the reference's micro-benchmark does
@@ -1008,7 +1052,18 @@ def main():
     N, F, Fb = eq.mesh.n_cells, eq.mesh.n_facets, eq.dev.n_bc
     lib = _lib.load()
     from fvm_solver_b200.autotune import autotune
-    tuned_full = autotune(eq)
+    if args.launch:
+        # fixed launch configuration (reproducing a profile of the benchmark's own kernels on a
+        # smaller box): "cell=128,face=128,div_stage=64"; no prefetch, per-thread record loads
+        from fvm_solver_b200 import autotune as AT
+        AT.reset()
+        tuned_full = {}
+        for item in args.launch.split(","):
+            k, _, bs = item.partition("=")
+            AT.set_block_size(k, int(bs))
+            tuned_full[k] = {"threads": int(bs), "prefetch": 0, "variant": "registers", "ms": {}}
+    else:
+        tuned_full = autotune(eq)
     tuned = {k: v["threads"] for k, v in tuned_full.items()}
     prefetch = {k: v["prefetch"] for k, v in tuned_full.items()}
     variants = {k: v["variant"] for k, v in tuned_full.items()}

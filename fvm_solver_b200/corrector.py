@@ -79,6 +79,53 @@ def geometry_features(kt, case_params: torch.Tensor | None, lengths=(2.0, 1.0)) 
     return torch.cat(feats, 1).float().contiguous()
 
 
+def _group_world(group) -> int:
+    import torch.distributed as dist
+    return dist.get_world_size(group) if dist.is_available() and dist.is_initialized() else 1
+
+
+def broadcast_from_first(tensors, group=None):
+    """Overwrite ``tensors`` on every rank of ``group`` with the first rank's values (no-op on one
+    rank)."""
+    import torch.distributed as dist
+    if _group_world(group) == 1:
+        return
+    src = dist.get_global_rank(group, 0) if group is not None else 0
+    for t in tensors:
+        dist.broadcast(t, src=src, group=group)
+
+
+class GradBucket:
+    """Data-parallel gradient exchange: the gradients of all parameters live in one flat buffer
+    (``views`` holds one view per parameter), so a training iteration averages them over the ranks
+    of ``group`` with a single all-reduce (NCCL between GPUs, gloo on CPU) before the optimiser
+    step.  With one rank (or no process group) ``average`` does nothing."""
+
+    def __init__(self, tensors: dict):
+        first = next(iter(tensors.values()))
+        total = sum(t.numel() for t in tensors.values())
+        self.flat = torch.zeros(total, dtype=first.dtype, device=first.device)
+        self.views, o = {}, 0
+        for k, t in tensors.items():
+            v = self.flat[o:o + t.numel()].view(t.shape)
+            v.copy_(t)
+            self.views[k] = v
+            o += t.numel()
+        self.group = None
+        self.world = 1
+
+    def attach(self, group=None):
+        self.group = group
+        self.world = _group_world(group)
+
+    def average(self):
+        if self.world == 1:
+            return
+        import torch.distributed as dist
+        dist.all_reduce(self.flat, op=dist.ReduceOp.SUM, group=self.group)
+        self.flat.div_(self.world)
+
+
 class CorrectorNet:
     """Parameters, forward, backward and Adam of the message-passing corrector (see module doc)."""
 
@@ -94,7 +141,8 @@ class CorrectorNet:
             self.params[f"b{l}"] = torch.zeros(W, device=self.dev)
         self.params["W_out"] = U((n_out, W), W) * 0.1
         self.params["b_out"] = torch.zeros(n_out, device=self.dev)
-        self.grads = {k: torch.zeros_like(v) for k, v in self.params.items()}
+        self.bucket = GradBucket({k: torch.zeros_like(v) for k, v in self.params.items()})
+        self.grads = self.bucket.views
         self.m = {k: torch.zeros_like(v) for k, v in self.params.items()}
         self.v = {k: torch.zeros_like(v) for k, v in self.params.items()}
         self.bf = {k: _bf(self.params[k]) for k in ["W_in"] + [f"W{l}" for l in range(layers)]}
@@ -210,8 +258,21 @@ class CorrectorNet:
         _lib.check(self.lib.fvm_transpose_bf16(b["X"].data_ptr(), N, XW, XW, b["XT"].data_ptr(), Np, s),
                    "fvm_transpose_bf16")
         self._gemm(b["dZT"], Np, b["XT"], Np, W, XW, Np, Df=g["W_in"], ldd=XW, k_splits=splits)
+        self.bucket.average()
         self.adam()
         return b["loss"]
+
+    def data_parallel(self, group=None):
+        """Train data-parallel over the ranks of ``group`` (one process per GPU): the first rank's
+        weights are broadcast, and every ``train_step`` averages the gradients of all ranks (one
+        all-reduce of the flat gradient buffer) before Adam, so the ranks' weights stay identical."""
+        self.bucket.attach(group)
+        broadcast_from_first(list(self.params.values()), group)
+        for k in self.bf:
+            self.bf[k].copy_(_bf(self.params[k]))
+        for k in self.bfT:
+            self.bfT[k].copy_(_bf(self.params[k].t()))
+        return self
 
     def adam(self, beta1=0.9, beta2=0.999, eps=1e-8):
         self.step_count += 1
@@ -324,10 +385,12 @@ class CorrectorModel:
         return (self.k * self.batch.t_solver.dt)[self.cell_case].unsqueeze(1)
 
     def set_normalisation(self, feats: torch.Tensor, targets: torch.Tensor):
-        """feats [S][N][2C] = [U, base]; targets [S][N][C] = U_{t+k} - U_t - base."""
+        """feats [S][N][2C] = [U, base]; targets [S][N][C] = U_{t+k} - U_t - base.  In
+        data-parallel training the first rank's statistics are used by every rank."""
         self.fmean = feats.mean(dim=(0, 1)).float().contiguous()
         self.finv = (1.0 / (feats.std(dim=(0, 1)) + 1e-12)).float().contiguous()
         self.scale = (targets.std(dim=(0, 1)) + 1e-12).float().contiguous()
+        broadcast_from_first([self.fmean, self.finv, self.scale], self.net.bucket.group)
 
     def inputs(self, state: torch.Tensor, r0: torch.Tensor):
         """Writes base = k dt r0 and the network input features for (state, base); returns them."""
@@ -408,7 +471,8 @@ def train(model: CorrectorModel, traj: torch.Tensor, iters: int, seed: int = 0, 
 
 
 def train_streaming(make_batch, n_batches: int, iters: int, k: int = 8, record: int = 100, spinup: int = 200,
-                    seed: int = 0, lr: float = 1e-3, prefetch=None, log=None, keep: dict | None = None) -> tuple:
+                    seed: int = 0, lr: float = 1e-3, prefetch=None, log=None, keep: dict | None = None,
+                    group=None) -> tuple:
     """Train one network on a stream of mesh batches (many more cases than fit on the device).
 
     ``make_batch(b)`` -> (BatchedFVM with its time steps set, case parameters [cases][2]) builds
@@ -416,7 +480,9 @@ def train_streaming(make_batch, n_batches: int, iters: int, k: int = 8, record: 
     spun up ``spinup`` steps and ``record`` + k steps are recorded; ``iters / n_batches`` Adam
     iterations then draw random windows from it.  The normalisation comes from the first batch,
     and the network and the Adam moments carry over.  ``keep`` (a dict), when given, holds the
-    current model under "model" after each batch (for periodic saving by ``log``).  Returns
+    current model under "model" after each batch (for periodic saving by ``log``).  ``group``:
+    data-parallel training over its ranks (each rank streams its own batches, all ranks take the
+    same number of batches and iterations; gradients are averaged every iteration).  Returns
     (model, loss history, cases seen)."""
     model, hist, cases = None, [], 0
     per = max(1, iters // n_batches)
@@ -426,8 +492,11 @@ def train_streaming(make_batch, n_batches: int, iters: int, k: int = 8, record: 
             prefetch(b + 1)
         batch, prm = make_batch(b)
         traj = record_trajectory(batch, steps=record + k, spinup=spinup)
-        m = CorrectorModel(batch, prm, k=k, seed=seed, lr=lr) if model is None else \
-            CorrectorModel(batch, prm, like=model)
+        if model is None:
+            m = CorrectorModel(batch, prm, k=k, seed=seed, lr=lr)
+            m.net.data_parallel(group)
+        else:
+            m = CorrectorModel(batch, prm, like=model)
         n_it = per if b < n_batches - 1 else max(per, iters - done)
         h = train(m, traj, iters=n_it, seed=seed + b, log_every=max(1, n_it // 2), normalise=model is None)
         hist.extend((done + it, loss) for it, loss in h)
