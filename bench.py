@@ -710,8 +710,10 @@ def corrector_train_streaming(args, three_d: bool, group=None):
     pending = {}
 
     def new_pool():
+        # workers are replaced every 16 tables (long-lived table workers died on the GPU machine
+        # after about 80 tables each, with host memory to spare)
         state["pool"] = cfut.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn"),
-                                                 initializer=B._worker_init)
+                                                 initializer=B._worker_init, max_tasks_per_child=16)
 
     def cases_of(b):                                     # local batch b -> global batch b W + r
         gb = b * world + rank
@@ -722,10 +724,12 @@ def corrector_train_streaming(args, three_d: bool, group=None):
 
     def restart(err):
         # a worker that died (out of host memory, signal) breaks the whole pool: replace it and
-        # resubmit every batch still pending; give up after three replacements
+        # resubmit every batch still pending; give up after a hundred replacements
         state["restarts"] += 1
-        print(f"table pool restarted ({type(err).__name__}: {err}); {host_memory()}", file=sys.stderr, flush=True)
-        if state["restarts"] > 3:
+        codes = sorted({p.exitcode for p in getattr(state["pool"], "_processes", {}).values() if p.exitcode})
+        print(f"table pool restarted ({type(err).__name__}: {err}; worker exit codes {codes}); {host_memory()}",
+              file=sys.stderr, flush=True)
+        if state["restarts"] > 100:
             raise err
         state["pool"].shutdown(wait=False, cancel_futures=True)
         new_pool()

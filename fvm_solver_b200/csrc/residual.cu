@@ -142,17 +142,6 @@ __device__ __forceinline__ float ld1_mut(const float* p) {
     if constexpr (COH) return __ldcg(p);
     else return __ldg(p);
 }
-// The first C floats of a padded row (C = 4 or 5; the row starts on a 16-byte boundary): one
-// 128-bit load and, for C = 5, one 32-bit load of the same 32-byte sector, so the row's padding
-// takes no registers.  COH as for ld_mut.
-template <bool COH, int C>
-__device__ __forceinline__ void ld_used(const float* p, float (&v)[C]) {
-    static_assert(C == 4 || C == 5, "row width");
-    const float4 t = COH ? __ldcg(reinterpret_cast<const float4*>(p)) : __ldg(reinterpret_cast<const float4*>(p));
-    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-    if constexpr (C == 5) v[4] = COH ? __ldcg(p + 4) : __ldg(p + 4);
-}
-
 template <int N>
 __device__ __forceinline__ void st_vec(float* p, const float (&v)[N]) {
     static_assert(N % 4 == 0, "row width");
@@ -446,14 +435,14 @@ __device__ __forceinline__ void cell_body(const fvm_mesh_t& m, const Phys& p, co
             next_cols<DIM>(m, i + stride, NA, cols, skip_frozen);
             continue;
         }
-        float X[KG][C];
+        float X[KG][RS];
 #pragma unroll
         for (int k = 0; k < KG; ++k) {
-            if (cols[k] < N) ld_used<COH, C>(prims + (int64_t)cols[k] * RS, X[k]);
-            else ld_used<true, C>(bcv + (int64_t)(cols[k] - N) * RS, X[k]);
+            if (cols[k] < N) ld_mut<COH, RS>(prims + (int64_t)cols[k] * RS, X[k]);
+            else ld_vec_cg<RS>(bcv + (int64_t)(cols[k] - N) * RS, X[k]);
         }
-        float U[C];
-        ld_used<COH, C>(prims + (int64_t)i * RS, U);
+        float U[RS];
+        ld_mut<COH, RS>(prims + (int64_t)i * RS, U);
         float rec[Ly::CR];
         ld_vec<Ly::CR>(m.cell_rec + (int64_t)i * Ly::CR, rec);
         next_cols<DIM>(m, i + stride, NA, cols, skip_frozen);
@@ -632,7 +621,7 @@ __global__ void __maxnreg__(FVM_CELL_MAXNREG) k_cell(fvm_mesh_t m, Phys p, const
 template <int DIM>
 __device__ __forceinline__ void face_eval(const fvm_mesh_t& m, const Phys& p, const float* __restrict__ bcv,
                                           int f, int ca, int cb, const float (&rec)[L<DIM>::FR],
-                                          const float (&P0)[L<DIM>::C], const float (&P1)[L<DIM>::C],
+                                          const float (&P0)[L<DIM>::RS], const float (&P1)[L<DIM>::RS],
                                           const float (&G0)[L<DIM>::GS], const float (&G1)[L<DIM>::GS],
                                           float (&F)[L<DIM>::RS]) {
     using Ly = L<DIM>;
@@ -825,9 +814,9 @@ __device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, co
     // the boundary value, and its gradient is the interior cell's (facet_process.py:364-368).
     const int cell0 = ca >= 0 ? ca : cb;
     const int cell1 = cb >= 0 ? cb : ca;
-    float P0[Ly::C], P1[Ly::C], G0[GS], G1[GS];
-    ld_used<COH, Ly::C>(prims + (int64_t)cell0 * RS, P0);
-    ld_used<COH, Ly::C>(prims + (int64_t)cell1 * RS, P1);
+    float P0[RS], P1[RS], G0[GS], G1[GS];
+    ld_mut<COH, RS>(prims + (int64_t)cell0 * RS, P0);
+    ld_mut<COH, RS>(prims + (int64_t)cell1 * RS, P1);
     ld_vec_cg<GS>(grads + (int64_t)cell0 * GS, G0);
     ld_vec_cg<GS>(grads + (int64_t)cell1 * GS, G1);
     float rec[Ly::FR];
@@ -928,9 +917,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_face_staged(fvm_mesh_t m, Phys p,
             const int ca = as_int(rec[Ly::FA]), cb = as_int(rec[Ly::FB]);
             const int cell0 = ca >= 0 ? ca : cb;
             const int cell1 = cb >= 0 ? cb : ca;
-            float P0[Ly::C], P1[Ly::C], G0[GS], G1[GS];
-            ld_used<false, Ly::C>(prims + (int64_t)cell0 * RS, P0);
-            ld_used<false, Ly::C>(prims + (int64_t)cell1 * RS, P1);
+            float P0[RS], P1[RS], G0[GS], G1[GS];
+            ld_vec<RS>(prims + (int64_t)cell0 * RS, P0);
+            ld_vec<RS>(prims + (int64_t)cell1 * RS, P1);
             ld_vec_cg<GS>(grads + (int64_t)cell0 * GS, G0);
             ld_vec_cg<GS>(grads + (int64_t)cell1 * GS, G1);
             float F[RS];
@@ -997,9 +986,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_face_div(fvm_mesh_t m, Phys p, co
             const int ca = as_int(rec[Ly::FA]), cb = as_int(rec[Ly::FB]);
             const int cell0 = ca >= 0 ? ca : cb;
             const int cell1 = cb >= 0 ? cb : ca;
-            float P0[Ly::C], P1[Ly::C], G0[GS], G1[GS];
-            ld_used<false, Ly::C>(prims + (int64_t)cell0 * RS, P0);
-            ld_used<false, Ly::C>(prims + (int64_t)cell1 * RS, P1);
+            float P0[RS], P1[RS], G0[GS], G1[GS];
+            ld_vec<RS>(prims + (int64_t)cell0 * RS, P0);
+            ld_vec<RS>(prims + (int64_t)cell1 * RS, P1);
             ld_vec_cg<GS>(grads + (int64_t)cell0 * GS, G0);
             ld_vec_cg<GS>(grads + (int64_t)cell1 * GS, G1);
             face_eval<DIM>(m, p, bcv, f, ca, cb, rec, P0, P1, G0, G1, F);
