@@ -68,8 +68,9 @@ struct L {
     static constexpr int C = DIM + 2, K = DIM + 1, KG = DIM + 2;
     static constexpr int RS = FVM_ROW(DIM), GS = FVM_GROW(DIM);
     static constexpr int CR = FVM_CELL_REC(DIM), FR = FVM_FACE_REC(DIM), DR = FVM_DIV_REC;
-    // compact cell record offsets: weights [DIM][KG], neighbour columns [KG - 1], displacements, eps
-    static constexpr int GV = 0, GC = DIM * KG, DISP = GC + KG - 1, EPS = DISP + K * DIM;
+    // compact cell record offsets: neighbour columns [KG - 1] (padded to 4, one 128-bit load),
+    // weights [DIM][KG], displacements [K][DIM], eps
+    static constexpr int GC = 0, GV = 4, DISP = GV + DIM * KG, EPS = DISP + K * DIM;
     static constexpr int SELF_SHIFT = 28;                 // own slot: bits 28..30 of the first column
     // face record offsets
     static constexpr int FA = 0, FB = 1, INVD = 2, SIZE = 3, NRM = 4, XO = 4 + DIM, RA = 4 + 2 * DIM,
@@ -202,17 +203,20 @@ __device__ __forceinline__ int2 next_codes(const fvm_mesh_t& m, int f, int nF, b
     return on ? ld_codes(m.face_rec + (int64_t)f * L<DIM>::FR) : make_int2(0, 0);
 }
 // The KG stencil columns of cell i in slot order, from its compact record: the KG - 1 stored
-// neighbour columns with the cell's own index inserted at its slot (selects only, no indexing of
-// register arrays by a runtime value).  Items not loaded get the column 0 everywhere.
+// neighbour columns with the cell's own index inserted at its slot `own` (selects only, no
+// indexing of register arrays by a runtime value).  Items not loaded get the column 0 everywhere.
 template <int DIM>
-__device__ __forceinline__ void next_cols(const fvm_mesh_t& m, int i, int NA, int* cols, bool skip_frozen) {
+__device__ __forceinline__ void next_cols(const fvm_mesh_t& m, int i, int NA, int* cols, int& own,
+                                          bool skip_frozen) {
     using Ly = L<DIM>;
     const bool on = i < NA && (!skip_frozen || case_on(m, m.cell_case, i));
+    static_assert(Ly::KG - 1 <= 4 && Ly::GC == 0, "columns in the record's first 16 bytes");
+    const int4 q = on ? __ldg(reinterpret_cast<const int4*>(m.cell_rec + (int64_t)i * Ly::CR)) : make_int4(0, 0, 0, 0);
+    const int nq[4] = {q.x, q.y, q.z, q.w};
     int nb[Ly::KG - 1];
 #pragma unroll
-    for (int k = 0; k < Ly::KG - 1; ++k)
-        nb[k] = on ? __ldg(reinterpret_cast<const int*>(m.cell_rec) + (int64_t)i * Ly::CR + Ly::GC + k) : 0;
-    const int own = (nb[0] >> Ly::SELF_SHIFT) & 7;
+    for (int k = 0; k < Ly::KG - 1; ++k) nb[k] = nq[k];
+    own = (nb[0] >> Ly::SELF_SHIFT) & 7;
     nb[0] &= (1 << Ly::SELF_SHIFT) - 1;
     const int self = on ? i : 0;
 #pragma unroll
@@ -427,12 +431,12 @@ __device__ __forceinline__ void cell_body(const fvm_mesh_t& m, const Phys& p, co
     int i = lo + blockIdx.x * blockDim.x + threadIdx.x;
     if (blockIdx.x == 0 && threadIdx.x == 0) *has_grads = 1;
     const bool skip_frozen = frozen_skip(m, NA - lo, stride);
-    int cols[KG];
-    next_cols<DIM>(m, i, NA, cols, skip_frozen);
+    int cols[KG], own;
+    next_cols<DIM>(m, i, NA, cols, own, skip_frozen);
     for (int64_t tile = blockIdx.x; i < NA; i += stride, tile += gridDim.x) {
         if (waves > 0) prefetch_tile(m.cell_rec + (int64_t)lo * Ly::CR, NA - lo, Ly::CR, tile + (int64_t)waves * gridDim.x);
         if (m.case_active && !case_on(m, m.cell_case, i)) {
-            next_cols<DIM>(m, i + stride, NA, cols, skip_frozen);
+            next_cols<DIM>(m, i + stride, NA, cols, own, skip_frozen);
             continue;
         }
         float X[KG][RS];
@@ -441,11 +445,17 @@ __device__ __forceinline__ void cell_body(const fvm_mesh_t& m, const Phys& p, co
             if (cols[k] < N) ld_mut<COH, RS>(prims + (int64_t)cols[k] * RS, X[k]);
             else ld_vec_cg<RS>(bcv + (int64_t)(cols[k] - N) * RS, X[k]);
         }
-        float U[RS];
-        ld_mut<COH, RS>(prims + (int64_t)i * RS, U);
+        // the cell's own primitives are its stencil row at slot `own` (no second load of the row)
+        float U[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            U[c] = X[0][c];
+#pragma unroll
+            for (int k = 1; k < KG; ++k) U[c] = own == k ? X[k][c] : U[c];
+        }
         float rec[Ly::CR];
         ld_vec<Ly::CR>(m.cell_rec + (int64_t)i * Ly::CR, rec);
-        next_cols<DIM>(m, i + stride, NA, cols, skip_frozen);
+        next_cols<DIM>(m, i + stride, NA, cols, own, skip_frozen);
         float g[DIM][C];
 #pragma unroll
         for (int d = 0; d < DIM; ++d)

@@ -215,10 +215,11 @@ class KernelTables:
     def records(self) -> dict:
         """The device record layout of ``include/fvm_b200.h`` (cell, divergence and facet records).
 
-        Cell record [N][CR]: G weights [dim][KG], then for the reference's stencil (compact, CR =
-        20 / 32) the KG - 1 neighbour columns in slot order (int32 bits, the own slot in bits
-        28..30 of the first), centroid->facet displacements [K][dim], limiter epsilon; for a
-        widened stencil G columns [KG], displacements, epsilon, meta (int32 bits), zero padding.
+        Cell record [N][CR]: for the reference's stencil (compact, CR = 20 / 32) the KG - 1
+        neighbour columns in slot order (int32 bits, the own slot in bits 28..30 of the first;
+        padded to four), G weights [dim][KG], centroid->facet displacements [K][dim], limiter
+        epsilon; for a widened stencil G weights [dim][KG], G columns [KG], displacements,
+        epsilon, meta (int32 bits), zero padding.
         Divergence record [N][8]: weights [kf], facet indices [kf] (int32 bits), padding.
         Facet record [F][FR]: side-0 cell, side-1 cell (int32 bits; a boundary side holds
         -1 - boundary index), +-1/d (negative: side 1's cell has the lower index), |S|, normal [dim],
@@ -229,9 +230,7 @@ class KernelTables:
         CR, FR, DR = record_sizes(dim, kg)
         bits = lambda t: t.to(torch.int32).view(torch.float32)
         cell = torch.zeros((N, CR), dtype=torch.float32)
-        o = 0
-        cell[:, o:o + dim * kg] = self.g_vals.permute(2, 0, 1).reshape(N, dim * kg)
-        o += dim * kg
+        weights = self.g_vals.permute(2, 0, 1).reshape(N, dim * kg)
         if kg == dim + 1 + 1:
             # compact record (the reference's stencil: every slot valid, the cell itself in one of
             # them): the kg - 1 neighbour columns in slot order, the own slot in the top bits of the
@@ -249,12 +248,16 @@ class KernelTables:
             slot = is_self.int().argmax(1)
             nbr = cols[~is_self].view(N, kg - 1)
             nbr[:, 0] |= slot.long() << SELF_SLOT_SHIFT
-            cell[:, o:o + kg - 1] = bits(nbr.to(torch.int32))
-            o += kg - 1
+            cell[:, 0:kg - 1] = bits(nbr.to(torch.int32))    # one 128-bit load (padded to 4 slots)
+            o = 4
+            cell[:, o:o + dim * kg] = weights
+            o += dim * kg
             cell[:, o:o + K * dim] = self.disp.permute(2, 0, 1).reshape(N, K * dim)
             o += K * dim
             cell[:, o] = self.eps
         else:
+            cell[:, 0:dim * kg] = weights
+            o = dim * kg
             cell[:, o:o + kg] = bits(self.g_cols.t().contiguous())
             o += kg
             cell[:, o:o + K * dim] = self.disp.permute(2, 0, 1).reshape(N, K * dim)

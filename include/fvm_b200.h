@@ -64,10 +64,11 @@ extern "C" {
  * Integer fields inside float records are stored bit-cast (int32 bits in a float slot). */
 typedef struct fvm_mesh {
     int32_t dim, n_comp, n_cells, n_facets, n_bc, n_char, kg, kf;
-    /* Cell records.  kg = dim + 2 (the reference's stencil): [N][FVM_CELL_REC] = LSQ gradient
-     * weights [dim][KG] in slot order, the KG - 1 neighbour columns in slot order (into
-     * [cells ; boundary facets]; bits 28..30 of the first hold the slot of the cell itself, whose
-     * column is its own index), centroid->facet displacements [K][dim], limiter epsilon.
+    /* Cell records.  kg = dim + 2 (the reference's stencil): [N][FVM_CELL_REC] = the KG - 1
+     * neighbour columns in slot order (into [cells ; boundary facets]; bits 28..30 of the first
+     * hold the slot of the cell itself, whose column is its own index), padded to 4 slots, then
+     * LSQ gradient weights [dim][KG] in slot order, centroid->facet displacements [K][dim],
+     * limiter epsilon.
      * kg > dim + 2: [N][FVM_CELL_REC_KG] = weights [dim][KG], columns [KG], displacements, epsilon,
      * meta (bits 4j..4j+3: slot of face neighbour j; bits 24..28: valid slots), padding. */
     const float *cell_rec;

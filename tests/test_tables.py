@@ -52,9 +52,10 @@ def test_device_records_encode_tables(golden):
     R = K.records()
     dim, N, F, kg = K.dim, K.n_cells, K.n_facets, K.kg
     cell, face, div = R["cell_rec"], R["face_rec"], R["div_rec"]
-    assert torch.equal(cell[:, :dim * kg].reshape(N, dim, kg), K.g_vals.permute(2, 0, 1))
-    # compact record: the kg - 1 neighbour columns, the cell's own slot in bits 28..30 of the first
-    nb = cell[:, dim * kg:dim * kg + kg - 1].contiguous().view(torch.int32).long()
+    # compact record: the kg - 1 neighbour columns (padded to 4), the cell's own slot in bits
+    # 28..30 of the first, then the weights
+    assert torch.equal(cell[:, 4:4 + dim * kg].reshape(N, dim, kg), K.g_vals.permute(2, 0, 1))
+    nb = cell[:, :kg - 1].contiguous().view(torch.int32).long()
     own = (nb[:, 0] >> 28) & 7
     nb[:, 0] &= (1 << 28) - 1
     cols = torch.empty((N, kg), dtype=torch.long)
@@ -62,7 +63,7 @@ def test_device_records_encode_tables(golden):
         cols[:, k] = torch.where(k < own, nb[:, min(k, kg - 2)],
                                  torch.where(k == own, torch.arange(N), nb[:, max(k - 1, 0)]))
     assert torch.equal(cols, K.g_cols.t().long())
-    o = dim * kg + kg - 1
+    o = 4 + dim * kg
     assert torch.equal(cell[:, o:o + (dim + 1) * dim].reshape(N, dim + 1, dim), K.disp.permute(2, 0, 1))
     assert torch.equal(cell[:, o + (dim + 1) * dim], K.eps)
     assert torch.equal(div[:, :K.kf], K.f_vals.t())
