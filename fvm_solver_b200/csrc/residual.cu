@@ -514,10 +514,10 @@ __device__ __forceinline__ void cell_body(const fvm_mesh_t& m, const Phys& p, co
 // order, as cell_body does); the limiter's bounds take the face neighbours only (their slots are in
 // the record's meta, 4 bits each), which for the dim + 2 stencil are all valid slots but the cell
 // itself.  Stencil columns stream through in groups of four, so registers do not grow with kg.
-template <int DIM>
-__global__ void __launch_bounds__(kBlock) k_cell_wide(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
-                                                       const float* __restrict__ bcv, float* __restrict__ grads,
-                                                       int32_t* __restrict__ has_grads) {
+template <int DIM, bool COH>
+__device__ __forceinline__ void cell_wide_body(const fvm_mesh_t& m, const Phys& p, const float* __restrict__ prims,
+                                               const float* __restrict__ bcv, float* __restrict__ grads,
+                                               int32_t* __restrict__ has_grads) {
     using Ly = L<DIM>;
     constexpr int C = Ly::C, K = Ly::K, RS = Ly::RS;
     const int kg = m.kg;
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(kBlock) k_cell_wide(fvm_mesh_t m, Phys p, cons
 #pragma unroll
         for (int j = 0; j < K; ++j) face |= 1u << ((meta >> (4 * j)) & 15);
         float U[RS];
-        ld_vec<RS>(prims + (int64_t)i * RS, U);
+        ld_mut<COH, RS>(prims + (int64_t)i * RS, U);
         float g[DIM][C];
 #pragma unroll
         for (int d = 0; d < DIM; ++d)
@@ -552,7 +552,7 @@ __global__ void __launch_bounds__(kBlock) k_cell_wide(fvm_mesh_t m, Phys p, cons
             for (int q = 0; q < 4; ++q) {
                 if (k0 + q < nvalid) {
                     const int col = as_int(__ldg(rec + GC + k0 + q));
-                    if (col < N) ld_vec<RS>(prims + (int64_t)col * RS, X[q]);
+                    if (col < N) ld_mut<COH, RS>(prims + (int64_t)col * RS, X[q]);
                     else ld_vec_cg<RS>(bcv + (int64_t)(col - N) * RS, X[q]);
                 }
             }
@@ -606,6 +606,13 @@ __global__ void __launch_bounds__(kBlock) k_cell_wide(fvm_mesh_t m, Phys p, cons
             for (int c = 0; c < C; ++c) go[Ly::gi(d, c)] = g[d][c] * phim[c];
         st_vec<Ly::GS>(grads + (int64_t)i * Ly::GS, go);
     }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) k_cell_wide(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
+                                                       const float* __restrict__ bcv, float* __restrict__ grads,
+                                                       int32_t* __restrict__ has_grads) {
+    cell_wide_body<DIM, false>(m, p, prims, bcv, grads, has_grads);
 }
 
 #ifndef FVM_CELL_MAXNREG
@@ -1457,7 +1464,8 @@ __global__ void __launch_bounds__(kBlock) k_step_fused(fvm_mesh_t m, Phys p, Fus
                 bc_item<DIM, true>(m, p, f.prims, f.grads, f.has_grads, f.bcv, f.red, b, scale);
             grid_barrier(f.bar, f.status);
         }
-        cell_body<DIM, true>(m, p, f.prims, f.bcv, f.grads, f.has_grads, 0);
+        if (m.kg == DIM + 2) cell_body<DIM, true>(m, p, f.prims, f.bcv, f.grads, f.has_grads, 0);
+        else cell_wide_body<DIM, true>(m, p, f.prims, f.bcv, f.grads, f.has_grads);
         grid_barrier(f.bar, f.status);
         face_body<DIM, true>(m, p, f.prims, f.bcv, f.grads, f.flux, 0);
         grid_barrier(f.bar, f.status);
@@ -2237,7 +2245,6 @@ extern "C" int fvm_step_fused(const fvm_mesh_t* mesh, const fvm_physics_t* phys,
     if (!phys || !tab_ok(tab) || !bufs_ok(bufs) || !work_ok(mesh, work)) return FVM_E_ARG;
     if (mesh->n_cases > 0 && tab->adaptive) return FVM_E_UNSUPPORTED;
     if (mesh->n_owned > 0 || mesh->char_scale_given) return FVM_E_UNSUPPORTED;   // partitions use the split stages
-    if (mesh->kg != mesh->dim + 2) return FVM_E_UNSUPPORTED;                      // widened stencils: separate launches
     if (mesh->cell_lo || mesh->facet_lo) return FVM_E_UNSUPPORTED;
     FusedArgs f{};
     f.stages = tab->stages;
@@ -2258,9 +2265,7 @@ extern "C" int fvm_multistep_fused(const fvm_mesh_t* mesh, const fvm_physics_t* 
     if (!phys || !bufs_ok(bufs) || !work_ok(mesh, work) || n_terms < 0 || n_terms > FVM_MAX_STAGES ||
         (n_terms > 0 && (!idx || !coef)) || store < 0)
         return FVM_E_ARG;
-    if (mesh->n_owned > 0 || mesh->char_scale_given || mesh->kg != mesh->dim + 2 || mesh->cell_lo ||
-        mesh->facet_lo)
-        return FVM_E_UNSUPPORTED;
+    if (mesh->n_owned > 0 || mesh->char_scale_given || mesh->cell_lo || mesh->facet_lo) return FVM_E_UNSUPPORTED;
     FusedArgs f{};
     f.stages = 1;
     StageArgs& a = f.st[0];

@@ -29,6 +29,20 @@ def test_fused_step_bitwise(case, solver, extra, cfl):
     assert b.t_solver.fused_status() == 0
 
 
+@pytest.mark.parametrize("case,width", [("c2d", 7), ("b3d", 9), ("b3d", 16)])
+def test_fused_step_widened_stencil_bitwise(case, width):
+    """Widened gradient stencils (the wide cell body) inside the fused step: bitwise equal too."""
+    from gpu_helpers import make_equation
+    a, b = _pair(lambda: make_equation(case, "Butcher", "RK4", cfl=0.5, grad_stencil=width)[1])
+    assert a.dev.kg > (2 if case == "c2d" else 3) + 2
+    a.t_solver.step(4)
+    b.t_solver.step(4)
+    torch.cuda.synchronize()
+    assert torch.equal(a.cells.state, b.cells.state)
+    assert torch.equal(a.grads, b.grads)
+    assert b.t_solver.fused_status() == 0
+
+
 def test_fused_adaptive_close():
     from gpu_helpers import make_equation
     a, b = _pair(lambda: make_equation("c2d", "Butcher_adapt", "RK3_SSP4")[1])
