@@ -688,10 +688,7 @@ def corrector_train_streaming(args, three_d: bool, group=None):
     process group of W ranks, training is data-parallel: rank r streams the global batches
     r, r + W, r + 2W, ... (the cases are split, not repeated) and every iteration averages the
     gradients of all ranks, so each iteration sees W batches of cases."""
-    import concurrent.futures as cfut
     import copy
-    import multiprocessing as mp
-    from concurrent.futures.process import BrokenProcessPool
     from fvm_solver_b200 import batched as B, workloads as W
     from fvm_solver_b200.corrector import train_streaming
     params, seeds = _corrector_family(three_d)
@@ -706,53 +703,24 @@ def corrector_train_streaming(args, three_d: bool, group=None):
     cfg = copy.deepcopy(case0.cfg)
     cfg.solver_name, cfg.solver_extra, cfg.cfl = "Butcher", "SSP_RK3", None
     workers = max(1, min(12, (os.cpu_count() or 2) - 2))
-    state = {"pool": None, "restarts": 0}
-    pending = {}
-
-    def new_pool():
-        # workers are replaced every 16 tables (long-lived table workers died on the GPU machine
-        # after about 80 tables each, with host memory to spare)
-        state["pool"] = cfut.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn"),
-                                                 initializer=B._worker_init, max_tasks_per_child=16)
+    state = {}
+    pool = B.TableWorkers(workers)
+    queued = set()
 
     def cases_of(b):                                     # local batch b -> global batch b W + r
         gb = b * world + rank
         return range(gb * per, (gb + 1) * per)
 
-    def jobs_of(b):
-        return [(i, seeds[0], family, (300_000, 800_000)) for i in cases_of(b)]
-
-    def restart(err):
-        # a worker that died (out of host memory, signal) breaks the whole pool: replace it and
-        # resubmit every batch still pending; give up after a hundred replacements
-        state["restarts"] += 1
-        codes = sorted({p.exitcode for p in getattr(state["pool"], "_processes", {}).values() if p.exitcode})
-        print(f"table pool restarted ({type(err).__name__}: {err}; worker exit codes {codes}); {host_memory()}",
-              file=sys.stderr, flush=True)
-        if state["restarts"] > 100:
-            raise err
-        state["pool"].shutdown(wait=False, cancel_futures=True)
-        new_pool()
-        for b in list(pending):
-            pending[b] = [state["pool"].submit(B._ensemble_worker, j) for j in jobs_of(b)]
-
     def prefetch(b):
-        if b not in pending:
-            try:
-                pending[b] = [state["pool"].submit(B._ensemble_worker, j) for j in jobs_of(b)]
-            except BrokenProcessPool as e:
-                pending[b] = []
-                restart(e)
+        if b not in queued:
+            for i in cases_of(b):
+                pool.submit(i, (i, seeds[0], family, (300_000, 800_000)))
+            queued.add(b)
 
     def make_batch(b):
         prefetch(b)
-        while True:
-            try:
-                parts = [f.result() for f in pending[b]]
-                break
-            except BrokenProcessPool as e:
-                restart(e)
-        pending.pop(b)
+        parts = [pool.get(i) for i in cases_of(b)]
+        queued.discard(b)
         batch = B.BatchedFVM(parts, cfg, device="cuda")
         batch.t_solver.update_cfl_dt(0.5)
         prm = torch.tensor([[params(i, seeds[0])["mach"], np.log10(params(i, seeds[0])["reynolds"])]
@@ -762,21 +730,22 @@ def corrector_train_streaming(args, three_d: bool, group=None):
     def log(b, done, cases, loss):
         if rank == 0 and (b % max(1, n_batches // 20) == 0 or b == n_batches - 1):
             print(f"batch {b + 1}/{n_batches}: {done} iterations, {cases} cases, loss {loss:.4g}, "
-                  f"{time.time() - t0:.0f} s; {host_memory()}", file=sys.stderr, flush=True)
+                  f"{time.time() - t0:.0f} s; {host_memory()}; table workers replaced {pool.restarts} "
+                  f"(exit codes {sorted(set(pool.exit_codes))})", file=sys.stderr, flush=True)
         if save_every and (b + 1) % save_every == 0 and args.save_checkpoint and rank == 0:
             state["model"].save(args.save_checkpoint + ".partial", meta={"batches_done": b + 1, "iters_done": done})
 
     save_every = max(1, n_batches // 10)
     t0 = time.time()
-    new_pool()
     try:
         model, hist, cases = train_streaming(make_batch, n_batches, args.iters, k=8, record=args.record_steps,
                                              spinup=200, prefetch=prefetch, log=log, keep=state, group=group)
     finally:
-        state["pool"].shutdown(cancel_futures=True)
+        pool.close()
     torch.cuda.synchronize()
     info = {"train_cases": cases * world, "cases_per_batch": per, "batches": n_batches * world, "iters": args.iters,
-            "table_workers": workers, "pool_restarts": state["restarts"], "data_parallel_ranks": world,
+            "table_workers": workers, "worker_restarts": pool.restarts,
+            "worker_exit_codes": sorted(set(pool.exit_codes)), "data_parallel_ranks": world,
             "recorded_steps_per_case": args.record_steps + 8, "loss_first": hist[0][1], "loss_last": hist[-1][1],
             "loss_history": hist[:: max(1, len(hist) // 20)], "seconds": time.time() - t0}
     return model, info

@@ -59,6 +59,80 @@ def _worker_init():
     torch.set_num_threads(1)
 
 
+def _table_worker_loop(jobs, results):
+    _worker_init()
+    while True:
+        item = jobs.get()
+        if item is None:
+            return
+        jid, job = item
+        results.put((jid, _ensemble_worker(job)))
+
+
+class TableWorkers:
+    """Spawned host processes that build case tables for a long stream of jobs (corrector
+    training).  Each worker takes (id, job) items from one queue and puts (id, tables) on another.
+    A worker that dies (whatever the cause) is replaced and every job that has not come back is
+    queued again; a result that arrives twice is kept once.  ``restarts`` counts replaced workers,
+    ``exit_codes`` their exit codes."""
+
+    def __init__(self, workers: int):
+        self.ctx = mp.get_context("spawn")
+        self.jobs, self.results = self.ctx.Queue(), self.ctx.Queue()
+        self.procs = [self._start() for _ in range(max(1, workers))]
+        self.pending: dict = {}           # id -> job, submitted and not yet returned
+        self.done: dict = {}              # id -> tables, returned and not yet taken
+        self.taken: set = set()
+        self.restarts, self.exit_codes = 0, []
+
+    def _start(self):
+        p = self.ctx.Process(target=_table_worker_loop, args=(self.jobs, self.results), daemon=True)
+        p.start()
+        return p
+
+    def submit(self, jid, job):
+        self.pending[jid] = job
+        self.jobs.put((jid, job))
+
+    def _replace_dead(self):
+        dead = [i for i, p in enumerate(self.procs) if not p.is_alive()]
+        if not dead:
+            return
+        for i in dead:
+            self.exit_codes.append(self.procs[i].exitcode)
+            self.procs[i] = self._start()
+        self.restarts += len(dead)
+        for jid, job in self.pending.items():          # whichever job a dead worker held
+            self.jobs.put((jid, job))
+
+    def get(self, jid, timeout: float = 3600.0):
+        import queue
+        import time
+        t0 = time.time()
+        while jid not in self.done:
+            if time.time() - t0 > timeout:
+                raise TimeoutError(f"table job {jid} did not come back in {timeout:.0f} s")
+            self._replace_dead()
+            try:
+                rid, res = self.results.get(timeout=5.0)
+            except queue.Empty:
+                continue
+            if rid in self.taken or rid in self.done:
+                continue                                 # a resubmitted job's second result
+            self.pending.pop(rid, None)
+            self.done[rid] = res
+        self.taken.add(jid)
+        return self.done.pop(jid)
+
+    def close(self):
+        for _ in self.procs:
+            self.jobs.put(None)
+        for p in self.procs:
+            p.join(timeout=10)
+            if p.is_alive():
+                p.terminate()
+
+
 def build_ensemble_tables(n_cases: int, base_seed: int = 1234, workers: int = 0, family: str = "channel",
                           cells=(300_000, 800_000), indices=None) -> list:
     """Per-case tables of a seeded ensemble -- ``family`` "channel" (2D channel-cylinder cases) or
