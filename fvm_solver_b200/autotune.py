@@ -47,6 +47,12 @@ def set_variant(kernel: str, variant: int):
     _lib.check(_lib.load().fvm_set_variant(kid, int(variant)), "fvm_set_variant")
 
 
+def set_launch_overlap(on: bool):
+    """Programmatic dependent launches for the stage kernels (``fvm_set_launch_overlap``; on by
+    default): each kernel is launched while its predecessor drains and waits on the device."""
+    _lib.check(_lib.load().fvm_set_launch_overlap(int(bool(on))), "fvm_set_launch_overlap")
+
+
 STAGED = "staged"           # facet kernel: records staged in shared memory by the bulk-copy unit
 
 

@@ -149,8 +149,17 @@ void prof_end(cudaStream_t s) {
     ++g_prof.n;
 }
 
+int g_launch_overlap = 1;
+static thread_local cudaError_t g_pending_launch_error = cudaSuccess;
+
+void note_launch_error(cudaError_t e) {
+    if (g_pending_launch_error == cudaSuccess) g_pending_launch_error = e;
+}
+
 int launch_status() {
-    const cudaError_t e = cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = g_pending_launch_error;
+    g_pending_launch_error = cudaSuccess;
     if (e != cudaSuccess) {
         g_last_cuda_error = (int)e;
         return FVM_E_CUDA;
@@ -158,6 +167,12 @@ int launch_status() {
     return FVM_OK;
 }
 }  // namespace fvm
+
+extern "C" int fvm_set_launch_overlap(int32_t on) {
+    if (on != 0 && on != 1) return FVM_E_ARG;
+    fvm::g_launch_overlap = on;
+    return FVM_OK;
+}
 
 extern "C" int fvm_last_cuda_error(void) { return fvm::g_last_cuda_error; }
 

@@ -24,6 +24,33 @@ enum KernelId {
 void prof_begin(int kid, cudaStream_t s);
 void prof_end(cudaStream_t s);
 
+// Launches of the stage kernels (boundary, cell, facet, divergence, finalisation) go through
+// `launch`: with launch overlap on (fvm_set_launch_overlap, default on) each carries the
+// programmatic-stream-serialisation attribute, so the next kernel of a stream (or of a CUDA graph)
+// is launched while the previous one drains; every such kernel starts with `dependency_wait`
+// (griddepcontrol.wait), which returns once the previous kernel has completed and its writes are
+// visible, so results are unchanged.  A launch error is kept for launch_status().
+extern int g_launch_overlap;
+void note_launch_error(cudaError_t e);
+
+__device__ __forceinline__ void dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = g_launch_overlap ? 1 : 0;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+    if (e != cudaSuccess) note_launch_error(e);
+}
+
 #define FVM_LAUNCH(kid, stream, ...)          \
     do {                                      \
         ::fvm::prof_begin((kid), (stream));   \

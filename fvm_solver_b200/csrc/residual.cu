@@ -308,6 +308,7 @@ __device__ __forceinline__ void char_scale_case(const fvm_mesh_t& m, const Phys&
 template <int DIM>
 __global__ void __launch_bounds__(kBlock) k_char_scale(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
                                                         double* __restrict__ red_out) {
+    dependency_wait();
     char_scale_case<DIM, false>(m, p, prims, red_out, blockIdx.x);
 }
 
@@ -407,6 +408,7 @@ __global__ void __launch_bounds__(kBlock) k_bc(fvm_mesh_t m, Phys p, const float
                                                 const float* __restrict__ grads,
                                                 const int32_t* __restrict__ has_grads,
                                                 float* __restrict__ bcv, const double* __restrict__ wred) {
+    dependency_wait();
     const float scale = bc_block_scale<DIM, false>(m, p, prims);
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b < m.n_bc) bc_item<DIM, false>(m, p, prims, grads, has_grads, bcv, wred, b, scale);
@@ -612,6 +614,7 @@ template <int DIM>
 __global__ void __launch_bounds__(kBlock) k_cell_wide(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
                                                        const float* __restrict__ bcv, float* __restrict__ grads,
                                                        int32_t* __restrict__ has_grads) {
+    dependency_wait();
     cell_wide_body<DIM, false>(m, p, prims, bcv, grads, has_grads);
 }
 
@@ -625,6 +628,7 @@ template <int DIM>
 __global__ void __maxnreg__(FVM_CELL_MAXNREG) k_cell(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
                                                   const float* __restrict__ bcv, float* __restrict__ grads,
                                                   int32_t* __restrict__ has_grads, int waves) {
+    dependency_wait();
     cell_body<DIM, false>(m, p, prims, bcv, grads, has_grads, waves);
 }
 
@@ -885,6 +889,7 @@ template <int DIM>
 __global__ void __launch_bounds__(kMaxBlock) k_face_staged(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
                                                          const float* __restrict__ bcv,
                                                          const float* __restrict__ grads, float* __restrict__ flux) {
+    dependency_wait();
     using Ly = L<DIM>;
     constexpr int RS = Ly::RS, GS = Ly::GS, FR = Ly::FR;
     extern __shared__ __align__(128) float s_rec[];       // [2][blockDim.x][FR]
@@ -964,6 +969,7 @@ __global__ void FVM_FACE_BOUNDS k_face(fvm_mesh_t m, Phys p, const float* __rest
                                                   const float* __restrict__ bcv,
                                                   const float* __restrict__ grads, float* __restrict__ flux,
                                                   int waves) {
+    dependency_wait();
     face_body<DIM, false>(m, p, prims, bcv, grads, flux, waves);
 }
 
@@ -980,6 +986,7 @@ template <int DIM>
 __global__ void __launch_bounds__(kMaxBlock) k_face_div(fvm_mesh_t m, Phys p, const float* __restrict__ prims,
                                                       const float* __restrict__ bcv,
                                                       const float* __restrict__ grads, float* __restrict__ dudt) {
+    dependency_wait();
     using Ly = L<DIM>;
     constexpr int C = Ly::C, RS = Ly::RS, GS = Ly::GS, FR = Ly::FR, K = Ly::K;
     static_assert(K <= 4, "four lanes per cell");
@@ -1298,6 +1305,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_div_stage(fvm_mesh_t m, Phys p, c
                                                        const float* __restrict__ dt,
                                                        double* __restrict__ red,
                                                        float* __restrict__ dudt, int waves) {
+    dependency_wait();
     div_body<DIM, MODE, false>(m, p, flux, a, state, prims, kbuf, dt, red, dudt, waves);
 }
 
@@ -1358,6 +1366,7 @@ __device__ __forceinline__ void finalize_body(int C, int adaptive, float atol, f
 __global__ void k_finalize(int C, int adaptive, float atol, float rtol, float mtol, float alpha_hi,
                            float alpha_lo, float order, float cfl, int cons, double* red, float* dt,
                            double* cons_out, int n_cases, const uint8_t* __restrict__ active) {
+    dependency_wait();
     finalize_body(C, adaptive, atol, rtol, mtol, alpha_hi, alpha_lo, order, cfl, cons, red, dt, cons_out, n_cases,
                   active);
 }
@@ -1487,6 +1496,7 @@ __global__ void __launch_bounds__(kBlock) k_step_fused(fvm_mesh_t m, Phys p, Fus
 template <int DIM>
 __global__ void __launch_bounds__(kBlock) k_state_to_prims(int N, float inv_Cv, const float* __restrict__ state,
                                                             float* __restrict__ prims) {
+    dependency_wait();
     using Ly = L<DIM>;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
@@ -1500,6 +1510,7 @@ __global__ void __launch_bounds__(kBlock) k_state_to_prims(int N, float inv_Cv, 
 // [N][C] primitives -> padded [N][RS] rows (fvm_residual takes the reference's layout).
 template <int DIM>
 __global__ void __launch_bounds__(kBlock) k_pad_prims(int N, const float* __restrict__ src, float* __restrict__ dst) {
+    dependency_wait();
     using Ly = L<DIM>;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
@@ -1731,19 +1742,19 @@ static int launch_begin(const fvm_mesh_t* m, const Phys& p, const float* prims, 
                         int32_t* has_grads, const fvm_work_t* w, cudaStream_t s) {
     if (m->n_bc > 0) {
         if (m->n_cases > 0 && m->n_char > 0)
-            FVM_LAUNCH(KID_BC, s, k_char_scale<DIM><<<m->n_cases, kBlock, 0, s>>>(*m, p, prims, w->red));
-        FVM_LAUNCH(KID_BC, s, k_bc<DIM><<<blocks_for(m->n_bc), kBlock, 0, s>>>(*m, p, prims, grads, has_grads,
+            FVM_LAUNCH(KID_BC, s, launch(k_char_scale<DIM>, dim3(m->n_cases), dim3(kBlock), 0, s, *m, p, prims, w->red));
+        FVM_LAUNCH(KID_BC, s, launch(k_bc<DIM>, dim3(blocks_for(m->n_bc)), dim3(kBlock), 0, s, *m, p, prims, grads, has_grads,
                                                                                w->bc_vals, w->red));
     }
     if (owned_cells(m) - m->cell_lo <= 0) return launch_status();   // empty range: nothing to launch
     if (m->kg != DIM + 2) {
         const unsigned gw = persistent_grid(owned_cells(m) - m->cell_lo, kBlock, wave_blocks(k_cell_wide<DIM>, kBlock));
-        FVM_LAUNCH(KID_CELL, s, k_cell_wide<DIM><<<gw, kBlock, 0, s>>>(*m, p, prims, w->bc_vals, grads, has_grads));
+        FVM_LAUNCH(KID_CELL, s, launch(k_cell_wide<DIM>, dim3(gw), dim3(kBlock), 0, s, *m, p, prims, w->bc_vals, grads, has_grads));
         return launch_status();
     }
     const unsigned gc =
         persistent_grid(owned_cells(m) - m->cell_lo, g_block_cell, wave_blocks(k_cell<DIM>, g_block_cell));
-    FVM_LAUNCH(KID_CELL, s, k_cell<DIM><<<gc, g_block_cell, 0, s>>>(*m, p, prims, w->bc_vals, grads, has_grads,
+    FVM_LAUNCH(KID_CELL, s, launch(k_cell<DIM>, dim3(gc), dim3(g_block_cell), 0, s, *m, p, prims, w->bc_vals, grads, has_grads,
                                                                     waves_of(g_pf_cell)));
     return launch_status();
 }
@@ -1785,13 +1796,13 @@ static int launch_face(const fvm_mesh_t* m, const Phys& p, const float* prims, c
         }
         const unsigned gf = persistent_grid(m->n_facets - m->facet_lo, g_block_face, wave);
         const size_t smem = (size_t)2 * g_block_face * L<DIM>::FR * 4;
-        FVM_LAUNCH(KID_FACE, s, k_face_staged<DIM><<<gf, g_block_face, smem, s>>>(*m, p, prims, w->bc_vals, grads,
+        FVM_LAUNCH(KID_FACE, s, launch(k_face_staged<DIM>, dim3(gf), dim3(g_block_face), smem, s, *m, p, prims, w->bc_vals, grads,
                                                                                   w->flux));
         return launch_status();
     }
     const unsigned gf =
         persistent_grid(m->n_facets - m->facet_lo, g_block_face, wave_blocks(k_face<DIM>, g_block_face));
-    FVM_LAUNCH(KID_FACE, s, k_face<DIM><<<gf, g_block_face, 0, s>>>(*m, p, prims, w->bc_vals, grads, w->flux,
+    FVM_LAUNCH(KID_FACE, s, launch(k_face<DIM>, dim3(gf), dim3(g_block_face), 0, s, *m, p, prims, w->bc_vals, grads, w->flux,
                                                                     waves_of(g_pf_face)));
     return launch_status();
 }
@@ -1809,7 +1820,7 @@ static void launch_div_mode(const fvm_mesh_t* m, const Phys& p, const float* flu
                             float* prims, float* kbuf, const float* dt, double* red, float* dudt, cudaStream_t s) {
     const unsigned grid =
         persistent_grid(owned_cells(m), g_block_div, wave_blocks(k_div_stage<DIM, MODE>, g_block_div));
-    FVM_LAUNCH(KID_DIV_STAGE, s, k_div_stage<DIM, MODE><<<grid, g_block_div, 0, s>>>(
+    FVM_LAUNCH(KID_DIV_STAGE, s, launch(k_div_stage<DIM, MODE>, dim3(grid), dim3(g_block_div), 0, s, 
                                      *m, p, flux, a, state, prims, kbuf, dt, red, dudt, waves_of(g_pf_div)));
 }
 
@@ -1838,7 +1849,7 @@ static int launch_residual(const fvm_mesh_t* m, const Phys& p, float* grads, int
         if (rc) return rc;
         const unsigned g = persistent_grid(4 * (int64_t)owned_cells(m), g_block_face,
                                            wave_blocks(k_face_div<DIM>, g_block_face));
-        FVM_LAUNCH(KID_DIV_STAGE, s, k_face_div<DIM><<<g, g_block_face, 0, s>>>(*m, p, w->prims, w->bc_vals, grads,
+        FVM_LAUNCH(KID_DIV_STAGE, s, launch(k_face_div<DIM>, dim3(g), dim3(g_block_face), 0, s, *m, p, w->prims, w->bc_vals, grads,
                                                                                 dudt));
         return launch_status();
     }
@@ -1851,7 +1862,7 @@ static int launch_residual(const fvm_mesh_t* m, const Phys& p, float* grads, int
 template <int DIM>
 static int residual_impl(const fvm_mesh_t* m, const Phys& p, const float* prims_user, float* grads,
                          int32_t* has_grads, float* dudt, const fvm_work_t* w, cudaStream_t s) {
-    FVM_LAUNCH(KID_STATE_TO_PRIMS, s, k_pad_prims<DIM><<<blocks_for(m->n_cells), kBlock, 0, s>>>(
+    FVM_LAUNCH(KID_STATE_TO_PRIMS, s, launch(k_pad_prims<DIM>, dim3(blocks_for(m->n_cells)), dim3(kBlock), 0, s, 
                                           m->n_cells, prims_user, w->prims));
     return launch_residual<DIM>(m, p, grads, has_grads, dudt, w, s);
 }
@@ -1861,7 +1872,7 @@ static int residual_impl(const fvm_mesh_t* m, const Phys& p, const float* prims_
 template <int DIM>
 static int residual_state_impl(const fvm_mesh_t* m, const Phys& p, const float* state, float* grads,
                                int32_t* has_grads, float* dudt, const fvm_work_t* w, cudaStream_t s) {
-    FVM_LAUNCH(KID_STATE_TO_PRIMS, s, k_state_to_prims<DIM><<<blocks_for(m->n_cells), kBlock, 0, s>>>(
+    FVM_LAUNCH(KID_STATE_TO_PRIMS, s, launch(k_state_to_prims<DIM>, dim3(blocks_for(m->n_cells)), dim3(kBlock), 0, s, 
                                           m->n_cells, p.inv_Cv, state, w->prims));
     return launch_residual<DIM>(m, p, grads, has_grads, dudt, w, s);
 }
@@ -1903,7 +1914,7 @@ static StageArgs stage_args(const fvm_tableau_t* tab, int s) {
 static int finalize_impl(const fvm_mesh_t* m, const fvm_tableau_t* tab, const fvm_solver_bufs_t* b,
                          const fvm_work_t* w, int cons, cudaStream_t st) {
     FVM_LAUNCH(KID_FINALIZE, st,
-               k_finalize<<<fin_blocks(m), 128, 0, st>>>(m->n_comp, tab->adaptive, tab->atol, tab->rtol, tab->mtol,
+               launch(k_finalize, dim3(fin_blocks(m)), dim3(128), 0, st, m->n_comp, tab->adaptive, tab->atol, tab->rtol, tab->mtol,
                                                          tab->alpha_hi_err, tab->alpha_lo_err, tab->order, tab->cfl,
                                                          cons, w->red, b->dt, b->cons, m->n_cases, m->case_active));
     return launch_status();
@@ -1992,7 +2003,7 @@ static int multistep_impl(const fvm_mesh_t* m, const Phys& p, int store, int n_t
     rc = launch_div<DIM>(m, p, w->flux, a, b->state, b->prims, b->k, b->dt, w->red, nullptr, st);
     if (rc) return rc;
     if (a.cons) {
-        FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(m), 128, 0, st>>>(m->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f,
+        FVM_LAUNCH(KID_FINALIZE, st, launch(k_finalize, dim3(fin_blocks(m)), dim3(128), 0, st, m->n_comp, 0, 0.f, 0.f, 0.f, 0.f, 0.f,
                                                                               1.f, 0.f, 1, w->red, b->dt, b->cons,
                                                                               m->n_cases, m->case_active));
         rc = launch_status();
@@ -2325,10 +2336,10 @@ extern "C" int fvm_state_to_prims(const fvm_mesh_t* mesh, const fvm_physics_t* p
     const Phys p = make_phys(phys);
     cudaStream_t st = (cudaStream_t)stream;
     if (mesh->dim == 2)
-        FVM_LAUNCH(KID_STATE_TO_PRIMS, st, k_state_to_prims<2><<<blocks_for(owned_cells(mesh)), kBlock, 0, st>>>(
+        FVM_LAUNCH(KID_STATE_TO_PRIMS, st, launch(k_state_to_prims<2>, dim3(blocks_for(owned_cells(mesh))), dim3(kBlock), 0, st, 
                                                owned_cells(mesh), p.inv_Cv, state, prims));
     else
-        FVM_LAUNCH(KID_STATE_TO_PRIMS, st, k_state_to_prims<3><<<blocks_for(owned_cells(mesh)), kBlock, 0, st>>>(
+        FVM_LAUNCH(KID_STATE_TO_PRIMS, st, launch(k_state_to_prims<3>, dim3(blocks_for(owned_cells(mesh))), dim3(kBlock), 0, st, 
                                                owned_cells(mesh), p.inv_Cv, state, prims));
     return launch_status();
 }
@@ -2346,7 +2357,7 @@ extern "C" int fvm_cfl_dt(const fvm_mesh_t* mesh, const fvm_physics_t* phys, con
                                              *mesh, p, state, 1, 0, work->red));
     int rc = launch_status();
     if (rc) return rc;
-    FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(mesh), 128, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f,
+    FVM_LAUNCH(KID_FINALIZE, st, launch(k_finalize, dim3(fin_blocks(mesh)), dim3(128), 0, st, mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f,
                                                                              0.f, 1.f, cfl, 0, work->red, dt,
                                                                              nullptr, mesh->n_cases, nullptr));
     return launch_status();
@@ -2365,7 +2376,7 @@ extern "C" int fvm_conservation(const fvm_mesh_t* mesh, const float* state, doub
                                              *mesh, p, state, 0, 1, work->red));
     int rc = launch_status();
     if (rc) return rc;
-    FVM_LAUNCH(KID_FINALIZE, st, k_finalize<<<fin_blocks(mesh), 128, 0, st>>>(mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f,
+    FVM_LAUNCH(KID_FINALIZE, st, launch(k_finalize, dim3(fin_blocks(mesh)), dim3(128), 0, st, mesh->n_comp, 0, 0.f, 0.f, 0.f, 0.f,
                                                                              0.f, 1.f, 0.f, 1, work->red, nullptr,
                                                                              out, mesh->n_cases, nullptr));
     return launch_status();

@@ -185,6 +185,12 @@ int fvm_profile_start(int32_t capacity);
  * no flux array, every interior facet evaluated from both sides), 0 = facet kernel then divergence
  * kernel; stages always use 0. */
 int fvm_set_variant(int32_t kernel_id, int32_t variant);
+/* Launch overlap (no reference counterpart; results unchanged; default 1): 1 = the boundary,
+ * cell, facet, divergence, conversion and finalisation kernels are launched with programmatic
+ * stream serialisation, so each is launched while the previous kernel of its stream (or CUDA
+ * graph) drains and waits on the device (griddepcontrol.wait) for that kernel's completion and
+ * writes; 0 = plain stream order. */
+int fvm_set_launch_overlap(int32_t on);
 /* Launch configuration (no reference counterpart): threads per block of the cell (id 3), facet
  * (id 4) and divergence/stage (id 5) kernels for all later launches of this process; a multiple
  * of 32 in [64, 512].  Results do not depend on it (each thread's arithmetic is unchanged); the

@@ -429,3 +429,25 @@ def test_owner_computes_residual_bitwise(case):
         assert torch.equal(rs, ref[1]), k
     with pytest.raises(RuntimeError):
         autotune.set_variant("div_stage", 2)
+
+
+@pytest.mark.parametrize("case,solver,extra", [("c2d", "Butcher", "SSP_RK3"), ("b3d", "Butcher", "RK4"),
+                                               ("c2d", "AB3", "")])
+def test_launch_overlap_bitwise(case, solver, extra):
+    """Programmatic dependent launches (each stage kernel launched while its predecessor drains,
+    waiting on the device) change nothing: eager steps and graph-replayed steps with the overlap
+    on equal those with it off, bit for bit."""
+    from fvm_solver_b200 import autotune
+    outs = []
+    try:
+        for on in (False, True):
+            autotune.set_launch_overlap(on)
+            g, eq, T, cfg = make_equation(case, solver, extra, cfl=0.5 if solver != "AB3" else None)
+            eq.t_solver.step(3)
+            eq.t_solver.graph_steps(3)()
+            torch.cuda.synchronize()
+            outs.append((eq.cells.state.clone(), eq.grads.clone(), eq.t_solver.dt.clone()))
+    finally:
+        autotune.set_launch_overlap(True)
+    for a, b in zip(*outs):
+        assert torch.equal(a, b)
