@@ -817,15 +817,63 @@ def corrector_evaluate(model_src, args, three_d: bool, gates=None, spinup: int =
         e[1].record(stream)
         torch.cuda.synchronize()
     ms_plain = e[0].elapsed_time(e[1])
+    n_cases = args.eval_cases
+    curve_at = [w for w in (10, 25, 50, 100, 250, 500, 1000) if w <= args.windows]
 
-    def rollout(ratio, consistency):
+    def case_rel(a_state, b_state, batch) -> torch.Tensor:
+        """Per-case rel-L2 of a_state against b_state (FP64)."""
+        cc = batch.dev.case["cell_case"].long()
+        d = torch.zeros(n_cases, dtype=torch.float64, device=a_state.device)
+        r = torch.zeros_like(d)
+        d.index_add_(0, cc, (a_state.double() - b_state.double()).square().sum(1))
+        r.index_add_(0, cc, b_state.double().square().sum(1))
+        return (d / r).sqrt()
+
+    def make_corr():
         corr = B.BatchedFVM(eparts, ecfg, device="cuda")
         corr.t_solver.update_cfl_dt(0.5)
         corr.t_solver.step(spinup)
-        if isinstance(model_src, str):
-            model = CorrectorModel.load(model_src, corr, eprm)
-        else:
-            model = CorrectorModel(corr, eprm, like=model_src)
+        model = CorrectorModel.load(model_src, corr, eprm) if isinstance(model_src, str) else \
+            CorrectorModel(corr, eprm, like=model_src)
+        return corr, model
+
+    # reference trajectory (untimed): plain states at the curve points, and the teacher-forced
+    # one-window error -- the proposal from the plain state U_w against 8 plain steps from U_w,
+    # per case, so no error carries over from earlier windows
+    ref = B.BatchedFVM(eparts, ecfg, device="cuda")
+    ref.t_solver.update_cfl_dt(0.5)
+    ref.t_solver.step(spinup)
+    ref_window = ref.t_solver.graph_steps(8)
+    tf_corr, tf_model = make_corr()
+    tf_ro = CheckedRollout(tf_model, residual_ratio=gates[0][0], consistency=gates[0][1])
+    tf_windows = min(args.windows, 50)
+    tf_all, tf_ok = [], []
+    ref_at = {}
+    for w in range(1, args.windows + 1):
+        if w <= tf_windows:
+            tf_corr.cells.state = ref.cells.state
+            tf_corr.t_solver._sync_prims()
+            tf_ro._run_propose()
+        ref_window()
+        if w <= tf_windows:
+            rel = case_rel(tf_ro.prop, ref.cells.state, ref)
+            tf_all.append(rel)
+            tf_ok.append(rel[tf_ro.ok])
+        if w in curve_at:
+            ref_at[w] = ref.cells.state.clone()
+    tf_all, tf_ok = torch.cat(tf_all), torch.cat(tf_ok)
+    fin = torch.isfinite(tf_all)
+    teacher_forced = {
+        "windows": tf_windows, "gate": {"residual_ratio": gates[0][0], "trapezoid_consistency": gates[0][1] or None},
+        "rel_l2_all": {"mean": float(tf_all[fin].mean()), "max": float(tf_all[fin].max()),
+                       "frac_below_1e-2": float((tf_all[fin] <= 1e-2).float().mean())},
+        "rel_l2_accepted": ({"mean": float(tf_ok.mean()), "max": float(tf_ok.max()),
+                             "frac_below_1e-2": float((tf_ok <= 1e-2).float().mean())} if tf_ok.numel() else None),
+        "accept_rate": tf_ok.numel() / max(tf_all.numel(), 1)}
+    del tf_corr, tf_model, tf_ro, ref, ref_window
+
+    def rollout(ratio, consistency):
+        corr, model = make_corr()
         ro = CheckedRollout(model, residual_ratio=ratio, consistency=consistency)
         # capture every CUDA graph before timing (capturing executes nothing; the state stays put)
         ro._run_propose()
@@ -856,8 +904,22 @@ def corrector_evaluate(model_src, args, three_d: bool, gates=None, spinup: int =
             bad_corr += not fa
             if fa and fr:
                 err.append(float(((a - r).norm() / r.norm()).item()))
+        # drift curve (untimed second rollout from the same start): rel-L2 vs the plain trajectory
+        corr2, model2 = make_corr()
+        ro2 = CheckedRollout(model2, residual_ratio=ratio, consistency=consistency)
+        curve = {}
+        for w in range(1, (curve_at[-1] if curve_at else 0) + 1):
+            ro2.window()
+            if w in curve_at:
+                rel = case_rel(corr2.cells.state, ref_at[w], corr2)
+                ok = torch.isfinite(rel)
+                curve[str(w)] = {"mean": float(rel[ok].mean()) if bool(ok.any()) else None,
+                                 "max": float(rel[ok].max()) if bool(ok.any()) else None,
+                                 "nonfinite_cases": int((~ok).sum())}
+        del corr2, model2, ro2
         return {"residual_ratio": ratio, "trapezoid_consistency": consistency or None,
                 "speedup": ms_plain / ms_corr, "ms_corrected": ms_corr,
+                "rel_l2_curve_by_window": curve,
                 "ms_per_window": {"corrected": ms_corr / args.windows, "plain": ms_plain / args.windows,
                                   "proposal_and_checks": ms_propose},
                 "accept_rate": ro.accepted / max(ro.windows, 1),
@@ -877,7 +939,8 @@ def corrector_evaluate(model_src, args, three_d: bool, gates=None, spinup: int =
                        "net": "4 message-passing layers, width 64, SiLU, tcgen05 BF16 GEMMs",
                        "checks": f"drift <= 1e-4, residual norm <= {gates[0][0]}x, admissible state"
                                  + (f", trapezoid distance <= {gates[0][1]} k dt |r0|" if gates[0][1] else "")},
-            "ms_plain": ms_plain, **{k: v for k, v in main.items() if k != "speedup"},
+            "ms_plain": ms_plain, "teacher_forced_window_error": teacher_forced,
+            **{k: v for k, v in main.items() if k != "speedup"},
             "other_checks": others, "clocks": clk.summary()}
 
 
