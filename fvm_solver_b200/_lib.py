@@ -113,7 +113,6 @@ _SIGS = [
     ("fvm_corrector_checks", ct.c_int, [_P, _P, _P, _P, _P, _P, ct.c_int32, ct.c_int32, ct.c_int32, _P, ct.c_int32,
                                         ct.c_double, ct.c_double, ct.c_double, _P, _P, _P, _P]),
     ("fvm_set_launch_overlap", ct.c_int, [ct.c_int32]),
-    ("fvm_ell_set_variant", ct.c_int, [ct.c_int32]),
     ("fvm_profile_stop", ct.c_int, []),
     ("fvm_profile_read", ct.c_int, [ct.c_int32, _P, _P]),
 ]

@@ -648,12 +648,13 @@ extern "C" int fvm_corrector_combine(const float* state, const float* base, cons
 //   and, for the last layer, out_i = W_out h'_i + b_out instead of storing h'.
 //
 // One CTA per SM slot runs a grid-stride loop over 128-row tiles with three roles:
-//   * warps 0-3 (loaders): stage tile k's A operand (128 x 128 bf16, canonical no-swizzle K-major
+//   * warps 0-7 (loaders): stage tile k's A operand (128 x 128 bf16, canonical no-swizzle K-major
 //     core-matrix layout, two K slices: own row, neighbour mean) into shared-memory stage k % 2;
-//     the neighbour mean is an fp32 sum over the valid neighbours in table order times 1 / count;
+//     the neighbour mean is an fp32 sum over the valid neighbours in table order times 1 / count
+//     (the gathers are latency-bound: eight warps, each thread with two rows' loads in flight);
 //   * thread 0 (a loader) issues the tile's eight tcgen05.mma (M 128, N 64, K 16) into tensor-memory
 //     accumulator k % 2 and commits to two mbarriers: "stage free" and "accumulator full";
-//   * warps 4-7 (epilogue): read accumulator k % 2 (warp 4 + w owns TMEM lanes 32w..32w+31 = tile
+//   * warps 8-11 (epilogue): read accumulator k % 2 (warp 8 + w owns TMEM lanes 32w..32w+31 = tile
 //     rows), free it for tile k + 2 (an mbarrier), add bias, SiLU, the fp32 residual and store h'
 //     (or the decoder's outputs) with 256-bit accesses.
 // So the gathers of tile k + 1, the MMAs of tile k and the epilogue of tile k - 1 overlap.  The
@@ -664,7 +665,8 @@ extern "C" int fvm_corrector_combine(const float* state, const float* base, cons
 namespace fvm {
 namespace corr {
 
-constexpr int kLayerThreads = 256;
+constexpr int kLayerLoaders = 256;                       // warps 0-7: gathers (+ the MMA issuer)
+constexpr int kLayerThreads = kLayerLoaders + 128;       // warps 8-11: epilogue
 constexpr int kLayerW = 64;                              // channels
 constexpr int kLayerStageBytes = 2 * TM * TK * 2;        // two K slices of 128 x 64 bf16
 constexpr int kLayerWBytes = kLayerW * 2 * kLayerW * 2;  // W: 64 x 128 bf16
@@ -694,15 +696,15 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
 }
-__device__ __forceinline__ void loader_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
-// Named barrier of the 128 loader threads that also returns whether any of them passed v != 0,
+__device__ __forceinline__ void loader_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+// Named barrier of the 256 loader threads that also returns whether any of them passed v != 0,
 // so every loader takes the same branch afterwards.
 __device__ __forceinline__ int loader_sync_or(int v) {
     int r;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\t"
         "setp.ne.b32 p, %1, 0;\n\t"
-        "bar.red.or.pred q, 1, 128, p;\n\t"
+        "bar.red.or.pred q, 1, 256, p;\n\t"
         "selp.b32 %0, 1, 0, q;\n\t}\n"
         : "=r"(r)
         : "r"(v)
@@ -724,17 +726,79 @@ __device__ __forceinline__ void tmem_ld32(uint32_t addr, uint32_t (&r)[32]) {
 }
 
 // Stage rows [m0, m0 + 128) of tile into the two K slices at sA (own row, neighbour mean), bf16.
-// Loader thread lt (0..127) handles the 8-channel units u = (lt >> 3) & 7 of rows
-// (lt & 7) + 8 * (lt >> 6) + 16 q, q = 0..7: a warp covers 8 rows x 4 units per q, so its 16-byte
+// Loader thread lt (0..255) handles the 8-channel unit u = (lt >> 3) & 7 of rows
+// (lt & 7) + 8 * (lt >> 6) + 32 q, q = 0..3: a warp covers 8 rows x 4 units per q, so its 16-byte
 // shared-memory stores hit all 32 banks once per 8 lanes and its global reads are 128-byte row
-// segments.
+// segments.  With at most KM <= 4 neighbours the loads of two rows (own + KM neighbours each) are
+// all issued before any is used -- a missing neighbour reads the row itself and contributes +0,
+// which leaves the sum unchanged (the sum starts at +0 and is never -0) -- so a thread keeps ten
+// 32-byte loads in flight instead of one; wider neighbour lists take the row-by-row loop.
+__device__ __forceinline__ void stage_store(uint8_t* sA, int r, int u, const float (&own)[8], const float (&acc)[8],
+                                            float inv) {
+    const int slice_bytes = (TM / 8) * 256;
+    __align__(16) __nv_bfloat16 a[8], b[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        a[e] = __float2bfloat16(own[e]);
+        b[e] = __float2bfloat16(acc[e] * inv);
+    }
+    const int off = (u >> 1) * slice_bytes + (r >> 3) * 256 + (u & 1) * 128 + (r & 7) * 16;
+    *reinterpret_cast<uint4*>(sA + off) = *reinterpret_cast<const uint4*>(a);
+    *reinterpret_cast<uint4*>(sA + TM * TK * 2 + off) = *reinterpret_cast<const uint4*>(b);
+}
+
+template <int KM>
+__device__ __forceinline__ void stage_layer_tile_batched(uint8_t* sA, const LayerArgs& g, int m0, const int* s_nb,
+                                                         const float* s_inv, int lt) {
+    const int u = (lt >> 3) & 7;
+#pragma unroll 1
+    for (int q0 = 0; q0 < 4; q0 += 2) {
+        float own[2][8], nb[2][KM][8];
+        bool use[2][KM];
+        int rs[2];
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const int r = (lt & 7) + 8 * (lt >> 6) + 32 * (q0 + b);
+            rs[b] = r;
+            const int64_t row = (int64_t)m0 + r;
+            const bool valid = row < g.M;
+            const int64_t self = valid ? row : 0;
+            ld8(g.h + self * kLayerW + 8 * u, own[b]);
+#pragma unroll
+            for (int k = 0; k < KM; ++k) {
+                const int j = k < g.KN ? s_nb[r * 8 + k] : -1;
+                use[b][k] = valid && j >= 0;
+                ld8(g.h + (use[b][k] ? (int64_t)j : self) * kLayerW + 8 * u, nb[b][k]);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const bool valid = (int64_t)m0 + rs[b] < g.M;
+            float o[8], acc[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                o[e] = valid ? own[b][e] : 0.f;
+                acc[e] = 0.f;
+            }
+#pragma unroll
+            for (int k = 0; k < KM; ++k)
+#pragma unroll
+                for (int e = 0; e < 8; ++e) acc[e] += use[b][k] ? nb[b][k][e] : 0.f;
+            stage_store(sA, rs[b], u, o, acc, s_inv[rs[b]]);
+        }
+    }
+}
+
 __device__ __forceinline__ void stage_layer_tile(uint8_t* sA, const LayerArgs& g, int m0, const int* s_nb,
                                                  const float* s_inv, int lt) {
+    if (g.KN <= 4) {
+        stage_layer_tile_batched<4>(sA, g, m0, s_nb, s_inv, lt);
+        return;
+    }
     const int u = (lt >> 3) & 7;
-    const int slice_bytes = (TM / 8) * 256;
-#pragma unroll 2
-    for (int q = 0; q < 8; ++q) {
-        const int r = (lt & 7) + 8 * (lt >> 6) + 16 * q;
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {
+        const int r = (lt & 7) + 8 * (lt >> 6) + 32 * q;
         const int64_t row = (int64_t)m0 + r;
         const bool valid = row < g.M;
         float own[8], acc[8];
@@ -753,16 +817,7 @@ __device__ __forceinline__ void stage_layer_tile(uint8_t* sA, const LayerArgs& g
                 for (int e = 0; e < 8; ++e) acc[e] += v[e];
             }
         }
-        const float inv = s_inv[r];
-        __align__(16) __nv_bfloat16 a[8], b[8];
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            a[e] = __float2bfloat16(own[e]);
-            b[e] = __float2bfloat16(acc[e] * inv);
-        }
-        const int off = (u >> 1) * slice_bytes + (r >> 3) * 256 + (u & 1) * 128 + (r & 7) * 16;
-        *reinterpret_cast<uint4*>(sA + off) = *reinterpret_cast<const uint4*>(a);
-        *reinterpret_cast<uint4*>(sA + TM * TK * 2 + off) = *reinterpret_cast<const uint4*>(b);
+        stage_store(sA, r, u, own, acc, s_inv[r]);
     }
 }
 
@@ -817,7 +872,7 @@ __global__ void __launch_bounds__(kLayerThreads, 1) k_mp_layer(LayerArgs g) {
     const uint32_t taddr = s_taddr;
     const uint32_t idesc = make_idesc(kLayerW);
 
-    if (warp < 4) {
+    if (warp < kLayerLoaders / 32) {
         // ---- loaders (and, thread 0, the MMA issuer) ----
         // Every decision to stop is taken together (loader_sync_or), so no loader is left waiting
         // at a named barrier: a loader's own bounded wait that gave up, or thread 0's, counts.
@@ -831,7 +886,7 @@ __global__ void __launch_bounds__(kLayerThreads, 1) k_mp_layer(LayerArgs g) {
                 fail = !mbar_wait(&bar_free[s], (uint32_t)(((k >> 1) - 1) & 1));
             // this tile's neighbour lists (every loader finished reading the last ones before the
             // previous loader_sync)
-            {
+            if (lt < TM) {
                 const int64_t row = (int64_t)m0 + lt;
                 int cnt = 0;
 #pragma unroll
@@ -879,7 +934,7 @@ __global__ void __launch_bounds__(kLayerThreads, 1) k_mp_layer(LayerArgs g) {
         if (fail) atomicExch(&s_fail, 1);
     } else {
         // ---- epilogue ----
-        const int we = warp - 4;                          // TMEM lane quarter = warp % 4
+        const int we = warp - kLayerLoaders / 32;         // TMEM lane quarter = warp % 4
         for (int k = 0; k < nlocal; ++k) {
             const int tile = (int)blockIdx.x + k * (int)gridDim.x;
             const int a = k & 1;

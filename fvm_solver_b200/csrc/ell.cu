@@ -117,40 +117,6 @@ __global__ void __launch_bounds__(kBlock) k_ell_spmm4(const float* __restrict__ 
     store_row<4>(Y + 4 * r, a);
 }
 
-// Five columns (the 3D state): a group of five lanes per row, lane j owning column j -- each slot's
-// value and column index are one broadcast load per group, and the group's five gathers of the
-// operand row are one contiguous 20-byte access, where a thread-per-row kernel issues five
-// separate gathers per slot (the operand rows are 20 bytes, too narrow and unaligned for vector
-// loads).  Six rows per warp (lanes 30, 31 idle); the slots are summed in order k = 0, 1, ...
-// and the bias added last, as in k_ell_spmm.
-template <int KT>
-__global__ void __launch_bounds__(kBlock) k_ell_spmm5(const float* __restrict__ vals,
-                                                       const int32_t* __restrict__ cols, int64_t M,
-                                                       int K, const float* __restrict__ X, int64_t ldx,
-                                                       const float* __restrict__ bias,
-                                                       float* __restrict__ Y, int64_t ldy) {
-    const int lane = threadIdx.x & 31;
-    const int j = lane % 5;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t r = warp * 6 + lane / 5;
-    if (lane >= 30 || r >= M) return;
-    float v[KT], x[KT];
-#pragma unroll
-    for (int k = 0; k < KT; ++k) {
-        v[k] = 0.f;
-        x[k] = 0.f;
-        if (k < K) {
-            v[k] = __ldg(vals + k * M + r);
-            x[k] = __ldg(X + (int64_t)__ldg(cols + k * M + r) * ldx + j);
-        }
-    }
-    float acc = 0.f;
-#pragma unroll
-    for (int k = 0; k < KT; ++k)
-        if (k < K) acc = fmaf(v[k], x[k], acc);
-    Y[r * ldy + j] = bias ? acc + __ldg(bias + r) : acc;
-}
-
 }  // namespace fvm
 
 #include <vector>
@@ -268,15 +234,6 @@ extern "C" int fvm_ell_spmv(const float* vals, const int32_t* cols, int64_t M, i
     return launch_status();
 }
 
-// Five-column products on k_ell_spmm5 (1) or on the thread-per-row kernel (0); same results.
-static int g_ell_coop = 1;
-
-extern "C" int fvm_ell_set_variant(int32_t five_column_groups) {
-    if (five_column_groups != 0 && five_column_groups != 1) return FVM_E_ARG;
-    g_ell_coop = five_column_groups;
-    return FVM_OK;
-}
-
 extern "C" int fvm_ell_spmm(const float* vals, const int32_t* cols, int64_t M, int32_t K,
                             const float* X, int64_t ldx, int32_t B, const float* bias, float* Y,
                             int64_t ldy, void* stream) {
@@ -294,15 +251,6 @@ extern "C" int fvm_ell_spmm(const float* vals, const int32_t* cols, int64_t M, i
         else if (K <= 8) FVM_SPMM4(8);
         else FVM_SPMM4(16);
 #undef FVM_SPMM4
-    } else if (B == 5 && g_ell_coop) {
-        const int64_t warps = (M + 5) / 6;
-        const unsigned g5 = (unsigned)((warps * 32 + fvm::kBlock - 1) / fvm::kBlock);
-#define FVM_SPMM5(KT) FVM_LAUNCH(fvm::KID_ELL_SPMM, s, fvm::k_ell_spmm5<KT><<<g5, fvm::kBlock, 0, s>>>( \
-                                     vals, cols, M, K, X, ldx, bias, Y, ldy))
-        if (K <= 4) FVM_SPMM5(4);
-        else if (K <= 8) FVM_SPMM5(8);
-        else FVM_SPMM5(16);
-#undef FVM_SPMM5
     } else {
         const unsigned gy = (unsigned)((B + 7) / 8);
 #define FVM_SPMM(KT) FVM_LAUNCH(fvm::KID_ELL_SPMM, s, fvm::k_ell_spmm<KT, 8><<<dim3((unsigned)gx, gy), fvm::kBlock, 0, s>>>( \

@@ -214,9 +214,6 @@ int fvm_ell_spmv(const float *vals, const int32_t *cols, int64_t M, int32_t K,
 int fvm_ell_spmm(const float *vals, const int32_t *cols, int64_t M, int32_t K,
                  const float *X, int64_t ldx, int32_t B, const float *bias, float *Y, int64_t ldy,
                  void *stream);
-/* ELL kernel variant (no reference counterpart; results unchanged; default 1): 1 = products with
- * B = 5 columns run five lanes per row (one lane per column), 0 = one thread per row. */
-int fvm_ell_set_variant(int32_t five_column_groups);
 
 /* dU/dt [N][C] (conserved variables) of the primitives prims [N][C].  grads [N][FVM_GROW] is
  * read as the previous limited gradient when the device flag *has_grads != 0 (the reference's

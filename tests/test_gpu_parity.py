@@ -52,36 +52,6 @@ def test_ell_random_vs_torch_sparse(K, B):
     assert rel_l2(to_np(y), to_np(torch.sparse.mm(Ad, x[:, None])[:, 0] + b)) < 1e-6
 
 
-@pytest.mark.parametrize("K", [1, 4, 5, 16])
-def test_ell_five_column_groups_bitwise(K):
-    """Five-column products: the five-lanes-per-row kernel equals the thread-per-row kernel bit for
-    bit (same slot order, bias last), contiguous and strided operands, with and without bias."""
-    from fvm_solver_b200 import _lib
-    from fvm_solver_b200.sparse import SPMB200
-    g = torch.Generator().manual_seed(K)
-    M, N = 4099, 2003
-    nnz_row = torch.randint(0, K + 1, (M,), generator=g)
-    rows = torch.repeat_interleave(torch.arange(M), nnz_row)
-    cols = torch.randint(0, N, (rows.numel(),), generator=g)
-    A = torch.sparse_coo_tensor(torch.stack([rows, cols]), torch.randn(rows.numel(), generator=g), (M, N)).coalesce()
-    op = SPMB200(A, "cuda")
-    X = torch.randn(N, 5, generator=g).cuda()
-    Xs = torch.randn(N, 8, generator=g).cuda()[:, 1:6]               # row stride 8
-    b = torch.randn(M, generator=g).cuda()
-    lib = _lib.load()
-    outs = []
-    try:
-        for v in (0, 1):
-            _lib.check(lib.fvm_ell_set_variant(v), "fvm_ell_set_variant")
-            outs.append([op.spMM(X), op.spMM(X, b), op.spMM(Xs), op.spMM(Xs, b)])
-    finally:
-        _lib.check(lib.fvm_ell_set_variant(1), "fvm_ell_set_variant")
-    for a, c in zip(*outs):
-        assert torch.equal(a, c)
-    ref = torch.sparse.mm(A.cuda(), X)
-    assert rel_l2(to_np(outs[1][0]), to_np(ref)) < 1e-6
-
-
 def test_ell_empty_and_zero_width():
     from fvm_solver_b200.sparse import SPMB200
     A = torch.sparse_coo_tensor(torch.zeros((2, 0), dtype=torch.long), torch.zeros(0), (7, 5))
