@@ -872,6 +872,28 @@ def corrector_evaluate(model_src, args, three_d: bool, gates=None, spinup: int =
         "accept_rate": tf_ok.numel() / max(tf_all.numel(), 1)}
     del tf_corr, tf_model, tf_ro, ref, ref_window
 
+    # control: the plain solver itself, its start state perturbed once by a seeded relative noise
+    # of the corrector's mean one-window error -- how far the unsteady flow carries an error of
+    # that size by itself over the same windows
+    eps = teacher_forced["rel_l2_all"]["mean"]
+    ctl = B.BatchedFVM(eparts, ecfg, device="cuda")
+    ctl.t_solver.update_cfl_dt(0.5)
+    ctl.t_solver.step(spinup)
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    noise = torch.randn(ctl.cells.state.shape, generator=gen, device="cuda")
+    ctl.cells.state = ctl.cells.state * (1.0 + eps * noise)
+    ctl_window = ctl.t_solver.graph_steps(8)
+    control = {"perturbation_rel": eps, "rel_l2_curve_by_window": {}}
+    for w in range(1, (curve_at[-1] if curve_at else 0) + 1):
+        ctl_window()
+        if w in curve_at:
+            rel = case_rel(ctl.cells.state, ref_at[w], ctl)
+            ok = torch.isfinite(rel)
+            control["rel_l2_curve_by_window"][str(w)] = {
+                "mean": float(rel[ok].mean()) if bool(ok.any()) else None,
+                "max": float(rel[ok].max()) if bool(ok.any()) else None}
+    del ctl, ctl_window
+
     def rollout(ratio, consistency):
         corr, model = make_corr()
         ro = CheckedRollout(model, residual_ratio=ratio, consistency=consistency)
@@ -940,6 +962,7 @@ def corrector_evaluate(model_src, args, three_d: bool, gates=None, spinup: int =
                        "checks": f"drift <= 1e-4, residual norm <= {gates[0][0]}x, admissible state"
                                  + (f", trapezoid distance <= {gates[0][1]} k dt |r0|" if gates[0][1] else "")},
             "ms_plain": ms_plain, "teacher_forced_window_error": teacher_forced,
+            "plain_perturbed_control": control,
             **{k: v for k, v in main.items() if k != "speedup"},
             "other_checks": others, "clocks": clk.summary()}
 
