@@ -878,6 +878,16 @@ __global__ void __launch_bounds__(kLayerThreads, 1) k_mp_layer(LayerArgs g) {
         // at a named barrier: a loader's own bounded wait that gave up, or thread 0's, counts.
         const int lt = threadIdx.x;
         int fail = 0;
+        // neighbour lists are fetched one tile ahead (the gathers of a tile then wait for one
+        // memory round trip, not two)
+        int nxt[8];
+        auto fetch_nbr = [&](int tile) {
+            const int64_t row = (int64_t)tile * TM + lt;
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                nxt[q] = (lt < TM && row < g.M && q < g.KN) ? __ldg(g.nbr + row * g.KN + q) : -1;
+        };
+        if (nlocal > 0) fetch_nbr((int)blockIdx.x);
         for (int k = 0; k < nlocal; ++k) {
             const int tile = (int)blockIdx.x + k * (int)gridDim.x;
             const int m0 = tile * TM, s = k & 1;
@@ -887,16 +897,15 @@ __global__ void __launch_bounds__(kLayerThreads, 1) k_mp_layer(LayerArgs g) {
             // this tile's neighbour lists (every loader finished reading the last ones before the
             // previous loader_sync)
             if (lt < TM) {
-                const int64_t row = (int64_t)m0 + lt;
                 int cnt = 0;
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
-                    const int j = (row < g.M && q < g.KN) ? __ldg(g.nbr + row * g.KN + q) : -1;
-                    s_nb[lt * 8 + q] = j;
-                    cnt += j >= 0;
+                    s_nb[lt * 8 + q] = nxt[q];
+                    cnt += nxt[q] >= 0;
                 }
                 s_inv[lt] = cnt > 0 ? 1.f / (float)cnt : 0.f;
             }
+            if (k + 1 < nlocal) fetch_nbr(tile + (int)gridDim.x);
             fail = loader_sync_or(fail);
             if (fail) break;
             stage_layer_tile(sA, g, m0, s_nb, s_inv, lt);
