@@ -124,7 +124,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     return done != 0;
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
+// z sigmoid(z) with the fast-division intrinsic: the denominator is >= 1, so the intrinsic's range
+// limit only matters where exp overflows and the quotient is 0 anyway (within 2 ulp elsewhere).
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.f + __expf(-z)); }
 
 // 8 consecutive floats (32-byte aligned) with one 256-bit access.
 __device__ __forceinline__ void ld8(const float* p, float* v) {
@@ -947,6 +949,13 @@ __global__ void __launch_bounds__(kLayerThreads, 1) k_mp_layer(LayerArgs g) {
         for (int k = 0; k < nlocal; ++k) {
             const int tile = (int)blockIdx.x + k * (int)gridDim.x;
             const int a = k & 1;
+            {   // the residual row is read after the accumulator: ask for it into L1 now
+                const int64_t prow = (int64_t)tile * TM + 32 * we + lane;
+                if (prow < g.M) {
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(g.h + prow * kLayerW));
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(g.h + prow * kLayerW + 32));
+                }
+            }
             bool ok = mbar_wait(&bar_full[a], (uint32_t)((k >> 1) & 1));
             if (!__all_sync(0xffffffffu, ok)) {
                 if (lane == 0) atomicExch(&s_fail, 1);
