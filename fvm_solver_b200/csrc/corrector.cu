@@ -126,6 +126,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 
 // z sigmoid(z) with the fast-division intrinsic: the denominator is >= 1, so the intrinsic's range
 // limit only matters where exp overflows and the quotient is 0 anyway (within 2 ulp elsewhere).
+// Every residual added to it goes through __fadd_rn, so no kernel fuses the quotient's multiply
+// with that add and all kernels round alike (the fused layer equals GEMM + epilogue bitwise).
 __device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.f + __expf(-z)); }
 
 // 8 consecutive floats (32-byte aligned) with one 256-bit access.
@@ -164,7 +166,7 @@ __device__ __forceinline__ void epilogue_vec(const GemmArgs& g, int64_t row, int
 #pragma unroll
         for (int q = 0; q < 4; ++q) ld8(g.resid + row * g.ldr + c0 + 8 * q, x + 8 * q);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) v[j] += x[j];
+        for (int j = 0; j < 32; ++j) v[j] = __fadd_rn(v[j], x[j]);
     }
     if (g.Df)
 #pragma unroll
@@ -309,7 +311,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(GemmArgs g) {
                     if (g.bias) v += g.bias[col];
                     if (g.preact) g.preact[(int64_t)row * g.ldd + col] = v;
                     if (g.act == 1) v = silu(v);
-                    if (g.resid) v += g.resid[(int64_t)row * g.ldr + col];
+                    if (g.resid) v = __fadd_rn(v, g.resid[(int64_t)row * g.ldr + col]);
                     if (g.Df) g.Df[(int64_t)row * g.ldd + col] = v;
                     if (g.Db) g.Db[(int64_t)row * g.ldd + col] = __float2bfloat16(v);
                 }
@@ -982,7 +984,7 @@ __global__ void __launch_bounds__(kLayerThreads, 1) k_mp_layer(LayerArgs g) {
 #pragma unroll
                     for (int q = 0; q < 4; ++q) ld8(g.h + row * kLayerW + c0 + 8 * q, x + 8 * q);
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) v[j] = silu(__uint_as_float(r[j]) + s_bias[c0 + j]) + x[j];
+                    for (int j = 0; j < 32; ++j) v[j] = __fadd_rn(silu(__uint_as_float(r[j]) + s_bias[c0 + j]), x[j]);
                     if (g.h_out)
 #pragma unroll
                         for (int q = 0; q < 4; ++q) st8(g.h_out + row * kLayerW + c0 + 8 * q, v + 8 * q);
