@@ -184,9 +184,6 @@ __device__ __forceinline__ bool case_on(const fvm_mesh_t& m, const int32_t* case
     return m.case_active == nullptr || m.case_active[__ldg(case_of + idx)] != 0;
 }
 
-// The two side codes (first two words) of a facet record.
-__device__ __forceinline__ int2 ld_codes(const float* rec) { return __ldg(reinterpret_cast<const int2*>(rec)); }
-
 // Whether a persistent loop over n items with `stride` threads checks the case of each next item
 // before loading its record: only with a case mask and more than four items per thread.
 __device__ __forceinline__ bool frozen_skip(const fvm_mesh_t& m, int n, int stride) {
@@ -197,11 +194,35 @@ __device__ __forceinline__ bool frozen_skip(const fvm_mesh_t& m, int n, int stri
 // of a frozen case (case mask), so a masked-out case costs one case-id read per item; the check
 // puts two dependent loads before the record load, so launches whose threads have only a few
 // items (latency-bound) leave it off (see frozen_skip).
+// The first 8 floats of facet f's record (its side codes, 1/d, |S|, normal, ...), fetched one
+// iteration ahead by the facet loop: the codes come with it, so the record's head is read once.
+// Rows of 16 floats (3D) start on 32-byte boundaries (one 256-bit load), rows of 12 (2D) on
+// 16-byte ones (two 128-bit loads).  Items not loaded read as zeros (side codes 0, 0).
 template <int DIM>
-__device__ __forceinline__ int2 next_codes(const fvm_mesh_t& m, int f, int nF, bool skip_frozen) {
+__device__ __forceinline__ void next_head(const fvm_mesh_t& m, int f, int nF, bool skip_frozen, float (&h)[8]) {
     const bool on = f < nF && (!skip_frozen || case_on(m, m.face_case, f));
-    return on ? ld_codes(m.face_rec + (int64_t)f * L<DIM>::FR) : make_int2(0, 0);
+    const float* r = m.face_rec + (int64_t)f * L<DIM>::FR;
+    if (!on) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) h[q] = 0.f;
+    } else if constexpr (L<DIM>::FR % 8 == 0) {
+        ld8_nc(r, h);
+    } else {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(r)), b = __ldg(reinterpret_cast<const float4*>(r) + 1);
+        h[0] = a.x; h[1] = a.y; h[2] = a.z; h[3] = a.w; h[4] = b.x; h[5] = b.y; h[6] = b.z; h[7] = b.w;
+    }
 }
+// The rest of the record (floats 8 .. FR - 1).
+template <int DIM>
+__device__ __forceinline__ void record_tail(const fvm_mesh_t& m, int f, float (&rec)[L<DIM>::FR]) {
+    constexpr int T = L<DIM>::FR - 8;
+    static_assert(T == 8 || T == 4, "facet record width");
+    float t[T];
+    ld_vec<T>(m.face_rec + (int64_t)f * L<DIM>::FR + 8, t);
+#pragma unroll
+    for (int q = 0; q < T; ++q) rec[8 + q] = t[q];
+}
+
 // The KG stencil columns of cell i in slot order, from its compact record: the KG - 1 stored
 // neighbour columns with the cell's own index inserted at its slot `own` (selects only, no
 // indexing of register arrays by a runtime value).  Items not loaded get the column 0 everywhere.
@@ -823,12 +844,13 @@ __device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, co
     const int stride = gridDim.x * blockDim.x;
     int f = lo + blockIdx.x * blockDim.x + threadIdx.x;
     const bool skip_frozen = frozen_skip(m, nF - lo, stride);
-    int2 nxt = next_codes<DIM>(m, f, nF, skip_frozen);
+    float head[8];
+    next_head<DIM>(m, f, nF, skip_frozen, head);
     for (int64_t tile = blockIdx.x; f < nF; f += stride, tile += gridDim.x) {
     if (waves > 0) prefetch_tile(m.face_rec + (int64_t)lo * Ly::FR, nF - lo, Ly::FR, tile + (int64_t)waves * gridDim.x);
-    const int ca = nxt.x, cb = nxt.y;
+    const int ca = as_int(head[Ly::FA]), cb = as_int(head[Ly::FB]);
     if (m.case_active && !case_on(m, m.face_case, f)) {
-        nxt = next_codes<DIM>(m, f + stride, nF, skip_frozen);
+        next_head<DIM>(m, f + stride, nF, skip_frozen, head);
         continue;
     }
     // Both sides: primitives and limited gradient of the cell(s); a boundary side (code < 0) takes
@@ -841,8 +863,10 @@ __device__ __forceinline__ void face_body(const fvm_mesh_t& m, const Phys& p, co
     ld_vec_cg<GS>(grads + (int64_t)cell0 * GS, G0);
     ld_vec_cg<GS>(grads + (int64_t)cell1 * GS, G1);
     float rec[Ly::FR];
-    ld_vec<Ly::FR>(m.face_rec + (int64_t)f * Ly::FR, rec);
-    nxt = next_codes<DIM>(m, f + stride, nF, skip_frozen);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) rec[q] = head[q];
+    record_tail<DIM>(m, f, rec);
+    next_head<DIM>(m, f + stride, nF, skip_frozen, head);
     float F[RS];
     face_eval<DIM>(m, p, bcv, f, ca, cb, rec, P0, P1, G0, G1, F);
     st_vec<RS>(flux + (int64_t)f * RS, F);
