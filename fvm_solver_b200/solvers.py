@@ -360,6 +360,28 @@ class TSolver:
         tab = getattr(self, "tab", None)
         return bool(self.cfl) or bool(tab is not None and tab.adaptive)
 
+    def solve_profile(self, warmup: int = 10, steps: int = 10, trace_path: str = "trace.json") -> str:
+        """The reference's ``cfg.profile`` mode (``TSolver._solve_profile``, ``t_solvers.py:179-196``):
+        ``warmup`` steps, then ``steps`` steps under ``torch.profiler`` (CPU and CUDA activity,
+        shapes, stacks), the ten entries with the most CUDA time printed and a Chrome trace written
+        to ``trace_path``.  Each profiled step is also an NVTX range ("fvm step <n>"), so external
+        profilers can filter by it.  Returns the printed table."""
+        from torch.profiler import ProfilerActivity, profile
+        self.step(warmup)
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CPU, ProfilerActivity.CUDA], record_shapes=True,
+                     with_stack=True) as prof:
+            for _ in range(steps):
+                prof.step()
+                torch.cuda.nvtx.range_push(f"fvm step {self.steps_done}")
+                self._solve_step()
+                torch.cuda.nvtx.range_pop()
+            torch.cuda.synchronize()
+        table = prof.key_averages().table(sort_by="self_cuda_time_total", row_limit=10)
+        print(table)
+        prof.export_chrome_trace(trace_path)
+        return table
+
     def solve(self):
         """The reference's main loop (``TSolver._solve``, ``t_solvers.py:77-154``) on the device solver.
 
@@ -371,8 +393,12 @@ class TSolver:
         ``save_t`` and ``save_dir``: snapshots in the reference's ``Saver`` format, the initial
         state at t = 0 and then every ``save_t`` (``trajectory_io.TrajectorySaver``); with
         ``exact_interval`` the step that would cross a save time is shortened to land on it and
-        the step size is restored afterwards.  Returns the final time."""
+        the step size is restored afterwards.  Returns the final time.  With ``cfg.profile`` the
+        reference's profiling mode runs instead (``solve_profile``)."""
         cfg = self.cfg
+        if getattr(cfg, "profile", False):
+            self.solve_profile()
+            return self.t
         if self.n_steps is None and self.end_t is None:
             raise ValueError("Either n_iter or end_t must be set in ConfigFVM")
         saver = None

@@ -62,3 +62,16 @@ def test_solve_nan_check():
     sol.n_steps, sol.end_t, sol.print_i = 3, None, 1
     with pytest.raises(ValueError, match="Nan"):
         sol.solve()
+
+
+def test_profile_mode_writes_trace(tmp_path):
+    """cfg.profile: the reference's profiling mode -- warm-up, profiled steps, a table of the
+    top CUDA entries naming the library's kernels, a Chrome trace file."""
+    from gpu_helpers import make_equation
+    g, eq, T, cfg = make_equation("c2d", "Butcher", "SSP_RK3")
+    path = str(tmp_path / "trace.json")
+    table = eq.t_solver.solve_profile(warmup=2, steps=3, trace_path=path)
+    assert os.path.getsize(path) > 0
+    assert "k_face" in table or "k_cell" in table
+    assert eq.t_solver.steps_done == 5
+    assert torch.isfinite(eq.cells.state).all()
