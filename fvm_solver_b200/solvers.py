@@ -370,7 +370,7 @@ class TSolver:
         self.step(warmup)
         torch.cuda.synchronize()
         with profile(activities=[ProfilerActivity.CPU, ProfilerActivity.CUDA], record_shapes=True,
-                     with_stack=True) as prof:
+                     with_stack=True, acc_events=True) as prof:      # keep every profiled step's events
             for _ in range(steps):
                 prof.step()
                 torch.cuda.nvtx.range_push(f"fvm step {self.steps_done}")
